@@ -1,0 +1,292 @@
+/*
+ * jurassic_b200.h -- public C interface of the B200 forward model.
+ *
+ * Two layers are declared here.
+ *
+ * 1. The drop-in layer.  formod(), brightness() and planck() keep the exact
+ *    signatures of the reference forward model (src/forwardmodel.h:16-19,
+ *    :282-283, :339-340), and the structs below keep the reference's memory
+ *    layout (src/jurassic.h:228-570) field for field, so a program built
+ *    against the reference headers links this library in place of
+ *    forwardmodel.o.  Field names are the reference's because callers use
+ *    them; sizes and offsets are checked by the test suite.
+ *
+ * 2. The plain C-ABI (jsc_*).  Opaque handles, plain pointers and sizes, no
+ *    C++ or torch types.  formod() is a thin client of it; batch callers
+ *    (many atmospheres and rays in one launch) call it directly.
+ */
+#ifndef JURASSIC_B200_H
+#define JURASSIC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Dimensions.  They size the fixed arrays of the boundary structs and must
+ * equal the reference's compile-time values (src/jurassic.h:135-196).
+ * ------------------------------------------------------------------------ */
+#define LEN      5000   /* characters per text field */
+#define NWMAX    5      /* spectral windows */
+#define NDMAX    130    /* radiance channels */
+#define NGMAX    25     /* emitters */
+#define NLOS     10000  /* points per line of sight */
+#define NPMAX    1000   /* atmospheric data points */
+#define NRMAX    1000   /* ray paths per obs_t */
+#define NSHAPE   10000  /* points of a filter or field-of-view shape */
+#define NFOV     50     /* rays used for the field-of-view convolution */
+#define TBLNPMAX 50     /* pressure levels per emissivity table */
+#define TBLNSMAX 1201   /* temperatures of the Planck source table */
+#define TBLNTMAX 30     /* temperatures per pressure level */
+#define TBLNUMAX 320    /* column densities per (pressure, temperature) */
+#define SCAMOD   30     /* aerosol/cloud models */
+#define NLMAX    10     /* aerosol/cloud layers */
+#define NTHETA   181    /* phase-function angles, 0..180 deg */
+#define NRAD     170    /* Gauss-Hermite nodes of the size integral */
+#define REFMAX   5000   /* refractive-index records */
+
+/* Physical constants with the reference's values (src/jurassic.h:113-126;
+ * GSL 1.15 gsl_const_mksa.h / gsl_const_num.h for the last three). */
+#define JSC_C1        1.19104259e-8   /* 2hc^2 [W/(m^2 sr cm^-4)] */
+#define JSC_C2        1.43877506      /* hc/k  [K/cm^-1] */
+#define JSC_P0        1013.25         /* standard pressure [hPa] */
+#define JSC_RE        6367.421        /* mean Earth radius [km] */
+#define JSC_TSUN      5780.           /* solar temperature [K] */
+#define JSC_KBOLTZ    1.3806504e-23   /* Boltzmann constant [J/K] */
+#define JSC_RGAS      8.314472        /* molar gas constant [J/(mol K)] */
+#define JSC_AVOGADRO  6.02214199e23   /* [1/mol] */
+
+/* ------------------------------------------------------------------------
+ * Boundary structs (layout of src/jurassic.h:13-25 and :228-570).
+ * ------------------------------------------------------------------------ */
+
+/* Work-queue bookkeeping carried inside ctl_t (src/workqueue.h:13-25).  The
+ * GPU path keeps its own device-resident queue; these fields are only kept
+ * for layout compatibility and are not touched by formod(). */
+typedef struct {
+  void *input;
+  void *result;
+  int ir;
+} queue_item_t;
+
+typedef struct {
+  queue_item_t *items;
+  int capacity;
+  int begin;
+  int end;
+  int state;
+} queue_t;
+
+/* Forward-model control parameters, as filled by the reference's read_ctl. */
+typedef struct {
+  int ng;                       /* emitters */
+  char emitter[NGMAX][LEN];     /* emitter names (table file suffixes) */
+  int nd;                       /* channels */
+  int nw;                       /* spectral windows */
+  double nu[NDMAX];             /* channel centre wavenumbers [cm^-1] */
+  int window[NDMAX];            /* window index of each channel */
+  char tblbase[LEN];            /* base name of table and filter files */
+  double hydz;                  /* hydrostatic reference height, <0: off [km] */
+  int ctm_co2, ctm_h2o, ctm_n2, ctm_o2;   /* continua switches */
+  int sca_n;                    /* aerosol/cloud models */
+  int sca_mult;                 /* scattering depth: 0 none, 1 single, >=2 multiple */
+  char sca_ext[LEN];            /* "beta_a" or "beta_e" when sca_mult==0 */
+  int ip;                       /* atmosphere interpolation: 1 profile, 2, 3 */
+  double cz, cx;                /* influence lengths for ip 2/3 [km] */
+  int refrac;                   /* refraction on/off */
+  double rayds;                 /* maximum ray step [km] */
+  double raydz;                 /* vertical ray step [km] */
+  double transs;                /* transition-layer sampling step [km] */
+  char fov[LEN];                /* field-of-view file, "-" for none */
+  double retp_zmin, retp_zmax;
+  double rett_zmin, rett_zmax;
+  double retq_zmin[NGMAX], retq_zmax[NGMAX];
+  double retk_zmin[NWMAX], retk_zmax[NWMAX];
+  double retnn_zmin, retnn_zmax;
+  int retnn, retrr, retss;      /* aerosol retrieval switches */
+  int write_bbt;                /* convert output to brightness temperature */
+  int write_matrix;
+  queue_t queue;
+} ctl_t;
+
+/* Observation geometry and results for up to NRMAX rays. */
+typedef struct {
+  int nr;
+  double time[NRMAX];
+  double obsz[NRMAX], obslon[NRMAX], obslat[NRMAX];
+  double vpz[NRMAX], vplon[NRMAX], vplat[NRMAX];
+  double tpz[NRMAX], tplon[NRMAX], tplat[NRMAX];
+  double tau[NDMAX][NRMAX];     /* path transmittance */
+  double rad[NDMAX][NRMAX];     /* radiance [W/(m^2 sr cm^-1)]; NaN = masked */
+} obs_t;
+
+/* Aerosol/cloud models and the optical properties derived from them. */
+typedef struct {
+  int nm;
+  double top_mod[SCAMOD], bottom_mod[SCAMOD], trans_mod[SCAMOD];
+  char type[SCAMOD][LEN];
+  char filepath[SCAMOD][LEN];
+  double nn[SCAMOD], rr[SCAMOD], ss[SCAMOD];
+  int nl;
+  int nmod[NLMAX];
+  double top[NLMAX], bottom[NLMAX], trans[NLMAX];
+  double beta_e[NLMAX][NDMAX];  /* extinction [1/km] */
+  double beta_s[NLMAX][NDMAX];  /* scattering [1/km] */
+  double beta_a[NLMAX][NDMAX];  /* absorption [1/km] */
+  double p[NLMAX][NDMAX][NTHETA];  /* phase function */
+} aero_t;
+
+/* Atmospheric state (one or more profiles). */
+typedef struct {
+  int np;
+  double time[NPMAX];
+  double z[NPMAX], lon[NPMAX], lat[NPMAX];
+  double p[NPMAX], t[NPMAX];
+  double q[NGMAX][NPMAX];
+  double k[NWMAX][NPMAX];
+  int init;
+} atm_t;
+
+/* ------------------------------------------------------------------------
+ * Drop-in entry points.
+ * ------------------------------------------------------------------------ */
+
+/* Replaces formod (src/forwardmodel.c:15-116): saves the NaN mask of
+ * obs->rad, applies hydrostatic balance to atm->p (ctl->hydz >= 0), traces
+ * every ray, evaluates EGA transmittances, continua, Planck source and
+ * radiative transfer on the GPU (single/multiple scattering when
+ * ctl->sca_mult > 0 and ctl->sca_n > 0), converts to brightness temperature
+ * when ctl->write_bbt, and restores the mask.  Writes obs->rad, obs->tau and
+ * obs->tpz/tplon/tplat.  Errors follow the reference's ERRMSG convention
+ * (message, exit(EXIT_FAILURE)) unless jsc_set_exit_on_error(0). */
+void formod(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero);
+
+/* Brightness temperature of a radiance (src/forwardmodel.c:7-11). */
+double brightness(double rad, double nu);
+
+/* Planck function (src/forwardmodel.c:569-573). */
+double planck(double t, double nu);
+
+/* ------------------------------------------------------------------------
+ * Plain C-ABI.
+ * ------------------------------------------------------------------------ */
+
+/* Status codes returned by every jsc_* call. */
+enum {
+  JSC_OK = 0,
+  JSC_ERR_ARG = 1,        /* invalid argument or size */
+  JSC_ERR_CUDA = 2,       /* CUDA runtime error */
+  JSC_ERR_FILE = 3,       /* missing or unreadable input file */
+  JSC_ERR_TABLE = 4,      /* emissivity table exceeds a dimension */
+  JSC_ERR_NLOS = 5,       /* a ray needs more than NLOS points */
+  JSC_ERR_OBSERVER = 6,   /* observer below the surface */
+  JSC_ERR_QUEUE = 7,      /* scattering work queue over capacity */
+  JSC_ERR_WATCHDOG = 8,   /* a device-side wait gave up */
+  JSC_ERR_UNSUPPORTED = 9,/* feature outside the GPU path (ip != 1, FOV) */
+  JSC_ERR_NOMEM = 10      /* host or device allocation failed */
+};
+
+/* Message of a status code. */
+const char *jsc_status_string(int status);
+
+/* Status of the last formod() call on this thread. */
+int jsc_last_status(void);
+
+/* formod() error behaviour: 1 (default) prints and exits like the
+ * reference's ERRMSG, 0 returns with jsc_last_status() set. */
+void jsc_set_exit_on_error(int on);
+
+/* Message describing the last error on this thread. */
+const char *jsc_last_error_message(void);
+
+/* Release the model and batch that formod() caches between calls. */
+void jsc_release_cache(void);
+
+/* Number of CUDA kernels this library has launched since load. */
+uint64_t jsc_launch_count(void);
+
+/* Model: device-resident emissivity tables, Planck source tables and
+ * per-channel continuum coefficients for one set of emitters, channels and
+ * table files.  Built from ctl->ng/emitter/nd/nu/tblbase: reads
+ * <tblbase>_<nu>_<emitter>.bin (or .tab) like read_tbl
+ * (src/forwardmodel.c:610-739) and <tblbase>_<nu>.filt like srcfunc_planck
+ * (src/forwardmodel.c:743-786). */
+typedef struct jsc_model jsc_model;
+int jsc_model_create(const ctl_t *ctl, int device, jsc_model **out);
+void jsc_model_destroy(jsc_model *m);
+
+/* Device bytes held by the model's tables. */
+size_t jsc_model_table_bytes(const jsc_model *m);
+
+/* Batch: device buffers for many independent rays over many atmospheres.
+ *
+ * Atmospheres are 1-D profiles (ctl->ip == 1) stored ragged: profile a has
+ * levels [atm_off[a], atm_off[a+1]) of z/p/t and of q[g] and k[w], where the
+ * q block is laid out [ng][n_levels_total] and k [nw][n_levels_total].
+ * Ray r is traced through profile ray_atm[r].  Outputs are [n_rays][nd]. */
+typedef struct jsc_batch jsc_batch;
+
+typedef struct {
+  int n_atm;
+  int n_levels;              /* total levels of all profiles */
+  const int *atm_off;        /* [n_atm+1] */
+  const double *z, *lon, *lat, *p, *t;   /* [n_levels] */
+  const double *q;           /* [ng][n_levels] */
+  const double *k;           /* [nw][n_levels] */
+  int n_rays;
+  const int *ray_atm;        /* [n_rays] */
+  const double *time;        /* [n_rays] (solar geometry) */
+  const double *obsz, *obslon, *obslat;  /* [n_rays] */
+  const double *vpz, *vplon, *vplat;     /* [n_rays] */
+} jsc_batch_input;
+
+typedef struct {
+  double *rad;               /* [n_rays][nd] */
+  double *tau;               /* [n_rays][nd] */
+  double *tpz, *tplon, *tplat;  /* [n_rays], may be NULL */
+  int *nlos;                 /* [n_rays] LOS points per ray, may be NULL */
+} jsc_batch_output;
+
+/* Allocate device buffers for up to max_atm profiles, max_levels levels and
+ * max_rays rays (max_seg: LOS points over all rays; 0 picks a bound). */
+int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
+                     int max_levels, int max_rays, int64_t max_seg,
+                     jsc_batch **out);
+void jsc_batch_destroy(jsc_batch *b);
+
+/* Copy a batch's inputs from host memory to the device on stream (a
+ * cudaStream_t passed as void*, NULL = default stream).  The host arrays may
+ * be reused once the stream has passed this point. */
+int jsc_batch_upload(jsc_batch *b, const jsc_batch_input *in, void *stream);
+
+/* Run the forward model on the uploaded batch: hydrostatic balance (when
+ * ctl->hydz >= 0), ray tracing, EGA + continua + Planck + radiative
+ * transfer, all on the device, asynchronously on stream. */
+int jsc_batch_run(jsc_batch *b, void *stream);
+
+/* Copy results to host memory (waits for the stream). */
+int jsc_batch_download(jsc_batch *b, const jsc_batch_output *out, void *stream);
+
+/* upload + run + download in one call. */
+int jsc_formod_batch(jsc_model *m, const ctl_t *ctl, const jsc_batch_input *in,
+                     const jsc_batch_output *out, void *stream);
+
+/* Per-kernel timing of the last jsc_batch_run (CUDA events on its stream).
+ * kernel: "hydrostatic", "raytrace", "ega_rt".  Returns milliseconds, or a
+ * negative value when timing is off or the kernel did not run. */
+void jsc_batch_set_timing(jsc_batch *b, int on);
+double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel);
+
+/* Work counters of the last run: total LOS points, and the number of
+ * (point, channel, emitter) EGA interpolations actually evaluated. */
+int jsc_batch_counters(const jsc_batch *b, int64_t *n_points,
+                       int64_t *n_ega);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JURASSIC_B200_H */

@@ -1,0 +1,405 @@
+// Batches: device buffers for many rays over many atmospheric profiles, and
+// the launch sequence of one forward model over them.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <strings.h>
+
+#include "kernels.cuh"
+
+static void batch_free_los(jsc_batch *b) {
+  cudaFree(b->d_geo);
+  cudaFree(b->d_pts);
+  b->d_geo = b->d_pts = nullptr;
+}
+
+static int batch_alloc_los(jsc_batch *b, int64_t max_seg) {
+  batch_free_los(b);
+  int st;
+  if ((st = jsc_dmalloc(&b->d_geo, (size_t)max_seg * 4))) return st;
+  if ((st = jsc_dmalloc(&b->d_pts, (size_t)max_seg * b->W))) return st;
+  b->max_seg = max_seg;
+  return JSC_OK;
+}
+
+extern "C" void jsc_batch_destroy(jsc_batch *b) {
+  if (!b) return;
+  cudaFree(b->d_atm_off);
+  cudaFree(b->d_z);
+  cudaFree(b->d_lon);
+  cudaFree(b->d_lat);
+  cudaFree(b->d_p_in);
+  cudaFree(b->d_t);
+  cudaFree(b->d_q);
+  cudaFree(b->d_k);
+  cudaFree(b->d_p);
+  cudaFree(b->d_zmin);
+  cudaFree(b->d_zmax);
+  cudaFree(b->d_ray_atm);
+  cudaFree(b->d_ray);
+  cudaFree(b->d_nlos);
+  cudaFree(b->d_los_off);
+  batch_free_los(b);
+  cudaFree(b->d_tsurf);
+  cudaFree(b->d_tp);
+  cudaFree(b->d_rad);
+  cudaFree(b->d_tau);
+  cudaFree(b->d_status);
+  cudaFree(b->d_counters);
+  if (b->h_total) cudaFreeHost(b->h_total);
+  for (int i = 0; i < 2 * JSC_T_N; i++)
+    if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+  free(b);
+}
+
+extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
+                                int max_levels, int max_rays, int64_t max_seg,
+                                jsc_batch **out) {
+  if (!m || !ctl || !out || max_atm < 1 || max_levels < 2 || max_rays < 1) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_create: invalid arguments");
+    return JSC_ERR_ARG;
+  }
+  *out = nullptr;
+  if (ctl->ng != m->ng || ctl->nd != m->nd || ctl->nw != m->nw) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_create: ctl does not match the model");
+    return JSC_ERR_ARG;
+  }
+  if (ctl->ip != 1) {
+    jsc_set_error(JSC_ERR_UNSUPPORTED, "only IP=1 (profile interpolation) runs on the GPU");
+    return JSC_ERR_UNSUPPORTED;
+  }
+  JSC_CUDA_TRY(cudaSetDevice(m->device));
+  jsc_batch *b = (jsc_batch *)calloc(1, sizeof(jsc_batch));
+  if (!b) return JSC_ERR_NOMEM;
+  b->m = m;
+  jsc_run_cfg &c = b->cfg;
+  c.ng = ctl->ng;
+  c.nd = ctl->nd;
+  c.nw = ctl->nw;
+  c.ctm_co2 = ctl->ctm_co2;
+  c.ctm_h2o = ctl->ctm_h2o;
+  c.ctm_n2 = ctl->ctm_n2;
+  c.ctm_o2 = ctl->ctm_o2;
+  c.refrac = ctl->refrac;
+  c.rayds = ctl->rayds;
+  c.raydz = ctl->raydz;
+  c.hydz = ctl->hydz;
+  c.sca_n = ctl->sca_n;
+  c.sca_mult = ctl->sca_mult;
+  c.sca_ext_beta_a = strcmp(ctl->sca_ext, "beta_a") == 0;
+  b->max_atm = max_atm;
+  b->max_levels = max_levels;
+  b->max_rays = max_rays;
+  b->W = 4 + ctl->nw + ctl->ng;
+  const int ng = ctl->ng > 0 ? ctl->ng : 1, nw = ctl->nw > 0 ? ctl->nw : 1;
+  int st = JSC_OK;
+  st = st ? st : jsc_dmalloc(&b->d_atm_off, (size_t)max_atm + 1);
+  st = st ? st : jsc_dmalloc(&b->d_z, (size_t)max_levels);
+  st = st ? st : jsc_dmalloc(&b->d_lon, (size_t)max_levels);
+  st = st ? st : jsc_dmalloc(&b->d_lat, (size_t)max_levels);
+  st = st ? st : jsc_dmalloc(&b->d_p_in, (size_t)max_levels);
+  st = st ? st : jsc_dmalloc(&b->d_t, (size_t)max_levels);
+  st = st ? st : jsc_dmalloc(&b->d_q, (size_t)max_levels * ng);
+  st = st ? st : jsc_dmalloc(&b->d_k, (size_t)max_levels * nw);
+  st = st ? st : jsc_dmalloc(&b->d_p, (size_t)max_levels);
+  st = st ? st : jsc_dmalloc(&b->d_zmin, (size_t)max_atm);
+  st = st ? st : jsc_dmalloc(&b->d_zmax, (size_t)max_atm);
+  st = st ? st : jsc_dmalloc(&b->d_ray_atm, (size_t)max_rays);
+  st = st ? st : jsc_dmalloc(&b->d_ray, (size_t)max_rays * 9);
+  st = st ? st : jsc_dmalloc(&b->d_nlos, (size_t)max_rays);
+  st = st ? st : jsc_dmalloc(&b->d_los_off, (size_t)max_rays + 1);
+  st = st ? st : jsc_dmalloc(&b->d_tsurf, (size_t)max_rays);
+  st = st ? st : jsc_dmalloc(&b->d_tp, (size_t)max_rays * 3);
+  st = st ? st : jsc_dmalloc(&b->d_rad, (size_t)max_rays * ctl->nd);
+  st = st ? st : jsc_dmalloc(&b->d_tau, (size_t)max_rays * ctl->nd);
+  st = st ? st : jsc_dmalloc(&b->d_status, 1);
+  st = st ? st : jsc_dmalloc(&b->d_counters, 2);
+  if (!st) st = batch_alloc_los(b, max_seg > 0 ? max_seg : (int64_t)max_rays * 512);
+  if (!st && cudaMallocHost((void **)&b->h_total, sizeof(int64_t)) != cudaSuccess) {
+    jsc_set_error(JSC_ERR_NOMEM, "pinned host allocation");
+    st = JSC_ERR_NOMEM;
+  }
+  for (int i = 0; i < 2 * JSC_T_N && !st; i++)
+    if (cudaEventCreate(&b->ev[i]) != cudaSuccess) st = JSC_ERR_CUDA;
+  if (st) {
+    jsc_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return JSC_OK;
+}
+
+#define CPY(dst, src, n, s)                                                  \
+  JSC_CUDA_TRY(cudaMemcpyAsync((dst), (src), (size_t)(n) * sizeof(*(src)),   \
+                               cudaMemcpyHostToDevice, (cudaStream_t)(s)))
+
+extern "C" int jsc_batch_upload(jsc_batch *b, const jsc_batch_input *in,
+                                void *stream) {
+  if (!b || !in) return JSC_ERR_ARG;
+  const int ng = b->cfg.ng, nw = b->cfg.nw;
+  if (in->n_atm < 1 || in->n_atm > b->max_atm || in->n_levels < 2 ||
+      in->n_levels > b->max_levels || in->n_rays < 0 || in->n_rays > b->max_rays) {
+    jsc_set_error(JSC_ERR_ARG, "batch input exceeds the batch capacity");
+    return JSC_ERR_ARG;
+  }
+  // Validate every index the kernels follow, so no device access leaves its
+  // buffer: profile offsets increase and stay inside the level arrays, every
+  // profile has two levels or more, every ray names an existing profile.
+  if (in->atm_off[0] != 0 || in->atm_off[in->n_atm] != in->n_levels) {
+    jsc_set_error(JSC_ERR_ARG, "atm_off must start at 0 and end at n_levels");
+    return JSC_ERR_ARG;
+  }
+  for (int a = 0; a < in->n_atm; a++)
+    if (in->atm_off[a + 1] - in->atm_off[a] < 2) {
+      jsc_set_error(JSC_ERR_ARG, "profile %d has fewer than 2 levels", a);
+      return JSC_ERR_ARG;
+    }
+  for (int r = 0; r < in->n_rays; r++)
+    if (in->ray_atm[r] < 0 || in->ray_atm[r] >= in->n_atm) {
+      jsc_set_error(JSC_ERR_ARG, "ray %d names profile %d of %d", r,
+                    in->ray_atm[r], in->n_atm);
+      return JSC_ERR_ARG;
+    }
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  b->n_atm = in->n_atm;
+  b->n_levels = in->n_levels;
+  b->n_rays = in->n_rays;
+  const int nl = in->n_levels, nr = in->n_rays;
+  CPY(b->d_atm_off, in->atm_off, in->n_atm + 1, stream);
+  CPY(b->d_z, in->z, nl, stream);
+  CPY(b->d_lon, in->lon, nl, stream);
+  CPY(b->d_lat, in->lat, nl, stream);
+  CPY(b->d_p_in, in->p, nl, stream);
+  CPY(b->d_t, in->t, nl, stream);
+  if (ng > 0) CPY(b->d_q, in->q, (size_t)ng * nl, stream);
+  if (nw > 0) CPY(b->d_k, in->k, (size_t)nw * nl, stream);
+  if (nr > 0) {
+    CPY(b->d_ray_atm, in->ray_atm, nr, stream);
+    const double *cols[7] = {in->time, in->obsz, in->obslon, in->obslat,
+                             in->vpz, in->vplon, in->vplat};
+    for (int i = 0; i < 7; i++) {
+      if (cols[i]) {
+        CPY(b->d_ray + (size_t)i * nr, cols[i], nr, stream);
+      } else {
+        JSC_CUDA_TRY(cudaMemsetAsync(b->d_ray + (size_t)i * nr, 0,
+                                     (size_t)nr * sizeof(double),
+                                     (cudaStream_t)stream));
+      }
+    }
+  }
+  return JSC_OK;
+}
+
+static void ev_record(jsc_batch *b, int k, int end, cudaStream_t s) {
+  if (b->timing) cudaEventRecord(b->ev[2 * k + end], s);
+  if (end) b->ran[k] = 1;
+}
+
+extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
+  if (!b) return JSC_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const jsc_model *m = b->m;
+  const int nr = b->n_rays;
+  JSC_CUDA_TRY(cudaSetDevice(m->device));
+  for (int k = 0; k < JSC_T_N; k++) b->ran[k] = 0;
+  JSC_CUDA_TRY(cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s));
+  JSC_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(unsigned long long), s));
+
+  AtmArgs aa;
+  aa.n_atm = b->n_atm;
+  aa.n_levels = b->n_levels;
+  aa.ng = b->cfg.ng;
+  aa.nw = b->cfg.nw;
+  aa.ig_h2o = m->dv.ig_h2o;
+  aa.off = b->d_atm_off;
+  aa.z = b->d_z;
+  aa.lon = b->d_lon;
+  aa.lat = b->d_lat;
+  aa.p_in = b->d_p_in;
+  aa.t = b->d_t;
+  aa.q = b->d_q;
+  aa.k = b->d_k;
+  aa.p = b->d_p;
+  aa.zmin = b->d_zmin;
+  aa.zmax = b->d_zmax;
+  aa.hydz = b->cfg.hydz;
+  ev_record(b, JSC_T_HYDRO, 0, s);
+  hydro_kernel<<<(b->n_atm + 127) / 128, 128, 0, s>>>(aa);
+  JSC_LAUNCH_CHECK();
+  ev_record(b, JSC_T_HYDRO, 1, s);
+  if (nr == 0) return JSC_OK;
+
+  RayArgs ra;
+  ra.n_rays = nr;
+  ra.ng = b->cfg.ng;
+  ra.nw = b->cfg.nw;
+  ra.ig_h2o = m->dv.ig_h2o;
+  ra.n_levels = b->n_levels;
+  ra.refrac = b->cfg.refrac;
+  ra.rayds = b->cfg.rayds;
+  ra.raydz = b->cfg.raydz;
+  ra.ray_atm = b->d_ray_atm;
+  ra.atm_off = b->d_atm_off;
+  ra.time = b->d_ray;
+  ra.obsz = b->d_ray + (size_t)nr;
+  ra.obslon = b->d_ray + 2 * (size_t)nr;
+  ra.obslat = b->d_ray + 3 * (size_t)nr;
+  ra.vpz = b->d_ray + 4 * (size_t)nr;
+  ra.vplon = b->d_ray + 5 * (size_t)nr;
+  ra.vplat = b->d_ray + 6 * (size_t)nr;
+  ra.z = b->d_z;
+  ra.p = b->d_p;
+  ra.t = b->d_t;
+  ra.q = b->d_q;
+  ra.k = b->d_k;
+  ra.zmin = b->d_zmin;
+  ra.zmax = b->d_zmax;
+  ra.nlos = b->d_nlos;
+  ra.los_off = b->d_los_off;
+  ra.W = b->W;
+  ra.tsurf = b->d_tsurf;
+  ra.tp = b->d_tp;
+  ra.status = b->d_status;
+
+  ev_record(b, JSC_T_RAYTRACE, 0, s);
+  ra.geo = b->d_geo;
+  ra.pts = b->d_pts;
+  ra.max_seg = b->max_seg;
+  raytrace_kernel<false><<<(nr + 127) / 128, 128, 0, s>>>(ra);
+  JSC_LAUNCH_CHECK();
+  scan_kernel<<<1, 1024, 0, s>>>(b->d_nlos, nr, b->d_los_off);
+  JSC_LAUNCH_CHECK();
+  // The LOS buffer is sized from the counting pass (one small copy).
+  JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, b->d_los_off + nr, sizeof(int64_t),
+                               cudaMemcpyDeviceToHost, s));
+  JSC_CUDA_TRY(cudaStreamSynchronize(s));
+  if (*b->h_total > b->max_seg) {
+    int st = batch_alloc_los(b, *b->h_total + *b->h_total / 4 + 1024);
+    if (st) return st;
+  }
+  ra.geo = b->d_geo;
+  ra.pts = b->d_pts;
+  ra.max_seg = b->max_seg;
+  raytrace_kernel<true><<<(nr + 127) / 128, 128, 0, s>>>(ra);
+  JSC_LAUNCH_CHECK();
+  ev_record(b, JSC_T_RAYTRACE, 1, s);
+
+  EgaArgs ea;
+  ea.m = m->dv;
+  ea.cfg = b->cfg;
+  ea.n_rays = nr;
+  ea.W = b->W;
+  int gl = 1, gl_log2 = 0;
+  while (gl < m->nd && gl < 32) {
+    gl <<= 1;
+    gl_log2++;
+  }
+  ea.gl_log2 = gl_log2;
+  ea.cpl = (m->nd + gl - 1) / gl;
+  ea.nlos = b->d_nlos;
+  ea.los_off = b->d_los_off;
+  ea.pts = b->d_pts;
+  ea.tsurf = b->d_tsurf;
+  ea.rad = b->d_rad;
+  ea.tau = b->d_tau;
+  ea.counters = b->d_counters;
+  const size_t per_thread = (size_t)ea.cpl * (m->ng > 0 ? m->ng : 1) * (sizeof(double) + sizeof(int));
+  int blk = 128;
+  while (blk > 32 && per_thread * blk > 96 * 1024) blk >>= 1;
+  const size_t smem = per_thread * blk;
+  if (smem > 48 * 1024)
+    JSC_CUDA_TRY(cudaFuncSetAttribute(ega_rt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+  const int64_t threads = (int64_t)nr * gl;
+  ev_record(b, JSC_T_EGA, 0, s);
+  ega_rt_kernel<<<(unsigned)((threads + blk - 1) / blk), blk, smem, s>>>(ea);
+  JSC_LAUNCH_CHECK();
+  ev_record(b, JSC_T_EGA, 1, s);
+  // LOS point total for the work counters.
+  JSC_CUDA_TRY(cudaMemcpyAsync(b->d_counters, b->d_los_off + nr, sizeof(int64_t),
+                               cudaMemcpyDeviceToDevice, s));
+  return JSC_OK;
+}
+
+static int map_status(unsigned st) {
+  if (st & JSC_DEV_ERR_OBSERVER) {
+    jsc_set_error(JSC_ERR_OBSERVER, "Observer below surface!");
+    return JSC_ERR_OBSERVER;
+  }
+  if (st & JSC_DEV_ERR_NLOS) {
+    jsc_set_error(JSC_ERR_NLOS, "Too many LOS points!");
+    return JSC_ERR_NLOS;
+  }
+  if (st & JSC_DEV_ERR_QUEUE) {
+    jsc_set_error(JSC_ERR_QUEUE, "Too many queue items!");
+    return JSC_ERR_QUEUE;
+  }
+  if (st & JSC_DEV_ERR_WATCHDOG) {
+    jsc_set_error(JSC_ERR_WATCHDOG, "device wait gave up");
+    return JSC_ERR_WATCHDOG;
+  }
+  return JSC_OK;
+}
+
+#define DCPY(dst, src, n, s)                                                 \
+  JSC_CUDA_TRY(cudaMemcpyAsync((dst), (src), (size_t)(n) * sizeof(*(src)),   \
+                               cudaMemcpyDeviceToHost, (cudaStream_t)(s)))
+
+extern "C" int jsc_batch_download(jsc_batch *b, const jsc_batch_output *out,
+                                  void *stream) {
+  if (!b || !out) return JSC_ERR_ARG;
+  const int nr = b->n_rays, nd = b->cfg.nd;
+  unsigned status = 0;
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  if (nr > 0) {
+    if (out->rad) DCPY(out->rad, b->d_rad, (size_t)nr * nd, stream);
+    if (out->tau) DCPY(out->tau, b->d_tau, (size_t)nr * nd, stream);
+    if (out->tpz) DCPY(out->tpz, b->d_tp, nr, stream);
+    if (out->tplon) DCPY(out->tplon, b->d_tp + nr, nr, stream);
+    if (out->tplat) DCPY(out->tplat, b->d_tp + 2 * (size_t)nr, nr, stream);
+    if (out->nlos) DCPY(out->nlos, b->d_nlos, nr, stream);
+  }
+  DCPY(&status, b->d_status, 1, stream);
+  JSC_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  return map_status(status);
+}
+
+extern "C" int jsc_formod_batch(jsc_model *m, const ctl_t *ctl,
+                                const jsc_batch_input *in,
+                                const jsc_batch_output *out, void *stream) {
+  jsc_batch *b = nullptr;
+  int st = jsc_batch_create(m, ctl, in->n_atm, in->n_levels,
+                            in->n_rays > 0 ? in->n_rays : 1, 0, &b);
+  if (!st) st = jsc_batch_upload(b, in, stream);
+  if (!st) st = jsc_batch_run(b, stream);
+  if (!st) st = jsc_batch_download(b, out, stream);
+  jsc_batch_destroy(b);
+  return st;
+}
+
+extern "C" void jsc_batch_set_timing(jsc_batch *b, int on) {
+  if (b) b->timing = on;
+}
+
+extern "C" double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel) {
+  if (!b || !b->timing || !kernel) return -1;
+  int k = -1;
+  if (!strcmp(kernel, "hydrostatic")) k = JSC_T_HYDRO;
+  else if (!strcmp(kernel, "raytrace")) k = JSC_T_RAYTRACE;
+  else if (!strcmp(kernel, "ega_rt")) k = JSC_T_EGA;
+  if (k < 0 || !b->ran[k]) return -1;
+  float ms = -1;
+  if (cudaEventSynchronize(b->ev[2 * k + 1]) != cudaSuccess) return -1;
+  if (cudaEventElapsedTime(&ms, b->ev[2 * k], b->ev[2 * k + 1]) != cudaSuccess) return -1;
+  return ms;
+}
+
+extern "C" int jsc_batch_counters(const jsc_batch *b, int64_t *n_points,
+                                  int64_t *n_ega) {
+  if (!b) return JSC_ERR_ARG;
+  unsigned long long c[2] = {0, 0};
+  JSC_CUDA_TRY(cudaMemcpy(c, b->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+  if (n_points) *n_points = (int64_t)c[0];
+  if (n_ega) *n_ega = (int64_t)c[1];
+  return JSC_OK;
+}

@@ -1,0 +1,172 @@
+/*
+ * Internal interface between the C host code (tables, filters, continua,
+ * formod drop-in) and the CUDA layer (model upload, kernels, batches).
+ * Not installed; the public interface is include/jurassic_b200.h.
+ */
+#ifndef JSC_INTERNAL_H
+#define JSC_INTERNAL_H
+
+#include "jurassic_b200.h"
+
+#ifdef __CUDACC__
+#define JSC_HD __host__ __device__ __forceinline__
+#define JSC_ALIGN(n) __align__(n)
+#else
+#define JSC_HD static inline
+#define JSC_ALIGN(n) __attribute__((aligned(n)))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Planck source table: 1201 temperatures from 100 K to 400 K in 0.25 K
+ * steps (src/forwardmodel.c:747-784). */
+#define JSC_NPLANCK 1201
+#define JSC_PLANCK_TMIN 100.0
+#define JSC_PLANCK_TMAX 400.0
+
+/* ------------------------------------------------------------------------
+ * Small numerical helpers shared by host and device.  They keep the exact
+ * operation order of the reference macros, so results agree bit for bit
+ * when no FMA contraction is applied (device code is built --fmad=false).
+ * ------------------------------------------------------------------------ */
+
+/* LIN macro of src/jurassic.h:72-73. */
+JSC_HD double jsc_lin(double x0, double y0, double x1, double y1, double x) {
+  return y0 + (y1 - y0) / (x1 - x0) * (x - x0);
+}
+
+/* GSL_MAX(GSL_MIN(x, 1), 0) with GSL's ternary semantics (NaN -> 1). */
+JSC_HD double jsc_clamp01(double x) {
+  double m = (x < 1.0 ? x : 1.0);
+  return (m > 0.0 ? m : 0.0);
+}
+
+/* Bisection of src/misc.c:237-265 on an ascending or descending double
+ * array; n >= 2 (n < 2 returns 0 without reading). */
+JSC_HD int jsc_locate(const double *xx, int n, double x) {
+  int ilo = 0, ihi = n - 1, i;
+  if (n < 2) return 0;
+  i = (ihi + ilo) >> 1;
+  if (xx[i] < xx[i + 1]) {
+    while (ihi > ilo + 1) {
+      i = (ihi + ilo) >> 1;
+      if (xx[i] > x) ihi = i; else ilo = i;
+    }
+  } else {
+    while (ihi > ilo + 1) {
+      i = (ihi + ilo) >> 1;
+      if (xx[i] <= x) ihi = i; else ilo = i;
+    }
+  }
+  return ilo;
+}
+
+/* ------------------------------------------------------------------------
+ * Host staging of the emissivity tables (what read_tbl produces, but only
+ * for the tables that exist, in compact arrays).
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  int np;                                  /* pressure levels, < 2: no table */
+  double p[TBLNPMAX];
+  int nt[TBLNPMAX];
+  double t[TBLNPMAX][TBLNTMAX];
+  int nu[TBLNPMAX][TBLNTMAX];              /* points per (p, T) row */
+  int64_t off[TBLNPMAX][TBLNTMAX];         /* first point in u[]/eps[] */
+} jsc_host_table;
+
+typedef struct {
+  int ng, nd;
+  jsc_host_table *tab;                     /* [nd][ng] (index id*ng+ig) */
+  float *u, *eps;                          /* all rows back to back */
+  int64_t n_points, cap_points;
+} jsc_host_tables;
+
+/* Per-channel continuum coefficients (ctmco2/ctmh2o/ctmn2/ctmo2 of
+ * src/continua.c with the wavenumber interpolation done once per channel). */
+typedef struct {
+  int co2_on;      /* CO2 continuum active for this channel */
+  double co2_c230, co2_c260, co2_c296;
+  int h2o_on;
+  double h2o_self296;   /* sfac * cw296 */
+  double h2o_ratio;     /* cw260 / cw296 */
+  double h2o_frn;       /* cwfrn * fscal */
+  int n2_on;
+  double n2_b, n2_beta;
+  int o2_on;
+  double o2_b, o2_beta;
+} jsc_ctm_coef;
+
+/* Everything the host reads or derives before upload. */
+typedef struct {
+  int ng, nd, nw;
+  double nu[NDMAX];
+  int window[NDMAX];
+  int ig_co2, ig_h2o;          /* emitter indices, -1 when absent */
+  int ctm_co2, ctm_h2o, ctm_n2, ctm_o2;
+  jsc_host_tables tables;
+  double *planck_b;            /* [nd][JSC_NPLANCK] */
+  double *planck_s;            /* [nd][JSC_NPLANCK] slope to the next node */
+  jsc_ctm_coef ctm[NDMAX];
+} jsc_host_model;
+
+/* Readers and derived data (model_host.c).  Return JSC_* status. */
+int jsc_host_model_load(const ctl_t *ctl, jsc_host_model *hm);
+void jsc_host_model_free(jsc_host_model *hm);
+int jsc_read_filter(const char *filename, double *nu, double *f, int *n);
+void jsc_ctm_coefficients(const ctl_t *ctl, jsc_ctm_coef *c, int id);
+double jsc_gsl_expm1(double x);
+double jsc_gsl_log1p(double x);
+int jsc_find_emitter(const ctl_t *ctl, const char *name);
+
+/* Error reporting shared by C and CUDA parts. */
+void jsc_set_error(int status, const char *fmt, ...);
+
+/* ------------------------------------------------------------------------
+ * Device layout of a model (device pointers; passed by value to kernels).
+ * ------------------------------------------------------------------------ */
+
+/* One interval [k, k+1] of an emissivity-table row: the bracketing points
+ * and both interpolation slopes, computed in double exactly as the
+ * reference's LIN computes them at run time (src/forwardmodel.c:519-541). */
+typedef struct JSC_ALIGN(16) {
+  float u0, e0, u1, e1;
+  double s_ue;      /* (u1-u0)/(e1-e0): eps -> u  (intpol_tbl_u) */
+  double s_eu;      /* (e1-e0)/(u1-u0): u -> eps  (intpol_tbl_eps) */
+} jsc_interval;
+
+/* Row descriptor: first interval of the row and n | flags << 16, where n is
+ * the number of points of the row. */
+typedef struct JSC_ALIGN(8) {
+  int off;
+  int nf;
+} jsc_row;
+
+/* Row descriptor flags. */
+#define JSC_ROW_STRICT 1   /* u and eps strictly increasing */
+
+typedef struct {
+  int ng, nd, nw;
+  int ig_co2, ig_h2o;
+  int n_grid;
+  /* (p, T) grids shared by tables; grid g occupies
+   * p[g*TBLNPMAX], nt[g*TBLNPMAX], t[(g*TBLNPMAX+ip)*TBLNTMAX+it]. */
+  const int *grid_np;
+  const double *grid_p;
+  const int *grid_nt;
+  const double *grid_t;
+  const int *tab_grid;       /* [nd*ng] grid id, -1: table unusable (np<2) */
+  const jsc_row *rows;       /* [nd*ng][TBLNPMAX][TBLNTMAX] */
+  const jsc_interval *iv;
+  const double *planck_b, *planck_s;   /* [nd][JSC_NPLANCK] */
+  const jsc_ctm_coef *ctm;             /* [nd] */
+  const double *nu;                    /* [nd] */
+  const int *window;                   /* [nd] */
+} jsc_dev_model;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JSC_INTERNAL_H */

@@ -1,0 +1,68 @@
+// Definitions of the opaque handles declared in jurassic_b200.h (CUDA side).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "jsc_internal.h"
+
+struct jsc_model {
+  int device;
+  int ng, nd, nw;
+  int n_grid;
+  int64_t n_intervals;
+  size_t table_bytes;
+  double nu[NDMAX];
+  jsc_dev_model dv;  // device view passed to kernels
+  int *d_grid_np, *d_grid_nt, *d_tab_grid, *d_window;
+  double *d_grid_p, *d_grid_t, *d_planck_b, *d_planck_s, *d_nu;
+  jsc_row *d_rows;
+  jsc_interval *d_iv;
+  jsc_ctm_coef *d_ctm;
+};
+
+// Forward-model switches copied from ctl_t when a batch is created.
+struct jsc_run_cfg {
+  int ng, nd, nw;
+  int ctm_co2, ctm_h2o, ctm_n2, ctm_o2;
+  int refrac;
+  double rayds, raydz, hydz;
+  int sca_n, sca_mult, sca_ext_beta_a;
+};
+
+// Kernel timers of a batch.
+enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_N };
+
+struct jsc_batch {
+  jsc_model *m;
+  jsc_run_cfg cfg;
+  int max_atm, max_levels, max_rays;
+  int64_t max_seg;
+  int n_atm, n_levels, n_rays;
+  int W;  // doubles per LOS point record for the radiative transfer
+
+  // Inputs.
+  int *d_atm_off;
+  double *d_z, *d_lon, *d_lat, *d_p_in, *d_t, *d_q, *d_k;
+  double *d_p;              // pressure after hydrostatic balance
+  double *d_zmin, *d_zmax;  // per profile
+  int *d_ray_atm;
+  double *d_ray;            // [9][max_rays]: time obsz obslon obslat vpz vplon vplat + 2 spare
+
+  // Line of sight.
+  int *d_nlos;
+  int64_t *d_los_off;       // [max_rays+1]
+  double *d_geo;            // [max_seg][4]: z lon lat raw-ds
+  double *d_pts;            // [max_seg][W]: p t ds qh2o k[nw] u[ng]
+  double *d_tsurf;          // [max_rays]
+  double *d_tp;             // [3][max_rays]
+
+  // Outputs and status.
+  double *d_rad, *d_tau;    // [max_rays][nd]
+  unsigned *d_status;
+  unsigned long long *d_counters;  // [0] LOS points, [1] EGA evaluations
+  int64_t *h_total;         // pinned: LOS points of the current batch
+
+  int timing;
+  cudaEvent_t ev[2 * JSC_T_N];
+  int ran[JSC_T_N];
+};

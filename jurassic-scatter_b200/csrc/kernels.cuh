@@ -1,0 +1,647 @@
+// Device kernels of the clear-air forward model.
+//
+//   hydro_kernel      one thread per profile: hydrostatic pressure
+//                     (src/atmosphere.c:163-243) and the profile's z range.
+//   raytrace_kernel   one thread per ray, FP64 refracted ray march
+//                     (src/lineofsight.c:5-190); a counting pass sizes the
+//                     line of sight, a storing pass writes the LOS records.
+//   scan_kernel       exclusive prefix sum of LOS points per ray.
+//   ega_rt_kernel     a group of lanes per ray, lanes over channels: EGA
+//                     table interpolation (src/forwardmodel.c:409-565),
+//                     continua (src/forwardmodel.c:120-152, src/continua.c),
+//                     Planck source (src/forwardmodel.c:743-794) and the
+//                     radiative-transfer recursion
+//                     (src/forwardmodel.c:302-399), fused, serial along the
+//                     ray because the EGA carries the path transmittance.
+//
+// All arithmetic that decides a table index is FP64 in the reference's
+// operation order (the library is built with --fmad=false), so the indices
+// and segment counts agree with the reference.
+#pragma once
+#include <math.h>
+#include <stdint.h>
+
+#include "jsc_model.h"
+#include "physics.h"
+#include "cuda_util.cuh"
+
+#define JSC_ZREFRAC 60.0   // refraction is evaluated up to this altitude [km]
+#define JSC_FD_STEP 0.02   // finite-difference step of the refractivity gradient [km]
+
+// ----------------------------------------------------------------- inputs --
+
+struct AtmArgs {
+  int n_atm, n_levels, ng, nw, ig_h2o;
+  const int *off;
+  const double *z, *lon, *lat, *p_in, *t, *q, *k;
+  double *p, *zmin, *zmax;
+  double hydz;
+};
+
+// Hydrostatic balance and altitude range of each profile.
+__global__ void hydro_kernel(AtmArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_atm) return;
+  const int lo = a.off[i], n = a.off[i + 1] - lo;
+  for (int l = 0; l < n; l++) a.p[lo + l] = a.p_in[lo + l];
+  if (a.hydz >= 0 && n > 0) {
+    const double *qh = a.ig_h2o >= 0 ? a.q + (size_t)a.ig_h2o * a.n_levels + lo : nullptr;
+    jsc_hydrostatic(a.hydz, n, a.z + lo, a.lon + lo, a.lat + lo, a.t + lo, qh,
+                    a.p + lo);
+  }
+  // gsl_stats_min/max: first element, then strict comparisons; NaN wins.
+  double mn = n > 0 ? a.z[lo] : 0.0, mx = mn;
+  bool nan = false;
+  for (int l = 0; l < n; l++) {
+    double v = a.z[lo + l];
+    if (v < mn) mn = v;
+    if (v > mx) mx = v;
+    if (isnan(v)) nan = true;
+  }
+  a.zmin[i] = nan ? NAN : mn;
+  a.zmax[i] = nan ? NAN : mx;
+}
+
+// --------------------------------------------------------------- raytrace --
+
+struct RayArgs {
+  int n_rays, ng, nw, ig_h2o, n_levels;
+  int refrac;
+  double rayds, raydz;
+  const int *ray_atm, *atm_off;
+  const double *time, *obsz, *obslon, *obslat, *vpz, *vplon, *vplat;
+  const double *z, *p, *t, *q, *k, *zmin, *zmax;
+  int *nlos;
+  const int64_t *los_off;
+  int64_t max_seg;
+  int W;
+  double *geo, *pts, *tsurf, *tp;  // tp: [3][n_rays]
+  unsigned *status;
+};
+
+struct Profile {
+  const double *z, *p, *t, *q, *k;
+  int n, stride;  // levels; stride between emitter/window blocks
+};
+
+// Pressure and temperature at altitude z0 (src/atmosphere.c:298-315).
+__device__ __forceinline__ void atm_pt(const Profile &a, double z0, double *p,
+                                       double *t) {
+  int ip = jsc_locate(a.z, a.n, z0);
+  *p = jsc_exp_interp(a.z[ip], a.p[ip], a.z[ip + 1], a.p[ip + 1], z0);
+  *t = jsc_lin(a.z[ip], a.t[ip], a.z[ip + 1], a.t[ip + 1], z0);
+}
+
+// Pressure and temperature at altitude z0; returns the profile level below
+// z0 for the remaining LIN interpolations (src/atmosphere.c:298-320).
+__device__ __forceinline__ int atm_full(const Profile &a, double z0, double *p,
+                                        double *t) {
+  int ip = jsc_locate(a.z, a.n, z0);
+  *p = jsc_exp_interp(a.z[ip], a.p[ip], a.z[ip + 1], a.p[ip + 1], z0);
+  *t = jsc_lin(a.z[ip], a.t[ip], a.z[ip + 1], a.t[ip + 1], z0);
+  return ip;
+}
+
+__device__ __forceinline__ double atm_lin(const double *v, const Profile &a,
+                                          int ip, double z0) {
+  return jsc_lin(a.z[ip], v[ip], a.z[ip + 1], v[ip + 1], z0);
+}
+
+// One LOS point: geometry, state, raw step.  Written by the storing pass.
+template <bool STORE>
+__device__ __forceinline__ void emit_point(const RayArgs &A, const Profile &a,
+                                           int64_t idx, double z, double lon,
+                                           double lat, double p, double t,
+                                           int ipz, double zq, double raw_ds,
+                                           double ds) {
+  if (!STORE) return;
+  double *g = A.geo + idx * 4;
+  g[0] = z;
+  g[1] = lon;
+  g[2] = lat;
+  g[3] = raw_ds;
+  double *r = A.pts + idx * A.W;
+  r[0] = p;
+  r[1] = t;
+  r[2] = ds;
+  r[3] = A.ig_h2o >= 0 ? atm_lin(a.q + (size_t)A.ig_h2o * a.stride, a, ipz, zq) : 0.0;
+  for (int w = 0; w < A.nw; w++) r[4 + w] = atm_lin(a.k + (size_t)w * a.stride, a, ipz, zq);
+  // Column density (src/lineofsight.c:182-185) with the final step length.
+  for (int g2 = 0; g2 < A.ng; g2++) {
+    double q = atm_lin(a.q + (size_t)g2 * a.stride, a, ipz, zq);
+    r[4 + A.nw + g2] = 10 * q * p / (JSC_KBOLTZ * t) * ds;
+  }
+}
+
+// Ray march of one ray (src/lineofsight.c:5-190 without the aerosol layer
+// refinement).  COUNT pass: returns the number of LOS points.  STORE pass:
+// writes the points at los_off[r], the tangent point and surface temperature.
+template <bool STORE>
+__device__ int trace_ray(const RayArgs &A, int r) {
+  const int ai = A.ray_atm[r];
+  const int lo = A.atm_off[ai];
+  Profile a;
+  a.n = A.atm_off[ai + 1] - lo;
+  a.stride = A.n_levels;
+  a.z = A.z + lo;
+  a.p = A.p + lo;
+  a.t = A.t + lo;
+  a.q = A.q + lo;
+  a.k = A.k + lo;
+  const double zmin = A.zmin[ai], zmax = A.zmax[ai];
+  const double obsz = A.obsz[r], vpz = A.vpz[r];
+  int64_t base = 0;
+  if (STORE) {
+    base = A.los_off[r];
+    A.tp[r] = vpz;
+    A.tp[A.n_rays + r] = A.vplon[r];
+    A.tp[2 * A.n_rays + r] = A.vplat[r];
+    A.tsurf[r] = -999;
+  }
+  if (obsz < zmin) {
+    atomicOr(A.status, JSC_DEV_ERR_OBSERVER);
+    return 0;
+  }
+  if (vpz > zmax - 0.001) return 0;
+
+  double xobs[3], xvp[3], ex0[3], ex1[3], x[3], xh[3], ng[3];
+  jsc_geo2cart(obsz, A.obslon[r], A.obslat[r], xobs);
+  jsc_geo2cart(vpz, A.vplon[r], A.vplat[r], xvp);
+  for (int i = 0; i < 3; i++) ex0[i] = xvp[i] - xobs[i];
+  double norm = sqrt(ex0[0] * ex0[0] + ex0[1] * ex0[1] + ex0[2] * ex0[2]);
+  for (int i = 0; i < 3; i++) ex0[i] /= norm;
+  for (int i = 0; i < 3; i++) x[i] = xobs[i];
+
+  double z = 1e99, lon = 0, lat = 0, p = 0, t = 0;
+  // Observer above the atmosphere: bisect for the entry point.
+  if (obsz > zmax) {
+    double dmin = 0, dmax = norm, d;
+    while (fabs(dmin - dmax) > 0.001) {
+      d = (dmax + dmin) / 2;
+      for (int i = 0; i < 3; i++) x[i] = xobs[i] + d * ex0[i];
+      jsc_cart2geo(x, &z, &lon, &lat);
+      if (z <= zmax && z > zmax - 0.001) break;
+      if (z < zmax - 0.0005) dmax = d; else dmin = d;
+    }
+  }
+
+  int np = 0, stop = 0;
+  double zprev = 0, lonprev = 0, latprev = 0, rprev = 0, rprev2 = 0, dprev = 0;
+  while (1) {
+    double ds = A.rayds;
+    if (A.raydz > 0) {
+      norm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+      for (int i = 0; i < 3; i++) xh[i] = x[i] / norm;
+      double cosa = fabs(ex0[0] * xh[0] + ex0[1] * xh[1] + ex0[2] * xh[2]);
+      if (cosa != 0) {
+        const double dz = A.raydz / cosa;
+        ds = (A.rayds < dz ? A.rayds : dz);  // GSL_MIN
+      }
+    }
+    jsc_cart2geo(x, &z, &lon, &lat);
+
+    double pz, plon, plat, pp, pt, raw;
+    if (z < zmin + 0.001 || z > zmax + 0.001) {
+      // Last point: where the segment from the previous point crosses the
+      // boundary (intersection_point, src/lineofsight.c:385-407).
+      stop = (z < zmin + 0.001 ? 2 : 1);
+      const double zlim = (stop == 2 ? zmin : zmax);
+      const double z0 = np > 0 ? zprev : z, lon0 = np > 0 ? lonprev : lon,
+                   lat0 = np > 0 ? latprev : lat;
+      double x1[3], x2[3];
+      const double frac = (z0 - zlim) / (z0 - z);
+      jsc_geo2cart(z0, lon0, lat0, x1);
+      jsc_geo2cart(z, lon, lat, x2);
+      for (int i = 0; i < 3; i++) x2[i] = x1[i] + frac * (x2[i] - x1[i]);
+      jsc_cart2geo(x2, &pz, &plon, &plat);
+      raw = 0.;
+    } else {
+      pz = z;
+      plon = lon;
+      plat = lat;
+      raw = ds;
+    }
+    int ipz = 0;
+    pp = pt = 0;
+    if (STORE || !stop) ipz = atm_full(a, pz, &pp, &pt);
+    if (!stop) {
+      p = pp;
+      t = pt;
+    }
+    if (np >= NLOS) {
+      atomicOr(A.status, JSC_DEV_ERR_NLOS);
+      return np;
+    }
+    // Step lengths are smoothed in place along the ray
+    // (src/lineofsight.c:177-179): d[0] = r[0]/2, d[i] = (d[i-1] + r[i])/2.
+    const double dsm = (np == 0) ? 0.5 * raw : 0.5 * (dprev + raw);
+    if (STORE) {
+      if (base + np >= A.max_seg) {
+        atomicOr(A.status, JSC_DEV_ERR_NLOS);
+        return np;
+      }
+      emit_point<true>(A, a, base + np, pz, plon, plat, pp, pt, ipz, pz, raw, dsm);
+    }
+    np++;
+    rprev2 = rprev;
+    rprev = raw;
+    dprev = dsm;
+    zprev = pz;
+    lonprev = plon;
+    latprev = plat;
+    if (stop) {
+      if (STORE) A.tsurf[r] = (stop == 2 ? t : -999);
+      break;
+    }
+
+    // Refraction (src/lineofsight.c:122-166).
+    double n = (A.refrac && z <= JSC_ZREFRAC) ? 1 + jsc_refractivity(p, t) : 1;
+    for (int i = 0; i < 3; i++) ex1[i] = ex0[i] * n;
+    if (A.refrac && z <= JSC_ZREFRAC) {
+      for (int i = 0; i < 3; i++) xh[i] = x[i] + 0.5 * ds * ex0[i];
+      jsc_cart2geo(xh, &z, &lon, &lat);
+      atm_pt(a, z, &p, &t);
+      n = jsc_refractivity(p, t);
+      for (int i = 0; i < 3; i++) {
+        xh[i] += JSC_FD_STEP;
+        jsc_cart2geo(xh, &z, &lon, &lat);
+        atm_pt(a, z, &p, &t);
+        const double naux = jsc_refractivity(p, t);
+        ng[i] = (naux - n) / JSC_FD_STEP;
+        xh[i] -= JSC_FD_STEP;
+      }
+    } else {
+      for (int i = 0; i < 3; i++) ng[i] = 0;
+    }
+    for (int i = 0; i < 3; i++) ex1[i] += ds * ng[i];
+    norm = sqrt(ex1[0] * ex1[0] + ex1[1] * ex1[1] + ex1[2] * ex1[2]);
+    for (int i = 0; i < 3; i++) ex1[i] /= norm;
+    for (int i = 0; i < 3; i++) x[i] += 0.5 * ds * (ex0[i] + ex1[i]);
+    for (int i = 0; i < 3; i++) ex0[i] = ex1[i];
+  }
+
+  // Drop a last point that follows a too-short step (src/lineofsight.c:170-171).
+  if (np >= 3 && rprev2 < 1e-3) np--;
+
+  if (STORE) {
+    // Tangent point (src/lineofsight.c:411-452) from the stored geometry.
+    const double *g = A.geo + base * 4;
+    size_t m = 0;
+    double mn = g[0];
+    for (int i = 0; i < np; i++) {
+      const double v = g[(size_t)i * 4];
+      if (v < mn) {
+        mn = v;
+        m = (size_t)i;
+      }
+      if (isnan(v)) {
+        m = (size_t)i;
+        break;
+      }
+    }
+    double tpz, tplon, tplat;
+    if (m <= 0 || m >= (size_t)np - 1) {
+      tpz = g[(size_t)(np - 1) * 4];
+      tplon = g[(size_t)(np - 1) * 4 + 1];
+      tplat = g[(size_t)(np - 1) * 4 + 2];
+    } else {
+      const double yy0 = g[(m - 1) * 4], yy1 = g[m * 4], yy2 = g[(m + 1) * 4];
+      const double d1 = g[m * 4 + 3], d2 = g[(m + 1) * 4 + 3];
+      const double x1 = sqrt(d1 * d1 - (yy1 - yy0) * (yy1 - yy0));
+      const double x2 = x1 + sqrt(d2 * d2 - (yy2 - yy1) * (yy2 - yy1));
+      const double aa = 1 / (x1 - x2) * (-(yy0 - yy1) / x1 + (yy0 - yy2) / x2);
+      const double bb = -(yy0 - yy1) / x1 - aa * x1;
+      const double cc = yy0;
+      const double xx = -bb / (2 * aa);
+      double v0[3], v2[3], v[3], dummy;
+      tpz = aa * xx * xx + bb * xx + cc;
+      jsc_geo2cart(g[(m - 1) * 4], g[(m - 1) * 4 + 1], g[(m - 1) * 4 + 2], v0);
+      jsc_geo2cart(g[(m + 1) * 4], g[(m + 1) * 4 + 1], g[(m + 1) * 4 + 2], v2);
+      for (int i = 0; i < 3; i++) v[i] = jsc_lin(0.0, v0[i], x2, v2[i], xx);
+      jsc_cart2geo(v, &dummy, &tplon, &tplat);
+    }
+    A.tp[r] = tpz;
+    A.tp[A.n_rays + r] = tplon;
+    A.tp[2 * A.n_rays + r] = tplat;
+  }
+  return np;
+}
+
+template <bool STORE>
+__global__ void __launch_bounds__(128) raytrace_kernel(RayArgs A) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.n_rays) return;
+  const int np = trace_ray<STORE>(A, r);
+  if (!STORE) A.nlos[r] = np;
+  else if (np != A.nlos[r]) atomicOr(A.status, JSC_DEV_ERR_NLOS);
+}
+
+// Exclusive scan of nlos into off[0..n] by one block.
+__global__ void scan_kernel(const int *nlos, int n, int64_t *off) {
+  __shared__ int64_t part[1024];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int chunk = (n + nt - 1) / nt;
+  const int b = tid * chunk, e = min(n, b + chunk);
+  int64_t s = 0;
+  for (int i = b; i < e; i++) s += nlos[i];
+  part[tid] = s;
+  __syncthreads();
+  for (int d = 1; d < nt; d <<= 1) {
+    int64_t v = tid >= d ? part[tid - d] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  int64_t run = part[tid] - s;
+  for (int i = b; i < e; i++) {
+    off[i] = run;
+    run += nlos[i];
+  }
+  if (tid == nt - 1) off[n] = part[nt - 1];
+}
+
+// ------------------------------------------------------------- EGA + RT --
+
+struct EgaArgs {
+  jsc_dev_model m;
+  jsc_run_cfg cfg;
+  int n_rays, W, gl_log2, cpl;
+  const int *nlos;
+  const int64_t *los_off;
+  const double *pts, *tsurf;
+  double *rad, *tau;
+  unsigned long long *counters;
+};
+
+__device__ __forceinline__ double planck_temp(int i) {
+  return jsc_lin(0.0, JSC_PLANCK_TMIN, JSC_NPLANCK - 1.0, JSC_PLANCK_TMAX, (double)i);
+}
+
+// Result of locate() on the uniform Planck temperature grid: the bracket
+// from the grid spacing, corrected against the exact node values.
+__device__ __forceinline__ int planck_index(double t) {
+  if (!(t == t)) return JSC_NPLANCK - 2;
+  const double f = floor((t - JSC_PLANCK_TMIN) * 4.0);
+  int i = f < 0 ? 0 : (f > JSC_NPLANCK - 2 ? JSC_NPLANCK - 2 : (int)f);
+  while (i > 0 && planck_temp(i) > t) i--;
+  while (i < JSC_NPLANCK - 2 && planck_temp(i + 1) <= t) i++;
+  return i;
+}
+
+__device__ __forceinline__ double planck_src(const jsc_dev_model &m, int d,
+                                             int it, double t) {
+  const size_t o = (size_t)d * JSC_NPLANCK + it;
+  return m.planck_b[o] + m.planck_s[o] * (t - planck_temp(it));
+}
+
+// Continuum extinction of one channel at one LOS point
+// (src/forwardmodel.c:120-152 with src/continua.c:5-2049).
+__device__ __forceinline__ double continua(const jsc_dev_model &m,
+                                           const jsc_run_cfg &cfg,
+                                           const jsc_ctm_coef &c, double nu,
+                                           double kwin, double P, double T,
+                                           double DS, double qh2o,
+                                           const double *u) {
+  double beta = kwin;
+  if (cfg.ctm_co2) {
+    double ctm = 0;
+    if (m.ig_co2 >= 0 && c.co2_on) {
+      const double dt230 = T - 230, dt260 = T - 260, dt296 = T - 296;
+      const double ctw = dt260 * 5.050505e-4 * dt296 * c.co2_c230 -
+                         dt230 * 9.259259e-4 * dt296 * c.co2_c260 +
+                         dt230 * 4.208754e-4 * dt260 * c.co2_c296;
+      ctm = u[m.ig_co2] / JSC_AVOGADRO / 1000 * P / JSC_P0 * ctw;
+    }
+    beta += ctm / DS;
+  }
+  if (cfg.ctm_h2o) {
+    double ctm = 0;
+    if (m.ig_h2o >= 0 && c.h2o_on) {
+      const double ctwslf = c.h2o_self296 * pow(c.h2o_ratio, (296 - T) / (296 - 260));
+      const double a1 = nu * u[m.ig_h2o] * tanh(.7193876 / T * nu);
+      const double a2 = 296 / T;
+      const double a3 = P / JSC_P0 * (qh2o * ctwslf + (1 - qh2o) * c.h2o_frn) * 1e-20;
+      ctm = a1 * a2 * a3;
+    }
+    beta += ctm / DS;
+  }
+  if (cfg.ctm_n2 && c.n2_on) {
+    const double t0 = 273, tr = 296, q_n2 = 0.79;
+    const double pp = P / JSC_P0, tt = t0 / T;
+    beta += 0.1 * (pp * pp) * (tt * tt) * q_n2 * c.n2_b *
+            exp(c.n2_beta * (1 / tr - 1 / T)) *
+            (q_n2 + (1 - q_n2) * (1.294 - 0.4545 * T / tr));
+  }
+  if (cfg.ctm_o2 && c.o2_on) {
+    const double t0 = 273, tr = 296, q_o2 = 0.21;
+    const double pp = P / JSC_P0, tt = t0 / T;
+    beta += 0.1 * (pp * pp) * (tt * tt) * q_o2 * c.o2_b *
+            exp(c.o2_beta * (1 / tr - 1 / T));
+  }
+  return beta;
+}
+
+// Lower key of interval i (u or eps).
+template <bool U>
+__device__ __forceinline__ float ikey(const jsc_interval *row, int i) {
+  return U ? __ldg(&row[i].u0) : __ldg(&row[i].e0);
+}
+
+// locate_tbl (src/forwardmodel.c:546-565) on one table row of n >= 2
+// points.  key > x is evaluated as key > RD(x) (x rounded down to float),
+// which is exact for float keys.
+template <bool U>
+__device__ __forceinline__ int bisect_row(const jsc_interval *row, int n, double x) {
+  const float xf = __double2float_rd(x);
+  const bool nan = !(x == x);
+  int ilo = 0, ihi = n - 1;
+  while (ihi > ilo + 1) {
+    const int i = (ihi + ilo) >> 1;
+    if (!nan && ikey<U>(row, i) > xf) ihi = i; else ilo = i;
+  }
+  return ilo;
+}
+
+// Same result as bisect_row for a row with strictly increasing keys,
+// found by an exponential search from the guess h: the largest i <= n-2
+// with key[i] <= x, or 0.
+template <bool U>
+__device__ __forceinline__ int search_row(const jsc_interval *row, int n, double x, int h) {
+  if (!(x == x)) return n - 2;
+  const float xf = __double2float_rd(x);
+  const int last = n - 2;
+  int i = h < 0 ? 0 : (h > last ? last : h);
+  const float4 r = __ldg(reinterpret_cast<const float4 *>(row + i));
+  const float klo = U ? r.x : r.y, khi = U ? r.z : r.w;
+  int lo, hi;
+  if (!(klo > xf)) {
+    if (khi > xf || i == last) return i;
+    lo = i + 1;
+    int step = 1;
+    while (true) {
+      const int pr = lo + step;
+      if (pr > last) { hi = last + 1; break; }
+      if (ikey<U>(row, pr) > xf) { hi = pr; break; }
+      lo = pr;
+      step <<= 1;
+    }
+  } else {
+    if (i == 0) return 0;
+    hi = i;
+    int step = 1;
+    while (true) {
+      const int pr = hi - step;
+      if (pr <= 0) { lo = 0; break; }
+      if (!(ikey<U>(row, pr) > xf)) { lo = pr; break; }
+      hi = pr;
+      step <<= 1;
+    }
+  }
+  while (hi > lo + 1) {
+    const int mid = (lo + hi) >> 1;
+    if (ikey<U>(row, mid) > xf) hi = mid; else lo = mid;
+  }
+  return lo;
+}
+
+// Emissivity of the extended path at one (p, T) node of a table
+// (intpol_tbl_u then intpol_tbl_eps, src/forwardmodel.c:460-474): invert
+// the path emissivity x1 to a column density, add the segment's column,
+// look the emissivity up again, clamp to [0, 1].
+__device__ __forceinline__ double ega_node(const jsc_interval *iv, jsc_row rd,
+                                           double x1, double useg, int hint,
+                                           int *jout) {
+  const int n = rd.nf & 0xffff;
+  const bool strict = (rd.nf >> 16) & JSC_ROW_STRICT;
+  const jsc_interval *row = iv + rd.off;
+  const int k = strict ? search_row<false>(row, n, x1, hint) : bisect_row<false>(row, n, x1);
+  const float4 rk = __ldg(reinterpret_cast<const float4 *>(row + k));
+  const double2 sk = __ldg(reinterpret_cast<const double2 *>(row + k) + 1);
+  const double ustar = (double)rk.x + sk.x * (x1 - (double)rk.y);
+  const double x2 = ustar + useg;
+  const int j = strict ? search_row<true>(row, n, x2, k) : bisect_row<true>(row, n, x2);
+  double e;
+  if (j == k) {
+    e = (double)rk.y + sk.y * (x2 - (double)rk.x);
+  } else {
+    const float4 rj = __ldg(reinterpret_cast<const float4 *>(row + j));
+    const double2 sj = __ldg(reinterpret_cast<const double2 *>(row + j) + 1);
+    e = (double)rj.y + sj.y * (x2 - (double)rj.x);
+  }
+  *jout = j;
+  return jsc_clamp01(e);
+}
+
+__global__ void __launch_bounds__(128) ega_rt_kernel(EgaArgs A) {
+  extern __shared__ unsigned char smem_raw[];
+  const jsc_dev_model &m = A.m;
+  const int tid = threadIdx.x, BLK = blockDim.x;
+  const int GL = 1 << A.gl_log2;
+  const int sub = tid & (GL - 1);
+  const int r = (blockIdx.x * BLK + tid) >> A.gl_log2;
+  if (r >= A.n_rays) return;
+  const int ng = m.ng, nd = m.nd, cpl = A.cpl, nslot = cpl * ng;
+  double *s_tp = reinterpret_cast<double *>(smem_raw);
+  int *s_hint = reinterpret_cast<int *>(s_tp + (size_t)nslot * BLK);
+  double rad[5], tau[5];
+  for (int c = 0; c < 5; c++) {
+    rad[c] = 0;
+    tau[c] = 1;
+  }
+  for (int s = 0; s < nslot; s++) {
+    s_tp[s * BLK + tid] = 1;
+    s_hint[s * BLK + tid] = 0;
+  }
+  const int np = A.nlos[r];
+  const double *rec0 = A.pts + (size_t)A.los_off[r] * A.W;
+  unsigned long long n_ega = 0;
+
+  for (int ip = 0; ip < np; ip++) {
+    const double *rec = rec0 + (size_t)ip * A.W;
+    const double P = rec[0], T = rec[1], DS = rec[2], QH = rec[3];
+    const double *kw = rec + 4;
+    const double *u = rec + 4 + m.nw;
+    const int itp = planck_index(T);
+    int memo_g = -1, ipr = 0, it0 = 0, it1 = 0;
+    bool ntok = false;
+    for (int c = 0; c < cpl; c++) {
+      const int d = sub + c * GL;
+      if (d >= nd) break;
+      double tau_gas = 1;
+      for (int g = 0; g < ng; g++) {
+        const int slot = (c * ng + g) * BLK + tid;
+        const int ti = d * ng + g;
+        double tp = s_tp[slot];
+        double eps;
+        const int gid = m.tab_grid[ti];
+        if (gid < 0) {
+          eps = 0;
+        } else if (tp < 1e-9) {
+          eps = 1;
+        } else {
+          const double *gp = m.grid_p + (size_t)gid * TBLNPMAX;
+          const int *gnt = m.grid_nt + (size_t)gid * TBLNPMAX;
+          const double *gt = m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX;
+          if (gid != memo_g) {
+            memo_g = gid;
+            ipr = jsc_locate(gp, m.grid_np[gid], P);
+            it0 = jsc_locate(gt + ipr * TBLNTMAX, gnt[ipr], T);
+            it1 = jsc_locate(gt + (ipr + 1) * TBLNTMAX, gnt[ipr + 1], T);
+            ntok = gnt[ipr] >= 2 && gnt[ipr + 1] >= 2;
+          }
+          eps = 0;
+          if (ntok) {
+            const jsc_row *rw = m.rows + (size_t)ti * (TBLNPMAX * TBLNTMAX);
+            const jsc_row r00 = rw[ipr * TBLNTMAX + it0];
+            const jsc_row r01 = rw[ipr * TBLNTMAX + it0 + 1];
+            const jsc_row r10 = rw[(ipr + 1) * TBLNTMAX + it1];
+            const jsc_row r11 = rw[(ipr + 1) * TBLNTMAX + it1 + 1];
+            if ((r00.nf & 0xffff) >= 2 && (r01.nf & 0xffff) >= 2 &&
+                (r10.nf & 0xffff) >= 2 && (r11.nf & 0xffff) >= 2) {
+              const double x1 = 1 - tp, useg = u[g];
+              const int hint = s_hint[slot];
+              int j00, jx;
+              const double e00 = ega_node(m.iv, r00, x1, useg, hint, &j00);
+              const double e01 = ega_node(m.iv, r01, x1, useg, hint, &jx);
+              const double e10 = ega_node(m.iv, r10, x1, useg, hint, &jx);
+              const double e11 = ega_node(m.iv, r11, x1, useg, hint, &jx);
+              s_hint[slot] = j00;
+              double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
+                                              gt[ipr * TBLNTMAX + it0 + 1], e01, T));
+              double eb = jsc_clamp01(jsc_lin(gt[(ipr + 1) * TBLNTMAX + it1], e10,
+                                              gt[(ipr + 1) * TBLNTMAX + it1 + 1], e11, T));
+              ea = jsc_clamp01(jsc_lin(gp[ipr], ea, gp[ipr + 1], eb, P));
+              eps = 1 - (1 - ea) / tp;
+              n_ega++;
+            }
+          }
+        }
+        s_tp[slot] = tp * (1 - eps);
+        tau_gas *= (1 - eps);
+      }
+      const jsc_ctm_coef cc = m.ctm[d];
+      const int w = m.window[d];
+      const double beta = continua(m, A.cfg, cc, m.nu[d], w < m.nw ? kw[w] : 0.0,
+                                   P, T, DS, QH, u);
+      const double src = planck_src(m, d, itp, T);
+      if (tau_gas > 0) {
+        const double eps = 1 - tau_gas * exp(-1. * beta * DS);
+        rad[c] += src * eps * tau[c];
+        tau[c] *= (1 - eps);
+      }
+    }
+  }
+  const double ts = A.tsurf[r];
+  const int its = planck_index(ts);
+  for (int c = 0; c < cpl; c++) {
+    const int d = sub + c * GL;
+    if (d >= nd) break;
+    if (ts > 0) rad[c] += planck_src(m, d, its, ts) * tau[c];
+    A.rad[(size_t)r * nd + d] = rad[c];
+    A.tau[(size_t)r * nd + d] = tau[c];
+  }
+  // Work counter: one atomic per warp.
+  const unsigned mask = __activemask();
+  const unsigned tot = __reduce_add_sync(mask, (unsigned)n_ega);
+  if ((tid & 31) == __ffs(mask) - 1) atomicAdd(&A.counters[1], (unsigned long long)tot);
+}

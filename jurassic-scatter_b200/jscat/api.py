@@ -1,0 +1,172 @@
+"""Python host mirror of the forward-model interface.
+
+formod(ctl, atm, obs, aero) calls the drop-in C entry point with the
+reference's structs (src/forwardmodel.c:15).  Model/Batch wrap the batch
+C-ABI for many atmospheres and rays per launch; arrays are numpy, copies
+to and from the device happen inside the C library.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import lib as L
+from . import structs as S
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+def _iptr(a):
+    return a.ctypes.data_as(_I) if a is not None else None
+
+
+def formod(ctl, atm, obs, aero=None, exit_on_error=False):
+    """Drop-in forward model on the structs; raises JscError on failure
+    (unless exit_on_error, which keeps the reference's exit behaviour)."""
+    lib = L.load()
+    if aero is None:
+        aero = S.AeroT()
+    lib.jsc_set_exit_on_error(1 if exit_on_error else 0)
+    lib.formod(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero))
+    L.check(lib.jsc_last_status(), "formod")
+
+
+def brightness(rad, nu):
+    return L.load().brightness(float(rad), float(nu))
+
+
+class Model:
+    """Device-resident tables, Planck and continuum data for one ctl."""
+
+    def __init__(self, ctl, device=0):
+        lib = L.load()
+        self.ctl = ctl
+        self.h = C.c_void_p()
+        L.check(lib.jsc_model_create(C.byref(ctl), int(device), C.byref(self.h)),
+                "jsc_model_create")
+
+    @property
+    def table_bytes(self):
+        return L.load().jsc_model_table_bytes(self.h)
+
+    def close(self):
+        if self.h:
+            L.load().jsc_model_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Device buffers for up to max_rays rays over max_atm profiles."""
+
+    def __init__(self, model, ctl, max_atm, max_levels, max_rays, max_seg=0):
+        lib = L.load()
+        self.model = model
+        self.ctl = ctl
+        self.nd = ctl.nd
+        self.h = C.c_void_p()
+        L.check(lib.jsc_batch_create(model.h, C.byref(ctl), int(max_atm),
+                                     int(max_levels), int(max_rays),
+                                     int(max_seg), C.byref(self.h)),
+                "jsc_batch_create")
+        self._keep = None
+
+    def upload(self, inp, stream=None):
+        """inp: dict with atm_off (int32 [n_atm+1]), z/lon/lat/p/t
+        ([n_levels]), q ([ng][n_levels]), k ([nw][n_levels]), ray_atm
+        (int32 [n_rays]) and time/obsz/obslon/obslat/vpz/vplon/vplat."""
+        a = {}
+        for k in ("z", "lon", "lat", "p", "t", "time", "obsz", "obslon",
+                  "obslat", "vpz", "vplon", "vplat"):
+            v = inp.get(k)
+            a[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        for k in ("q", "k"):
+            v = inp.get(k)
+            a[k] = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        a["atm_off"] = np.ascontiguousarray(inp["atm_off"], dtype=np.int32)
+        a["ray_atm"] = np.ascontiguousarray(inp["ray_atm"], dtype=np.int32)
+        bi = L.BatchInput()
+        bi.n_atm = len(a["atm_off"]) - 1
+        bi.n_levels = len(a["z"])
+        bi.atm_off = _iptr(a["atm_off"])
+        for k in ("z", "lon", "lat", "p", "t", "q", "k", "time", "obsz",
+                  "obslon", "obslat", "vpz", "vplon", "vplat"):
+            setattr(bi, k, _dptr(a[k]))
+        bi.n_rays = len(a["ray_atm"])
+        bi.ray_atm = _iptr(a["ray_atm"])
+        self._keep = (a, bi)  # alive until the stream has consumed them
+        self.n_rays = bi.n_rays
+        L.check(L.load().jsc_batch_upload(self.h, C.byref(bi), stream),
+                "jsc_batch_upload")
+
+    def run(self, stream=None):
+        L.check(L.load().jsc_batch_run(self.h, stream), "jsc_batch_run")
+
+    def download(self, stream=None, out=None):
+        nr, nd = self.n_rays, self.nd
+        if out is None:
+            out = {"rad": np.empty((nr, nd)), "tau": np.empty((nr, nd)),
+                   "tpz": np.empty(nr), "tplon": np.empty(nr),
+                   "tplat": np.empty(nr), "nlos": np.empty(nr, np.int32)}
+        bo = L.BatchOutput()
+        bo.rad = _dptr(out.get("rad"))
+        bo.tau = _dptr(out.get("tau"))
+        bo.tpz = _dptr(out.get("tpz"))
+        bo.tplon = _dptr(out.get("tplon"))
+        bo.tplat = _dptr(out.get("tplat"))
+        bo.nlos = _iptr(out.get("nlos"))
+        L.check(L.load().jsc_batch_download(self.h, C.byref(bo), stream),
+                "jsc_batch_download")
+        return out
+
+    def set_timing(self, on=True):
+        L.load().jsc_batch_set_timing(self.h, 1 if on else 0)
+
+    def kernel_ms(self, name):
+        return L.load().jsc_batch_kernel_ms(self.h, name.encode())
+
+    def counters(self):
+        a, b = C.c_int64(), C.c_int64()
+        L.check(L.load().jsc_batch_counters(self.h, C.byref(a), C.byref(b)),
+                "jsc_batch_counters")
+        return a.value, b.value
+
+    def close(self):
+        if self.h:
+            L.load().jsc_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def formod_batch(ctl, inp, device=0, model=None):
+    """One-shot batch forward model: returns dict of rad/tau/tp*/nlos."""
+    own = model is None
+    m = Model(ctl, device) if own else model
+    nl = len(inp["z"])
+    b = Batch(m, ctl, len(inp["atm_off"]) - 1, nl, max(1, len(inp["ray_atm"])))
+    try:
+        b.upload(inp)
+        b.run()
+        return b.download()
+    finally:
+        b.close()
+        if own:
+            m.close()
+
+
+def launch_count():
+    return int(L.load().jsc_launch_count())

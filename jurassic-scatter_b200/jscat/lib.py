@@ -1,0 +1,107 @@
+"""Loads libjurassic_b200.so and declares the C-ABI of
+include/jurassic_b200.h.  There is no fallback: if the library is missing
+the import fails with instructions to build it."""
+import ctypes as C
+import os
+
+from . import structs as S
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "lib", "libjurassic_b200.so")
+
+# Every symbol the public header declares.
+EXPORTS = [
+    "formod", "brightness", "planck", "jsc_status_string", "jsc_last_status",
+    "jsc_set_exit_on_error", "jsc_last_error_message", "jsc_release_cache",
+    "jsc_launch_count", "jsc_model_create", "jsc_model_destroy",
+    "jsc_model_table_bytes", "jsc_batch_create", "jsc_batch_destroy",
+    "jsc_batch_upload", "jsc_batch_run", "jsc_batch_download",
+    "jsc_formod_batch", "jsc_batch_set_timing", "jsc_batch_kernel_ms",
+    "jsc_batch_counters",
+]
+
+
+class BatchInput(C.Structure):
+    _fields_ = [
+        ("n_atm", C.c_int), ("n_levels", C.c_int),
+        ("atm_off", C.POINTER(C.c_int)),
+        ("z", C.POINTER(C.c_double)), ("lon", C.POINTER(C.c_double)),
+        ("lat", C.POINTER(C.c_double)), ("p", C.POINTER(C.c_double)),
+        ("t", C.POINTER(C.c_double)),
+        ("q", C.POINTER(C.c_double)), ("k", C.POINTER(C.c_double)),
+        ("n_rays", C.c_int),
+        ("ray_atm", C.POINTER(C.c_int)),
+        ("time", C.POINTER(C.c_double)),
+        ("obsz", C.POINTER(C.c_double)), ("obslon", C.POINTER(C.c_double)),
+        ("obslat", C.POINTER(C.c_double)),
+        ("vpz", C.POINTER(C.c_double)), ("vplon", C.POINTER(C.c_double)),
+        ("vplat", C.POINTER(C.c_double)),
+    ]
+
+
+class BatchOutput(C.Structure):
+    _fields_ = [
+        ("rad", C.POINTER(C.c_double)), ("tau", C.POINTER(C.c_double)),
+        ("tpz", C.POINTER(C.c_double)), ("tplon", C.POINTER(C.c_double)),
+        ("tplat", C.POINTER(C.c_double)), ("nlos", C.POINTER(C.c_int)),
+    ]
+
+
+_lib = None
+
+
+def load():
+    """The library handle, loaded once with the C-ABI signatures set."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "libjurassic_b200.so not found at %s; build it with "
+            "'python jurassic-scatter_b200/build.py' (or __graft_entry__.build())"
+            % LIB_PATH)
+    lib = C.CDLL(LIB_PATH)
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    P = C.POINTER
+    sig = {
+        "formod": (None, [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT)]),
+        "brightness": (d, [d, d]),
+        "planck": (d, [d, d]),
+        "jsc_status_string": (C.c_char_p, [i]),
+        "jsc_last_status": (i, []),
+        "jsc_set_exit_on_error": (None, [i]),
+        "jsc_last_error_message": (C.c_char_p, []),
+        "jsc_release_cache": (None, []),
+        "jsc_launch_count": (C.c_uint64, []),
+        "jsc_model_create": (i, [P(S.CtlT), i, P(vp)]),
+        "jsc_model_destroy": (None, [vp]),
+        "jsc_model_table_bytes": (C.c_size_t, [vp]),
+        "jsc_batch_create": (i, [vp, P(S.CtlT), i, i, i, C.c_int64, P(vp)]),
+        "jsc_batch_destroy": (None, [vp]),
+        "jsc_batch_upload": (i, [vp, P(BatchInput), vp]),
+        "jsc_batch_run": (i, [vp, vp]),
+        "jsc_batch_download": (i, [vp, P(BatchOutput), vp]),
+        "jsc_formod_batch": (i, [vp, P(S.CtlT), P(BatchInput), P(BatchOutput), vp]),
+        "jsc_batch_set_timing": (None, [vp, i]),
+        "jsc_batch_kernel_ms": (d, [vp, C.c_char_p]),
+        "jsc_batch_counters": (i, [vp, P(C.c_int64), P(C.c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+class JscError(RuntimeError):
+    def __init__(self, status, where=""):
+        lib = load()
+        msg = lib.jsc_last_error_message().decode(errors="replace")
+        super().__init__("%s: %s (%s)" % (where, lib.jsc_status_string(status).decode(), msg))
+        self.status = status
+
+
+def check(status, where=""):
+    if status != 0:
+        raise JscError(status, where)

@@ -1,0 +1,164 @@
+"""Run the reference forward model as the oracle.  TEST INFRASTRUCTURE ONLY:
+imported by tests/, __graft_entry__.smoke() and bench.py's CPU baseline,
+never by the product.
+
+oracle/_ref/libjurassic_ref.so is the reference's own src/*.c compiled by
+oracle/Makefile.  The reference keeps its emissivity tables, Planck table
+and emitter indices in static variables initialised by the first call
+(src/forwardmodel.c:231-292, :747-786; src/continua.c:846,1894), so every
+run happens in a fresh spawned process.
+"""
+import ctypes as C
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+REF_LIB = os.path.join(HERE, "_ref", "libjurassic_ref.so")
+sys.path.insert(0, os.path.join(REPO, "jurassic-scatter_b200"))
+
+from jscat import structs as S  # noqa: E402
+
+
+class LosT(C.Structure):
+    """los_t of src/jurassic.h:352-393 (raytrace output)."""
+    _fields_ = [
+        ("np", C.c_int),
+        ("z", C.c_double * S.NLOS), ("lon", C.c_double * S.NLOS),
+        ("lat", C.c_double * S.NLOS), ("p", C.c_double * S.NLOS),
+        ("t", C.c_double * S.NLOS),
+        ("q", (C.c_double * S.NGMAX) * S.NLOS),
+        ("k", (C.c_double * S.NWMAX) * S.NLOS),
+        ("aeroi", C.c_int * S.NLOS),
+        ("aerofac", C.c_double * S.NLOS),
+        ("tsurf", C.c_double),
+        ("ds", C.c_double * S.NLOS),
+        ("u", (C.c_double * S.NGMAX) * S.NLOS),
+    ]
+
+
+def available():
+    return os.path.exists(REF_LIB)
+
+
+def _silence():
+    fd = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(fd, 1)
+    os.close(fd)
+
+
+def _atm_struct(a):
+    return S.make_atm(a["z"], a["p"], a["t"], a["q"], a.get("k"),
+                      a.get("lon"), a.get("lat"))
+
+
+def _child(job):
+    if job.get("threads"):
+        os.environ["OMP_NUM_THREADS"] = str(job["threads"])
+    _silence()
+    lib = C.CDLL(job.get("lib", REF_LIB))
+    P = C.POINTER
+    lib.formod.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT)]
+    lib.formod.restype = None
+    lib.raytrace.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT), P(LosT), C.c_int]
+    lib.raytrace.restype = None
+    ctl = S.make_ctl(**job["ctl"])
+    aero = job.get("aero") or S.AeroT()
+    atms, ray_atm, geom = job["atms"], np.asarray(job["ray_atm"]), job["geom"]
+    nr, nd = len(ray_atm), ctl.nd
+    out = {"rad": np.zeros((nr, nd)), "tau": np.zeros((nr, nd)),
+           "tpz": np.zeros(nr), "tplon": np.zeros(nr), "tplat": np.zeros(nr)}
+    if job.get("los"):
+        out["nlos"] = np.zeros(nr, np.int32)
+        out["los"] = []
+    groups = []
+    for ai in np.unique(ray_atm):
+        idx = np.nonzero(ray_atm == ai)[0]
+        for s in range(0, len(idx), S.NRMAX):
+            groups.append((int(ai), idx[s:s + S.NRMAX]))
+
+    def call(ai, idx):
+        atm = _atm_struct(atms[ai])
+        obs = S.make_obs(geom["obsz"][idx], geom["obslat"][idx],
+                         geom["vpz"][idx], geom["vplat"][idx],
+                         geom["obslon"][idx], geom["vplon"][idx],
+                         geom["time"][idx])
+        lib.formod(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero))
+        return atm, obs
+
+    if job.get("warmup"):
+        call(*groups[0])
+    t0 = time.perf_counter()
+    for ai, idx in groups:
+        atm, obs = call(ai, idx)
+        n = len(idx)
+        out["rad"][idx] = S.arr(obs.rad)[:nd, :n].T
+        out["tau"][idx] = S.arr(obs.tau)[:nd, :n].T
+        out["tpz"][idx] = S.arr(obs.tpz)[:n]
+        out["tplon"][idx] = S.arr(obs.tplon)[:n]
+        out["tplat"][idx] = S.arr(obs.tplat)[:n]
+    out["seconds"] = time.perf_counter() - t0
+    if job.get("los"):
+        los = LosT()
+        for ai, idx in groups:
+            atm = _atm_struct(atms[ai])
+            # formod applied hydrostatic balance to its copy; do the same
+            obs = S.make_obs(geom["obsz"][idx], geom["obslat"][idx],
+                             geom["vpz"][idx], geom["vplat"][idx],
+                             geom["obslon"][idx], geom["vplon"][idx],
+                             geom["time"][idx])
+            lib.hydrostatic.argtypes = [P(S.CtlT), P(S.AtmT)]
+            lib.hydrostatic(C.byref(ctl), C.byref(atm))
+            for j, r in enumerate(idx):
+                lib.raytrace(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero),
+                             C.byref(los), j)
+                out["nlos"][r] = los.np
+                if job["los"] == "full":
+                    n = los.np
+                    ng = ctl.ng
+                    out["los"].append({
+                        "z": S.arr(los.z)[:n].copy(), "p": S.arr(los.p)[:n].copy(),
+                        "t": S.arr(los.t)[:n].copy(), "ds": S.arr(los.ds)[:n].copy(),
+                        "u": S.arr(los.u)[:n, :ng].copy(), "tsurf": los.tsurf})
+    return out
+
+
+def run(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False,
+        los=False, lib=None, timeout=1800):
+    """Reference formod over profiles atms (list of dicts) and rays.
+    Returns rad/tau [n_rays][nd], tpz/tplon/tplat, seconds (wall time of
+    the formod calls after the optional warm-up call), and with los=True
+    the LOS point count per ray (los='full' also returns the LOS records)."""
+    import pickle
+    import subprocess
+    import tempfile
+    job = {"ctl": ctl_kw, "atms": atms, "ray_atm": np.asarray(ray_atm),
+           "geom": geom, "aero": None if aero is None else bytes(aero),
+           "threads": threads, "warmup": warmup, "los": los}
+    if lib:
+        job["lib"] = lib
+    with tempfile.TemporaryDirectory() as d:
+        jf, of = os.path.join(d, "job.pkl"), os.path.join(d, "out.pkl")
+        with open(jf, "wb") as f:
+            pickle.dump(job, f)
+        res = subprocess.run([sys.executable, os.path.abspath(__file__), jf, of],
+                             capture_output=True, text=True, timeout=timeout)
+        if res.returncode != 0 or not os.path.exists(of):
+            raise RuntimeError("reference run failed (%d): %s" %
+                               (res.returncode, res.stderr[-2000:]))
+        with open(of, "rb") as f:
+            return pickle.load(f)
+
+
+if __name__ == "__main__":
+    import pickle
+    with open(sys.argv[1], "rb") as f:
+        _job = pickle.load(f)
+    if _job.get("aero") is not None:
+        _job["aero"] = S.AeroT.from_buffer_copy(_job["aero"])
+    _out = _child(_job)
+    with open(sys.argv[2], "wb") as f:
+        pickle.dump(_out, f)

@@ -1,0 +1,6 @@
+"""Re-exports the case definitions of tests/golden/make_golden.py."""
+import os
+import sys
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+from make_golden import mixed_case, tables_digest  # noqa: E402,F401

@@ -1,0 +1,66 @@
+"""GPU parity against the reference forward model.
+
+Golden fixtures hold the reference's own FP64 outputs (tests/golden,
+made by make_golden.py with the reference compiled from its sources) for
+seeded synthetic inputs regenerated here.  Bars: LOS point counts exactly
+equal, brightness temperature within 0.01 K, and radiance/transmittance
+within 1e-9 relative (the GPU keeps the reference's FP64 operation order;
+only libm last-bit differences remain)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from helpers import bt_error, max_rel
+
+pytestmark = pytest.mark.gpu
+
+BT_TOL_K = 0.01
+REL_TOL = 1e-9
+
+
+def _load(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def _geom(g):
+    return {k[5:]: v for k, v in g.items() if k.startswith("geom_")}
+
+
+def _check_tables(g, ctlkw):
+    from make_golden_shim import tables_digest
+    assert tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]) == str(g["table_sha256"])
+
+
+def test_clear_limb_dropin_formod(workdir):
+    from jscat import structs as S, synth, api
+    g = _load("clear_limb")
+    ctlkw, atm, geom = synth.clear_limb_case(workdir)
+    _check_tables(g, ctlkw)
+    ctl = S.make_ctl(**ctlkw)
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm["k"])
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"])
+    api.formod(ctl, a, obs)
+    nr, nd = obs.nr, ctl.nd
+    rad = S.arr(obs.rad)[:nd, :nr].T
+    tau = S.arr(obs.tau)[:nd, :nr].T
+    assert bt_error(rad, g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(rad, g["rad"]) <= REL_TOL
+    assert max_rel(tau, g["tau"]) <= REL_TOL
+    np.testing.assert_allclose(S.arr(obs.tpz)[:nr], g["tpz"], rtol=1e-9, atol=1e-9)
+
+
+def test_mixed_batch(workdir):
+    from jscat import synth, api, structs as S
+    from make_golden_shim import mixed_case
+    g = _load("mixed_batch")
+    ctlkw, atms, ray_atm, geom = mixed_case(workdir)
+    _check_tables(g, ctlkw)
+    ctl = S.make_ctl(**ctlkw)
+    out = api.formod_batch(ctl, synth.batch_from(atms, ray_atm, geom))
+    np.testing.assert_array_equal(out["nlos"], g["nlos"])
+    assert bt_error(out["rad"], g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(out["rad"], g["rad"]) <= REL_TOL
+    assert max_rel(out["tau"], g["tau"]) <= REL_TOL
+    np.testing.assert_allclose(out["tpz"], g["tpz"], rtol=1e-9, atol=1e-9)
