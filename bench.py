@@ -133,14 +133,16 @@ def cpu_baseline(ctlkw, atms, ray_atm, geom, n_sample):
     sel = np.nonzero(ray_atm < n_atm)[0]
     sub_geom = {k: v[sel] for k, v in geom.items()}
     cores = os.cpu_count() or 1
+    # SCA_MULT=0: the clear-air arithmetic without the reference's read of
+    # the uninitialised los->aerofac (see tests/golden/make_golden.py).
+    ref_kw = dict(ctlkw, sca_mult=0)
     if refrun.available():
-        res = refrun.run(ctlkw, atms[:n_atm], ray_atm[sel], sub_geom,
+        res = refrun.run(ref_kw, atms[:n_atm], ray_atm[sel], sub_geom,
                          threads=cores, warmup=True, timeout=3600)
         kind = "reference"
     else:
-        from oracle import port
-        res = port.run(ctlkw, atms[:n_atm], ray_atm[sel], sub_geom,
-                       threads=cores, warmup=True)
+        res = refrun.run_port(ctlkw, atms[:n_atm], ray_atm[sel], sub_geom,
+                              threads=cores, warmup=True, timeout=3600)
         kind = "port"
     v = len(sel) * ctlkw_nd(ctlkw) / res["seconds"]
     return {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
@@ -165,8 +167,13 @@ def run_reference_arm(args, rank, world):
         sel_atm = list(range(a0, a0 + n_atm))
         sel = np.nonzero(np.isin(ray_atm, sel_atm))[0]
         sub = {k: v[sel] for k, v in geom.items()}
-        res = refrun.run(ctlkw, [atms[i] for i in sel_atm], ray_atm[sel] - a0, sub,
-                         threads=cores, warmup=True, timeout=3600)
+        if refrun.available():
+            res = refrun.run(dict(ctlkw, sca_mult=0), [atms[i] for i in sel_atm],
+                             ray_atm[sel] - a0, sub, threads=cores, warmup=True,
+                             timeout=3600)
+        else:
+            res = refrun.run_port(ctlkw, [atms[i] for i in sel_atm], ray_atm[sel] - a0,
+                                  sub, threads=cores, warmup=True, timeout=3600)
         if step >= args.warmup:
             times.append((len(sel), res["seconds"]))
     n = sum(t[0] for t in times)

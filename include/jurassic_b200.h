@@ -280,6 +280,17 @@ int jsc_formod_batch(jsc_model *m, const ctl_t *ctl, const jsc_batch_input *in,
 void jsc_batch_set_timing(jsc_batch *b, int on);
 double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel);
 
+/* Per-(ray, channel) checksum of every emissivity-table index the EGA
+ * interpolation selected in the last run, for parity checks against the
+ * reference's indices: for each LOS point and emitter with a full
+ * interpolation, fold d = d*1000003 + v over the (p, T) bracket code
+ * ipr*961 + it0*31 + it1 and then, for the (p, T) nodes (ipr,it0),
+ * (ipr,it0+1), (ipr+1,it1), (ipr+1,it1+1), the interval found for the
+ * path emissivity (intpol_tbl_u) and the one found for the extended column
+ * (intpol_tbl_eps).  Enable before jsc_batch_run; out is [n_rays][nd]. */
+int jsc_batch_set_digest(jsc_batch *b, int on);
+int jsc_batch_index_digest(jsc_batch *b, uint64_t *out);
+
 /* Work counters of the last run: total LOS points, and the number of
  * (point, channel, emitter) EGA interpolations actually evaluated. */
 int jsc_batch_counters(const jsc_batch *b, int64_t *n_points,

@@ -46,6 +46,7 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   cudaFree(b->d_tau);
   cudaFree(b->d_status);
   cudaFree(b->d_counters);
+  cudaFree(b->d_digest);
   if (b->h_total) cudaFreeHost(b->h_total);
   for (int i = 0; i < 2 * JSC_T_N; i++)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
@@ -303,6 +304,7 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   ea.rad = b->d_rad;
   ea.tau = b->d_tau;
   ea.counters = b->d_counters;
+  ea.digest = b->digest ? b->d_digest : nullptr;
   const size_t per_thread = (size_t)ea.cpl * (m->ng > 0 ? m->ng : 1) * (sizeof(double) + sizeof(int));
   int blk = 128;
   while (blk > 32 && per_thread * blk > 96 * 1024) blk >>= 1;
@@ -375,6 +377,24 @@ extern "C" int jsc_formod_batch(jsc_model *m, const ctl_t *ctl,
   if (!st) st = jsc_batch_download(b, out, stream);
   jsc_batch_destroy(b);
   return st;
+}
+
+extern "C" int jsc_batch_set_digest(jsc_batch *b, int on) {
+  if (!b) return JSC_ERR_ARG;
+  if (on && !b->d_digest) {
+    int st = jsc_dmalloc(&b->d_digest, (size_t)b->max_rays * b->cfg.nd);
+    if (st) return st;
+  }
+  b->digest = on;
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_index_digest(jsc_batch *b, uint64_t *out) {
+  if (!b || !out || !b->digest) return JSC_ERR_ARG;
+  JSC_CUDA_TRY(cudaMemcpy(out, b->d_digest,
+                          (size_t)b->n_rays * b->cfg.nd * sizeof(uint64_t),
+                          cudaMemcpyDeviceToHost));
+  return JSC_OK;
 }
 
 extern "C" void jsc_batch_set_timing(jsc_batch *b, int on) {

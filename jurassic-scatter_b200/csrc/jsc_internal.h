@@ -127,16 +127,18 @@ void jsc_set_error(int status, const char *fmt, ...);
  * Device layout of a model (device pointers; passed by value to kernels).
  * ------------------------------------------------------------------------ */
 
-/* One interval [k, k+1] of an emissivity-table row: the bracketing points
- * and both interpolation slopes, computed in double exactly as the
- * reference's LIN computes them at run time (src/forwardmodel.c:519-541). */
+/* One point k of an emissivity-table row with the slopes of the interval
+ * [k, k+1] (zero at the last point).  The reference's LIN on float table
+ * entries evaluates (y1-y0)/(x1-x0) in single precision
+ * (src/forwardmodel.c:519-541 with the LIN macro of src/jurassic.h:72), so
+ * the slopes are stored as the float values it computes. */
 typedef struct JSC_ALIGN(16) {
-  float u0, e0, u1, e1;
-  double s_ue;      /* (u1-u0)/(e1-e0): eps -> u  (intpol_tbl_u) */
-  double s_eu;      /* (e1-e0)/(u1-u0): u -> eps  (intpol_tbl_eps) */
-} jsc_interval;
+  float u, e;
+  float s_ue;       /* (u1-u0)/(e1-e0): eps -> u  (intpol_tbl_u) */
+  float s_eu;       /* (e1-e0)/(u1-u0): u -> eps  (intpol_tbl_eps) */
+} jsc_node;
 
-/* Row descriptor: first interval of the row and n | flags << 16, where n is
+/* Row descriptor: first node of the row and n | flags << 16, where n is
  * the number of points of the row. */
 typedef struct JSC_ALIGN(8) {
   int off;
@@ -158,7 +160,7 @@ typedef struct {
   const double *grid_t;
   const int *tab_grid;       /* [nd*ng] grid id, -1: table unusable (np<2) */
   const jsc_row *rows;       /* [nd*ng][TBLNPMAX][TBLNTMAX] */
-  const jsc_interval *iv;
+  const jsc_node *nodes;
   const double *planck_b, *planck_s;   /* [nd][JSC_NPLANCK] */
   const jsc_ctm_coef *ctm;             /* [nd] */
   const double *nu;                    /* [nd] */

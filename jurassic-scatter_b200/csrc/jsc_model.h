@@ -9,14 +9,14 @@ struct jsc_model {
   int device;
   int ng, nd, nw;
   int n_grid;
-  int64_t n_intervals;
+  int64_t n_nodes;
   size_t table_bytes;
   double nu[NDMAX];
   jsc_dev_model dv;  // device view passed to kernels
   int *d_grid_np, *d_grid_nt, *d_tab_grid, *d_window;
   double *d_grid_p, *d_grid_t, *d_planck_b, *d_planck_s, *d_nu;
   jsc_row *d_rows;
-  jsc_interval *d_iv;
+  jsc_node *d_nodes;
   jsc_ctm_coef *d_ctm;
 };
 
@@ -62,6 +62,8 @@ struct jsc_batch {
   unsigned long long *d_counters;  // [0] LOS points, [1] EGA evaluations
   int64_t *h_total;         // pinned: LOS points of the current batch
 
+  unsigned long long *d_digest;  // [max_rays][nd] when index digests are on
+  int digest;
   int timing;
   cudaEvent_t ev[2 * JSC_T_N];
   int ran[JSC_T_N];

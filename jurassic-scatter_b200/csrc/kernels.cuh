@@ -371,6 +371,7 @@ struct EgaArgs {
   const double *pts, *tsurf;
   double *rad, *tau;
   unsigned long long *counters;
+  unsigned long long *digest;  // optional [n_rays][nd] EGA index checksums
 };
 
 __device__ __forceinline__ double planck_temp(int i) {
@@ -441,23 +442,23 @@ __device__ __forceinline__ double continua(const jsc_dev_model &m,
   return beta;
 }
 
-// Lower key of interval i (u or eps).
+// Key of node i (u or eps).
 template <bool U>
-__device__ __forceinline__ float ikey(const jsc_interval *row, int i) {
-  return U ? __ldg(&row[i].u0) : __ldg(&row[i].e0);
+__device__ __forceinline__ float nkey(const jsc_node *row, int i) {
+  return U ? __ldg(&row[i].u) : __ldg(&row[i].e);
 }
 
 // locate_tbl (src/forwardmodel.c:546-565) on one table row of n >= 2
 // points.  key > x is evaluated as key > RD(x) (x rounded down to float),
 // which is exact for float keys.
 template <bool U>
-__device__ __forceinline__ int bisect_row(const jsc_interval *row, int n, double x) {
+__device__ __forceinline__ int bisect_row(const jsc_node *row, int n, double x) {
   const float xf = __double2float_rd(x);
   const bool nan = !(x == x);
   int ilo = 0, ihi = n - 1;
   while (ihi > ilo + 1) {
     const int i = (ihi + ilo) >> 1;
-    if (!nan && ikey<U>(row, i) > xf) ihi = i; else ilo = i;
+    if (!nan && nkey<U>(row, i) > xf) ihi = i; else ilo = i;
   }
   return ilo;
 }
@@ -466,13 +467,12 @@ __device__ __forceinline__ int bisect_row(const jsc_interval *row, int n, double
 // found by an exponential search from the guess h: the largest i <= n-2
 // with key[i] <= x, or 0.
 template <bool U>
-__device__ __forceinline__ int search_row(const jsc_interval *row, int n, double x, int h) {
+__device__ __forceinline__ int search_row(const jsc_node *row, int n, double x, int h) {
   if (!(x == x)) return n - 2;
   const float xf = __double2float_rd(x);
   const int last = n - 2;
   int i = h < 0 ? 0 : (h > last ? last : h);
-  const float4 r = __ldg(reinterpret_cast<const float4 *>(row + i));
-  const float klo = U ? r.x : r.y, khi = U ? r.z : r.w;
+  const float klo = nkey<U>(row, i), khi = nkey<U>(row, i + 1);
   int lo, hi;
   if (!(klo > xf)) {
     if (khi > xf || i == last) return i;
@@ -481,7 +481,7 @@ __device__ __forceinline__ int search_row(const jsc_interval *row, int n, double
     while (true) {
       const int pr = lo + step;
       if (pr > last) { hi = last + 1; break; }
-      if (ikey<U>(row, pr) > xf) { hi = pr; break; }
+      if (nkey<U>(row, pr) > xf) { hi = pr; break; }
       lo = pr;
       step <<= 1;
     }
@@ -492,42 +492,48 @@ __device__ __forceinline__ int search_row(const jsc_interval *row, int n, double
     while (true) {
       const int pr = hi - step;
       if (pr <= 0) { lo = 0; break; }
-      if (!(ikey<U>(row, pr) > xf)) { lo = pr; break; }
+      if (!(nkey<U>(row, pr) > xf)) { lo = pr; break; }
       hi = pr;
       step <<= 1;
     }
   }
   while (hi > lo + 1) {
     const int mid = (lo + hi) >> 1;
-    if (ikey<U>(row, mid) > xf) hi = mid; else lo = mid;
+    if (nkey<U>(row, mid) > xf) hi = mid; else lo = mid;
   }
   return lo;
+}
+
+// LIN on float table entries with the slope already in float, as the
+// reference evaluates it: y0 + slope * (x - x0), promoted to double.
+__device__ __forceinline__ double lin_node(float x0, float y0, float slope, double x) {
+  return (double)y0 + (double)slope * (x - (double)x0);
 }
 
 // Emissivity of the extended path at one (p, T) node of a table
 // (intpol_tbl_u then intpol_tbl_eps, src/forwardmodel.c:460-474): invert
 // the path emissivity x1 to a column density, add the segment's column,
-// look the emissivity up again, clamp to [0, 1].
-__device__ __forceinline__ double ega_node(const jsc_interval *iv, jsc_row rd,
+// look the emissivity up again, clamp to [0, 1].  dig, when non-null,
+// folds in both interval indices.
+__device__ __forceinline__ double ega_node(const jsc_node *nodes, jsc_row rd,
                                            double x1, double useg, int hint,
-                                           int *jout) {
+                                           int *jout, unsigned long long *dig) {
   const int n = rd.nf & 0xffff;
   const bool strict = (rd.nf >> 16) & JSC_ROW_STRICT;
-  const jsc_interval *row = iv + rd.off;
+  const jsc_node *row = nodes + rd.off;
   const int k = strict ? search_row<false>(row, n, x1, hint) : bisect_row<false>(row, n, x1);
   const float4 rk = __ldg(reinterpret_cast<const float4 *>(row + k));
-  const double2 sk = __ldg(reinterpret_cast<const double2 *>(row + k) + 1);
-  const double ustar = (double)rk.x + sk.x * (x1 - (double)rk.y);
+  const double ustar = lin_node(rk.y, rk.x, rk.z, x1);
   const double x2 = ustar + useg;
   const int j = strict ? search_row<true>(row, n, x2, k) : bisect_row<true>(row, n, x2);
   double e;
   if (j == k) {
-    e = (double)rk.y + sk.y * (x2 - (double)rk.x);
+    e = lin_node(rk.x, rk.y, rk.w, x2);
   } else {
     const float4 rj = __ldg(reinterpret_cast<const float4 *>(row + j));
-    const double2 sj = __ldg(reinterpret_cast<const double2 *>(row + j) + 1);
-    e = (double)rj.y + sj.y * (x2 - (double)rj.x);
+    e = lin_node(rj.x, rj.y, rj.w, x2);
   }
+  if (dig) *dig = (*dig * 1000003ull + (unsigned long long)k) * 1000003ull + (unsigned long long)j;
   *jout = j;
   return jsc_clamp01(e);
 }
@@ -544,9 +550,11 @@ __global__ void __launch_bounds__(128) ega_rt_kernel(EgaArgs A) {
   double *s_tp = reinterpret_cast<double *>(smem_raw);
   int *s_hint = reinterpret_cast<int *>(s_tp + (size_t)nslot * BLK);
   double rad[5], tau[5];
+  unsigned long long dig[5];
   for (int c = 0; c < 5; c++) {
     rad[c] = 0;
     tau[c] = 1;
+    dig[c] = 0;
   }
   for (int s = 0; s < nslot; s++) {
     s_tp[s * BLK + tid] = 1;
@@ -601,10 +609,12 @@ __global__ void __launch_bounds__(128) ega_rt_kernel(EgaArgs A) {
               const double x1 = 1 - tp, useg = u[g];
               const int hint = s_hint[slot];
               int j00, jx;
-              const double e00 = ega_node(m.iv, r00, x1, useg, hint, &j00);
-              const double e01 = ega_node(m.iv, r01, x1, useg, hint, &jx);
-              const double e10 = ega_node(m.iv, r10, x1, useg, hint, &jx);
-              const double e11 = ega_node(m.iv, r11, x1, useg, hint, &jx);
+              unsigned long long *dg = A.digest ? &dig[c] : nullptr;
+              if (dg) *dg = *dg * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
+              const double e00 = ega_node(m.nodes, r00, x1, useg, hint, &j00, dg);
+              const double e01 = ega_node(m.nodes, r01, x1, useg, hint, &jx, dg);
+              const double e10 = ega_node(m.nodes, r10, x1, useg, hint, &jx, dg);
+              const double e11 = ega_node(m.nodes, r11, x1, useg, hint, &jx, dg);
               s_hint[slot] = j00;
               double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
                                               gt[ipr * TBLNTMAX + it0 + 1], e01, T));
@@ -639,6 +649,7 @@ __global__ void __launch_bounds__(128) ega_rt_kernel(EgaArgs A) {
     if (ts > 0) rad[c] += planck_src(m, d, its, ts) * tau[c];
     A.rad[(size_t)r * nd + d] = rad[c];
     A.tau[(size_t)r * nd + d] = tau[c];
+    if (A.digest) A.digest[(size_t)r * nd + d] = dig[c];
   }
   // Work counter: one atomic per warp.
   const unsigned mask = __activemask();

@@ -3,10 +3,10 @@
 // Device layout (all in HBM, read-only during a forward model):
 //  * (p, T) grids, deduplicated across tables (most table sets share one);
 //  * a row descriptor per (channel, emitter, p level, T) slot;
-//  * one 32-byte interval record per pair of neighbouring table points:
-//    both points (u, eps as float) and both interpolation slopes in double,
-//    computed on the device with the same IEEE operations the reference's
-//    LIN evaluates at run time, so a lookup needs one 32-byte sector;
+//  * one 16-byte node per table point: u, eps and both slopes of the
+//    interval to the next point, computed on the device with the same IEEE
+//    single-precision operations the reference's LIN evaluates at run time,
+//    so a lookup reads two neighbouring nodes (one 32-byte sector);
 //  * Planck source tables with slopes, continuum coefficients per channel.
 #include <stdio.h>
 #include <stdlib.h>
@@ -22,11 +22,10 @@ static std::atomic<uint64_t> g_launches{0};
 extern "C" void jsc_count_launch(void) { g_launches.fetch_add(1); }
 extern "C" uint64_t jsc_launch_count(void) { return g_launches.load(); }
 
-// One warp per row slot builds the row's interval records.
-__global__ void build_intervals_kernel(const jsc_row *rows,
-                                       const int64_t *row_pt, int nrows,
-                                       const float *u, const float *e,
-                                       jsc_interval *iv) {
+// One warp per row slot builds the row's nodes.
+__global__ void build_nodes_kernel(const jsc_row *rows, const int64_t *row_pt,
+                                   int nrows, const float *u, const float *e,
+                                   jsc_node *nodes) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -35,17 +34,18 @@ __global__ void build_intervals_kernel(const jsc_row *rows,
     if (n < 2) continue;
     const int64_t pt = row_pt[r];
     const int off = rows[r].off;
-    for (int k = lane; k < n - 1; k += 32) {
-      jsc_interval v;
-      v.u0 = u[pt + k];
-      v.e0 = e[pt + k];
-      v.u1 = u[pt + k + 1];
-      v.e1 = e[pt + k + 1];
-      const double du = (double)v.u1 - (double)v.u0;
-      const double de = (double)v.e1 - (double)v.e0;
-      v.s_ue = du / de;
-      v.s_eu = de / du;
-      iv[off + k] = v;
+    for (int k = lane; k < n; k += 32) {
+      jsc_node v;
+      v.u = u[pt + k];
+      v.e = e[pt + k];
+      v.s_ue = 0.0f;
+      v.s_eu = 0.0f;
+      if (k + 1 < n) {
+        const float u1 = u[pt + k + 1], e1 = e[pt + k + 1];
+        v.s_ue = __fdiv_rn(__fsub_rn(u1, v.u), __fsub_rn(e1, v.e));
+        v.s_eu = __fdiv_rn(__fsub_rn(e1, v.e), __fsub_rn(u1, v.u));
+      }
+      nodes[off + k] = v;
     }
   }
 }
@@ -130,7 +130,7 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
     }
   }
 
-  // Row descriptors and interval offsets.
+  // Row descriptors and node offsets.
   std::vector<jsc_row> rows(nslots > 0 ? nslots : 1);
   std::vector<int64_t> row_pt(nslots > 0 ? nslots : 1, 0);
   int64_t niv = 0;
@@ -155,9 +155,9 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
         rows[s].off = (int)niv;
         rows[s].nf = n | (strict ? (JSC_ROW_STRICT << 16) : 0);
         row_pt[s] = pt;
-        if (n >= 2) niv += n - 1;
+        if (n >= 2) niv += n;
         if (niv > 0x7fffffff) {
-          jsc_set_error(JSC_ERR_TABLE, "emissivity tables exceed 2^31 intervals");
+          jsc_set_error(JSC_ERR_TABLE, "emissivity tables exceed 2^31 points");
           return JSC_ERR_TABLE;
         }
       }
@@ -170,8 +170,8 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
   if ((st = upload(&m->d_grid_t, g_t.data(), g_t.size()))) return st;
   if ((st = upload(&m->d_tab_grid, tab_grid.data(), tab_grid.size()))) return st;
   if ((st = upload(&m->d_rows, rows.data(), rows.size()))) return st;
-  if ((st = jsc_dmalloc(&m->d_iv, (size_t)niv))) return st;
-  m->n_intervals = niv;
+  if ((st = jsc_dmalloc(&m->d_nodes, (size_t)niv))) return st;
+  m->n_nodes = niv;
   m->n_grid = ngrid;
 
   if (niv > 0) {
@@ -180,15 +180,15 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
     if ((st = upload(&du, ht->u, (size_t)ht->n_points))) return st;
     if ((st = upload(&de, ht->eps, (size_t)ht->n_points))) return st;
     if ((st = upload(&drp, row_pt.data(), row_pt.size()))) return st;
-    build_intervals_kernel<<<148 * 8, 256>>>(m->d_rows, drp, (int)nslots, du,
-                                              de, m->d_iv);
+    build_nodes_kernel<<<148 * 8, 256>>>(m->d_rows, drp, (int)nslots, du, de,
+                                          m->d_nodes);
     jsc_count_launch();
     cudaError_t e = cudaDeviceSynchronize();
     cudaFree(du);
     cudaFree(de);
     cudaFree(drp);
     if (e != cudaSuccess) {
-      jsc_set_error(JSC_ERR_CUDA, "build_intervals: %s", cudaGetErrorString(e));
+      jsc_set_error(JSC_ERR_CUDA, "build_nodes: %s", cudaGetErrorString(e));
       return JSC_ERR_CUDA;
     }
   }
@@ -200,7 +200,7 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
   if ((st = upload(&m->d_nu, hm->nu, (size_t)nd))) return st;
   if ((st = upload(&m->d_window, hm->window, (size_t)nd))) return st;
 
-  m->table_bytes = (size_t)niv * sizeof(jsc_interval) + rows.size() * sizeof(jsc_row);
+  m->table_bytes = (size_t)niv * sizeof(jsc_node) + rows.size() * sizeof(jsc_row);
 
   jsc_dev_model &d = m->dv;
   d.ng = ng;
@@ -215,7 +215,7 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
   d.grid_t = m->d_grid_t;
   d.tab_grid = m->d_tab_grid;
   d.rows = m->d_rows;
-  d.iv = m->d_iv;
+  d.nodes = m->d_nodes;
   d.planck_b = m->d_planck_b;
   d.planck_s = m->d_planck_s;
   d.ctm = m->d_ctm;
@@ -266,7 +266,7 @@ extern "C" void jsc_model_destroy(jsc_model *m) {
   cudaFree(m->d_grid_t);
   cudaFree(m->d_tab_grid);
   cudaFree(m->d_rows);
-  cudaFree(m->d_iv);
+  cudaFree(m->d_nodes);
   cudaFree(m->d_planck_b);
   cudaFree(m->d_planck_s);
   cudaFree(m->d_ctm);

@@ -128,6 +128,15 @@ class Batch:
                 "jsc_batch_download")
         return out
 
+    def set_digest(self, on=True):
+        L.check(L.load().jsc_batch_set_digest(self.h, 1 if on else 0), "jsc_batch_set_digest")
+
+    def index_digest(self):
+        out = np.empty((self.n_rays, self.nd), np.uint64)
+        L.check(L.load().jsc_batch_index_digest(self.h, out.ctypes.data_as(C.POINTER(C.c_uint64))),
+                "jsc_batch_index_digest")
+        return out
+
     def set_timing(self, on=True):
         L.load().jsc_batch_set_timing(self.h, 1 if on else 0)
 
@@ -152,16 +161,22 @@ class Batch:
             pass
 
 
-def formod_batch(ctl, inp, device=0, model=None):
-    """One-shot batch forward model: returns dict of rad/tau/tp*/nlos."""
+def formod_batch(ctl, inp, device=0, model=None, digest=False):
+    """One-shot batch forward model: returns dict of rad/tau/tp*/nlos (and
+    the per-(ray, channel) EGA index digests when digest=True)."""
     own = model is None
     m = Model(ctl, device) if own else model
     nl = len(inp["z"])
     b = Batch(m, ctl, len(inp["atm_off"]) - 1, nl, max(1, len(inp["ray_atm"])))
     try:
+        if digest:
+            b.set_digest(True)
         b.upload(inp)
         b.run()
-        return b.download()
+        out = b.download()
+        if digest:
+            out["digest"] = b.index_digest()
+        return out
     finally:
         b.close()
         if own:

@@ -17,7 +17,7 @@ EXPORTS = [
     "jsc_model_table_bytes", "jsc_batch_create", "jsc_batch_destroy",
     "jsc_batch_upload", "jsc_batch_run", "jsc_batch_download",
     "jsc_formod_batch", "jsc_batch_set_timing", "jsc_batch_kernel_ms",
-    "jsc_batch_counters",
+    "jsc_batch_counters", "jsc_batch_set_digest", "jsc_batch_index_digest",
 ]
 
 
@@ -85,6 +85,8 @@ def load():
         "jsc_batch_set_timing": (None, [vp, i]),
         "jsc_batch_kernel_ms": (d, [vp, C.c_char_p]),
         "jsc_batch_counters": (i, [vp, P(C.c_int64), P(C.c_int64)]),
+        "jsc_batch_set_digest": (i, [vp, i]),
+        "jsc_batch_index_digest": (i, [vp, P(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -61,10 +61,13 @@ def _child(job):
     _silence()
     lib = C.CDLL(job.get("lib", REF_LIB))
     P = C.POINTER
-    lib.formod.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT)]
-    lib.formod.restype = None
-    lib.raytrace.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT), P(LosT), C.c_int]
-    lib.raytrace.restype = None
+    port = job.get("port", False)
+    fm = lib.oracle_formod if port else lib.formod
+    fm.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT)]
+    fm.restype = C.c_int if port else None
+    if not port:
+        lib.raytrace.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT), P(LosT), C.c_int]
+        lib.raytrace.restype = None
     ctl = S.make_ctl(**job["ctl"])
     aero = job.get("aero") or S.AeroT()
     atms, ray_atm, geom = job["atms"], np.asarray(job["ray_atm"]), job["geom"]
@@ -86,7 +89,9 @@ def _child(job):
                          geom["vpz"][idx], geom["vplat"][idx],
                          geom["obslon"][idx], geom["vplon"][idx],
                          geom["time"][idx])
-        lib.formod(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero))
+        st = fm(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero))
+        if port and st:
+            raise RuntimeError("oracle_formod failed with status %d" % st)
         return atm, obs
 
     if job.get("warmup"):
@@ -101,7 +106,24 @@ def _child(job):
         out["tplon"][idx] = S.arr(obs.tplon)[:n]
         out["tplat"][idx] = S.arr(obs.tplat)[:n]
     out["seconds"] = time.perf_counter() - t0
-    if job.get("los"):
+    if job.get("los") and port:
+        lib.oracle_diagnostics.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT),
+                                           P(C.c_int), P(C.c_uint64)]
+        out["digest"] = np.zeros((nr, nd), np.uint64)
+        for ai, idx in groups:
+            atm = _atm_struct(atms[ai])
+            obs = S.make_obs(geom["obsz"][idx], geom["obslat"][idx],
+                             geom["vpz"][idx], geom["vplat"][idx],
+                             geom["obslon"][idx], geom["vplon"][idx],
+                             geom["time"][idx])
+            nl = np.zeros(len(idx), np.int32)
+            dg = np.zeros((len(idx), nd), np.uint64)
+            lib.oracle_diagnostics(C.byref(ctl), C.byref(atm), C.byref(obs),
+                                   nl.ctypes.data_as(P(C.c_int)),
+                                   dg.ctypes.data_as(P(C.c_uint64)))
+            out["nlos"][idx] = nl
+            out["digest"][idx] = dg
+    elif job.get("los"):
         los = LosT()
         for ai, idx in groups:
             atm = _atm_struct(atms[ai])
@@ -126,8 +148,24 @@ def _child(job):
     return out
 
 
+PORT_LIB = os.path.join(HERE, "build", "libjscat_oracle.so")
+
+
+def port_available():
+    return os.path.exists(PORT_LIB)
+
+
+def run_port(ctl_kw, atms, ray_atm, geom, threads=None, warmup=False, los=False,
+             timeout=1800):
+    """Same as run() with the C restatement (oracle/jurassic_oracle.c)
+    instead of the reference build; with los=True it also returns the
+    per-(ray, channel) EGA index digests."""
+    return run(ctl_kw, atms, ray_atm, geom, threads=threads, warmup=warmup,
+               los=los, lib=PORT_LIB, timeout=timeout, port=True)
+
+
 def run(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False,
-        los=False, lib=None, timeout=1800):
+        los=False, lib=None, timeout=1800, port=False):
     """Reference formod over profiles atms (list of dicts) and rays.
     Returns rad/tau [n_rays][nd], tpz/tplon/tplat, seconds (wall time of
     the formod calls after the optional warm-up call), and with los=True
@@ -137,7 +175,7 @@ def run(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False,
     import tempfile
     job = {"ctl": ctl_kw, "atms": atms, "ray_atm": np.asarray(ray_atm),
            "geom": geom, "aero": None if aero is None else bytes(aero),
-           "threads": threads, "warmup": warmup, "los": los}
+           "threads": threads, "warmup": warmup, "los": los, "port": port}
     if lib:
         job["lib"] = lib
     with tempfile.TemporaryDirectory() as d:

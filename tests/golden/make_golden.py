@@ -5,9 +5,11 @@ workloads of jscat.synth.
 
     make -C oracle ref && python tests/golden/make_golden.py
 
-Each fixture stores the reference's outputs in full FP64 precision plus a
-checksum of the generated table files, so a test can tell a changed input
-from a changed result.
+Each fixture stores the reference's outputs in full FP64 precision, the
+per-(ray, channel) EGA table-index digests of the C restatement (checked
+here to reproduce the reference's radiances bit for bit), and a checksum
+of the generated table files, so a test can tell a changed input from a
+changed result.
 """
 import hashlib
 import os
@@ -44,11 +46,23 @@ def mixed_case(workdir):
     return ctlkw, atms, ray_atm, geom
 
 
-def save(name, ctlkw, atms, ray_atm, geom, ref):
+def reference_ctl(ctlkw):
+    """Clear-air cases run the reference with SCA_MULT=0.  With the default
+    SCA_MULT=1 and no aerosol models the reference reads los->aerofac, which
+    it never initialises in clear air (src/lineofsight.c:188 skips
+    add_aerosol_layers, src/forwardmodel.c:317 tests it), so a recycled heap
+    block can send a ray down the scattering branch and return NaN.  With
+    SCA_MULT=0 the same clear-air arithmetic runs deterministically."""
+    return dict(ctlkw, sca_mult=0)
+
+
+def save(name, ctlkw, atms, ray_atm, geom, ref, port):
+    assert np.array_equal(port["rad"], ref["rad"]) and np.array_equal(port["tau"], ref["tau"]), \
+        "the C restatement must reproduce the reference bit for bit"
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"),
         rad=ref["rad"], tau=ref["tau"], tpz=ref["tpz"], tplon=ref["tplon"],
-        tplat=ref["tplat"], nlos=ref["nlos"],
+        tplat=ref["tplat"], nlos=ref["nlos"], digest=port["digest"],
         table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
         ray_atm=np.asarray(ray_atm), **{"geom_" + k: v for k, v in geom.items()})
 
@@ -56,11 +70,14 @@ def save(name, ctlkw, atms, ray_atm, geom, ref):
 def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
     ctlkw, atm, geom = synth.clear_limb_case(workdir)
-    ref = refrun.run(ctlkw, [atm], np.zeros(len(geom["obsz"]), int), geom, los=True)
-    save("clear_limb", ctlkw, [atm], np.zeros(len(geom["obsz"]), int), geom, ref)
+    ra = np.zeros(len(geom["obsz"]), int)
+    ref = refrun.run(reference_ctl(ctlkw), [atm], ra, geom, los=True)
+    port = refrun.run_port(ctlkw, [atm], ra, geom, los=True)
+    save("clear_limb", ctlkw, [atm], ra, geom, ref, port)
     ctlkw, atms, ray_atm, geom = mixed_case(workdir)
-    ref = refrun.run(ctlkw, atms, ray_atm, geom, los=True)
-    save("mixed_batch", ctlkw, atms, ray_atm, geom, ref)
+    ref = refrun.run(reference_ctl(ctlkw), atms, ray_atm, geom, los=True)
+    port = refrun.run_port(ctlkw, atms, ray_atm, geom, los=True)
+    save("mixed_batch", ctlkw, atms, ray_atm, geom, ref, port)
     print("fixtures written to", HERE)
 
 

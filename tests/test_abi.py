@@ -1,0 +1,104 @@
+"""The drop-in boundary: struct layouts and exported symbols (CPU only)."""
+import ctypes as C
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+
+import pytest
+
+from conftest import GOLDEN, REPO
+
+sys.path.insert(0, GOLDEN)
+
+
+def _golden_layout():
+    with open(os.path.join(GOLDEN, "struct_layout.json")) as f:
+        return json.load(f)
+
+
+def test_header_struct_layout_matches_reference():
+    """sizeof/offsetof of every field of include/jurassic_b200.h equal the
+    reference's src/jurassic.h (recorded by make_struct_layout.py)."""
+    from make_struct_layout import measure
+    mine = measure('#include "jurassic_b200.h"', ["-I" + os.path.join(REPO, "include")])
+    assert mine == _golden_layout()
+
+
+def test_ctypes_layout_matches_reference():
+    from jscat import structs as S
+    ref = _golden_layout()
+    classes = {"ctl_t": S.CtlT, "obs_t": S.ObsT, "aero_t": S.AeroT,
+               "atm_t": S.AtmT, "queue_t": S.QueueT}
+    for cname, cls in classes.items():
+        assert C.sizeof(cls) == ref[cname + ".sizeof"], cname
+        for f in cls._fields_:
+            assert getattr(cls, f[0]).offset == ref["%s.%s" % (cname, f[0])], (cname, f[0])
+
+
+def _header_functions():
+    src = open(os.path.join(REPO, "include", "jurassic_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b(\w+)\s*\([^;{]*\)\s*;", src)
+    return sorted(set(n for n in names if n not in ("sizeof",)))
+
+
+def test_library_exports_every_declared_symbol():
+    from jscat import lib as L
+    declared = _header_functions()
+    assert set(declared) == set(L.EXPORTS), set(declared) ^ set(L.EXPORTS)
+    res = subprocess.run(["nm", "-D", "--defined-only", L.LIB_PATH],
+                         capture_output=True, text=True, check=True)
+    exported = set(ln.split()[-1] for ln in res.stdout.splitlines() if " T " in ln)
+    missing = [n for n in declared if n not in exported]
+    assert not missing, missing
+
+
+def test_library_loads_without_gpu():
+    from jscat import lib as L
+    lib = L.load()
+    for n in L.EXPORTS:
+        assert hasattr(lib, n)
+    assert lib.jsc_status_string(0) == b"ok"
+
+
+# Values returned by the reference build for the two example invocations
+# of docu/modules.tex ("planck 270 960", "brightness 0.0231451 960").
+REF_PLANCK_270_960 = 0.06362961283311917
+REF_BRIGHTNESS_00231451_960 = 225.57541385238784
+
+
+def test_known_answers_planck_brightness():
+    from jscat import lib as L
+    lib = L.load()
+    assert lib.planck(270.0, 960.0) == REF_PLANCK_270_960
+    assert lib.brightness(0.0231451, 960.0) == REF_BRIGHTNESS_00231451_960
+    assert abs(lib.brightness(REF_PLANCK_270_960, 960.0) - 270.0) < 1e-9
+
+
+def test_drop_in_links_in_place_of_forwardmodel():
+    """A C program written against the reference's API (formod, brightness,
+    planck with the reference structs) compiles and links against the
+    library."""
+    prog = r'''
+#include <stdio.h>
+#include "jurassic_b200.h"
+int main(void) {
+  static ctl_t ctl; static atm_t atm; static obs_t obs; static aero_t aero;
+  void (*f)(ctl_t *, atm_t *, obs_t *, aero_t *) = formod;
+  printf("%p %.6f %.6f\n", (void *)f, brightness(0.0231451, 960.0), planck(270.0, 960.0));
+  (void)ctl; (void)atm; (void)obs; (void)aero;
+  return 0;
+}
+'''
+    from jscat import lib as L
+    with tempfile.TemporaryDirectory() as d:
+        src, exe = os.path.join(d, "p.c"), os.path.join(d, "p")
+        open(src, "w").write(prog)
+        subprocess.run(["gcc", "-I" + os.path.join(REPO, "include"), src, "-o", exe,
+                        L.LIB_PATH, "-Wl,-rpath," + os.path.dirname(L.LIB_PATH)],
+                       check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+        assert "225.575414 0.063630" in out

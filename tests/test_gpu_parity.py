@@ -2,10 +2,13 @@
 
 Golden fixtures hold the reference's own FP64 outputs (tests/golden,
 made by make_golden.py with the reference compiled from its sources) for
-seeded synthetic inputs regenerated here.  Bars: LOS point counts exactly
-equal, brightness temperature within 0.01 K, and radiance/transmittance
-within 1e-9 relative (the GPU keeps the reference's FP64 operation order;
-only libm last-bit differences remain)."""
+seeded synthetic inputs regenerated here, plus the per-(ray, channel)
+checksums of every emissivity-table index the EGA interpolation selected
+(from the C restatement, which reproduces the reference bit for bit).
+Bars: LOS point counts and table indices exactly equal, brightness
+temperature within 0.01 K, radiance/transmittance within 1e-9 relative
+(the GPU keeps the reference's FP64/FP32 operation order; only last-bit
+differences of the CUDA and glibc transcendental functions remain)."""
 import os
 
 import numpy as np
@@ -51,6 +54,18 @@ def test_clear_limb_dropin_formod(workdir):
     np.testing.assert_allclose(S.arr(obs.tpz)[:nr], g["tpz"], rtol=1e-9, atol=1e-9)
 
 
+def test_clear_limb_batch_indices(workdir):
+    from jscat import structs as S, synth, api
+    g = _load("clear_limb")
+    ctlkw, atm, geom = synth.clear_limb_case(workdir)
+    ctl = S.make_ctl(**ctlkw)
+    out = api.formod_batch(ctl, synth.batch_from([atm], np.zeros(len(geom["obsz"]), np.int32), geom),
+                           digest=True)
+    np.testing.assert_array_equal(out["nlos"], g["nlos"])
+    np.testing.assert_array_equal(out["digest"], g["digest"])
+    assert max_rel(out["rad"], g["rad"]) <= REL_TOL
+
+
 def test_mixed_batch(workdir):
     from jscat import synth, api, structs as S
     from make_golden_shim import mixed_case
@@ -58,8 +73,9 @@ def test_mixed_batch(workdir):
     ctlkw, atms, ray_atm, geom = mixed_case(workdir)
     _check_tables(g, ctlkw)
     ctl = S.make_ctl(**ctlkw)
-    out = api.formod_batch(ctl, synth.batch_from(atms, ray_atm, geom))
+    out = api.formod_batch(ctl, synth.batch_from(atms, ray_atm, geom), digest=True)
     np.testing.assert_array_equal(out["nlos"], g["nlos"])
+    np.testing.assert_array_equal(out["digest"], g["digest"])
     assert bt_error(out["rad"], g["rad"], ctlkw["nus"]) <= BT_TOL_K
     assert max_rel(out["rad"], g["rad"]) <= REL_TOL
     assert max_rel(out["tau"], g["tau"]) <= REL_TOL

@@ -1,0 +1,122 @@
+"""The CPU oracle (oracle/jurassic_oracle.c) pinned against the reference:
+bit for bit against the reference's outputs stored in tests/golden, and
+against the reference's own example goldens (examples/org) where the
+reference tree is present (this container; not on the GPU box)."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, REPO
+
+REF_EXAMPLES = "/root/reference/examples"
+PORT = os.path.join(REPO, "oracle", "build", "libjscat_oracle.so")
+
+
+def _golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+@pytest.fixture(scope="module")
+def port():
+    if not os.path.exists(PORT):
+        import subprocess
+        subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "port"], check=True)
+    return PORT
+
+
+def test_port_bit_exact_clear_limb(workdir, port):
+    from jscat import synth
+    from oracle import refrun
+    g = _golden("clear_limb")
+    ctlkw, atm, geom = synth.clear_limb_case(workdir)
+    r = refrun.run_port(ctlkw, [atm], np.zeros(len(geom["obsz"]), int), geom, los=True)
+    assert np.array_equal(r["rad"], g["rad"])
+    assert np.array_equal(r["tau"], g["tau"])
+    assert np.array_equal(r["tpz"], g["tpz"])
+    assert np.array_equal(r["nlos"], g["nlos"])
+    assert np.array_equal(r["digest"], g["digest"])
+
+
+def test_port_bit_exact_mixed_batch(workdir, port):
+    from make_golden_shim import mixed_case
+    from oracle import refrun
+    g = _golden("mixed_batch")
+    ctlkw, atms, ray_atm, geom = mixed_case(workdir)
+    r = refrun.run_port(ctlkw, atms, ray_atm, geom, los=True)
+    for k in ("rad", "tau", "tpz", "tplon", "tplat", "nlos", "digest"):
+        assert np.array_equal(r[k], g[k]), k
+
+
+def _read_cols(path):
+    rows = []
+    for ln in open(path):
+        ln = ln.strip()
+        if ln and not ln.startswith("#"):
+            rows.append(ln.split())
+    return rows
+
+
+def _port_lib():
+    lib = C.CDLL(PORT)
+    from jscat import structs as S
+    P = C.POINTER
+    lib.oracle_formod.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT)]
+    lib.oracle_formod.restype = C.c_int
+    lib.oracle_raytrace.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), C.c_int] + \
+        [P(C.c_double)] * 10
+    lib.oracle_raytrace.restype = C.c_int
+    return lib
+
+
+def _example_inputs():
+    from jscat import structs as S
+    ctl = S.make_ctl(["CO2", "H2O", "O3"], [792.0],
+                     os.path.join(REF_EXAMPLES, "tab", "boxcar"))
+    a = np.array(_read_cols(os.path.join(REF_EXAMPLES, "org", "atm.tab")), dtype=float)
+    atm = S.make_atm(a[:, 1], a[:, 4], a[:, 5], a[:, 6:9].T, a[:, 9:10].T, a[:, 2], a[:, 3])
+    return ctl, atm
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference tree not present")
+def test_port_reproduces_example_rad_clear(port):
+    """examples/clear.sh: 11 limb rays, CO2/H2O/O3 RFM tables at 792 cm-1;
+    the port's output formatted like write_obs (src/misc.c:377-384) equals
+    org/rad_clear.tab."""
+    from jscat import structs as S
+    ctl, atm = _example_inputs()
+    o = np.array(_read_cols(os.path.join(REF_EXAMPLES, "org", "obs.tab")), dtype=float)
+    obs = S.make_obs(o[:, 1], o[:, 3], o[:, 4], o[:, 6], o[:, 2], o[:, 5], o[:, 0])
+    lib = _port_lib()
+    assert lib.oracle_formod(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(S.AeroT())) == 0
+    mine = []
+    for ir in range(obs.nr):
+        vals = [obs.obsz[ir], obs.obslon[ir], obs.obslat[ir], obs.vpz[ir], obs.vplon[ir],
+                obs.vplat[ir], obs.tpz[ir], obs.tplon[ir], obs.tplat[ir],
+                obs.rad[0][ir], obs.tau[0][ir]]
+        mine.append(["%.2f" % obs.time[ir]] + ["%g" % v for v in vals])
+    assert mine == _read_cols(os.path.join(REF_EXAMPLES, "org", "rad_clear.tab"))
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference tree not present")
+def test_port_reproduces_example_los(port):
+    """examples/raytrace.sh: one 8 km limb ray; every LOS record formatted
+    like raytrace.c (src/raytrace.c:88-103) equals org/los.0."""
+    from jscat import structs as S
+    ctl, atm = _example_inputs()
+    o = np.array(_read_cols(os.path.join(REF_EXAMPLES, "org", "obs_raytrace.tab")), dtype=float)
+    obs = S.make_obs(o[:, 1], o[:, 3], o[:, 4], o[:, 6], o[:, 2], o[:, 5], o[:, 0])
+    lib = _port_lib()
+    n = 10000
+    bufs = [np.zeros(n) for _ in range(6)] + [np.zeros(n * 3), np.zeros(n), np.zeros(n * 3)]
+    ts = np.zeros(1)
+    np_ = lib.oracle_raytrace(C.byref(ctl), C.byref(atm), C.byref(obs), 0,
+                              *[b.ctypes.data_as(C.POINTER(C.c_double)) for b in bufs + [ts]])
+    z, lon, lat, p, t, ds, q, k, u = bufs
+    rows = []
+    for i in range(np_):
+        vals = [z[i], lon[i], lat[i], p[i], t[i]] + list(q[3 * i:3 * i + 3]) + [k[i]] + \
+            list(u[3 * i:3 * i + 3]) + [0.0, 0.0, 0.0, ds[i]]
+        rows.append(["%.2f" % 0.0] + ["%g" % v for v in vals])
+    assert rows == _read_cols(os.path.join(REF_EXAMPLES, "org", "los.0"))
