@@ -264,9 +264,12 @@ static void o_tangent_point(const olos_t *los, double *tpz, double *tplon, doubl
   }
 }
 
-/* src/lineofsight.c:5-190 (aerosol layer refinement not restated; the
- * oracle covers the clear-air path). */
-static int o_raytrace(const ctl_t *ctl, const atm_t *atm, obs_t *obs, olos_t *los, int ir) {
+static int o_add_aerosol_layers(const ctl_t *ctl, const atm_t *atm, olos_t *los,
+                                const aero_t *aero);
+
+/* src/lineofsight.c:5-190 */
+static int o_raytrace(const ctl_t *ctl, const atm_t *atm, obs_t *obs, const aero_t *aero,
+                      olos_t *los, int ir) {
   double cosa, d, dmax, dmin = 0, ds, ex0[3], ex1[3], h = 0.02, k[NWMAX], lat, lon,
          n, naux, ng[3], norm, p = 0, q[NGMAX], t = 0, x[3], xh[3], xobs[3], xvp[3],
          z = 1e99, zmax, zmin, zrefrac = 60;
@@ -366,6 +369,148 @@ static int o_raytrace(const ctl_t *ctl, const atm_t *atm, obs_t *obs, olos_t *lo
   for (int ip = 0; ip < los->np; ip++)
     for (int ig = 0; ig < ctl->ng; ig++)
       los->u[ip][ig] = 10 * los->q[ip][ig] * los->p[ip] / (JSC_KBOLTZ * los->t[ip]) * los->ds[ip];
+  for (int ip = 0; ip < los->np; ip++) {
+    los->aerofac[ip] = 0;   /* the reference leaves these unset in clear air */
+    los->aeroi[ip] = -999;
+  }
+  if (ctl->sca_n > 0) return o_add_aerosol_layers(ctl, atm, los, aero);
+  return 0;
+}
+
+static int cmp_desc(const void *a, const void *b) {
+  double x = *(const double *)a, y = *(const double *)b;
+  return (x < y) - (x > y);
+}
+
+#define DIST3(a, b) sqrt(((a)[0] - (b)[0]) * ((a)[0] - (b)[0]) + ((a)[1] - (b)[1]) * ((a)[1] - (b)[1]) + \
+                         ((a)[2] - (b)[2]) * ((a)[2] - (b)[2]))
+
+/* Extra LOS points at the aerosol/cloud layer edges and through the
+ * transition layers, chord step lengths, layer index and scaling factor
+ * per point (src/lineofsight.c:193-372). */
+static int o_add_aerosol_layers(const ctl_t *ctl, const atm_t *atm, olos_t *los,
+                                const aero_t *aero) {
+  double alti[4 * NLMAX + 2 * 1000], altimax, altimin, x1[3], x2[3], x3[3], eps = 0.005;
+  int jl = 0;
+  for (int il = 0; il < aero->nl; il++) {
+    alti[jl] = aero->top[il] + eps;
+    alti[jl + 1] = aero->top[il] - eps;
+    alti[jl + 2] = aero->bottom[il] + eps;
+    alti[jl + 3] = aero->bottom[il] - eps;
+    jl += 4;
+    if (aero->trans[il] > ctl->transs) {
+      double tt = aero->trans[il] / ctl->transs;
+      alti[jl] = aero->top[il] + aero->trans[il] + eps;
+      alti[jl + 1] = aero->top[il] + aero->trans[il] - eps;
+      alti[jl + 2] = aero->bottom[il] - aero->trans[il] + eps;
+      alti[jl + 3] = aero->bottom[il] - aero->trans[il] - eps;
+      jl += 4;
+      for (int it = 1; it < (int)tt; it++) {
+        if (jl + 2 > (int)(sizeof(alti) / sizeof(alti[0]))) return JSC_ERR_NLOS;
+        alti[jl++] = aero->top[il] + aero->trans[il] - eps - it * ctl->transs;
+        alti[jl++] = aero->bottom[il] - aero->trans[il] + eps + it * ctl->transs;
+      }
+    }
+  }
+  /* top-down order (the reference negates, sorts ascending, negates) */
+  qsort(alti, (size_t)jl, sizeof(double), cmp_desc);
+  altimax = alti[0];
+  altimin = alti[0];
+  for (int i = 0; i < jl; i++) {
+    if (alti[i] > altimax) altimax = alti[i];
+    if (alti[i] < altimin) altimin = alti[i];
+  }
+  olos_t *la = los_new();
+  la->tsurf = los->tsurf;
+  la->z[0] = los->z[0];
+  la->lat[0] = los->lat[0];
+  la->lon[0] = los->lon[0];
+  la->ds[0] = los->ds[0];
+  la->t[0] = los->t[0];
+  la->p[0] = los->p[0];
+  for (int ig = 0; ig < ctl->ng; ig++) la->q[0][ig] = los->q[0][ig];
+  for (int iw = 0; iw < ctl->nw; iw++) la->k[0][iw] = los->k[0][iw];
+  la->np = 1;
+  for (int ip = 1; ip < los->np; ip++) {
+    if ((los->z[ip - 1] < altimax || los->z[ip] < altimax) &&
+        (los->z[ip - 1] > altimin || los->z[ip] > altimin)) {
+      for (int il = 0; il < jl; il++) {
+        if (los->z[ip - 1] > alti[il] && los->z[ip] < alti[il]) {
+          if (la->np >= NLOS) { los_free(la); return JSC_ERR_NLOS; }
+          o_intersection(ctl, atm, alti[il], los, ip, la, la->np);
+          la->np++;
+        }
+        if (los->z[ip - 1] < alti[jl - il - 1] && los->z[ip] > alti[jl - il - 1]) {
+          if (la->np >= NLOS) { los_free(la); return JSC_ERR_NLOS; }
+          o_intersection(ctl, atm, alti[jl - il - 1], los, ip, la, la->np);
+          la->np++;
+        }
+      }
+    }
+    if (la->np >= NLOS) { los_free(la); return JSC_ERR_NLOS; }
+    la->z[la->np] = los->z[ip];
+    la->lat[la->np] = los->lat[ip];
+    la->lon[la->np] = los->lon[ip];
+    la->t[la->np] = los->t[ip];
+    la->p[la->np] = los->p[ip];
+    for (int ig = 0; ig < ctl->ng; ig++) la->q[la->np][ig] = los->q[ip][ig];
+    for (int iw = 0; iw < ctl->nw; iw++) la->k[la->np][iw] = los->k[ip][iw];
+    la->np++;
+  }
+  o_geo2cart(la->z[0], la->lon[0], la->lat[0], x1);
+  o_geo2cart(la->z[1], la->lon[1], la->lat[1], x2);
+  la->ds[0] = 0.5 * (DIST3(x1, x2));
+  for (int ip = 1; ip < la->np - 1; ip++) {
+    o_geo2cart(la->z[ip - 1], la->lon[ip - 1], la->lat[ip - 1], x1);
+    o_geo2cart(la->z[ip], la->lon[ip], la->lat[ip], x2);
+    o_geo2cart(la->z[ip + 1], la->lon[ip + 1], la->lat[ip + 1], x3);
+    la->ds[ip] = 0.5 * (DIST3(x1, x2) + DIST3(x2, x3));
+  }
+  o_geo2cart(la->z[la->np - 1], la->lon[la->np - 1], la->lat[la->np - 1], x1);
+  o_geo2cart(la->z[la->np - 2], la->lon[la->np - 2], la->lat[la->np - 2], x2);
+  la->ds[la->np - 1] = 0.5 * (DIST3(x1, x2));
+  for (int ip = 0; ip < la->np; ip++) {
+    for (int ig = 0; ig < ctl->ng; ig++)
+      la->u[ip][ig] = 10 * la->q[ip][ig] * la->p[ip] / (JSC_KBOLTZ * la->t[ip]) * la->ds[ip];
+    la->aeroi[ip] = -999;
+    la->aerofac[ip] = 0.;
+    /* at ip = 0 the reference reads z[-1]; z[0] stands in (the first
+     * point lies at the top of the atmosphere, outside every layer) */
+    double zprev = la->z[ip > 0 ? ip - 1 : 0];
+    if ((zprev < altimax || la->z[ip] < altimax) && (zprev > altimin || la->z[ip] > altimin)) {
+      for (int il = 0; il < aero->nl; il++) {
+        if (la->z[ip] <= aero->top[il] && la->z[ip] >= aero->bottom[il]) {
+          la->aeroi[ip] = il;
+          la->aerofac[ip] = 1.;
+        }
+        if (aero->trans[il] > ctl->transs && la->z[ip] <= (aero->top[il] + aero->trans[il]) &&
+            la->z[ip] > aero->top[il]) {
+          la->aeroi[ip] = il;
+          la->aerofac[ip] = (aero->top[il] + aero->trans[il] - la->z[ip]) / aero->trans[il];
+        }
+        if (aero->trans[il] > ctl->transs && la->z[ip] < aero->bottom[il] &&
+            la->z[ip] >= (aero->bottom[il] - aero->trans[il])) {
+          la->aeroi[ip] = il;
+          la->aerofac[ip] = fabs(aero->bottom[il] - aero->trans[il] - la->z[ip]) / aero->trans[il];
+        }
+      }
+    }
+  }
+  /* copy back */
+  los->np = la->np;
+  los->tsurf = la->tsurf;
+  memcpy(los->z, la->z, sizeof(double) * NLOS);
+  memcpy(los->lon, la->lon, sizeof(double) * NLOS);
+  memcpy(los->lat, la->lat, sizeof(double) * NLOS);
+  memcpy(los->p, la->p, sizeof(double) * NLOS);
+  memcpy(los->t, la->t, sizeof(double) * NLOS);
+  memcpy(los->ds, la->ds, sizeof(double) * NLOS);
+  memcpy(los->aerofac, la->aerofac, sizeof(double) * NLOS);
+  memcpy(los->aeroi, la->aeroi, sizeof(int) * NLOS);
+  memcpy(los->q, la->q, sizeof(double) * NLOS * NGMAX);
+  memcpy(los->k, la->k, sizeof(double) * NLOS * NWMAX);
+  memcpy(los->u, la->u, sizeof(double) * NLOS * NGMAX);
+  los_free(la);
   return 0;
 }
 
@@ -598,17 +743,26 @@ static void o_intpol_tbl(const ctl_t *ctl, const olos_t *los, int ip,
         else {
           if (dig) *dig = *dig * 1000003u + (uint64_t)(ipr * 961 + it0 * 31 + it1);
           double x = 1 - tau_path[ig][id], us = los->u[ip][ig], u, e00, e01, e10, e11;
+          /* assign, then clamp (the clamp macro evaluates its argument
+           * more than once) */
           u = o_tbl_u(tb, ipr, it0, x, dig);
-          e00 = CLAMP01(o_tbl_eps(tb, ipr, it0, u + us, dig));
+          e00 = o_tbl_eps(tb, ipr, it0, u + us, dig);
+          e00 = CLAMP01(e00);
           u = o_tbl_u(tb, ipr, it0 + 1, x, dig);
-          e01 = CLAMP01(o_tbl_eps(tb, ipr, it0 + 1, u + us, dig));
+          e01 = o_tbl_eps(tb, ipr, it0 + 1, u + us, dig);
+          e01 = CLAMP01(e01);
           u = o_tbl_u(tb, ipr + 1, it1, x, dig);
-          e10 = CLAMP01(o_tbl_eps(tb, ipr + 1, it1, u + us, dig));
+          e10 = o_tbl_eps(tb, ipr + 1, it1, u + us, dig);
+          e10 = CLAMP01(e10);
           u = o_tbl_u(tb, ipr + 1, it1 + 1, x, dig);
-          e11 = CLAMP01(o_tbl_eps(tb, ipr + 1, it1 + 1, u + us, dig));
-          e00 = CLAMP01(LINV(tb->t[ipr][it0], e00, tb->t[ipr][it0 + 1], e01, los->t[ip]));
-          e11 = CLAMP01(LINV(tb->t[ipr + 1][it1], e10, tb->t[ipr + 1][it1 + 1], e11, los->t[ip]));
-          e00 = CLAMP01(LINV(tb->p[ipr], e00, tb->p[ipr + 1], e11, los->p[ip]));
+          e11 = o_tbl_eps(tb, ipr + 1, it1 + 1, u + us, dig);
+          e11 = CLAMP01(e11);
+          e00 = LINV(tb->t[ipr][it0], e00, tb->t[ipr][it0 + 1], e01, los->t[ip]);
+          e00 = CLAMP01(e00);
+          e11 = LINV(tb->t[ipr + 1][it1], e10, tb->t[ipr + 1][it1 + 1], e11, los->t[ip]);
+          e11 = CLAMP01(e11);
+          e00 = LINV(tb->p[ipr], e00, tb->p[ipr + 1], e11, los->p[ip]);
+          e00 = CLAMP01(e00);
           eps = 1 - (1 - e00) / tau_path[ig][id];
         }
       }
@@ -700,13 +854,197 @@ static void o_continua(const ctl_t *ctl, const olos_t *los, int ip, double *beta
 
 /* ------------------------------------------------------------ formod -- */
 
-/* Clear-air pencil beam (src/forwardmodel.c:224-405, scattering == 0). */
-static int o_pencil(const ctl_t *ctl, const atm_t *atm, obs_t *obs, int ir, uint64_t *dig,
-                    int *nlos) {
-  double beta[NDMAX], src[NDMAX], tau_seg[NDMAX];
+static int o_pencil(const ctl_t *ctl, const atm_t *atm, obs_t *obs, const aero_t *aero,
+                    int scattering, int ir, uint64_t *dig, int *nlos);
+
+/* Orthonormal basis with ez along dz (src/scatter.c:6-52). */
+static void o_bascoord(const double *dz, const double *dy, double *ex, double *ey, double *ez) {
+  double dotp, norm = NRM(dz);
+  for (int i = 0; i < 3; i++) ez[i] = dz[i] / norm;
+  norm = NRM(dy);
+  for (int i = 0; i < 3; i++) ey[i] = dy[i] / norm;
+  dotp = DOT(ey, ez);
+  if (dotp == 1) {
+    ey[0] = 1;
+    ey[1] = 0;
+    ey[2] = 0;
+    dotp = ez[0];
+    if (dotp == 1) {
+      ey[0] = 0;
+      ey[1] = 1;
+      dotp = ez[1];
+    }
+  }
+  for (int i = 0; i < 3; i++) ey[i] -= dotp * ez[i];
+  norm = NRM(ey);
+  for (int i = 0; i < 3; i++) ey[i] /= norm;
+  ex[0] = ey[1] * ez[2] - ey[2] * ez[1];
+  ex[1] = ey[2] * ez[0] - ey[0] * ez[2];
+  ex[2] = ey[0] * ez[1] - ey[1] * ez[0];
+}
+
+/* ANGLE macro (src/jurassic.h:33-34). */
+static double o_angle(const double *a, const double *b) {
+  double c = DOT(a, b) / NRM(a) / NRM(b);
+  return acos(MIN(MAX(c, -1), 1));
+}
+
+/* Zenith angles of the secondary pencils (src/scatter.c:698-715). */
+static void o_sca_alpha(double *alpha, int nalpha) {
+  int n1 = 1, n2 = 2;
+  double midang = 83, up = 92, down = 81, step = 1 + 2;
+  alpha[0] = 0;
+  for (int ir = nalpha / 2 - 4; ir < nalpha / 2 + 4; ++ir) {
+    alpha[ir] = midang * M_PI / 180.;
+    midang++;
+  }
+  for (int ir = 0; ir < nalpha / 2 - 5; ++ir) {
+    alpha[nalpha / 2 + ir + 4] = up * M_PI / 180.;
+    alpha[nalpha / 2 - ir - 5] = down * M_PI / 180.;
+    up += step;
+    down -= step;
+    if (step < 13) {
+      step = (double)n1 + (double)n2;
+      n1 = n2;
+      n2 = (int)step;
+    }
+  }
+  alpha[nalpha - 1] = M_PI;
+}
+
+/* Thermal single scattering in 1-D atmospheres (src/scatter.c:666-807):
+ * 28 secondary pencils at fixed zenith angles, then the phase-function
+ * weighted integral over 180 x 180 directions. */
+static int o_srcfunc_sca_1d(const ctl_t *ctl, const atm_t *atm, const aero_t *aero,
+                            const double *x, const double *dx, int il, double *src_sca,
+                            int scattering) {
+  enum { NALPHA = 28, NPHI = 180, NTHETA2 = 180 };
+  double alpha[NALPHA], dnorth[3], ek[3], lx[3], ly[3], lz[3], sx[3], sy[3], sz[3],
+         theta[NTHETA], wsum[NDMAX], xv[3], mlz[3];
+  obs_t *obs2 = (obs_t *)calloc(1, sizeof(obs_t));
+  int st = 0;
+  for (int it = 0; it < NTHETA; it++) theta[it] = (double)it * M_PI / 180.;
+  dnorth[0] = -x[0];
+  dnorth[1] = -x[1];
+  dnorth[2] = 2 * JSC_RE - x[2];
+  o_bascoord(x, dnorth, lx, ly, lz);
+  o_sca_alpha(alpha, NALPHA);
+  for (int ir = 0; ir < NALPHA && !st; ir++) {
+    for (int i = 0; i < 3; i++)
+      xv[i] = x[i] + 10. * cos(alpha[ir]) * (-1) * lz[i] + 10. * sin(alpha[ir]) * ly[i];
+    obs2->nr = NALPHA;
+    o_cart2geo(x, &obs2->obsz[ir], &obs2->obslon[ir], &obs2->obslat[ir]);
+    o_cart2geo(xv, &obs2->vpz[ir], &obs2->vplon[ir], &obs2->vplat[ir]);
+    st = o_pencil(ctl, atm, obs2, aero, scattering - 1, ir, NULL, NULL);
+  }
+  o_bascoord(dx, x, sx, sy, sz);
+  for (int id = 0; id < ctl->nd; id++) {
+    src_sca[id] = 0;
+    wsum[id] = 0;
+  }
+  for (int i = 0; i < 3; i++) mlz[i] = -1. * lz[i];
+  for (int itheta = 0; itheta < NTHETA2; itheta++) {
+    double theta2 = (0.5 + itheta) * M_PI / 180.;
+    for (int iphi = 0; iphi < NPHI; iphi++) {
+      double phi = 2. * (0.5 + iphi) * M_PI / 180.;
+      for (int i = 0; i < 3; i++)
+        ek[i] = sin(theta2) * sin(phi) * sx[i] + sin(theta2) * cos(phi) * sy[i] + cos(theta2) * sz[i];
+      int idp = o_locate(theta, NTHETA, theta2);
+      double alpha2 = o_angle(mlz, ek);
+      int idx = o_locate(alpha, NALPHA, alpha2);
+      for (int id = 0; id < ctl->nd; id++) {
+        double phase2 = LINV(theta[idp], aero->p[il][id][idp], theta[idp + 1],
+                             aero->p[il][id][idp + 1], theta2);
+        double w = sin(theta2) * phase2;
+        double rad = LINV(alpha[idx], obs2->rad[id][idx], alpha[idx + 1], obs2->rad[id][idx + 1],
+                          alpha2);
+        src_sca[id] += w * rad;
+        wsum[id] += w;
+      }
+    }
+  }
+  for (int id = 0; id < ctl->nd; id++) src_sca[id] /= wsum[id];
+  free(obs2);
+  return st;
+}
+
+/* Solar position (src/scatter.c:999-1041). */
+static void o_suncoord(double sec, double lon, double lat, double *azi, double *sza) {
+  double D = sec / 86400 - 0.5;
+  double g = (357.529 + 0.98560028 * D) * M_PI / 180;
+  double q = 280.459 + 0.98564736 * D;
+  double L = (q + 1.915 * sin(g) + 0.020 * sin(2 * g)) * M_PI / 180;
+  double e = (23.439 - 0.00000036 * D) * M_PI / 180;
+  double dec = asin(sin(e) * sin(L));
+  double ra = atan2(cos(e) * sin(L), cos(L));
+  double GMST = 18.697374558 + 24.06570982441908 * D;
+  double LST = GMST + lon / 15;
+  double h = LST / 12 * M_PI - ra;
+  lat *= M_PI / 180;
+  *azi = atan2(-sin(h), cos(lat) * tan(dec) - sin(lat) * cos(h)) * 180 / M_PI;
+  *sza = acos(sin(lat) * sin(dec) + cos(lat) * cos(dec) * cos(h)) * 180 / M_PI;
+}
+
+/* Solar single scattering (src/scatter.c:899-995). */
+static int o_srcfunc_sca_sun(const ctl_t *ctl, const atm_t *atm, const aero_t *aero, double sec,
+                             const double *x, const double *dx, int il, double *src_sca) {
+  double azi, dnorth[3], dout[3], ek[3], lx[3], ly[3], lz[3], sza, sza_beam, sza_cor,
+         theta[NTHETA], x0[3], x1[3];
+  olos_t *los = los_new();
+  obs_t *obs = (obs_t *)calloc(1, sizeof(obs_t));
+  int st = 0;
+  for (int it = 0; it < NTHETA; it++) theta[it] = M_PI * (double)it / (NTHETA - 1);
+  dnorth[0] = -x[0];
+  dnorth[1] = -x[1];
+  dnorth[2] = 2 * JSC_RE - x[2];
+  o_bascoord(x, dnorth, lx, ly, lz);
+  obs->nr = 1;
+  o_cart2geo(x, &obs->obsz[0], &obs->obslon[0], &obs->obslat[0]);
+  o_suncoord(sec, obs->obslon[0], obs->obslat[0], &azi, &sza);
+  sza_cor = sza;
+  for (int i2 = 0; i2 < 10; i2++) {
+    for (int i = 0; i < 3; i++) {
+      ek[i] = sin(sza_cor * M_PI / 180) * sin(azi * M_PI / 180) * lx[i] +
+              sin(sza_cor * M_PI / 180) * cos(azi * M_PI / 180) * ly[i] +
+              cos(sza_cor * M_PI / 180) * lz[i];
+      x1[i] = x[i] + 10 * ek[i];
+    }
+    o_cart2geo(x1, &obs->vpz[0], &obs->vplon[0], &obs->vplat[0]);
+    st = o_raytrace(ctl, atm, obs, aero, los, 0);
+    if (st || los->np < 2) break;
+    o_geo2cart(los->z[los->np - 2], los->lon[los->np - 2], los->lat[los->np - 2], x0);
+    o_geo2cart(los->z[los->np - 1], los->lon[los->np - 1], los->lat[los->np - 1], x1);
+    for (int i = 0; i < 3; i++) dout[i] = x1[i] - x0[i];
+    sza_beam = o_angle(x, dout) * 180 / M_PI;
+    if (fabs(sza_beam - sza) < 0.01) break;
+    sza_cor -= 0.61803 * (sza_beam - sza);
+    sza_cor = MIN(MAX(sza_cor, 0), 180);
+  }
+  if (!st && los->tsurf < 0) {
+    st = o_pencil(ctl, atm, obs, aero, 0, 0, NULL, NULL);
+    double theta2 = o_angle(ek, dx);
+    int idx = o_locate(theta, NTHETA, theta2);
+    for (int id = 0; id < ctl->nd; id++) {
+      double phase2 = LINV(theta[idx], aero->p[il][id][idx], theta[idx + 1],
+                           aero->p[il][id][idx + 1], theta2);
+      src_sca[id] += 6.764e-5 * phase2 * oracle_planck(JSC_TSUN, ctl->nu[id]) * obs->tau[id][0];
+    }
+  }
+  los_free(los);
+  free(obs);
+  return st;
+}
+
+/* Pencil beam (src/forwardmodel.c:224-405): trace, then EGA, continua,
+ * Planck and radiative transfer per LOS point, with the scattering source
+ * at aerosol points when scattering > 0. */
+static int o_pencil(const ctl_t *ctl, const atm_t *atm, obs_t *obs, const aero_t *aero,
+                    int scattering, int ir, uint64_t *dig, int *nlos) {
+  double beta[NDMAX], src[NDMAX], tau_seg[NDMAX], src_sca[NDMAX], x[3], x0[3], x1[3], dx[3];
   double (*tau_path)[NDMAX] = malloc(sizeof(double) * NGMAX * NDMAX);
   olos_t *los = los_new();
-  int st = o_raytrace(ctl, atm, obs, los, ir);
+  int st = o_raytrace(ctl, atm, obs, aero, los, ir);
+  const int beta_a = strcmp(ctl->sca_ext, "beta_a") == 0;
   if (nlos) *nlos = los->np;
   for (int id = 0; id < ctl->nd; id++) {
     obs->rad[id][ir] = 0;
@@ -716,12 +1054,42 @@ static int o_pencil(const ctl_t *ctl, const atm_t *atm, obs_t *obs, int ir, uint
     o_intpol_tbl(ctl, los, ip, tau_path, tau_seg, dig);
     o_continua(ctl, los, ip, beta);
     o_srcfunc_planck(ctl, los->t[ip], src);
-    for (int id = 0; id < ctl->nd; id++)
-      if (tau_seg[id] > 0) {
-        double eps = 1 - tau_seg[id] * exp(-1. * beta[id] * los->ds[ip]);
-        obs->rad[id][ir] += src[id] * eps * obs->tau[id][ir];
-        obs->tau[id][ir] *= (1 - eps);
-      }
+    const double af = los->aerofac[ip];
+    const int ia = los->aeroi[ip];
+    if (scattering > 0 && af > 0) {
+      /* the reference's neighbour index is ip+1 even at the last point
+       * (src/forwardmodel.c:323); the last point stands in for itself */
+      int ip0 = (ip > 0 ? ip - 1 : ip), ip1 = (ip + 1 < los->np ? ip + 1 : ip);
+      o_geo2cart(los->z[ip], los->lon[ip], los->lat[ip], x);
+      o_geo2cart(los->z[ip0], los->lon[ip0], los->lat[ip0], x0);
+      o_geo2cart(los->z[ip1], los->lon[ip1], los->lat[ip1], x1);
+      for (int i = 0; i < 3; i++) dx[i] = x1[i] - x0[i];
+      st = o_srcfunc_sca_1d(ctl, atm, aero, x, dx, ia, src_sca, scattering);
+      if (!st && JSC_TSUN > 0)
+        st = o_srcfunc_sca_sun(ctl, atm, aero, obs->time[ir], x, dx, ia, src_sca);
+      for (int id = 0; id < ctl->nd; id++)
+        if (tau_seg[id] > 0) {
+          double bext = (-1.) * log(tau_seg[id]) / los->ds[ip] + beta[id] + af * aero->beta_e[ia][id];
+          double eps = 1 - exp(-1 * bext * los->ds[ip]);
+          double src_all = ((bext - af * aero->beta_s[ia][id]) * src[id] +
+                            af * aero->beta_s[ia][id] * src_sca[id]) / bext;
+          obs->rad[id][ir] += obs->tau[id][ir] * eps * src_all;
+          obs->tau[id][ir] *= exp(-1. * bext * los->ds[ip]);
+        }
+    } else {
+      for (int id = 0; id < ctl->nd; id++)
+        if (tau_seg[id] > 0) {
+          double eps;
+          if (ctl->sca_n == 0 || af == 0)
+            eps = 1 - tau_seg[id] * exp(-1. * beta[id] * los->ds[ip]);
+          else if (beta_a)
+            eps = 1 - tau_seg[id] * exp(-1. * (beta[id] + af * aero->beta_a[ia][id]) * los->ds[ip]);
+          else
+            eps = 1 - tau_seg[id] * exp(-1. * (beta[id] + af * aero->beta_e[ia][id]) * los->ds[ip]);
+          obs->rad[id][ir] += src[id] * eps * obs->tau[id][ir];
+          obs->tau[id][ir] *= (1 - eps);
+        }
+    }
   }
   if (!st && los->tsurf > 0) {
     o_srcfunc_planck(ctl, los->tsurf, src);
@@ -732,29 +1100,29 @@ static int o_pencil(const ctl_t *ctl, const atm_t *atm, obs_t *obs, int ir, uint
   return st;
 }
 
-static int run_rays(const ctl_t *ctl, atm_t *atm, obs_t *obs, uint64_t *dig, int *nlos) {
+static int run_rays(const ctl_t *ctl, atm_t *atm, obs_t *obs, const aero_t *aero, uint64_t *dig,
+                    int *nlos) {
   g_err = 0;
   o_hydrostatic(ctl, atm);
   int st = load_tables(ctl);
   if (st) return st;
 #pragma omp parallel for schedule(dynamic)
   for (int ir = 0; ir < obs->nr; ir++) {
-    int s = o_pencil(ctl, atm, obs, ir, dig ? dig + (size_t)ir * ctl->nd : NULL,
-                     nlos ? &nlos[ir] : NULL);
+    int s = o_pencil(ctl, atm, obs, aero, ctl->sca_mult, ir,
+                     dig ? dig + (size_t)ir * ctl->nd : NULL, nlos ? &nlos[ir] : NULL);
     if (s) fail(s);
   }
   return g_err;
 }
 
-/* formod (src/forwardmodel.c:15-116) for the clear-air path. */
+/* formod (src/forwardmodel.c:15-116), IP=1 without field of view. */
 int oracle_formod(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
-  (void)aero;
-  if (ctl->sca_n > 0 || ctl->ip != 1 || ctl->fov[0] != '-') return JSC_ERR_UNSUPPORTED;
+  if (ctl->ip != 1 || ctl->fov[0] != '-') return JSC_ERR_UNSUPPORTED;
   int nd = ctl->nd, nr = obs->nr;
   unsigned char *mask = (unsigned char *)malloc((size_t)nd * (nr > 0 ? nr : 1));
   for (int id = 0; id < nd; id++)
     for (int ir = 0; ir < nr; ir++) mask[id * nr + ir] = !isfinite(obs->rad[id][ir]);
-  int st = run_rays(ctl, atm, obs, NULL, NULL);
+  int st = run_rays(ctl, atm, obs, aero, NULL, NULL);
   if (ctl->write_bbt)
     for (int ir = 0; ir < nr; ir++)
       for (int id = 0; id < nd; id++)
@@ -772,8 +1140,9 @@ int oracle_formod(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
  * interval indices of the four (p, T) nodes in the order (ipr,it0),
  * (ipr,it0+1), (ipr+1,it1), (ipr+1,it1+1); fold: d = d*1000003 + v.
  * The radiances are computed as by oracle_formod. */
-int oracle_diagnostics(ctl_t *ctl, atm_t *atm, obs_t *obs, int *nlos, uint64_t *digest) {
-  return run_rays(ctl, atm, obs, digest, nlos);
+int oracle_diagnostics(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, int *nlos,
+                       uint64_t *digest) {
+  return run_rays(ctl, atm, obs, aero, digest, nlos);
 }
 
 /* One ray's LOS (after hydrostatic balance of atm by the caller): fills
@@ -783,7 +1152,9 @@ int oracle_raytrace(ctl_t *ctl, atm_t *atm, obs_t *obs, int ir, double *z, doubl
                     double *lat, double *p, double *t, double *ds, double *q, double *k,
                     double *u, double *tsurf) {
   olos_t *los = los_new();
-  int st = o_raytrace(ctl, atm, obs, los, ir), n = los->np;
+  aero_t *aero = (aero_t *)calloc(1, sizeof(aero_t));
+  int st = o_raytrace(ctl, atm, obs, aero, los, ir), n = los->np;
+  free(aero);
   if (st) n = -st;
   for (int i = 0; i < los->np; i++) {
     z[i] = los->z[i];

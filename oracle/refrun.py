@@ -107,7 +107,7 @@ def _child(job):
         out["tplat"][idx] = S.arr(obs.tplat)[:n]
     out["seconds"] = time.perf_counter() - t0
     if job.get("los") and port:
-        lib.oracle_diagnostics.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT),
+        lib.oracle_diagnostics.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT),
                                            P(C.c_int), P(C.c_uint64)]
         out["digest"] = np.zeros((nr, nd), np.uint64)
         for ai, idx in groups:
@@ -118,7 +118,7 @@ def _child(job):
                              geom["time"][idx])
             nl = np.zeros(len(idx), np.int32)
             dg = np.zeros((len(idx), nd), np.uint64)
-            lib.oracle_diagnostics(C.byref(ctl), C.byref(atm), C.byref(obs),
+            lib.oracle_diagnostics(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero),
                                    nl.ctypes.data_as(P(C.c_int)),
                                    dg.ctypes.data_as(P(C.c_uint64)))
             out["nlos"][idx] = nl
@@ -155,12 +155,32 @@ def port_available():
     return os.path.exists(PORT_LIB)
 
 
-def run_port(ctl_kw, atms, ray_atm, geom, threads=None, warmup=False, los=False,
+def _aero_child(job):
+    _silence()
+    lib = C.CDLL(REF_LIB)
+    P = C.POINTER
+    lib.read_aero.argtypes = [C.c_char_p, C.c_char_p, P(S.CtlT), P(S.AeroT)]
+    lib.get_opt_prop.argtypes = [P(S.CtlT), P(S.AeroT)]
+    ctl = S.make_ctl(**job["ctl"])
+    aero = S.AeroT()
+    os.chdir(job["cwd"])
+    lib.read_aero(None, job["aerofile"].encode(), C.byref(ctl), C.byref(aero))
+    lib.get_opt_prop(C.byref(ctl), C.byref(aero))
+    return bytes(aero)
+
+
+def reference_aero(ctl_kw, aerofile, cwd, timeout=600):
+    """aero_t (as bytes) from the reference's read_aero + get_opt_prop
+    (Mie optical properties, src/scatter.c:330-508,583-639), run in cwd."""
+    return _spawn({"aero_job": True, "ctl": ctl_kw, "aerofile": aerofile, "cwd": cwd}, timeout)
+
+
+def run_port(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False, los=False,
              timeout=1800):
     """Same as run() with the C restatement (oracle/jurassic_oracle.c)
     instead of the reference build; with los=True it also returns the
     per-(ray, channel) EGA index digests."""
-    return run(ctl_kw, atms, ray_atm, geom, threads=threads, warmup=warmup,
+    return run(ctl_kw, atms, ray_atm, geom, aero=aero, threads=threads, warmup=warmup,
                los=los, lib=PORT_LIB, timeout=timeout, port=True)
 
 
@@ -178,6 +198,13 @@ def run(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False,
            "threads": threads, "warmup": warmup, "los": los, "port": port}
     if lib:
         job["lib"] = lib
+    return _spawn(job, timeout)
+
+
+def _spawn(job, timeout):
+    import pickle
+    import subprocess
+    import tempfile
     with tempfile.TemporaryDirectory() as d:
         jf, of = os.path.join(d, "job.pkl"), os.path.join(d, "out.pkl")
         with open(jf, "wb") as f:
@@ -195,8 +222,11 @@ if __name__ == "__main__":
     import pickle
     with open(sys.argv[1], "rb") as f:
         _job = pickle.load(f)
-    if _job.get("aero") is not None:
-        _job["aero"] = S.AeroT.from_buffer_copy(_job["aero"])
-    _out = _child(_job)
+    if _job.get("aero_job"):
+        _out = _aero_child(_job)
+    else:
+        if _job.get("aero") is not None:
+            _job["aero"] = S.AeroT.from_buffer_copy(_job["aero"])
+        _out = _child(_job)
     with open(sys.argv[2], "wb") as f:
         pickle.dump(_out, f)

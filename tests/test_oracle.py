@@ -120,3 +120,51 @@ def test_port_reproduces_example_los(port):
             list(u[3 * i:3 * i + 3]) + [0.0, 0.0, 0.0, ds[i]]
         rows.append(["%.2f" % 0.0] + ["%g" % v for v in vals])
     assert rows == _read_cols(os.path.join(REF_EXAMPLES, "org", "los.0"))
+
+
+def _climatology_atm(ctlname, extra, tmpdir):
+    """Example atmosphere made by the reference's climatology program
+    (built by oracle/Makefile), as the example scripts do."""
+    import subprocess
+    clim = os.path.join(REPO, "oracle", "_ref", "climatology")
+    src = os.path.join(REF_EXAMPLES, ctlname)
+    ctl = os.path.join(tmpdir, ctlname)
+    txt = open(src, "rb").read().replace(b"../clim", b"/root/reference/clim")
+    open(ctl, "wb").write(txt)
+    out = os.path.join(tmpdir, ctlname + ".atm")
+    subprocess.run([clim, ctl, "-", out] + extra, check=True, capture_output=True)
+    a = np.array(_read_cols(out), dtype=float)
+    return {"z": a[:, 1], "lon": a[:, 2], "lat": a[:, 3], "p": a[:, 4], "t": a[:, 5],
+            "q": a[:, 6:9].T, "k": a[:, 9:10].T}
+
+
+@pytest.mark.skipif(not (os.path.isdir(REF_EXAMPLES) and
+                         os.path.exists(os.path.join(REPO, "oracle", "_ref", "climatology"))),
+                    reason="reference tree or reference build not present")
+@pytest.mark.parametrize("name,ctlname,extra,obsf,aerof,kw", [
+    ("ext1", "extinction1.ctl", [], "obs.tab", "aero0.tab", dict(sca_n=1, sca_mult=0)),
+    ("aero0", "aerosol0.ctl", ["CLIMZONE", "pwin"], "obs_nadir.tab", "aero0.tab",
+     dict(sca_n=1, sca_mult=1)),
+    ("aero1", "aerosol1.ctl", [], "obs.tab", "aero1.tab", dict(sca_n=6, sca_mult=1)),
+])
+def test_port_reproduces_example_scattering(port, tmp_path, name, ctlname, extra, obsf, aerof, kw):
+    """examples/extinction1.sh, aerosol0.sh (nadir, single scattering) and
+    aerosol1.sh (limb, 6 modes in 3 layers, single scattering): the port's
+    output equals org/rad_<name>.tab.  The aero_t input comes from the
+    reference's own read_aero + get_opt_prop (Mie)."""
+    from oracle import refrun
+    atm = _climatology_atm(ctlname, extra, str(tmp_path))
+    o = np.array(_read_cols(os.path.join(REF_EXAMPLES, "org", obsf)), dtype=float)
+    geom = {"time": o[:, 0], "obsz": o[:, 1], "obslon": o[:, 2], "obslat": o[:, 3],
+            "vpz": o[:, 4], "vplon": o[:, 5], "vplat": o[:, 6]}
+    ctlkw = dict(emitters=["CO2", "H2O", "O3"], nus=[792.0],
+                 tblbase=os.path.join(REF_EXAMPLES, "tab", "boxcar"), **kw)
+    aero = refrun.reference_aero(ctlkw, aerof, REF_EXAMPLES)
+    r = refrun.run_port(ctlkw, [atm], np.zeros(len(o), int), geom, aero=aero)
+    mine = []
+    for i in range(len(o)):
+        vals = [geom["obsz"][i], geom["obslon"][i], geom["obslat"][i], geom["vpz"][i],
+                geom["vplon"][i], geom["vplat"][i], r["tpz"][i], r["tplon"][i], r["tplat"][i],
+                r["rad"][i, 0], r["tau"][i, 0]]
+        mine.append(["%.2f" % geom["time"][i]] + ["%g" % v for v in vals])
+    assert mine == _read_cols(os.path.join(REF_EXAMPLES, "org", "rad_%s.tab" % name))
