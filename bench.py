@@ -228,6 +228,7 @@ def main():
 
     batch.upload(pinned, stream=sp)
     batch.set_timing(True)
+    tuned = batch.autotune(stream=sp)   # launch-variant autotuner (untimed)
     for _ in range(args.warmup):
         batch.run(stream=sp)
     stream.synchronize()
@@ -296,7 +297,8 @@ def main():
             "config": {"workload": WORKLOAD, "rays_per_gpu": args.rays,
                        "channels": nd, "emitters": ng, "los_points": n_points,
                        "ega_evaluations": n_ega, "l2": "inputs larger than L2, no flush",
-                       "parallelism": "rays sharded per GPU, no collective"},
+                       "parallelism": "rays sharded per GPU, no collective",
+                       "ega_launch": tuned},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),

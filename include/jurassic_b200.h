@@ -280,6 +280,13 @@ int jsc_formod_batch(jsc_model *m, const ctl_t *ctl, const jsc_batch_input *in,
 void jsc_batch_set_timing(jsc_batch *b, int on);
 double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel);
 
+/* Launch autotuner: runs the batch once, then times every launch variant
+ * of the EGA/radiative-transfer kernel (threads per block x register
+ * budget) on it and keeps the fastest for later runs of this batch.
+ * jsc_batch_variant reports the choice. */
+int jsc_batch_autotune(jsc_batch *b, void *stream);
+int jsc_batch_variant(const jsc_batch *b, int *variant, int *block, int *min_blocks);
+
 /* Per-(ray, channel) checksum of every emissivity-table index the EGA
  * interpolation selected in the last run, for parity checks against the
  * reference's indices: for each LOS point and emitter with a full

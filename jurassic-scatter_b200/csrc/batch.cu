@@ -91,7 +91,7 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   b->max_atm = max_atm;
   b->max_levels = max_levels;
   b->max_rays = max_rays;
-  b->W = 4 + ctl->nw + ctl->ng;
+  b->W = JSC_REC_W(ctl->nw, ctl->ng);
   const int ng = ctl->ng > 0 ? ctl->ng : 1, nw = ctl->nw > 0 ? ctl->nw : 1;
   int st = JSC_OK;
   st = st ? st : jsc_dmalloc(&b->d_atm_off, (size_t)max_atm + 1);
@@ -116,6 +116,7 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   st = st ? st : jsc_dmalloc(&b->d_status, 1);
   st = st ? st : jsc_dmalloc(&b->d_counters, 2);
   if (!st) st = batch_alloc_los(b, max_seg > 0 ? max_seg : (int64_t)max_rays * 512);
+  b->ega_variant = -1;
   if (!st && cudaMallocHost((void **)&b->h_total, sizeof(int64_t)) != cudaSuccess) {
     jsc_set_error(JSC_ERR_NOMEM, "pinned host allocation");
     st = JSC_ERR_NOMEM;
@@ -191,6 +192,50 @@ extern "C" int jsc_batch_upload(jsc_batch *b, const jsc_batch_input *in,
   return JSC_OK;
 }
 
+// Launch variants of ega_rt_kernel: (threads per block, minimum resident
+// blocks per SM).  The second number sets the register budget, i.e. the
+// trade between occupancy and spills; jsc_batch_autotune picks one.
+struct EgaVariant { int blk, minb; };
+static const EgaVariant kEgaVariants[] = {{128, 4}, {128, 6}, {128, 8}, {256, 3}, {256, 4}};
+static const int kNumEgaVariants = 5;
+static const int kEgaDefault = 1;
+
+template <int G, bool DIG>
+static void launch_g(const EgaArgs &ea, unsigned grid_128, unsigned grid_256, int v,
+                     cudaStream_t s) {
+  switch (v) {
+    case 0: ega_rt_kernel<G, DIG, 128, 4><<<grid_128, 128, 0, s>>>(ea); break;
+    case 2: ega_rt_kernel<G, DIG, 128, 8><<<grid_128, 128, 0, s>>>(ea); break;
+    case 3: ega_rt_kernel<G, DIG, 256, 3><<<grid_256, 256, 0, s>>>(ea); break;
+    case 4: ega_rt_kernel<G, DIG, 256, 4><<<grid_256, 256, 0, s>>>(ea); break;
+    default: ega_rt_kernel<G, DIG, 128, 6><<<grid_128, 128, 0, s>>>(ea); break;
+  }
+}
+
+static int launch_ega(const EgaArgs &ea, int nr, int ndp, int ng, int variant,
+                      cudaStream_t s) {
+  const int64_t threads = (int64_t)nr * ndp;
+  const unsigned g128 = (unsigned)((threads + 127) / 128);
+  const unsigned g256 = (unsigned)((threads + 255) / 256);
+  const int v = (variant >= 0 && variant < kNumEgaVariants) ? variant : kEgaDefault;
+  const bool dig = ea.digest != nullptr;
+  if (dig) {  // index digests: diagnostics, default variant only
+    if (ng <= 2) launch_g<2, true>(ea, g128, g256, kEgaDefault, s);
+    else if (ng <= 4) launch_g<4, true>(ea, g128, g256, kEgaDefault, s);
+    else if (ng <= 8) launch_g<8, true>(ea, g128, g256, kEgaDefault, s);
+    else if (ng <= 16) launch_g<16, true>(ea, g128, g256, kEgaDefault, s);
+    else launch_g<NGMAX, true>(ea, g128, g256, kEgaDefault, s);
+  } else {
+    if (ng <= 2) launch_g<2, false>(ea, g128, g256, v, s);
+    else if (ng <= 4) launch_g<4, false>(ea, g128, g256, v, s);
+    else if (ng <= 8) launch_g<8, false>(ea, g128, g256, v, s);
+    else if (ng <= 16) launch_g<16, false>(ea, g128, g256, kEgaDefault, s);
+    else launch_g<NGMAX, false>(ea, g128, g256, kEgaDefault, s);
+  }
+  JSC_LAUNCH_CHECK();
+  return JSC_OK;
+}
+
 static void ev_record(jsc_batch *b, int k, int end, cudaStream_t s) {
   if (b->timing) cudaEventRecord(b->ev[2 * k + end], s);
   if (end) b->ran[k] = 1;
@@ -261,6 +306,17 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   ra.tsurf = b->d_tsurf;
   ra.tp = b->d_tp;
   ra.status = b->d_status;
+  ra.grid_np = 0;
+  ra.grid_p = ra.grid_t = nullptr;
+  ra.grid_nt = nullptr;
+  if (m->n_grid == 1) {
+    int gnp = 0;
+    JSC_CUDA_TRY(cudaMemcpy(&gnp, m->d_grid_np, sizeof(int), cudaMemcpyDeviceToHost));
+    ra.grid_np = gnp;
+    ra.grid_p = m->d_grid_p;
+    ra.grid_nt = m->d_grid_nt;
+    ra.grid_t = m->d_grid_t;
+  }
 
   ev_record(b, JSC_T_RAYTRACE, 0, s);
   ra.geo = b->d_geo;
@@ -290,13 +346,14 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   ea.cfg = b->cfg;
   ea.n_rays = nr;
   ea.W = b->W;
-  int gl = 1, gl_log2 = 0;
-  while (gl < m->nd && gl < 32) {
-    gl <<= 1;
-    gl_log2++;
+  ea.single_grid = m->n_grid == 1;
+  int ndp = 1;
+  if (m->nd <= 32) {
+    while (ndp < m->nd) ndp <<= 1;
+  } else {
+    ndp = (m->nd + 31) / 32 * 32;
   }
-  ea.gl_log2 = gl_log2;
-  ea.cpl = (m->nd + gl - 1) / gl;
+  ea.ndp = ndp;
   ea.nlos = b->d_nlos;
   ea.los_off = b->d_los_off;
   ea.pts = b->d_pts;
@@ -305,16 +362,9 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   ea.tau = b->d_tau;
   ea.counters = b->d_counters;
   ea.digest = b->digest ? b->d_digest : nullptr;
-  const size_t per_thread = (size_t)ea.cpl * (m->ng > 0 ? m->ng : 1) * (sizeof(double) + sizeof(int));
-  int blk = 128;
-  while (blk > 32 && per_thread * blk > 96 * 1024) blk >>= 1;
-  const size_t smem = per_thread * blk;
-  if (smem > 48 * 1024)
-    JSC_CUDA_TRY(cudaFuncSetAttribute(ega_rt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-  const int64_t threads = (int64_t)nr * gl;
-  ev_record(b, JSC_T_EGA, 0, s);
-  ega_rt_kernel<<<(unsigned)((threads + blk - 1) / blk), blk, smem, s>>>(ea);
+  b->last_ega = ea;
+  int st = launch_ega(ea, nr, ndp, m->ng, b->ega_variant, s);
+  if (st) return st;
   JSC_LAUNCH_CHECK();
   ev_record(b, JSC_T_EGA, 1, s);
   // LOS point total for the work counters.
@@ -394,6 +444,49 @@ extern "C" int jsc_batch_index_digest(jsc_batch *b, uint64_t *out) {
   JSC_CUDA_TRY(cudaMemcpy(out, b->d_digest,
                           (size_t)b->n_rays * b->cfg.nd * sizeof(uint64_t),
                           cudaMemcpyDeviceToHost));
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_autotune(jsc_batch *b, void *stream) {
+  if (!b || b->n_rays < 1) return JSC_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = jsc_batch_run(b, stream);  // LOS records and a reference timing
+  if (st) return st;
+  EgaArgs ea = b->last_ega;
+  ea.digest = nullptr;
+  cudaEvent_t e0, e1;
+  JSC_CUDA_TRY(cudaEventCreate(&e0));
+  JSC_CUDA_TRY(cudaEventCreate(&e1));
+  int best = kEgaDefault;
+  float best_ms = 1e30f;
+  for (int v = 0; v < kNumEgaVariants; v++) {
+    JSC_CUDA_TRY(cudaEventRecord(e0, s));
+    st = launch_ega(ea, b->n_rays, ea.ndp, b->m->ng, v, s);
+    if (st) break;
+    JSC_CUDA_TRY(cudaEventRecord(e1, s));
+    JSC_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (v < 8) b->ega_variant_ms[v] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  b->ega_variant = best;
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_variant(const jsc_batch *b, int *variant, int *blk, int *minb) {
+  if (!b) return JSC_ERR_ARG;
+  const int v = (b->ega_variant >= 0 && b->ega_variant < kNumEgaVariants) ? b->ega_variant
+                                                                          : kEgaDefault;
+  if (variant) *variant = v;
+  if (blk) *blk = kEgaVariants[v].blk;
+  if (minb) *minb = kEgaVariants[v].minb;
   return JSC_OK;
 }
 

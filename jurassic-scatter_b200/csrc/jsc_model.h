@@ -29,6 +29,26 @@ struct jsc_run_cfg {
   int sca_n, sca_mult, sca_ext_beta_a;
 };
 
+// LOS point record for the radiative transfer (doubles): pressure,
+// temperature, smoothed step, H2O VMR, packed (p, T) table bracket of the
+// shared grid (-1 when tables use several grids), Planck table index, the
+// window extinctions, then the column densities.
+enum { REC_P = 0, REC_T, REC_DS, REC_QH2O, REC_GRID, REC_PLK, REC_K };
+#define JSC_REC_W(nw, ng) (REC_K + (nw) + (ng))
+
+// Arguments of the EGA + radiative-transfer kernel.
+struct EgaArgs {
+  jsc_dev_model m;
+  jsc_run_cfg cfg;
+  int n_rays, W, ndp, single_grid;
+  const int *nlos;
+  const int64_t *los_off;
+  const double *pts, *tsurf;
+  double *rad, *tau;
+  unsigned long long *counters;
+  unsigned long long *digest;  // optional [n_rays][nd] EGA index checksums
+};
+
 // Kernel timers of a batch.
 enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_N };
 
@@ -65,6 +85,9 @@ struct jsc_batch {
   unsigned long long *d_digest;  // [max_rays][nd] when index digests are on
   int digest;
   int timing;
+  int ega_variant;          // launch variant of ega_rt (autotuned), -1 = default
+  EgaArgs last_ega;         // arguments of the last ega_rt launch
+  float ega_variant_ms[8];  // autotuner timings
   cudaEvent_t ev[2 * JSC_T_N];
   int ran[JSC_T_N];
 };

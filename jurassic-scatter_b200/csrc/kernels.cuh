@@ -62,6 +62,27 @@ __global__ void hydro_kernel(AtmArgs a) {
   a.zmax[i] = nan ? NAN : mx;
 }
 
+__device__ __forceinline__ double planck_temp(int i) {
+  return jsc_lin(0.0, JSC_PLANCK_TMIN, JSC_NPLANCK - 1.0, JSC_PLANCK_TMAX, (double)i);
+}
+
+// Result of locate() on the uniform Planck temperature grid: the bracket
+// from the grid spacing, corrected against the exact node values.
+__device__ __forceinline__ int planck_index(double t) {
+  if (!(t == t)) return JSC_NPLANCK - 2;
+  const double f = floor((t - JSC_PLANCK_TMIN) * 4.0);
+  int i = f < 0 ? 0 : (f > JSC_NPLANCK - 2 ? JSC_NPLANCK - 2 : (int)f);
+  while (i > 0 && planck_temp(i) > t) i--;
+  while (i < JSC_NPLANCK - 2 && planck_temp(i + 1) <= t) i++;
+  return i;
+}
+
+__device__ __forceinline__ double planck_src(const jsc_dev_model &m, int d,
+                                             int it, double t) {
+  const size_t o = (size_t)d * JSC_NPLANCK + it;
+  return m.planck_b[o] + m.planck_s[o] * (t - planck_temp(it));
+}
+
 // --------------------------------------------------------------- raytrace --
 
 struct RayArgs {
@@ -77,7 +98,23 @@ struct RayArgs {
   int W;
   double *geo, *pts, *tsurf, *tp;  // tp: [3][n_rays]
   unsigned *status;
+  // (p, T) grid shared by every table, or null when there are several
+  int grid_np;
+  const double *grid_p, *grid_t;
+  const int *grid_nt;
 };
+
+// Packed (p, T) bracket of a point on the shared grid: ipr << 10 | it0 << 5
+// | it1, plus 1 << 16 when both temperature rows have two nodes or more.
+// locate() (src/misc.c:237-265) as intpol_tbl calls it (src/forwardmodel.c:447-449).
+__device__ __forceinline__ int grid_code(int np, const double *gp, const int *gnt,
+                                         const double *gt, double p, double t) {
+  const int ipr = jsc_locate(gp, np, p);
+  const int it0 = jsc_locate(gt + ipr * TBLNTMAX, gnt[ipr], t);
+  const int it1 = jsc_locate(gt + (ipr + 1) * TBLNTMAX, gnt[ipr + 1], t);
+  const int ok = (gnt[ipr] >= 2 && gnt[ipr + 1] >= 2) ? (1 << 16) : 0;
+  return ok | (ipr << 10) | (it0 << 5) | it1;
+}
 
 struct Profile {
   const double *z, *p, *t, *q, *k;
@@ -121,15 +158,17 @@ __device__ __forceinline__ void emit_point(const RayArgs &A, const Profile &a,
   g[2] = lat;
   g[3] = raw_ds;
   double *r = A.pts + idx * A.W;
-  r[0] = p;
-  r[1] = t;
-  r[2] = ds;
-  r[3] = A.ig_h2o >= 0 ? atm_lin(a.q + (size_t)A.ig_h2o * a.stride, a, ipz, zq) : 0.0;
-  for (int w = 0; w < A.nw; w++) r[4 + w] = atm_lin(a.k + (size_t)w * a.stride, a, ipz, zq);
+  r[REC_P] = p;
+  r[REC_T] = t;
+  r[REC_DS] = ds;
+  r[REC_QH2O] = A.ig_h2o >= 0 ? atm_lin(a.q + (size_t)A.ig_h2o * a.stride, a, ipz, zq) : 0.0;
+  r[REC_GRID] = A.grid_p ? (double)grid_code(A.grid_np, A.grid_p, A.grid_nt, A.grid_t, p, t) : -1.0;
+  r[REC_PLK] = (double)planck_index(t);
+  for (int w = 0; w < A.nw; w++) r[REC_K + w] = atm_lin(a.k + (size_t)w * a.stride, a, ipz, zq);
   // Column density (src/lineofsight.c:182-185) with the final step length.
   for (int g2 = 0; g2 < A.ng; g2++) {
     double q = atm_lin(a.q + (size_t)g2 * a.stride, a, ipz, zq);
-    r[4 + A.nw + g2] = 10 * q * p / (JSC_KBOLTZ * t) * ds;
+    r[REC_K + A.nw + g2] = 10 * q * p / (JSC_KBOLTZ * t) * ds;
   }
 }
 
@@ -362,38 +401,6 @@ __global__ void scan_kernel(const int *nlos, int n, int64_t *off) {
 
 // ------------------------------------------------------------- EGA + RT --
 
-struct EgaArgs {
-  jsc_dev_model m;
-  jsc_run_cfg cfg;
-  int n_rays, W, gl_log2, cpl;
-  const int *nlos;
-  const int64_t *los_off;
-  const double *pts, *tsurf;
-  double *rad, *tau;
-  unsigned long long *counters;
-  unsigned long long *digest;  // optional [n_rays][nd] EGA index checksums
-};
-
-__device__ __forceinline__ double planck_temp(int i) {
-  return jsc_lin(0.0, JSC_PLANCK_TMIN, JSC_NPLANCK - 1.0, JSC_PLANCK_TMAX, (double)i);
-}
-
-// Result of locate() on the uniform Planck temperature grid: the bracket
-// from the grid spacing, corrected against the exact node values.
-__device__ __forceinline__ int planck_index(double t) {
-  if (!(t == t)) return JSC_NPLANCK - 2;
-  const double f = floor((t - JSC_PLANCK_TMIN) * 4.0);
-  int i = f < 0 ? 0 : (f > JSC_NPLANCK - 2 ? JSC_NPLANCK - 2 : (int)f);
-  while (i > 0 && planck_temp(i) > t) i--;
-  while (i < JSC_NPLANCK - 2 && planck_temp(i + 1) <= t) i++;
-  return i;
-}
-
-__device__ __forceinline__ double planck_src(const jsc_dev_model &m, int d,
-                                             int it, double t) {
-  const size_t o = (size_t)d * JSC_NPLANCK + it;
-  return m.planck_b[o] + m.planck_s[o] * (t - planck_temp(it));
-}
 
 // Continuum extinction of one channel at one LOS point
 // (src/forwardmodel.c:120-152 with src/continua.c:5-2049).
@@ -512,147 +519,151 @@ __device__ __forceinline__ double lin_node(float x0, float y0, float slope, doub
 
 // Emissivity of the extended path at one (p, T) node of a table
 // (intpol_tbl_u then intpol_tbl_eps, src/forwardmodel.c:460-474): invert
-// the path emissivity x1 to a column density, add the segment's column,
-// look the emissivity up again, clamp to [0, 1].  dig, when non-null,
-// folds in both interval indices.
-__device__ __forceinline__ double ega_node(const jsc_node *nodes, jsc_row rd,
-                                           double x1, double useg, int hint,
-                                           int *jout, unsigned long long *dig) {
+// the path emissivity x1 to a column density on the row, add the segment's
+// column, look the emissivity up again, clamp to [0, 1].
+//
+// Fast path: the row is strictly increasing, the interval [h, h+1] of the
+// previous point still brackets x1 and the extended column stays in the
+// same interval -- then the two nodes h, h+1 (one 32-byte sector) answer
+// both lookups.  Otherwise the exact searches above find the intervals.
+template <bool DIG>
+__device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, jsc_row rd,
+                                           double x1, double useg, int hint, int *jout,
+                                           unsigned long long *dig) {
   const int n = rd.nf & 0xffff;
   const bool strict = (rd.nf >> 16) & JSC_ROW_STRICT;
   const jsc_node *row = nodes + rd.off;
-  const int k = strict ? search_row<false>(row, n, x1, hint) : bisect_row<false>(row, n, x1);
-  const float4 rk = __ldg(reinterpret_cast<const float4 *>(row + k));
-  const double ustar = lin_node(rk.y, rk.x, rk.z, x1);
-  const double x2 = ustar + useg;
-  const int j = strict ? search_row<true>(row, n, x2, k) : bisect_row<true>(row, n, x2);
-  double e;
-  if (j == k) {
-    e = lin_node(rk.x, rk.y, rk.w, x2);
-  } else {
-    const float4 rj = __ldg(reinterpret_cast<const float4 *>(row + j));
-    e = lin_node(rj.x, rj.y, rj.w, x2);
+  const int last = n - 2;
+  int k = hint < 0 ? 0 : (hint > last ? last : hint);
+  float4 a = __ldg(reinterpret_cast<const float4 *>(row + k));
+  float4 b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
+  const float x1f = __double2float_rd(x1);
+  // bracket for x1 on eps: (e[k] <= x1 or k == 0) and (x1 < e[k+1] or k == last)
+  if (!(strict && (!(a.y > x1f) || k == 0) && (b.y > x1f || k == last) && x1 == x1)) {
+    k = strict ? search_row<false>(row, n, x1, k) : bisect_row<false>(row, n, x1);
+    a = __ldg(reinterpret_cast<const float4 *>(row + k));
+    b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
   }
-  if (dig) *dig = (*dig * 1000003ull + (unsigned long long)k) * 1000003ull + (unsigned long long)j;
+  const double x2 = lin_node(a.y, a.x, a.z, x1) + useg;
+  const float x2f = __double2float_rd(x2);
+  int j = k;
+  if (!(strict && (!(a.x > x2f) || k == 0) && (b.x > x2f || k == last) && x2 == x2)) {
+    j = strict ? search_row<true>(row, n, x2, k) : bisect_row<true>(row, n, x2);
+    if (j != k) a = __ldg(reinterpret_cast<const float4 *>(row + j));
+  }
+  if (DIG) *dig = (*dig * 1000003ull + (unsigned long long)k) * 1000003ull + (unsigned long long)j;
   *jout = j;
-  return jsc_clamp01(e);
+  return jsc_clamp01(lin_node(a.x, a.y, a.w, x2));
 }
 
-__global__ void __launch_bounds__(128) ega_rt_kernel(EgaArgs A) {
-  extern __shared__ unsigned char smem_raw[];
+// One thread per (ray, channel).  The path state of every emitter lives in
+// registers (GMAX >= ng, the emitter loop is unrolled so the lookups of
+// different emitters overlap); LOS records are read by all threads of a
+// ray (broadcast loads).
+template <int GMAX, bool DIG, int BLK, int MINB>
+__global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
   const jsc_dev_model &m = A.m;
-  const int tid = threadIdx.x, BLK = blockDim.x;
-  const int GL = 1 << A.gl_log2;
-  const int sub = tid & (GL - 1);
-  const int r = (blockIdx.x * BLK + tid) >> A.gl_log2;
-  if (r >= A.n_rays) return;
-  const int ng = m.ng, nd = m.nd, cpl = A.cpl, nslot = cpl * ng;
-  double *s_tp = reinterpret_cast<double *>(smem_raw);
-  int *s_hint = reinterpret_cast<int *>(s_tp + (size_t)nslot * BLK);
-  double rad[5], tau[5];
-  unsigned long long dig[5];
-  for (int c = 0; c < 5; c++) {
-    rad[c] = 0;
-    tau[c] = 1;
-    dig[c] = 0;
-  }
-  for (int s = 0; s < nslot; s++) {
-    s_tp[s * BLK + tid] = 1;
-    s_hint[s * BLK + tid] = 0;
-  }
-  const int np = A.nlos[r];
-  const double *rec0 = A.pts + (size_t)A.los_off[r] * A.W;
-  unsigned long long n_ega = 0;
+  const int nd = m.nd, ng = m.ng;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = tid / A.ndp;
+  const int d = tid - r * A.ndp;
+  if (r >= A.n_rays || d >= nd) return;
 
-  for (int ip = 0; ip < np; ip++) {
-    const double *rec = rec0 + (size_t)ip * A.W;
-    const double P = rec[0], T = rec[1], DS = rec[2], QH = rec[3];
-    const double *kw = rec + 4;
-    const double *u = rec + 4 + m.nw;
-    const int itp = planck_index(T);
-    int memo_g = -1, ipr = 0, it0 = 0, it1 = 0;
-    bool ntok = false;
-    for (int c = 0; c < cpl; c++) {
-      const int d = sub + c * GL;
-      if (d >= nd) break;
-      double tau_gas = 1;
-      for (int g = 0; g < ng; g++) {
-        const int slot = (c * ng + g) * BLK + tid;
-        const int ti = d * ng + g;
-        double tp = s_tp[slot];
-        double eps;
-        const int gid = m.tab_grid[ti];
-        if (gid < 0) {
-          eps = 0;
-        } else if (tp < 1e-9) {
-          eps = 1;
-        } else {
-          const double *gp = m.grid_p + (size_t)gid * TBLNPMAX;
-          const int *gnt = m.grid_nt + (size_t)gid * TBLNPMAX;
-          const double *gt = m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX;
-          if (gid != memo_g) {
-            memo_g = gid;
-            ipr = jsc_locate(gp, m.grid_np[gid], P);
-            it0 = jsc_locate(gt + ipr * TBLNTMAX, gnt[ipr], T);
-            it1 = jsc_locate(gt + (ipr + 1) * TBLNTMAX, gnt[ipr + 1], T);
-            ntok = gnt[ipr] >= 2 && gnt[ipr + 1] >= 2;
-          }
-          eps = 0;
-          if (ntok) {
-            const jsc_row *rw = m.rows + (size_t)ti * (TBLNPMAX * TBLNTMAX);
-            const jsc_row r00 = rw[ipr * TBLNTMAX + it0];
-            const jsc_row r01 = rw[ipr * TBLNTMAX + it0 + 1];
-            const jsc_row r10 = rw[(ipr + 1) * TBLNTMAX + it1];
-            const jsc_row r11 = rw[(ipr + 1) * TBLNTMAX + it1 + 1];
-            if ((r00.nf & 0xffff) >= 2 && (r01.nf & 0xffff) >= 2 &&
-                (r10.nf & 0xffff) >= 2 && (r11.nf & 0xffff) >= 2) {
-              const double x1 = 1 - tp, useg = u[g];
-              const int hint = s_hint[slot];
-              int j00, jx;
-              unsigned long long *dg = A.digest ? &dig[c] : nullptr;
-              if (dg) *dg = *dg * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
-              const double e00 = ega_node(m.nodes, r00, x1, useg, hint, &j00, dg);
-              const double e01 = ega_node(m.nodes, r01, x1, useg, hint, &jx, dg);
-              const double e10 = ega_node(m.nodes, r10, x1, useg, hint, &jx, dg);
-              const double e11 = ega_node(m.nodes, r11, x1, useg, hint, &jx, dg);
-              s_hint[slot] = j00;
-              double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
-                                              gt[ipr * TBLNTMAX + it0 + 1], e01, T));
-              double eb = jsc_clamp01(jsc_lin(gt[(ipr + 1) * TBLNTMAX + it1], e10,
-                                              gt[(ipr + 1) * TBLNTMAX + it1 + 1], e11, T));
-              ea = jsc_clamp01(jsc_lin(gp[ipr], ea, gp[ipr + 1], eb, P));
-              eps = 1 - (1 - ea) / tp;
-              n_ega++;
-            }
+  // per-channel constants
+  const int w = m.window[d];
+  const bool has_w = w < m.nw;
+  const jsc_ctm_coef cc = m.ctm[d];
+  const double nu = m.nu[d];
+  const double *__restrict__ pb = m.planck_b + (size_t)d * JSC_NPLANCK;
+  const double *__restrict__ ps = m.planck_s + (size_t)d * JSC_NPLANCK;
+  const jsc_row *__restrict__ rows_d = m.rows + (size_t)d * ng * (TBLNPMAX * TBLNTMAX);
+  unsigned okmask = 0;
+  for (int g = 0; g < ng && g < GMAX; g++)
+    if (m.tab_grid[d * ng + g] >= 0) okmask |= 1u << g;
+
+  double tp[GMAX];
+  int hint[GMAX];
+#pragma unroll
+  for (int g = 0; g < GMAX; g++) {
+    tp[g] = 1;
+    hint[g] = 0;
+  }
+  double rad = 0, tau = 1;
+  unsigned long long dig = 0;
+  unsigned n_ega = 0;
+  const int np = A.nlos[r];
+  const double *__restrict__ rec = A.pts + (size_t)A.los_off[r] * A.W;
+
+  for (int ip = 0; ip < np; ip++, rec += A.W) {
+    const double P = rec[REC_P], T = rec[REC_T], DS = rec[REC_DS];
+    const int itp = (int)rec[REC_PLK];
+    int code = (int)rec[REC_GRID];
+    double tau_gas = 1;
+#pragma unroll
+    for (int g = 0; g < GMAX; g++) {
+      if (g >= ng) break;
+      double eps = 0;
+      const double tpg = tp[g];
+      if (!((okmask >> g) & 1u)) {
+        eps = 0;
+      } else if (tpg < 1e-9) {
+        eps = 1;
+      } else {
+        const int gid = A.single_grid ? 0 : m.tab_grid[d * ng + g];
+        if (!A.single_grid)
+          code = grid_code(m.grid_np[gid], m.grid_p + (size_t)gid * TBLNPMAX,
+                           m.grid_nt + (size_t)gid * TBLNPMAX,
+                           m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX, P, T);
+        if (code & (1 << 16)) {
+          const int ipr = (code >> 10) & 63, it0 = (code >> 5) & 31, it1 = code & 31;
+          const jsc_row *rw = rows_d + (size_t)g * (TBLNPMAX * TBLNTMAX);
+          const jsc_row r00 = rw[ipr * TBLNTMAX + it0];
+          const jsc_row r01 = rw[ipr * TBLNTMAX + it0 + 1];
+          const jsc_row r10 = rw[(ipr + 1) * TBLNTMAX + it1];
+          const jsc_row r11 = rw[(ipr + 1) * TBLNTMAX + it1 + 1];
+          if ((r00.nf & 0xffff) >= 2 && (r01.nf & 0xffff) >= 2 &&
+              (r10.nf & 0xffff) >= 2 && (r11.nf & 0xffff) >= 2) {
+            const double x1 = 1 - tpg, useg = rec[REC_K + m.nw + g];
+            if (DIG) dig = dig * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
+            int j00, jx;
+            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, hint[g], &j00, &dig);
+            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, hint[g], &jx, &dig);
+            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, hint[g], &jx, &dig);
+            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, hint[g], &jx, &dig);
+            hint[g] = j00;
+            const double *gp = m.grid_p + (size_t)gid * TBLNPMAX;
+            const double *gt = m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX;
+            double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
+                                            gt[ipr * TBLNTMAX + it0 + 1], e01, T));
+            const double eb = jsc_clamp01(jsc_lin(gt[(ipr + 1) * TBLNTMAX + it1], e10,
+                                                  gt[(ipr + 1) * TBLNTMAX + it1 + 1], e11, T));
+            ea = jsc_clamp01(jsc_lin(gp[ipr], ea, gp[ipr + 1], eb, P));
+            eps = 1 - (1 - ea) / tpg;
+            n_ega++;
           }
         }
-        s_tp[slot] = tp * (1 - eps);
-        tau_gas *= (1 - eps);
       }
-      const jsc_ctm_coef cc = m.ctm[d];
-      const int w = m.window[d];
-      const double beta = continua(m, A.cfg, cc, m.nu[d], w < m.nw ? kw[w] : 0.0,
-                                   P, T, DS, QH, u);
-      const double src = planck_src(m, d, itp, T);
-      if (tau_gas > 0) {
-        const double eps = 1 - tau_gas * exp(-1. * beta * DS);
-        rad[c] += src * eps * tau[c];
-        tau[c] *= (1 - eps);
-      }
+      tp[g] = tpg * (1 - eps);
+      tau_gas *= (1 - eps);
+    }
+    const double beta = continua(m, A.cfg, cc, nu, has_w ? rec[REC_K + w] : 0.0, P, T, DS,
+                                 rec[REC_QH2O], rec + REC_K + m.nw);
+    const double src = pb[itp] + ps[itp] * (T - planck_temp(itp));
+    if (tau_gas > 0) {
+      const double eps = 1 - tau_gas * exp(-1. * beta * DS);
+      rad += src * eps * tau;
+      tau *= (1 - eps);
     }
   }
   const double ts = A.tsurf[r];
-  const int its = planck_index(ts);
-  for (int c = 0; c < cpl; c++) {
-    const int d = sub + c * GL;
-    if (d >= nd) break;
-    if (ts > 0) rad[c] += planck_src(m, d, its, ts) * tau[c];
-    A.rad[(size_t)r * nd + d] = rad[c];
-    A.tau[(size_t)r * nd + d] = tau[c];
-    if (A.digest) A.digest[(size_t)r * nd + d] = dig[c];
+  if (ts > 0) {
+    const int its = planck_index(ts);
+    rad += (pb[its] + ps[its] * (ts - planck_temp(its))) * tau;
   }
-  // Work counter: one atomic per warp.
+  A.rad[(size_t)r * nd + d] = rad;
+  A.tau[(size_t)r * nd + d] = tau;
+  if (DIG) A.digest[(size_t)r * nd + d] = dig;
   const unsigned mask = __activemask();
-  const unsigned tot = __reduce_add_sync(mask, (unsigned)n_ega);
-  if ((tid & 31) == __ffs(mask) - 1) atomicAdd(&A.counters[1], (unsigned long long)tot);
+  const unsigned tot = __reduce_add_sync(mask, n_ega);
+  if ((threadIdx.x & 31) == __ffs(mask) - 1) atomicAdd(&A.counters[1], (unsigned long long)tot);
 }

@@ -137,6 +137,17 @@ class Batch:
                 "jsc_batch_index_digest")
         return out
 
+    def autotune(self, stream=None):
+        """Pick the fastest EGA kernel launch variant on this batch."""
+        L.check(L.load().jsc_batch_autotune(self.h, stream), "jsc_batch_autotune")
+        return self.variant()
+
+    def variant(self):
+        v, b, mb = C.c_int(), C.c_int(), C.c_int()
+        L.check(L.load().jsc_batch_variant(self.h, C.byref(v), C.byref(b), C.byref(mb)),
+                "jsc_batch_variant")
+        return {"variant": v.value, "block": b.value, "min_blocks": mb.value}
+
     def set_timing(self, on=True):
         L.load().jsc_batch_set_timing(self.h, 1 if on else 0)
 
