@@ -286,6 +286,11 @@ double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel);
  * jsc_batch_variant reports the choice. */
 int jsc_batch_autotune(jsc_batch *b, void *stream);
 int jsc_batch_variant(const jsc_batch *b, int *variant, int *block, int *min_blocks);
+double jsc_batch_variant_ms(const jsc_batch *b, int variant);
+
+/* Aerosol/cloud layers and optical properties for runs with ctl->sca_n > 0
+ * (the aero_t that read_aero + get_opt_prop fill, src/scatter.c:330,583). */
+int jsc_batch_set_aero(jsc_batch *b, const aero_t *aero);
 
 /* Per-(ray, channel) checksum of every emissivity-table index the EGA
  * interpolation selected in the last run, for parity checks against the

@@ -47,6 +47,13 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   cudaFree(b->d_status);
   cudaFree(b->d_counters);
   cudaFree(b->d_digest);
+  cudaFree(b->d_aero);
+  cudaFree(b->d_beta);
+  cudaFree(b->d_phase);
+  cudaFree(b->d_nlos_b);
+  cudaFree(b->d_los_off_b);
+  cudaFree(b->d_geo_b);
+  cudaFree(b->d_pts_b);
   if (b->h_total) cudaFreeHost(b->h_total);
   for (int i = 0; i < 2 * JSC_T_N; i++)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
@@ -88,6 +95,7 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   c.sca_n = ctl->sca_n;
   c.sca_mult = ctl->sca_mult;
   c.sca_ext_beta_a = strcmp(ctl->sca_ext, "beta_a") == 0;
+  c.transs = ctl->transs;
   b->max_atm = max_atm;
   b->max_levels = max_levels;
   b->max_rays = max_rays;
@@ -117,6 +125,7 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   st = st ? st : jsc_dmalloc(&b->d_counters, 2);
   if (!st) st = batch_alloc_los(b, max_seg > 0 ? max_seg : (int64_t)max_rays * 512);
   b->ega_variant = -1;
+  for (int v = 0; v < 8; v++) b->ega_variant_ms[v] = -1;
   if (!st && cudaMallocHost((void **)&b->h_total, sizeof(int64_t)) != cudaSuccess) {
     jsc_set_error(JSC_ERR_NOMEM, "pinned host allocation");
     st = JSC_ERR_NOMEM;
@@ -128,6 +137,115 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
     return st;
   }
   *out = b;
+  return JSC_OK;
+}
+
+static int cmp_desc(const void *a, const void *b) {
+  const double x = *(const double *)a, y = *(const double *)b;
+  return (x < y) - (x > y);
+}
+
+extern "C" int jsc_batch_set_aero(jsc_batch *b, const aero_t *aero) {
+  if (!b || !aero || aero->nl < 0 || aero->nl > NLMAX) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_set_aero: invalid aerosol layers");
+    return JSC_ERR_ARG;
+  }
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  const int nl = aero->nl, nd = b->cfg.nd;
+  // Layer edges +-5 m and transition sampling altitudes, top down
+  // (src/lineofsight.c:210-244).
+  const double eps = 0.005;
+  double *alti = (double *)malloc(sizeof(double) * (4 * NLMAX + 2 * 4096));
+  int jl = 0;
+  if (!alti) return JSC_ERR_NOMEM;
+  for (int il = 0; il < nl; il++) {
+    alti[jl] = aero->top[il] + eps;
+    alti[jl + 1] = aero->top[il] - eps;
+    alti[jl + 2] = aero->bottom[il] + eps;
+    alti[jl + 3] = aero->bottom[il] - eps;
+    jl += 4;
+    if (aero->trans[il] > b->cfg.transs) {
+      const double tt = aero->trans[il] / b->cfg.transs;
+      alti[jl] = aero->top[il] + aero->trans[il] + eps;
+      alti[jl + 1] = aero->top[il] + aero->trans[il] - eps;
+      alti[jl + 2] = aero->bottom[il] - aero->trans[il] + eps;
+      alti[jl + 3] = aero->bottom[il] - aero->trans[il] - eps;
+      jl += 4;
+      for (int it = 1; it < (int)tt; it++) {
+        if (jl + 2 > 4 * NLMAX + 2 * 4096) {
+          free(alti);
+          jsc_set_error(JSC_ERR_ARG, "too many transition-layer samples");
+          return JSC_ERR_ARG;
+        }
+        alti[jl++] = aero->top[il] + aero->trans[il] - eps - it * b->cfg.transs;
+        alti[jl++] = aero->bottom[il] - aero->trans[il] + eps + it * b->cfg.transs;
+      }
+    }
+  }
+  qsort(alti, (size_t)jl, sizeof(double), cmp_desc);
+  double amax = jl ? alti[0] : 0, amin = jl ? alti[0] : 0;
+  for (int i = 0; i < jl; i++) {
+    if (alti[i] > amax) amax = alti[i];
+    if (alti[i] < amin) amin = alti[i];
+  }
+  const size_t nh = 3 * NLMAX + (size_t)jl;
+  double *h = (double *)calloc(nh > 0 ? nh : 1, sizeof(double));
+  double *beta = (double *)calloc((size_t)3 * (nl > 0 ? nl : 1) * nd, sizeof(double));
+  double *phase = (double *)calloc((size_t)(nl > 0 ? nl : 1) * nd * NTHETA, sizeof(double));
+  if (!h || !beta || !phase) {
+    free(alti); free(h); free(beta); free(phase);
+    return JSC_ERR_NOMEM;
+  }
+  for (int il = 0; il < nl; il++) {
+    h[il] = aero->top[il];
+    h[NLMAX + il] = aero->bottom[il];
+    h[2 * NLMAX + il] = aero->trans[il];
+    for (int id = 0; id < nd; id++) {
+      beta[(size_t)il * nd + id] = aero->beta_e[il][id];
+      beta[(size_t)(nl + il) * nd + id] = aero->beta_s[il][id];
+      beta[(size_t)(2 * nl + il) * nd + id] = aero->beta_a[il][id];
+      for (int ia = 0; ia < NTHETA; ia++)
+        phase[((size_t)il * nd + id) * NTHETA + ia] = aero->p[il][id][ia];
+    }
+  }
+  memcpy(h + 3 * NLMAX, alti, sizeof(double) * (size_t)jl);
+  cudaFree(b->d_aero);
+  cudaFree(b->d_beta);
+  cudaFree(b->d_phase);
+  b->d_aero = nullptr;
+  b->d_beta = b->d_phase = nullptr;
+  int st = jsc_dmalloc(&b->d_aero, nh);
+  if (!st) st = jsc_dmalloc(&b->d_beta, (size_t)3 * (nl > 0 ? nl : 1) * nd);
+  if (!st) st = jsc_dmalloc(&b->d_phase, (size_t)(nl > 0 ? nl : 1) * nd * NTHETA);
+  if (!st && cudaMemcpy(b->d_aero, h, nh * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) st = JSC_ERR_CUDA;
+  if (!st && cudaMemcpy(b->d_beta, beta, (size_t)3 * (nl > 0 ? nl : 1) * nd * sizeof(double),
+                        cudaMemcpyHostToDevice) != cudaSuccess) st = JSC_ERR_CUDA;
+  if (!st && cudaMemcpy(b->d_phase, phase, (size_t)(nl > 0 ? nl : 1) * nd * NTHETA * sizeof(double),
+                        cudaMemcpyHostToDevice) != cudaSuccess) st = JSC_ERR_CUDA;
+  free(alti); free(h); free(beta); free(phase);
+  if (st) {
+    jsc_set_error(st, "jsc_batch_set_aero: device upload failed");
+    return st;
+  }
+  b->aero_nl = nl;
+  b->n_alti = jl;
+  b->altimax = amax;
+  b->altimin = amin;
+  if (!b->d_nlos_b) {
+    if ((st = jsc_dmalloc(&b->d_nlos_b, (size_t)b->max_rays))) return st;
+    if ((st = jsc_dmalloc(&b->d_los_off_b, (size_t)b->max_rays + 1))) return st;
+  }
+  return JSC_OK;
+}
+
+static int batch_alloc_los_b(jsc_batch *b, int64_t max_seg) {
+  cudaFree(b->d_geo_b);
+  cudaFree(b->d_pts_b);
+  b->d_geo_b = b->d_pts_b = nullptr;
+  int st;
+  if ((st = jsc_dmalloc(&b->d_geo_b, (size_t)max_seg * 4))) return st;
+  if ((st = jsc_dmalloc(&b->d_pts_b, (size_t)max_seg * b->W))) return st;
+  b->max_seg_b = max_seg;
   return JSC_OK;
 }
 
@@ -247,6 +365,7 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   const jsc_model *m = b->m;
   const int nr = b->n_rays;
   JSC_CUDA_TRY(cudaSetDevice(m->device));
+  (void)cudaGetLastError();  // launch checks below report this run's errors only
   for (int k = 0; k < JSC_T_N; k++) b->ran[k] = 0;
   JSC_CUDA_TRY(cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s));
   JSC_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(unsigned long long), s));
@@ -318,27 +437,99 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
     ra.grid_t = m->d_grid_t;
   }
 
+  const bool refine = b->cfg.sca_n > 0;
+  if (refine && !b->d_aero) {
+    jsc_set_error(JSC_ERR_ARG, "SCA_N > 0 needs jsc_batch_set_aero before jsc_batch_run");
+    return JSC_ERR_ARG;
+  }
+  ra.raw_q = refine;
+  ra.nlos = refine ? b->d_nlos_b : b->d_nlos;
+  ra.los_off = refine ? b->d_los_off_b : b->d_los_off;
   ev_record(b, JSC_T_RAYTRACE, 0, s);
-  ra.geo = b->d_geo;
-  ra.pts = b->d_pts;
-  ra.max_seg = b->max_seg;
   raytrace_kernel<false><<<(nr + 127) / 128, 128, 0, s>>>(ra);
   JSC_LAUNCH_CHECK();
-  scan_kernel<<<1, 1024, 0, s>>>(b->d_nlos, nr, b->d_los_off);
+  scan_kernel<<<1, 1024, 0, s>>>(ra.nlos, nr, (int64_t *)ra.los_off);
   JSC_LAUNCH_CHECK();
   // The LOS buffer is sized from the counting pass (one small copy).
-  JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, b->d_los_off + nr, sizeof(int64_t),
+  JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, ra.los_off + nr, sizeof(int64_t),
                                cudaMemcpyDeviceToHost, s));
   JSC_CUDA_TRY(cudaStreamSynchronize(s));
-  if (*b->h_total > b->max_seg) {
-    int st = batch_alloc_los(b, *b->h_total + *b->h_total / 4 + 1024);
-    if (st) return st;
+  if (refine) {
+    if (*b->h_total > b->max_seg_b) {
+      int st = batch_alloc_los_b(b, *b->h_total + *b->h_total / 4 + 1024);
+      if (st) return st;
+    }
+    ra.geo = b->d_geo_b;
+    ra.pts = b->d_pts_b;
+    ra.max_seg = b->max_seg_b;
+  } else {
+    if (*b->h_total > b->max_seg) {
+      int st = batch_alloc_los(b, *b->h_total + *b->h_total / 4 + 1024);
+      if (st) return st;
+    }
+    ra.geo = b->d_geo;
+    ra.pts = b->d_pts;
+    ra.max_seg = b->max_seg;
   }
-  ra.geo = b->d_geo;
-  ra.pts = b->d_pts;
-  ra.max_seg = b->max_seg;
   raytrace_kernel<true><<<(nr + 127) / 128, 128, 0, s>>>(ra);
   JSC_LAUNCH_CHECK();
+  if (refine) {
+    // Layer-edge points, chord steps and aerosol factors
+    // (add_aerosol_layers, src/lineofsight.c:193-372).
+    RefineArgs fa;
+    fa.n_rays = nr;
+    fa.ng = b->cfg.ng;
+    fa.nw = b->cfg.nw;
+    fa.W = b->W;
+    fa.n_levels = b->n_levels;
+    fa.ig_h2o = m->dv.ig_h2o;
+    fa.ray_atm = b->d_ray_atm;
+    fa.atm_off = b->d_atm_off;
+    fa.z = b->d_z;
+    fa.p = b->d_p;
+    fa.t = b->d_t;
+    fa.q = b->d_q;
+    fa.k = b->d_k;
+    fa.nlos_b = b->d_nlos_b;
+    fa.off_b = b->d_los_off_b;
+    fa.geo_b = b->d_geo_b;
+    fa.pts_b = b->d_pts_b;
+    fa.nlos = b->d_nlos;
+    fa.off = b->d_los_off;
+    fa.nl = b->aero_nl;
+    fa.n_alti = b->n_alti;
+    fa.altimax = b->altimax;
+    fa.altimin = b->altimin;
+    fa.transs = b->cfg.transs;
+    fa.top = b->d_aero;
+    fa.bottom = b->d_aero + NLMAX;
+    fa.trans = b->d_aero + 2 * NLMAX;
+    fa.alti = b->d_aero + 3 * NLMAX;
+    fa.grid_np = ra.grid_np;
+    fa.grid_p = ra.grid_p;
+    fa.grid_t = ra.grid_t;
+    fa.grid_nt = ra.grid_nt;
+    fa.status = b->d_status;
+    fa.geo = b->d_geo;
+    fa.pts = b->d_pts;
+    fa.max_seg = b->max_seg;
+    refine_kernel<false><<<(nr + 127) / 128, 128, 0, s>>>(fa);
+    JSC_LAUNCH_CHECK();
+    scan_kernel<<<1, 1024, 0, s>>>(b->d_nlos, nr, b->d_los_off);
+    JSC_LAUNCH_CHECK();
+    JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, b->d_los_off + nr, sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, s));
+    JSC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (*b->h_total > b->max_seg) {
+      int st = batch_alloc_los(b, *b->h_total + *b->h_total / 4 + 1024);
+      if (st) return st;
+    }
+    fa.geo = b->d_geo;
+    fa.pts = b->d_pts;
+    fa.max_seg = b->max_seg;
+    refine_kernel<true><<<(nr + 127) / 128, 128, 0, s>>>(fa);
+    JSC_LAUNCH_CHECK();
+  }
   ev_record(b, JSC_T_RAYTRACE, 1, s);
 
   EgaArgs ea;
@@ -362,6 +553,8 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   ea.tau = b->d_tau;
   ea.counters = b->d_counters;
   ea.digest = b->digest ? b->d_digest : nullptr;
+  ea.beta = b->d_beta;
+  ea.aero_nl = b->aero_nl;
   b->last_ega = ea;
   int st = launch_ega(ea, nr, ndp, m->ng, b->ega_variant, s);
   if (st) return st;
@@ -450,25 +643,32 @@ extern "C" int jsc_batch_index_digest(jsc_batch *b, uint64_t *out) {
 extern "C" int jsc_batch_autotune(jsc_batch *b, void *stream) {
   if (!b || b->n_rays < 1) return JSC_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  int st = jsc_batch_run(b, stream);  // LOS records and a reference timing
+  int st = jsc_batch_run(b, stream);  // LOS records for the timing runs
   if (st) return st;
   EgaArgs ea = b->last_ega;
   ea.digest = nullptr;
-  cudaEvent_t e0, e1;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
   JSC_CUDA_TRY(cudaEventCreate(&e0));
-  JSC_CUDA_TRY(cudaEventCreate(&e1));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    jsc_set_error(JSC_ERR_CUDA, "autotune: cudaEventCreate failed");
+    return JSC_ERR_CUDA;
+  }
   int best = kEgaDefault;
   float best_ms = 1e30f;
-  for (int v = 0; v < kNumEgaVariants; v++) {
-    JSC_CUDA_TRY(cudaEventRecord(e0, s));
-    st = launch_ega(ea, b->n_rays, ea.ndp, b->m->ng, v, s);
-    if (st) break;
-    JSC_CUDA_TRY(cudaEventRecord(e1, s));
-    JSC_CUDA_TRY(cudaEventSynchronize(e1));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (v < 8) b->ega_variant_ms[v] = ms;
-    if (ms < best_ms) {
+  for (int v = 0; v < kNumEgaVariants && !st; v++) {
+    cudaError_t e = cudaEventRecord(e0, s);
+    if (e == cudaSuccess) st = launch_ega(ea, b->n_rays, ea.ndp, b->m->ng, v, s);
+    if (!st && e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (!st && e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = -1;
+    if (!st && e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (!st && e != cudaSuccess) {
+      jsc_set_error(JSC_ERR_CUDA, "autotune variant %d: %s", v, cudaGetErrorString(e));
+      st = JSC_ERR_CUDA;
+    }
+    b->ega_variant_ms[v] = ms;
+    if (!st && ms < best_ms) {
       best_ms = ms;
       best = v;
     }
@@ -478,6 +678,11 @@ extern "C" int jsc_batch_autotune(jsc_batch *b, void *stream) {
   if (st) return st;
   b->ega_variant = best;
   return JSC_OK;
+}
+
+extern "C" double jsc_batch_variant_ms(const jsc_batch *b, int variant) {
+  if (!b || variant < 0 || variant >= kNumEgaVariants) return -1;
+  return b->ega_variant_ms[variant];
 }
 
 extern "C" int jsc_batch_variant(const jsc_batch *b, int *variant, int *blk, int *minb) {

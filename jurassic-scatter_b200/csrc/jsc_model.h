@@ -23,6 +23,7 @@ struct jsc_model {
 // Forward-model switches copied from ctl_t when a batch is created.
 struct jsc_run_cfg {
   int ng, nd, nw;
+  double transs;
   int ctm_co2, ctm_h2o, ctm_n2, ctm_o2;
   int refrac;
   double rayds, raydz, hydz;
@@ -30,10 +31,12 @@ struct jsc_run_cfg {
 };
 
 // LOS point record for the radiative transfer (doubles): pressure,
-// temperature, smoothed step, H2O VMR, packed (p, T) table bracket of the
-// shared grid (-1 when tables use several grids), Planck table index, the
-// window extinctions, then the column densities.
-enum { REC_P = 0, REC_T, REC_DS, REC_QH2O, REC_GRID, REC_PLK, REC_K };
+// temperature, step length, H2O VMR, packed (p, T) table bracket of the
+// shared grid (-1 when tables use several grids), Planck table index,
+// aerosol/cloud scaling factor and layer index (0 and -999 in clear air),
+// the window extinctions, then the column densities (volume mixing ratios
+// in the raw records the aerosol refinement reads).
+enum { REC_P = 0, REC_T, REC_DS, REC_QH2O, REC_GRID, REC_PLK, REC_AF, REC_AI, REC_K };
 #define JSC_REC_W(nw, ng) (REC_K + (nw) + (ng))
 
 // Arguments of the EGA + radiative-transfer kernel.
@@ -47,6 +50,8 @@ struct EgaArgs {
   double *rad, *tau;
   unsigned long long *counters;
   unsigned long long *digest;  // optional [n_rays][nd] EGA index checksums
+  const double *beta;          // aerosol beta_e/beta_s/beta_a [3][nl][nd]
+  int aero_nl;
 };
 
 // Kernel timers of a batch.
@@ -67,6 +72,18 @@ struct jsc_batch {
   double *d_zmin, *d_zmax;  // per profile
   int *d_ray_atm;
   double *d_ray;            // [9][max_rays]: time obsz obslon obslat vpz vplon vplat + 2 spare
+
+  // Aerosol/cloud layers (sca_n > 0): layer geometry, optics [nl][nd],
+  // phase functions [nl][nd][NTHETA], edge altitudes of the refinement.
+  int aero_nl, n_alti;
+  double altimax, altimin;
+  double *d_aero;           // top[NLMAX] bottom[NLMAX] trans[NLMAX] alti[...]
+  double *d_beta;           // beta_e, beta_s, beta_a: [3][nl][nd]
+  double *d_phase;          // [nl][nd][NTHETA]
+  int *d_nlos_b;            // LOS points before the refinement
+  int64_t *d_los_off_b;
+  double *d_geo_b, *d_pts_b;
+  int64_t max_seg_b;
 
   // Line of sight.
   int *d_nlos;

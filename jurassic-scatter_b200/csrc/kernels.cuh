@@ -102,6 +102,7 @@ struct RayArgs {
   int grid_np;
   const double *grid_p, *grid_t;
   const int *grid_nt;
+  int raw_q;  // store volume mixing ratios instead of column densities
 };
 
 // Packed (p, T) bracket of a point on the shared grid: ipr << 10 | it0 << 5
@@ -164,11 +165,13 @@ __device__ __forceinline__ void emit_point(const RayArgs &A, const Profile &a,
   r[REC_QH2O] = A.ig_h2o >= 0 ? atm_lin(a.q + (size_t)A.ig_h2o * a.stride, a, ipz, zq) : 0.0;
   r[REC_GRID] = A.grid_p ? (double)grid_code(A.grid_np, A.grid_p, A.grid_nt, A.grid_t, p, t) : -1.0;
   r[REC_PLK] = (double)planck_index(t);
+  r[REC_AF] = 0.0;
+  r[REC_AI] = -999.0;
   for (int w = 0; w < A.nw; w++) r[REC_K + w] = atm_lin(a.k + (size_t)w * a.stride, a, ipz, zq);
   // Column density (src/lineofsight.c:182-185) with the final step length.
   for (int g2 = 0; g2 < A.ng; g2++) {
     double q = atm_lin(a.q + (size_t)g2 * a.stride, a, ipz, zq);
-    r[REC_K + A.nw + g2] = 10 * q * p / (JSC_KBOLTZ * t) * ds;
+    r[REC_K + A.nw + g2] = A.raw_q ? q : 10 * q * p / (JSC_KBOLTZ * t) * ds;
   }
 }
 
@@ -373,6 +376,183 @@ __global__ void __launch_bounds__(128) raytrace_kernel(RayArgs A) {
   const int np = trace_ray<STORE>(A, r);
   if (!STORE) A.nlos[r] = np;
   else if (np != A.nlos[r]) atomicOr(A.status, JSC_DEV_ERR_NLOS);
+}
+
+// ------------------------------------------------------ aerosol layers --
+
+struct RefineArgs {
+  int n_rays, ng, nw, W, n_levels, ig_h2o;
+  const int *ray_atm, *atm_off;
+  const double *z, *p, *t, *q, *k;       // atmospheric profiles
+  const int *nlos_b;                     // ray-traced LOS (raw records)
+  const int64_t *off_b;
+  const double *geo_b, *pts_b;
+  int *nlos;                             // refined LOS
+  const int64_t *off;
+  double *geo, *pts;
+  int64_t max_seg;
+  int nl, n_alti;
+  double altimax, altimin, transs;
+  const double *top, *bottom, *trans, *alti;
+  int grid_np;
+  const double *grid_p, *grid_t;
+  const int *grid_nt;
+  unsigned *status;
+};
+
+// Point where the segment between raw points ip-1 and ip crosses znew, with
+// the atmospheric state there (intersection_point, src/lineofsight.c:385-407).
+__device__ __forceinline__ void refine_cross(const RefineArgs &A, const Profile &a,
+                                             const double *gb, int ip, double znew,
+                                             double *go, double *po) {
+  double x1[3], x2[3], zz, lon, lat, p, t;
+  const double *g0 = gb + (size_t)(ip - 1) * 4, *g1 = gb + (size_t)ip * 4;
+  const double frac = (g0[0] - znew) / (g0[0] - g1[0]);
+  jsc_geo2cart(g0[0], g0[1], g0[2], x1);
+  jsc_geo2cart(g1[0], g1[1], g1[2], x2);
+  for (int i = 0; i < 3; i++) x2[i] = x1[i] + frac * (x2[i] - x1[i]);
+  jsc_cart2geo(x2, &zz, &lon, &lat);
+  const int ipz = atm_full(a, zz, &p, &t);
+  go[0] = zz;
+  go[1] = lon;
+  go[2] = lat;
+  po[REC_P] = p;
+  po[REC_T] = t;
+  po[REC_QH2O] = A.ig_h2o >= 0 ? atm_lin(a.q + (size_t)A.ig_h2o * a.stride, a, ipz, zz) : 0.0;
+  for (int w = 0; w < A.nw; w++) po[REC_K + w] = atm_lin(a.k + (size_t)w * a.stride, a, ipz, zz);
+  for (int g = 0; g < A.ng; g++) po[REC_K + A.nw + g] = atm_lin(a.q + (size_t)g * a.stride, a, ipz, zz);
+}
+
+// Extra LOS points at the layer edges and through the transition layers,
+// chord step lengths, column densities, layer index and scaling factor per
+// point (add_aerosol_layers, src/lineofsight.c:193-372).  COUNT pass sizes
+// the refined LOS, STORE pass writes it.
+template <bool STORE>
+__global__ void __launch_bounds__(128) refine_kernel(RefineArgs A) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.n_rays) return;
+  const int nb = A.nlos_b[r];
+  if (nb == 0) {
+    if (!STORE) A.nlos[r] = 0;
+    return;
+  }
+  const int ai = A.ray_atm[r];
+  const int lo = A.atm_off[ai];
+  Profile a;
+  a.n = A.atm_off[ai + 1] - lo;
+  a.stride = A.n_levels;
+  a.z = A.z + lo;
+  a.p = A.p + lo;
+  a.t = A.t + lo;
+  a.q = A.q + lo;
+  a.k = A.k + lo;
+  const double *gb = A.geo_b + A.off_b[r] * 4, *pb = A.pts_b + A.off_b[r] * A.W;
+  const int64_t base = STORE ? A.off[r] : 0;
+  const int nmax = STORE ? A.nlos[r] : NLOS + 1;
+  int o = 0;
+  bool over = false;
+#define JSC_PUT_BASE(ip)                                                     \
+  do {                                                                       \
+    if (o >= nmax || base + o >= A.max_seg) { over = true; break; }          \
+    if (STORE) {                                                             \
+      double *go = A.geo + (base + o) * 4, *po = A.pts + (base + o) * A.W;   \
+      const double *gs = gb + (size_t)(ip) * 4, *ps = pb + (size_t)(ip) * A.W; \
+      go[0] = gs[0]; go[1] = gs[1]; go[2] = gs[2];                           \
+      for (int c = 0; c < A.W; c++) po[c] = ps[c];                           \
+    }                                                                        \
+    o++;                                                                     \
+  } while (0)
+  JSC_PUT_BASE(0);
+  for (int ip = 1; ip < nb && !over; ip++) {
+    const double zp = gb[(size_t)(ip - 1) * 4], zc = gb[(size_t)ip * 4];
+    if ((zp < A.altimax || zc < A.altimax) && (zp > A.altimin || zc > A.altimin)) {
+      for (int il = 0; il < A.n_alti && !over; il++) {
+        const double z1 = A.alti[il], z2 = A.alti[A.n_alti - il - 1];
+        if (zp > z1 && zc < z1) {
+          if (o >= nmax || base + o >= A.max_seg) { over = true; break; }
+          if (STORE) refine_cross(A, a, gb, ip, z1, A.geo + (base + o) * 4, A.pts + (base + o) * A.W);
+          o++;
+        }
+        if (zp < z2 && zc > z2) {
+          if (o >= nmax || base + o >= A.max_seg) { over = true; break; }
+          if (STORE) refine_cross(A, a, gb, ip, z2, A.geo + (base + o) * 4, A.pts + (base + o) * A.W);
+          o++;
+        }
+      }
+    }
+    if (!over) JSC_PUT_BASE(ip);
+  }
+#undef JSC_PUT_BASE
+  if (over || o > NLOS) {
+    atomicOr(A.status, JSC_DEV_ERR_NLOS);
+    if (!STORE) A.nlos[r] = 0;
+    return;
+  }
+  if (!STORE) {
+    A.nlos[r] = o;
+    return;
+  }
+  // Chord step lengths, column densities, layer index and factor.
+  double xp[3], xc[3], xn[3];
+  double *go = A.geo + base * 4;
+  jsc_geo2cart(go[0], go[1], go[2], xc);
+  if (o > 1) jsc_geo2cart(go[4], go[5], go[6], xn);
+  for (int i = 0; i < o; i++) {
+    double ds;
+    if (o == 1) {
+      ds = 0;
+    } else if (i == 0) {
+      ds = 0.5 * sqrt((xc[0] - xn[0]) * (xc[0] - xn[0]) + (xc[1] - xn[1]) * (xc[1] - xn[1]) +
+                      (xc[2] - xn[2]) * (xc[2] - xn[2]));
+    } else if (i == o - 1) {
+      ds = 0.5 * sqrt((xc[0] - xp[0]) * (xc[0] - xp[0]) + (xc[1] - xp[1]) * (xc[1] - xp[1]) +
+                      (xc[2] - xp[2]) * (xc[2] - xp[2]));
+    } else {
+      ds = 0.5 * (sqrt((xp[0] - xc[0]) * (xp[0] - xc[0]) + (xp[1] - xc[1]) * (xp[1] - xc[1]) +
+                       (xp[2] - xc[2]) * (xp[2] - xc[2])) +
+                  sqrt((xc[0] - xn[0]) * (xc[0] - xn[0]) + (xc[1] - xn[1]) * (xc[1] - xn[1]) +
+                       (xc[2] - xn[2]) * (xc[2] - xn[2])));
+    }
+    double *rec = A.pts + (base + i) * A.W;
+    const double p = rec[REC_P], t = rec[REC_T], z = go[(size_t)i * 4];
+    rec[REC_DS] = ds;
+    go[(size_t)i * 4 + 3] = ds;
+    for (int g = 0; g < A.ng; g++) {
+      const double q = rec[REC_K + A.nw + g];
+      rec[REC_K + A.nw + g] = 10 * q * p / (JSC_KBOLTZ * t) * ds;
+    }
+    rec[REC_GRID] = A.grid_p ? (double)grid_code(A.grid_np, A.grid_p, A.grid_nt, A.grid_t, p, t) : -1.0;
+    rec[REC_PLK] = (double)planck_index(t);
+    // At i = 0 the reference compares z[-1]; the first point, at the top
+    // of the atmosphere and outside every layer, stands in for it.
+    const double zprev = go[(size_t)(i > 0 ? i - 1 : 0) * 4];
+    int aeroi = -999;
+    double aerofac = 0.;
+    if ((zprev < A.altimax || z < A.altimax) && (zprev > A.altimin || z > A.altimin)) {
+      for (int il = 0; il < A.nl; il++) {
+        if (z <= A.top[il] && z >= A.bottom[il]) {
+          aeroi = il;
+          aerofac = 1.;
+        }
+        if (A.trans[il] > A.transs && z <= (A.top[il] + A.trans[il]) && z > A.top[il]) {
+          aeroi = il;
+          aerofac = (A.top[il] + A.trans[il] - z) / A.trans[il];
+        }
+        if (A.trans[il] > A.transs && z < A.bottom[il] && z >= (A.bottom[il] - A.trans[il])) {
+          aeroi = il;
+          aerofac = fabs(A.bottom[il] - A.trans[il] - z) / A.trans[il];
+        }
+      }
+    }
+    rec[REC_AF] = aerofac;
+    rec[REC_AI] = (double)aeroi;
+    for (int c = 0; c < 3; c++) {
+      xp[c] = xc[c];
+      xc[c] = xn[c];
+    }
+    if (i + 2 < o) jsc_geo2cart(go[(size_t)(i + 2) * 4], go[(size_t)(i + 2) * 4 + 1],
+                                go[(size_t)(i + 2) * 4 + 2], xn);
+  }
 }
 
 // Exclusive scan of nlos into off[0..n] by one block.
@@ -650,7 +830,17 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
                                  rec[REC_QH2O], rec + REC_K + m.nw);
     const double src = pb[itp] + ps[itp] * (T - planck_temp(itp));
     if (tau_gas > 0) {
-      const double eps = 1 - tau_gas * exp(-1. * beta * DS);
+      // clear air, or aerosol/cloud extinction without a scattering source
+      // (src/forwardmodel.c:365-389)
+      const double af = rec[REC_AF];
+      double eps;
+      if (A.cfg.sca_n == 0 || af == 0) {
+        eps = 1 - tau_gas * exp(-1. * beta * DS);
+      } else {
+        const int ia = (int)rec[REC_AI];
+        const double bx = A.beta[(A.cfg.sca_ext_beta_a ? 2 : 0) * A.aero_nl * nd + ia * nd + d];
+        eps = 1 - tau_gas * exp(-1. * (beta + af * bx) * DS);
+      }
       rad += src * eps * tau;
       tau *= (1 - eps);
     }

@@ -144,9 +144,16 @@ class Batch:
 
     def variant(self):
         v, b, mb = C.c_int(), C.c_int(), C.c_int()
-        L.check(L.load().jsc_batch_variant(self.h, C.byref(v), C.byref(b), C.byref(mb)),
+        lib = L.load()
+        L.check(lib.jsc_batch_variant(self.h, C.byref(v), C.byref(b), C.byref(mb)),
                 "jsc_batch_variant")
-        return {"variant": v.value, "block": b.value, "min_blocks": mb.value}
+        ms = [lib.jsc_batch_variant_ms(self.h, i) for i in range(5)]
+        return {"variant": v.value, "block": b.value, "min_blocks": mb.value,
+                "variant_ms": [round(x, 3) for x in ms]}
+
+    def set_aero(self, aero):
+        """Aerosol/cloud layers (an AeroT) for runs with ctl.sca_n > 0."""
+        L.check(L.load().jsc_batch_set_aero(self.h, C.byref(aero)), "jsc_batch_set_aero")
 
     def set_timing(self, on=True):
         L.load().jsc_batch_set_timing(self.h, 1 if on else 0)
@@ -172,14 +179,17 @@ class Batch:
             pass
 
 
-def formod_batch(ctl, inp, device=0, model=None, digest=False):
+def formod_batch(ctl, inp, device=0, model=None, digest=False, aero=None):
     """One-shot batch forward model: returns dict of rad/tau/tp*/nlos (and
-    the per-(ray, channel) EGA index digests when digest=True)."""
+    the per-(ray, channel) EGA index digests when digest=True).  aero: an
+    AeroT with the layers and optical properties when ctl.sca_n > 0."""
     own = model is None
     m = Model(ctl, device) if own else model
     nl = len(inp["z"])
     b = Batch(m, ctl, len(inp["atm_off"]) - 1, nl, max(1, len(inp["ray_atm"])))
     try:
+        if aero is not None:
+            b.set_aero(aero)
         if digest:
             b.set_digest(True)
         b.upload(inp)

@@ -18,7 +18,8 @@ EXPORTS = [
     "jsc_batch_upload", "jsc_batch_run", "jsc_batch_download",
     "jsc_formod_batch", "jsc_batch_set_timing", "jsc_batch_kernel_ms",
     "jsc_batch_counters", "jsc_batch_set_digest", "jsc_batch_index_digest",
-    "jsc_batch_autotune", "jsc_batch_variant",
+    "jsc_batch_autotune", "jsc_batch_variant", "jsc_batch_variant_ms",
+    "jsc_batch_set_aero",
 ]
 
 
@@ -90,6 +91,8 @@ def load():
         "jsc_batch_index_digest": (i, [vp, P(C.c_uint64)]),
         "jsc_batch_autotune": (i, [vp, vp]),
         "jsc_batch_variant": (i, [vp, P(i), P(i), P(i)]),
+        "jsc_batch_variant_ms": (d, [vp, i]),
+        "jsc_batch_set_aero": (i, [vp, P(S.AeroT)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

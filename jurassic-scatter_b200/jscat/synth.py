@@ -234,3 +234,64 @@ def batched_case(directory, n_rays=100_000, rays_per_atm=50, seed=20261203,
     base = write_tables(directory, emitters, nus, seed)
     ctlkw = dict(emitters=emitters, nus=nus, tblbase=base, hydz=0.0)
     return ctlkw, atms, ray_atm, geom
+
+
+# ------------------------------------------------------------- aerosols --
+
+CFG2_NU = list(np.linspace(780.0, 1250.0, 16))
+
+
+def sulfate_refractive_index(nu):
+    """n = 1.43 + 0.02 sin(nu/50), k = 0.05 + 0.1 exp(-((nu-1050)/40)^2)."""
+    nu = np.asarray(nu, dtype=np.float64)
+    return 1.43 + 0.02 * np.sin(nu / 50.0), 0.05 + 0.1 * np.exp(-((nu - 1050.0) / 40.0) ** 2)
+
+
+def ice_refractive_index(nu):
+    """n = 1.3 + 0.05 cos(nu/80), k varying smoothly between 0.02 and 0.4."""
+    nu = np.asarray(nu, dtype=np.float64)
+    return 1.3 + 0.05 * np.cos(nu / 80.0), 0.02 + 0.38 * (0.5 + 0.5 * np.sin((nu - 700.0) / 150.0)) ** 2
+
+
+def write_refractive_index(path, fn, lo=600.0, hi=1500.0, step=1.0):
+    """Refractive-index file: 'nu n k' lines (the Mie input of read_aero)."""
+    nu = np.arange(lo, hi + step / 2, step)
+    n, k = fn(nu)
+    with open(path, "w") as f:
+        for a, b, c in zip(nu, n, k):
+            f.write("%.4f %.8f %.8f\n" % (a, b, c))
+
+
+def write_aero_file(path, layers):
+    """Aerosol model file: top bottom transition type refractive-index-file
+    concentration radius width (one line per log-normal mode)."""
+    with open(path, "w") as f:
+        f.write("# $1 = top [km]\n# $2 = bottom [km]\n# $3 = transition [km]\n"
+                "# $4 = type\n# $5 = refractive index file\n# $6 = N [cm-3]\n"
+                "# $7 = median radius [um]\n# $8 = width\n\n")
+        for lay in layers:
+            f.write("%g %g %g MIE %s %g %g %g\n" % lay)
+
+
+def sulfate_layer_files(directory):
+    """aero.tab for a sulfate-like layer at 15-20 km (0.1 km transition),
+    median radius 0.1 um, width 1.5, 10 cm-3.  (The reference keeps the
+    layer-edge altitudes in a 4*NLMAX array, src/lineofsight.c:200, so a
+    transition layer may hold at most ~16 samples of TRANSS.)"""
+    os.makedirs(directory, exist_ok=True)
+    ri = os.path.join(directory, "sulfate_ri.dat")
+    write_refractive_index(ri, sulfate_refractive_index)
+    aero = os.path.join(directory, "aero_sulfate.tab")
+    write_aero_file(aero, [(20.0, 15.0, 0.1, ri, 10.0, 0.1, 1.5)])
+    return aero
+
+
+def ice_layer_files(directory):
+    """aero.tab for an ice-cloud-like layer at 9-11 km (0.1 km transition),
+    median radius 10 um, width 1.8, 0.1 cm-3."""
+    os.makedirs(directory, exist_ok=True)
+    ri = os.path.join(directory, "ice_ri.dat")
+    write_refractive_index(ri, ice_refractive_index)
+    aero = os.path.join(directory, "aero_ice.tab")
+    write_aero_file(aero, [(11.0, 9.0, 0.1, ri, 0.1, 10.0, 1.8)])
+    return aero

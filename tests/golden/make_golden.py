@@ -67,6 +67,34 @@ def save(name, ctlkw, atms, ray_atm, geom, ref, port):
         ray_atm=np.asarray(ray_atm), **{"geom_" + k: v for k, v in geom.items()})
 
 
+def aerosol_case(workdir, sca_mult, n_rays=24, nus=None, sca_ext="beta_a"):
+    """2 emitters, 4 channels of the 16-channel aerosol grid, limb rays with
+    tangent heights 8-30 km through the sulfate-like layer; sca_mult 0:
+    extinction only, 1: single scattering."""
+    nus = [synth.CFG2_NU[i] for i in (0, 5, 10, 15)] if nus is None else nus
+    rng = np.random.default_rng(20261204)
+    atm = synth.atmosphere(synth.CFG0_EMITTERS, rng)
+    geom = synth.limb_geometry(np.linspace(8.0, 30.0, n_rays))
+    base = synth.write_tables(workdir, synth.CFG0_EMITTERS, nus, 20261203)
+    aerofile = synth.sulfate_layer_files(os.path.join(workdir, "aero"))
+    ctlkw = dict(emitters=synth.CFG0_EMITTERS, nus=nus, tblbase=base, hydz=0.0, sca_n=1,
+                 sca_mult=sca_mult, sca_ext=sca_ext)
+    return ctlkw, atm, geom, aerofile
+
+
+def save_aero(name, ctlkw, atm, geom, ref, aero_bytes, port=None):
+    extra = {}
+    if port is not None:
+        assert np.array_equal(port["rad"], ref["rad"]), "port must match the reference"
+        extra["digest"] = port["digest"]
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        rad=ref["rad"], tau=ref["tau"], tpz=ref["tpz"], nlos=ref["nlos"],
+        aero=np.frombuffer(aero_bytes, dtype=np.uint8),
+        table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
+        **{"geom_" + k: v for k, v in geom.items()}, **extra)
+
+
 def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
     ctlkw, atm, geom = synth.clear_limb_case(workdir)
@@ -78,6 +106,13 @@ def main():
     ref = refrun.run(reference_ctl(ctlkw), atms, ray_atm, geom, los=True)
     port = refrun.run_port(ctlkw, atms, ray_atm, geom, los=True)
     save("mixed_batch", ctlkw, atms, ray_atm, geom, ref, port)
+    for ext in ("beta_a", "beta_e"):
+        ctlkw, atm, geom, aerofile = aerosol_case(workdir, 0, sca_ext=ext)
+        aero = refrun.reference_aero(ctlkw, aerofile, os.path.dirname(aerofile))
+        ra = np.zeros(len(geom["obsz"]), int)
+        ref = refrun.run(ctlkw, [atm], ra, geom, aero=aero, los=True)
+        port = refrun.run_port(ctlkw, [atm], ra, geom, aero=aero, los=True)
+        save_aero("aerosol_ext_" + ext, ctlkw, atm, geom, ref, aero, port)
     print("fixtures written to", HERE)
 
 

@@ -80,3 +80,23 @@ def test_mixed_batch(workdir):
     assert max_rel(out["rad"], g["rad"]) <= REL_TOL
     assert max_rel(out["tau"], g["tau"]) <= REL_TOL
     np.testing.assert_allclose(out["tpz"], g["tpz"], rtol=1e-9, atol=1e-9)
+
+
+@pytest.mark.parametrize("ext", ["beta_a", "beta_e"])
+def test_aerosol_extinction(workdir, ext):
+    """Aerosol layer with extinction only (SCA_MULT=0): layer-edge LOS
+    refinement (add_aerosol_layers) and the aerosol RT branch."""
+    from jscat import synth, api, structs as S
+    from make_golden_shim import aerosol_case
+    g = _load("aerosol_ext_" + ext)
+    ctlkw, atm, geom, aerofile = aerosol_case(workdir, 0, sca_ext=ext)
+    _check_tables(g, ctlkw)
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    ctl = S.make_ctl(**ctlkw)
+    out = api.formod_batch(ctl, synth.batch_from([atm], np.zeros(len(geom["obsz"]), np.int32), geom),
+                           digest=True, aero=aero)
+    np.testing.assert_array_equal(out["nlos"], g["nlos"])
+    np.testing.assert_array_equal(out["digest"], g["digest"])
+    assert bt_error(out["rad"], g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(out["rad"], g["rad"]) <= REL_TOL
+    assert max_rel(out["tau"], g["tau"]) <= REL_TOL
