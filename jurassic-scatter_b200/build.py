@@ -9,6 +9,7 @@ with --fmad=false: no multiply-add contraction, so floating-point results
 follow the reference's operation order.
 """
 import argparse
+import concurrent.futures as cf
 import os
 import subprocess
 import sys
@@ -22,9 +23,10 @@ LIB = os.path.join(OUT, "libjurassic_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 C_SRCS = ["model_host.c", "formod.c"]
-CU_SRCS = ["model_dev.cu", "batch.cu"]
+CU_SRCS = ["model_dev.cu", "batch.cu", "ega_g2.cu", "ega_g4.cu", "ega_g8.cu",
+           "ega_gmax.cu"]
 HEADERS = ["jsc_internal.h", "physics.h", "ckd_tables.h", "jsc_model.h",
-           "cuda_util.cuh", "kernels.cuh"]
+           "cuda_util.cuh", "device_common.cuh", "kernels.cuh", "ega_kernel.cuh"]
 
 INC = ["-I" + os.path.join(REPO, "include"), "-I" + CSRC]
 CFLAGS = ["-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-std=gnu11",
@@ -56,19 +58,24 @@ def build(force=False, verbose=False):
     hdrs = [os.path.join(CSRC, h) for h in HEADERS]
     hdrs.append(os.path.join(REPO, "include", "jurassic_b200.h"))
     objs = []
+    jobs = []
     for s in C_SRCS:
         src = os.path.join(CSRC, s)
         o = os.path.join(OBJ, s + ".o")
         if force or _newer(o, [src] + hdrs):
-            _run(["gcc"] + CFLAGS + INC + ["-c", src, "-o", o])
+            jobs.append((["gcc"] + CFLAGS + INC + ["-c", src, "-o", o], None))
         objs.append(o)
     for s in CU_SRCS:
         src = os.path.join(CSRC, s)
         o = os.path.join(OBJ, s + ".o")
         if force or _newer(o, [src] + hdrs):
-            _run([NVCC] + NVFLAGS + INC + ["-c", src, "-o", o],
-                 log=os.path.join(OBJ, s + ".ptxas.txt"))
+            jobs.append(([NVCC] + NVFLAGS + INC + ["-c", src, "-o", o],
+                         os.path.join(OBJ, s + ".ptxas.txt")))
         objs.append(o)
+    # the translation units compile independently: run them in parallel
+    with cf.ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(_run, cmd, log) for cmd, log in jobs]:
+            f.result()
     if force or _newer(LIB, objs):
         _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
               "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp",

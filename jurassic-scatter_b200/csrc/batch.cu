@@ -6,6 +6,7 @@
 #include <strings.h>
 
 #include "kernels.cuh"
+#include "ega_kernel.cuh"
 
 static void batch_free_los(jsc_batch *b) {
   cudaFree(b->d_geo);
@@ -318,38 +319,17 @@ static const EgaVariant kEgaVariants[] = {{128, 4}, {128, 6}, {128, 8}, {256, 3}
 static const int kNumEgaVariants = 5;
 static const int kEgaDefault = 1;
 
-template <int G, bool DIG>
-static void launch_g(const EgaArgs &ea, unsigned grid_128, unsigned grid_256, int v,
-                     cudaStream_t s) {
-  switch (v) {
-    case 0: ega_rt_kernel<G, DIG, 128, 4><<<grid_128, 128, 0, s>>>(ea); break;
-    case 2: ega_rt_kernel<G, DIG, 128, 8><<<grid_128, 128, 0, s>>>(ea); break;
-    case 3: ega_rt_kernel<G, DIG, 256, 3><<<grid_256, 256, 0, s>>>(ea); break;
-    case 4: ega_rt_kernel<G, DIG, 256, 4><<<grid_256, 256, 0, s>>>(ea); break;
-    default: ega_rt_kernel<G, DIG, 128, 6><<<grid_128, 128, 0, s>>>(ea); break;
-  }
-}
-
 static int launch_ega(const EgaArgs &ea, int nr, int ndp, int ng, int variant,
                       cudaStream_t s) {
   const int64_t threads = (int64_t)nr * ndp;
   const unsigned g128 = (unsigned)((threads + 127) / 128);
   const unsigned g256 = (unsigned)((threads + 255) / 256);
   const int v = (variant >= 0 && variant < kNumEgaVariants) ? variant : kEgaDefault;
-  const bool dig = ea.digest != nullptr;
-  if (dig) {  // index digests: diagnostics, default variant only
-    if (ng <= 2) launch_g<2, true>(ea, g128, g256, kEgaDefault, s);
-    else if (ng <= 4) launch_g<4, true>(ea, g128, g256, kEgaDefault, s);
-    else if (ng <= 8) launch_g<8, true>(ea, g128, g256, kEgaDefault, s);
-    else if (ng <= 16) launch_g<16, true>(ea, g128, g256, kEgaDefault, s);
-    else launch_g<NGMAX, true>(ea, g128, g256, kEgaDefault, s);
-  } else {
-    if (ng <= 2) launch_g<2, false>(ea, g128, g256, v, s);
-    else if (ng <= 4) launch_g<4, false>(ea, g128, g256, v, s);
-    else if (ng <= 8) launch_g<8, false>(ea, g128, g256, v, s);
-    else if (ng <= 16) launch_g<16, false>(ea, g128, g256, kEgaDefault, s);
-    else launch_g<NGMAX, false>(ea, g128, g256, kEgaDefault, s);
-  }
+  const bool dig = ea.digest != nullptr;  // index digests: default variant only
+  if (ng <= 2) jsc_ega_launch_g2(ea, g128, g256, v, dig, s);
+  else if (ng <= 4) jsc_ega_launch_g4(ea, g128, g256, v, dig, s);
+  else if (ng <= 8) jsc_ega_launch_g8(ea, g128, g256, v, dig, s);
+  else jsc_ega_launch_gmax(ea, g128, g256, v, dig, s);
   JSC_LAUNCH_CHECK();
   return JSC_OK;
 }
@@ -556,6 +536,7 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   ea.beta = b->d_beta;
   ea.aero_nl = b->aero_nl;
   b->last_ega = ea;
+  ev_record(b, JSC_T_EGA, 0, s);
   int st = launch_ega(ea, nr, ndp, m->ng, b->ega_variant, s);
   if (st) return st;
   JSC_LAUNCH_CHECK();

@@ -1,0 +1,201 @@
+// Device functions shared by the ray-tracing and radiative-transfer
+// kernels: Planck source lookup, (p, T) table brackets, continua and the
+// EGA table lookups.
+#pragma once
+#include <math.h>
+#include <stdint.h>
+
+#include "jsc_model.h"
+#include "physics.h"
+#include "cuda_util.cuh"
+
+__device__ __forceinline__ double planck_temp(int i) {
+  return jsc_lin(0.0, JSC_PLANCK_TMIN, JSC_NPLANCK - 1.0, JSC_PLANCK_TMAX, (double)i);
+}
+
+// Result of locate() on the uniform Planck temperature grid: the bracket
+// from the grid spacing, corrected against the exact node values.
+__device__ __forceinline__ int planck_index(double t) {
+  if (!(t == t)) return JSC_NPLANCK - 2;
+  const double f = floor((t - JSC_PLANCK_TMIN) * 4.0);
+  int i = f < 0 ? 0 : (f > JSC_NPLANCK - 2 ? JSC_NPLANCK - 2 : (int)f);
+  while (i > 0 && planck_temp(i) > t) i--;
+  while (i < JSC_NPLANCK - 2 && planck_temp(i + 1) <= t) i++;
+  return i;
+}
+
+__device__ __forceinline__ double planck_src(const jsc_dev_model &m, int d,
+                                             int it, double t) {
+  const size_t o = (size_t)d * JSC_NPLANCK + it;
+  return m.planck_b[o] + m.planck_s[o] * (t - planck_temp(it));
+}
+
+// Packed (p, T) bracket of a point on the shared grid: ipr << 10 | it0 << 5
+// | it1, plus 1 << 16 when both temperature rows have two nodes or more.
+// locate() (src/misc.c:237-265) as intpol_tbl calls it (src/forwardmodel.c:447-449).
+__device__ __forceinline__ int grid_code(int np, const double *gp, const int *gnt,
+                                         const double *gt, double p, double t) {
+  const int ipr = jsc_locate(gp, np, p);
+  const int it0 = jsc_locate(gt + ipr * TBLNTMAX, gnt[ipr], t);
+  const int it1 = jsc_locate(gt + (ipr + 1) * TBLNTMAX, gnt[ipr + 1], t);
+  const int ok = (gnt[ipr] >= 2 && gnt[ipr + 1] >= 2) ? (1 << 16) : 0;
+  return ok | (ipr << 10) | (it0 << 5) | it1;
+}
+
+// ------------------------------------------------------------- EGA + RT --
+
+
+// Continuum extinction of one channel at one LOS point
+// (src/forwardmodel.c:120-152 with src/continua.c:5-2049).
+__device__ __forceinline__ double continua(const jsc_dev_model &m,
+                                           const jsc_run_cfg &cfg,
+                                           const jsc_ctm_coef &c, double nu,
+                                           double kwin, double P, double T,
+                                           double DS, double qh2o,
+                                           const double *u) {
+  double beta = kwin;
+  if (cfg.ctm_co2) {
+    double ctm = 0;
+    if (m.ig_co2 >= 0 && c.co2_on) {
+      const double dt230 = T - 230, dt260 = T - 260, dt296 = T - 296;
+      const double ctw = dt260 * 5.050505e-4 * dt296 * c.co2_c230 -
+                         dt230 * 9.259259e-4 * dt296 * c.co2_c260 +
+                         dt230 * 4.208754e-4 * dt260 * c.co2_c296;
+      ctm = u[m.ig_co2] / JSC_AVOGADRO / 1000 * P / JSC_P0 * ctw;
+    }
+    beta += ctm / DS;
+  }
+  if (cfg.ctm_h2o) {
+    double ctm = 0;
+    if (m.ig_h2o >= 0 && c.h2o_on) {
+      const double ctwslf = c.h2o_self296 * pow(c.h2o_ratio, (296 - T) / (296 - 260));
+      const double a1 = nu * u[m.ig_h2o] * tanh(.7193876 / T * nu);
+      const double a2 = 296 / T;
+      const double a3 = P / JSC_P0 * (qh2o * ctwslf + (1 - qh2o) * c.h2o_frn) * 1e-20;
+      ctm = a1 * a2 * a3;
+    }
+    beta += ctm / DS;
+  }
+  if (cfg.ctm_n2 && c.n2_on) {
+    const double t0 = 273, tr = 296, q_n2 = 0.79;
+    const double pp = P / JSC_P0, tt = t0 / T;
+    beta += 0.1 * (pp * pp) * (tt * tt) * q_n2 * c.n2_b *
+            exp(c.n2_beta * (1 / tr - 1 / T)) *
+            (q_n2 + (1 - q_n2) * (1.294 - 0.4545 * T / tr));
+  }
+  if (cfg.ctm_o2 && c.o2_on) {
+    const double t0 = 273, tr = 296, q_o2 = 0.21;
+    const double pp = P / JSC_P0, tt = t0 / T;
+    beta += 0.1 * (pp * pp) * (tt * tt) * q_o2 * c.o2_b *
+            exp(c.o2_beta * (1 / tr - 1 / T));
+  }
+  return beta;
+}
+
+// Key of node i (u or eps).
+template <bool U>
+__device__ __forceinline__ float nkey(const jsc_node *row, int i) {
+  return U ? __ldg(&row[i].u) : __ldg(&row[i].e);
+}
+
+// locate_tbl (src/forwardmodel.c:546-565) on one table row of n >= 2
+// points.  key > x is evaluated as key > RD(x) (x rounded down to float),
+// which is exact for float keys.
+template <bool U>
+__device__ __forceinline__ int bisect_row(const jsc_node *row, int n, double x) {
+  const float xf = __double2float_rd(x);
+  const bool nan = !(x == x);
+  int ilo = 0, ihi = n - 1;
+  while (ihi > ilo + 1) {
+    const int i = (ihi + ilo) >> 1;
+    if (!nan && nkey<U>(row, i) > xf) ihi = i; else ilo = i;
+  }
+  return ilo;
+}
+
+// Same result as bisect_row for a row with strictly increasing keys,
+// found by an exponential search from the guess h: the largest i <= n-2
+// with key[i] <= x, or 0.
+template <bool U>
+__device__ __forceinline__ int search_row(const jsc_node *row, int n, double x, int h) {
+  if (!(x == x)) return n - 2;
+  const float xf = __double2float_rd(x);
+  const int last = n - 2;
+  int i = h < 0 ? 0 : (h > last ? last : h);
+  const float klo = nkey<U>(row, i), khi = nkey<U>(row, i + 1);
+  int lo, hi;
+  if (!(klo > xf)) {
+    if (khi > xf || i == last) return i;
+    lo = i + 1;
+    int step = 1;
+    while (true) {
+      const int pr = lo + step;
+      if (pr > last) { hi = last + 1; break; }
+      if (nkey<U>(row, pr) > xf) { hi = pr; break; }
+      lo = pr;
+      step <<= 1;
+    }
+  } else {
+    if (i == 0) return 0;
+    hi = i;
+    int step = 1;
+    while (true) {
+      const int pr = hi - step;
+      if (pr <= 0) { lo = 0; break; }
+      if (!(nkey<U>(row, pr) > xf)) { lo = pr; break; }
+      hi = pr;
+      step <<= 1;
+    }
+  }
+  while (hi > lo + 1) {
+    const int mid = (lo + hi) >> 1;
+    if (nkey<U>(row, mid) > xf) hi = mid; else lo = mid;
+  }
+  return lo;
+}
+
+// LIN on float table entries with the slope already in float, as the
+// reference evaluates it: y0 + slope * (x - x0), promoted to double.
+__device__ __forceinline__ double lin_node(float x0, float y0, float slope, double x) {
+  return (double)y0 + (double)slope * (x - (double)x0);
+}
+
+// Emissivity of the extended path at one (p, T) node of a table
+// (intpol_tbl_u then intpol_tbl_eps, src/forwardmodel.c:460-474): invert
+// the path emissivity x1 to a column density on the row, add the segment's
+// column, look the emissivity up again, clamp to [0, 1].
+//
+// Fast path: the row is strictly increasing, the interval [h, h+1] of the
+// previous point still brackets x1 and the extended column stays in the
+// same interval -- then the two nodes h, h+1 (one 32-byte sector) answer
+// both lookups.  Otherwise the exact searches above find the intervals.
+template <bool DIG>
+__device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, jsc_row rd,
+                                           double x1, double useg, int hint, int *jout,
+                                           unsigned long long *dig) {
+  const int n = rd.nf & 0xffff;
+  const bool strict = (rd.nf >> 16) & JSC_ROW_STRICT;
+  const jsc_node *row = nodes + rd.off;
+  const int last = n - 2;
+  int k = hint < 0 ? 0 : (hint > last ? last : hint);
+  float4 a = __ldg(reinterpret_cast<const float4 *>(row + k));
+  float4 b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
+  const float x1f = __double2float_rd(x1);
+  // bracket for x1 on eps: (e[k] <= x1 or k == 0) and (x1 < e[k+1] or k == last)
+  if (!(strict && (!(a.y > x1f) || k == 0) && (b.y > x1f || k == last) && x1 == x1)) {
+    k = strict ? search_row<false>(row, n, x1, k) : bisect_row<false>(row, n, x1);
+    a = __ldg(reinterpret_cast<const float4 *>(row + k));
+    b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
+  }
+  const double x2 = lin_node(a.y, a.x, a.z, x1) + useg;
+  const float x2f = __double2float_rd(x2);
+  int j = k;
+  if (!(strict && (!(a.x > x2f) || k == 0) && (b.x > x2f || k == last) && x2 == x2)) {
+    j = strict ? search_row<true>(row, n, x2, k) : bisect_row<true>(row, n, x2);
+    if (j != k) a = __ldg(reinterpret_cast<const float4 *>(row + j));
+  }
+  if (DIG) *dig = (*dig * 1000003ull + (unsigned long long)k) * 1000003ull + (unsigned long long)j;
+  *jout = j;
+  return jsc_clamp01(lin_node(a.x, a.y, a.w, x2));
+}
+

@@ -159,7 +159,7 @@ typedef struct {
   const int *grid_nt;
   const double *grid_t;
   const int *tab_grid;       /* [nd*ng] grid id, -1: table unusable (np<2) */
-  const jsc_row *rows;       /* [nd*ng][TBLNPMAX][TBLNTMAX] */
+  const jsc_row *rows;       /* [TBLNPMAX][TBLNTMAX][ng][nd] */
   const jsc_node *nodes;
   const double *planck_b, *planck_s;   /* [nd][JSC_NPLANCK] */
   const jsc_ctm_coef *ctm;             /* [nd] */

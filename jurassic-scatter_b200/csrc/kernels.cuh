@@ -6,13 +6,9 @@
 //                     (src/lineofsight.c:5-190); a counting pass sizes the
 //                     line of sight, a storing pass writes the LOS records.
 //   scan_kernel       exclusive prefix sum of LOS points per ray.
-//   ega_rt_kernel     a group of lanes per ray, lanes over channels: EGA
-//                     table interpolation (src/forwardmodel.c:409-565),
-//                     continua (src/forwardmodel.c:120-152, src/continua.c),
-//                     Planck source (src/forwardmodel.c:743-794) and the
-//                     radiative-transfer recursion
-//                     (src/forwardmodel.c:302-399), fused, serial along the
-//                     ray because the EGA carries the path transmittance.
+//   refine_kernel     aerosol/cloud layer-edge refinement of the LOS.
+//   (ega_rt_kernel, the EGA + continua + Planck + radiative-transfer
+//   kernel, is in ega_kernel.cuh.)
 //
 // All arithmetic that decides a table index is FP64 in the reference's
 // operation order (the library is built with --fmad=false), so the indices
@@ -24,6 +20,7 @@
 #include "jsc_model.h"
 #include "physics.h"
 #include "cuda_util.cuh"
+#include "device_common.cuh"
 
 #define JSC_ZREFRAC 60.0   // refraction is evaluated up to this altitude [km]
 #define JSC_FD_STEP 0.02   // finite-difference step of the refractivity gradient [km]
@@ -62,27 +59,6 @@ __global__ void hydro_kernel(AtmArgs a) {
   a.zmax[i] = nan ? NAN : mx;
 }
 
-__device__ __forceinline__ double planck_temp(int i) {
-  return jsc_lin(0.0, JSC_PLANCK_TMIN, JSC_NPLANCK - 1.0, JSC_PLANCK_TMAX, (double)i);
-}
-
-// Result of locate() on the uniform Planck temperature grid: the bracket
-// from the grid spacing, corrected against the exact node values.
-__device__ __forceinline__ int planck_index(double t) {
-  if (!(t == t)) return JSC_NPLANCK - 2;
-  const double f = floor((t - JSC_PLANCK_TMIN) * 4.0);
-  int i = f < 0 ? 0 : (f > JSC_NPLANCK - 2 ? JSC_NPLANCK - 2 : (int)f);
-  while (i > 0 && planck_temp(i) > t) i--;
-  while (i < JSC_NPLANCK - 2 && planck_temp(i + 1) <= t) i++;
-  return i;
-}
-
-__device__ __forceinline__ double planck_src(const jsc_dev_model &m, int d,
-                                             int it, double t) {
-  const size_t o = (size_t)d * JSC_NPLANCK + it;
-  return m.planck_b[o] + m.planck_s[o] * (t - planck_temp(it));
-}
-
 // --------------------------------------------------------------- raytrace --
 
 struct RayArgs {
@@ -104,18 +80,6 @@ struct RayArgs {
   const int *grid_nt;
   int raw_q;  // store volume mixing ratios instead of column densities
 };
-
-// Packed (p, T) bracket of a point on the shared grid: ipr << 10 | it0 << 5
-// | it1, plus 1 << 16 when both temperature rows have two nodes or more.
-// locate() (src/misc.c:237-265) as intpol_tbl calls it (src/forwardmodel.c:447-449).
-__device__ __forceinline__ int grid_code(int np, const double *gp, const int *gnt,
-                                         const double *gt, double p, double t) {
-  const int ipr = jsc_locate(gp, np, p);
-  const int it0 = jsc_locate(gt + ipr * TBLNTMAX, gnt[ipr], t);
-  const int it1 = jsc_locate(gt + (ipr + 1) * TBLNTMAX, gnt[ipr + 1], t);
-  const int ok = (gnt[ipr] >= 2 && gnt[ipr + 1] >= 2) ? (1 << 16) : 0;
-  return ok | (ipr << 10) | (it0 << 5) | it1;
-}
 
 struct Profile {
   const double *z, *p, *t, *q, *k;
@@ -579,281 +543,3 @@ __global__ void scan_kernel(const int *nlos, int n, int64_t *off) {
   if (tid == nt - 1) off[n] = part[nt - 1];
 }
 
-// ------------------------------------------------------------- EGA + RT --
-
-
-// Continuum extinction of one channel at one LOS point
-// (src/forwardmodel.c:120-152 with src/continua.c:5-2049).
-__device__ __forceinline__ double continua(const jsc_dev_model &m,
-                                           const jsc_run_cfg &cfg,
-                                           const jsc_ctm_coef &c, double nu,
-                                           double kwin, double P, double T,
-                                           double DS, double qh2o,
-                                           const double *u) {
-  double beta = kwin;
-  if (cfg.ctm_co2) {
-    double ctm = 0;
-    if (m.ig_co2 >= 0 && c.co2_on) {
-      const double dt230 = T - 230, dt260 = T - 260, dt296 = T - 296;
-      const double ctw = dt260 * 5.050505e-4 * dt296 * c.co2_c230 -
-                         dt230 * 9.259259e-4 * dt296 * c.co2_c260 +
-                         dt230 * 4.208754e-4 * dt260 * c.co2_c296;
-      ctm = u[m.ig_co2] / JSC_AVOGADRO / 1000 * P / JSC_P0 * ctw;
-    }
-    beta += ctm / DS;
-  }
-  if (cfg.ctm_h2o) {
-    double ctm = 0;
-    if (m.ig_h2o >= 0 && c.h2o_on) {
-      const double ctwslf = c.h2o_self296 * pow(c.h2o_ratio, (296 - T) / (296 - 260));
-      const double a1 = nu * u[m.ig_h2o] * tanh(.7193876 / T * nu);
-      const double a2 = 296 / T;
-      const double a3 = P / JSC_P0 * (qh2o * ctwslf + (1 - qh2o) * c.h2o_frn) * 1e-20;
-      ctm = a1 * a2 * a3;
-    }
-    beta += ctm / DS;
-  }
-  if (cfg.ctm_n2 && c.n2_on) {
-    const double t0 = 273, tr = 296, q_n2 = 0.79;
-    const double pp = P / JSC_P0, tt = t0 / T;
-    beta += 0.1 * (pp * pp) * (tt * tt) * q_n2 * c.n2_b *
-            exp(c.n2_beta * (1 / tr - 1 / T)) *
-            (q_n2 + (1 - q_n2) * (1.294 - 0.4545 * T / tr));
-  }
-  if (cfg.ctm_o2 && c.o2_on) {
-    const double t0 = 273, tr = 296, q_o2 = 0.21;
-    const double pp = P / JSC_P0, tt = t0 / T;
-    beta += 0.1 * (pp * pp) * (tt * tt) * q_o2 * c.o2_b *
-            exp(c.o2_beta * (1 / tr - 1 / T));
-  }
-  return beta;
-}
-
-// Key of node i (u or eps).
-template <bool U>
-__device__ __forceinline__ float nkey(const jsc_node *row, int i) {
-  return U ? __ldg(&row[i].u) : __ldg(&row[i].e);
-}
-
-// locate_tbl (src/forwardmodel.c:546-565) on one table row of n >= 2
-// points.  key > x is evaluated as key > RD(x) (x rounded down to float),
-// which is exact for float keys.
-template <bool U>
-__device__ __forceinline__ int bisect_row(const jsc_node *row, int n, double x) {
-  const float xf = __double2float_rd(x);
-  const bool nan = !(x == x);
-  int ilo = 0, ihi = n - 1;
-  while (ihi > ilo + 1) {
-    const int i = (ihi + ilo) >> 1;
-    if (!nan && nkey<U>(row, i) > xf) ihi = i; else ilo = i;
-  }
-  return ilo;
-}
-
-// Same result as bisect_row for a row with strictly increasing keys,
-// found by an exponential search from the guess h: the largest i <= n-2
-// with key[i] <= x, or 0.
-template <bool U>
-__device__ __forceinline__ int search_row(const jsc_node *row, int n, double x, int h) {
-  if (!(x == x)) return n - 2;
-  const float xf = __double2float_rd(x);
-  const int last = n - 2;
-  int i = h < 0 ? 0 : (h > last ? last : h);
-  const float klo = nkey<U>(row, i), khi = nkey<U>(row, i + 1);
-  int lo, hi;
-  if (!(klo > xf)) {
-    if (khi > xf || i == last) return i;
-    lo = i + 1;
-    int step = 1;
-    while (true) {
-      const int pr = lo + step;
-      if (pr > last) { hi = last + 1; break; }
-      if (nkey<U>(row, pr) > xf) { hi = pr; break; }
-      lo = pr;
-      step <<= 1;
-    }
-  } else {
-    if (i == 0) return 0;
-    hi = i;
-    int step = 1;
-    while (true) {
-      const int pr = hi - step;
-      if (pr <= 0) { lo = 0; break; }
-      if (!(nkey<U>(row, pr) > xf)) { lo = pr; break; }
-      hi = pr;
-      step <<= 1;
-    }
-  }
-  while (hi > lo + 1) {
-    const int mid = (lo + hi) >> 1;
-    if (nkey<U>(row, mid) > xf) hi = mid; else lo = mid;
-  }
-  return lo;
-}
-
-// LIN on float table entries with the slope already in float, as the
-// reference evaluates it: y0 + slope * (x - x0), promoted to double.
-__device__ __forceinline__ double lin_node(float x0, float y0, float slope, double x) {
-  return (double)y0 + (double)slope * (x - (double)x0);
-}
-
-// Emissivity of the extended path at one (p, T) node of a table
-// (intpol_tbl_u then intpol_tbl_eps, src/forwardmodel.c:460-474): invert
-// the path emissivity x1 to a column density on the row, add the segment's
-// column, look the emissivity up again, clamp to [0, 1].
-//
-// Fast path: the row is strictly increasing, the interval [h, h+1] of the
-// previous point still brackets x1 and the extended column stays in the
-// same interval -- then the two nodes h, h+1 (one 32-byte sector) answer
-// both lookups.  Otherwise the exact searches above find the intervals.
-template <bool DIG>
-__device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, jsc_row rd,
-                                           double x1, double useg, int hint, int *jout,
-                                           unsigned long long *dig) {
-  const int n = rd.nf & 0xffff;
-  const bool strict = (rd.nf >> 16) & JSC_ROW_STRICT;
-  const jsc_node *row = nodes + rd.off;
-  const int last = n - 2;
-  int k = hint < 0 ? 0 : (hint > last ? last : hint);
-  float4 a = __ldg(reinterpret_cast<const float4 *>(row + k));
-  float4 b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
-  const float x1f = __double2float_rd(x1);
-  // bracket for x1 on eps: (e[k] <= x1 or k == 0) and (x1 < e[k+1] or k == last)
-  if (!(strict && (!(a.y > x1f) || k == 0) && (b.y > x1f || k == last) && x1 == x1)) {
-    k = strict ? search_row<false>(row, n, x1, k) : bisect_row<false>(row, n, x1);
-    a = __ldg(reinterpret_cast<const float4 *>(row + k));
-    b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
-  }
-  const double x2 = lin_node(a.y, a.x, a.z, x1) + useg;
-  const float x2f = __double2float_rd(x2);
-  int j = k;
-  if (!(strict && (!(a.x > x2f) || k == 0) && (b.x > x2f || k == last) && x2 == x2)) {
-    j = strict ? search_row<true>(row, n, x2, k) : bisect_row<true>(row, n, x2);
-    if (j != k) a = __ldg(reinterpret_cast<const float4 *>(row + j));
-  }
-  if (DIG) *dig = (*dig * 1000003ull + (unsigned long long)k) * 1000003ull + (unsigned long long)j;
-  *jout = j;
-  return jsc_clamp01(lin_node(a.x, a.y, a.w, x2));
-}
-
-// One thread per (ray, channel).  The path state of every emitter lives in
-// registers (GMAX >= ng, the emitter loop is unrolled so the lookups of
-// different emitters overlap); LOS records are read by all threads of a
-// ray (broadcast loads).
-template <int GMAX, bool DIG, int BLK, int MINB>
-__global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
-  const jsc_dev_model &m = A.m;
-  const int nd = m.nd, ng = m.ng;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = tid / A.ndp;
-  const int d = tid - r * A.ndp;
-  if (r >= A.n_rays || d >= nd) return;
-
-  // per-channel constants
-  const int w = m.window[d];
-  const bool has_w = w < m.nw;
-  const jsc_ctm_coef cc = m.ctm[d];
-  const double nu = m.nu[d];
-  const double *__restrict__ pb = m.planck_b + (size_t)d * JSC_NPLANCK;
-  const double *__restrict__ ps = m.planck_s + (size_t)d * JSC_NPLANCK;
-  const jsc_row *__restrict__ rows_d = m.rows + (size_t)d * ng * (TBLNPMAX * TBLNTMAX);
-  unsigned okmask = 0;
-  for (int g = 0; g < ng && g < GMAX; g++)
-    if (m.tab_grid[d * ng + g] >= 0) okmask |= 1u << g;
-
-  double tp[GMAX];
-  int hint[GMAX];
-#pragma unroll
-  for (int g = 0; g < GMAX; g++) {
-    tp[g] = 1;
-    hint[g] = 0;
-  }
-  double rad = 0, tau = 1;
-  unsigned long long dig = 0;
-  unsigned n_ega = 0;
-  const int np = A.nlos[r];
-  const double *__restrict__ rec = A.pts + (size_t)A.los_off[r] * A.W;
-
-  for (int ip = 0; ip < np; ip++, rec += A.W) {
-    const double P = rec[REC_P], T = rec[REC_T], DS = rec[REC_DS];
-    const int itp = (int)rec[REC_PLK];
-    int code = (int)rec[REC_GRID];
-    double tau_gas = 1;
-#pragma unroll
-    for (int g = 0; g < GMAX; g++) {
-      if (g >= ng) break;
-      double eps = 0;
-      const double tpg = tp[g];
-      if (!((okmask >> g) & 1u)) {
-        eps = 0;
-      } else if (tpg < 1e-9) {
-        eps = 1;
-      } else {
-        const int gid = A.single_grid ? 0 : m.tab_grid[d * ng + g];
-        if (!A.single_grid)
-          code = grid_code(m.grid_np[gid], m.grid_p + (size_t)gid * TBLNPMAX,
-                           m.grid_nt + (size_t)gid * TBLNPMAX,
-                           m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX, P, T);
-        if (code & (1 << 16)) {
-          const int ipr = (code >> 10) & 63, it0 = (code >> 5) & 31, it1 = code & 31;
-          const jsc_row *rw = rows_d + (size_t)g * (TBLNPMAX * TBLNTMAX);
-          const jsc_row r00 = rw[ipr * TBLNTMAX + it0];
-          const jsc_row r01 = rw[ipr * TBLNTMAX + it0 + 1];
-          const jsc_row r10 = rw[(ipr + 1) * TBLNTMAX + it1];
-          const jsc_row r11 = rw[(ipr + 1) * TBLNTMAX + it1 + 1];
-          if ((r00.nf & 0xffff) >= 2 && (r01.nf & 0xffff) >= 2 &&
-              (r10.nf & 0xffff) >= 2 && (r11.nf & 0xffff) >= 2) {
-            const double x1 = 1 - tpg, useg = rec[REC_K + m.nw + g];
-            if (DIG) dig = dig * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
-            int j00, jx;
-            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, hint[g], &j00, &dig);
-            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, hint[g], &jx, &dig);
-            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, hint[g], &jx, &dig);
-            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, hint[g], &jx, &dig);
-            hint[g] = j00;
-            const double *gp = m.grid_p + (size_t)gid * TBLNPMAX;
-            const double *gt = m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX;
-            double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
-                                            gt[ipr * TBLNTMAX + it0 + 1], e01, T));
-            const double eb = jsc_clamp01(jsc_lin(gt[(ipr + 1) * TBLNTMAX + it1], e10,
-                                                  gt[(ipr + 1) * TBLNTMAX + it1 + 1], e11, T));
-            ea = jsc_clamp01(jsc_lin(gp[ipr], ea, gp[ipr + 1], eb, P));
-            eps = 1 - (1 - ea) / tpg;
-            n_ega++;
-          }
-        }
-      }
-      tp[g] = tpg * (1 - eps);
-      tau_gas *= (1 - eps);
-    }
-    const double beta = continua(m, A.cfg, cc, nu, has_w ? rec[REC_K + w] : 0.0, P, T, DS,
-                                 rec[REC_QH2O], rec + REC_K + m.nw);
-    const double src = pb[itp] + ps[itp] * (T - planck_temp(itp));
-    if (tau_gas > 0) {
-      // clear air, or aerosol/cloud extinction without a scattering source
-      // (src/forwardmodel.c:365-389)
-      const double af = rec[REC_AF];
-      double eps;
-      if (A.cfg.sca_n == 0 || af == 0) {
-        eps = 1 - tau_gas * exp(-1. * beta * DS);
-      } else {
-        const int ia = (int)rec[REC_AI];
-        const double bx = A.beta[(A.cfg.sca_ext_beta_a ? 2 : 0) * A.aero_nl * nd + ia * nd + d];
-        eps = 1 - tau_gas * exp(-1. * (beta + af * bx) * DS);
-      }
-      rad += src * eps * tau;
-      tau *= (1 - eps);
-    }
-  }
-  const double ts = A.tsurf[r];
-  if (ts > 0) {
-    const int its = planck_index(ts);
-    rad += (pb[its] + ps[its] * (ts - planck_temp(its))) * tau;
-  }
-  A.rad[(size_t)r * nd + d] = rad;
-  A.tau[(size_t)r * nd + d] = tau;
-  if (DIG) A.digest[(size_t)r * nd + d] = dig;
-  const unsigned mask = __activemask();
-  const unsigned tot = __reduce_add_sync(mask, n_ega);
-  if ((threadIdx.x & 31) == __ffs(mask) - 1) atomicAdd(&A.counters[1], (unsigned long long)tot);
-}

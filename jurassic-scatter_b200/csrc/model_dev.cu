@@ -2,7 +2,7 @@
 //
 // Device layout (all in HBM, read-only during a forward model):
 //  * (p, T) grids, deduplicated across tables (most table sets share one);
-//  * a row descriptor per (channel, emitter, p level, T) slot;
+//  * a row descriptor per (p level, T, emitter, channel) slot;
 //  * one 16-byte node per table point: u, eps and both slopes of the
 //    interval to the next point, computed on the device with the same IEEE
 //    single-precision operations the reference's LIN evaluates at run time,
@@ -130,38 +130,42 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
     }
   }
 
-  // Row descriptors and node offsets.
+  // Row descriptors and node offsets, ordered (p level, temperature,
+  // emitter, channel): the threads of a warp (neighbouring channels) look
+  // up the same (p, T) node of the same emitter at the same time, so their
+  // descriptors are contiguous and their nodes lie within a few hundred KB.
   std::vector<jsc_row> rows(nslots > 0 ? nslots : 1);
   std::vector<int64_t> row_pt(nslots > 0 ? nslots : 1, 0);
   int64_t niv = 0;
-  for (int ti = 0; ti < ntab; ti++) {
-    const jsc_host_table *t = &ht->tab[ti];
-    for (int ip = 0; ip < TBLNPMAX; ip++)
-      for (int it = 0; it < TBLNTMAX; it++) {
-        size_t s = (size_t)ti * slots_per_tab + (size_t)ip * TBLNTMAX + it;
-        rows[s].off = 0;
-        rows[s].nf = 0;
-        if (t->np < 2 || ip >= t->np || it >= t->nt[ip]) continue;
-        int n = t->nu[ip][it];
-        if (n < 0) n = 0;
-        int64_t pt = t->off[ip][it];
-        int strict = 1;
-        for (int k = 0; k + 1 < n; k++)
-          if (!(ht->u[pt + k] < ht->u[pt + k + 1]) ||
-              !(ht->eps[pt + k] < ht->eps[pt + k + 1])) {
-            strict = 0;
-            break;
+  for (int ip = 0; ip < TBLNPMAX; ip++)
+    for (int it = 0; it < TBLNTMAX; it++)
+      for (int ig = 0; ig < ng; ig++)
+        for (int id = 0; id < nd; id++) {
+          const int ti = id * ng + ig;
+          const jsc_host_table *t = &ht->tab[ti];
+          size_t s = (((size_t)ip * TBLNTMAX + it) * ng + ig) * nd + id;
+          rows[s].off = 0;
+          rows[s].nf = 0;
+          if (t->np < 2 || ip >= t->np || it >= t->nt[ip]) continue;
+          int n = t->nu[ip][it];
+          if (n < 0) n = 0;
+          int64_t pt = t->off[ip][it];
+          int strict = 1;
+          for (int k = 0; k + 1 < n; k++)
+            if (!(ht->u[pt + k] < ht->u[pt + k + 1]) ||
+                !(ht->eps[pt + k] < ht->eps[pt + k + 1])) {
+              strict = 0;
+              break;
+            }
+          rows[s].off = (int)niv;
+          rows[s].nf = n | (strict ? (JSC_ROW_STRICT << 16) : 0);
+          row_pt[s] = pt;
+          if (n >= 2) niv += n;
+          if (niv > 0x7fffffff) {
+            jsc_set_error(JSC_ERR_TABLE, "emissivity tables exceed 2^31 points");
+            return JSC_ERR_TABLE;
           }
-        rows[s].off = (int)niv;
-        rows[s].nf = n | (strict ? (JSC_ROW_STRICT << 16) : 0);
-        row_pt[s] = pt;
-        if (n >= 2) niv += n;
-        if (niv > 0x7fffffff) {
-          jsc_set_error(JSC_ERR_TABLE, "emissivity tables exceed 2^31 points");
-          return JSC_ERR_TABLE;
         }
-      }
-  }
 
   int st;
   if ((st = upload(&m->d_grid_np, g_np.data(), g_np.size()))) return st;
