@@ -274,6 +274,40 @@ int jsc_batch_download(jsc_batch *b, const jsc_batch_output *out, void *stream);
 int jsc_formod_batch(jsc_model *m, const ctl_t *ctl, const jsc_batch_input *in,
                      const jsc_batch_output *out, void *stream);
 
+/* jsc_formod_batch without any device or host allocation.  No counterpart
+ * in the reference: its formod (src/forwardmodel.c:15-116) keeps the line
+ * of sight in a heap-allocated los_t; this entry point exists for callers
+ * that must not allocate device memory while they run the forward model
+ * (see below).
+ *
+ * Same arguments, same clear-air kernels and launch variant, same results
+ * as jsc_formod_batch; host inputs and outputs as there.  Every per-call
+ * device buffer (inputs, hydrostatic pressures, LOS records, outputs) is
+ * carved from one static device array of JSC_NOALLOC_SCRATCH_BYTES per
+ * device, so the call neither allocates nor frees (jsc_formod_batch
+ * allocates and frees a whole batch per call, and cudaFree waits for the
+ * whole device).  The model (its tables) must exist already.
+ *
+ * Limits: ctl->sca_n must be 0 (clear air); the inputs, outputs and
+ * (4 + 8 + nw + ng) doubles per LOS point must fit the scratch, e.g.
+ * about 390,000 LOS points for 8 emitters and one window.  A larger input
+ * returns JSC_ERR_ARG with the sizes in jsc_last_error_message(), before
+ * any LOS record is written.
+ *
+ * Set-up: the first call on a device looks up the scratch's device address
+ * (cudaGetSymbolAddress, with the model's device current) and caches it;
+ * make that first call before any stream capture on the device.
+ *
+ * Concurrency: the scratch is one per device, so two calls whose GPU work
+ * overlaps would race on it.  The library holds a per-device lock for the
+ * whole call and every call waits for its stream before it returns, so
+ * calls from several host threads run one after another.  After a call that
+ * returned JSC_ERR_CUDA, synchronise the stream before the next call. */
+#define JSC_NOALLOC_SCRATCH_BYTES (64u << 20)
+int jsc_formod_batch_noalloc(jsc_model *m, const ctl_t *ctl,
+                             const jsc_batch_input *in,
+                             const jsc_batch_output *out, void *stream);
+
 /* Per-kernel timing of the last jsc_batch_run (CUDA events on its stream).
  * kernel: "hydrostatic", "raytrace", "ega_rt".  Returns milliseconds, or a
  * negative value when timing is off or the kernel did not run. */

@@ -36,7 +36,7 @@ struct AtmArgs {
 };
 
 // Hydrostatic balance and altitude range of each profile.
-__global__ void hydro_kernel(AtmArgs a) {
+static __global__ void hydro_kernel(AtmArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n_atm) return;
   const int lo = a.off[i], n = a.off[i + 1] - lo;
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(128) refine_kernel(RefineArgs A) {
 }
 
 // Exclusive scan of nlos into off[0..n] by one block.
-__global__ void scan_kernel(const int *nlos, int n, int64_t *off) {
+static __global__ void scan_kernel(const int *nlos, int n, int64_t *off) {
   __shared__ int64_t part[1024];
   const int tid = threadIdx.x, nt = blockDim.x;
   const int chunk = (n + nt - 1) / nt;

@@ -204,5 +204,36 @@ def formod_batch(ctl, inp, device=0, model=None, digest=False, aero=None):
             m.close()
 
 
+def formod_batch_noalloc(ctl, inp, model, stream=None):
+    """jsc_formod_batch_noalloc: the clear-air batch forward model with every
+    per-call device buffer taken from the library's static scratch (no device
+    allocation).  model: a Model for ctl.  Returns rad/tau/tp*/nlos."""
+    a = {k: None if inp.get(k) is None else np.ascontiguousarray(inp[k], dtype=np.float64)
+         for k in ("z", "lon", "lat", "p", "t", "q", "k", "time", "obsz", "obslon",
+                   "obslat", "vpz", "vplon", "vplat")}
+    a["atm_off"] = np.ascontiguousarray(inp["atm_off"], dtype=np.int32)
+    a["ray_atm"] = np.ascontiguousarray(inp["ray_atm"], dtype=np.int32)
+    bi = L.BatchInput()
+    bi.n_atm = len(a["atm_off"]) - 1
+    bi.n_levels = len(a["z"])
+    bi.n_rays = len(a["ray_atm"])
+    bi.atm_off = _iptr(a["atm_off"])
+    bi.ray_atm = _iptr(a["ray_atm"])
+    for k in ("z", "lon", "lat", "p", "t", "q", "k", "time", "obsz", "obslon",
+              "obslat", "vpz", "vplon", "vplat"):
+        setattr(bi, k, _dptr(a[k]))
+    nr, nd = bi.n_rays, ctl.nd
+    out = {"rad": np.empty((nr, nd)), "tau": np.empty((nr, nd)), "tpz": np.empty(nr),
+           "tplon": np.empty(nr), "tplat": np.empty(nr), "nlos": np.empty(nr, np.int32)}
+    bo = L.BatchOutput()
+    bo.rad, bo.tau = _dptr(out["rad"]), _dptr(out["tau"])
+    bo.tpz, bo.tplon, bo.tplat = _dptr(out["tpz"]), _dptr(out["tplon"]), _dptr(out["tplat"])
+    bo.nlos = _iptr(out["nlos"])
+    L.check(L.load().jsc_formod_batch_noalloc(model.h, C.byref(ctl), C.byref(bi),
+                                              C.byref(bo), stream),
+            "jsc_formod_batch_noalloc")
+    return out
+
+
 def launch_count():
     return int(L.load().jsc_launch_count())

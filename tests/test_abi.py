@@ -41,6 +41,7 @@ def test_ctypes_layout_matches_reference():
 def _header_functions():
     src = open(os.path.join(REPO, "include", "jurassic_b200.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"^\s*#.*$", "", src, flags=re.M)  # preprocessor lines
     names = re.findall(r"\b(\w+)\s*\([^;{]*\)\s*;", src)
     return sorted(set(n for n in names if n not in ("sizeof",)))
 
