@@ -309,7 +309,8 @@ int jsc_formod_batch_noalloc(jsc_model *m, const ctl_t *ctl,
                              const jsc_batch_output *out, void *stream);
 
 /* Per-kernel timing of the last jsc_batch_run (CUDA events on its stream).
- * kernel: "hydrostatic", "raytrace", "ega_rt".  Returns milliseconds, or a
+ * kernel: "hydrostatic", "raytrace", "scatter" (scattering sources: the
+ * secondary and solar pencils and the source integrals), "ega_rt".  Returns milliseconds, or a
  * negative value when timing is off or the kernel did not run. */
 void jsc_batch_set_timing(jsc_batch *b, int on);
 double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel);
@@ -325,6 +326,14 @@ double jsc_batch_variant_ms(const jsc_batch *b, int variant);
 /* Aerosol/cloud layers and optical properties for runs with ctl->sca_n > 0
  * (the aero_t that read_aero + get_opt_prop fill, src/scatter.c:330,583). */
 int jsc_batch_set_aero(jsc_batch *b, const aero_t *aero);
+
+/* Secondary pencils per scattering point of the thermal scattering source
+ * (srcfunc_sca_1d, src/scatter.c:666-807, which casts 28).  nalpha: an even
+ * count from 10 to 28; the zenith angles follow the reference's
+ * construction (0, a Fibonacci-spaced fan, 83..90 degrees in 1-degree
+ * steps, the mirrored fan, 180 degrees) with fewer fan steps.  Applies to
+ * every scattering order of the batch's later runs. */
+int jsc_batch_set_nalpha(jsc_batch *b, int nalpha);
 
 /* Per-(ray, channel) checksum of every emissivity-table index the EGA
  * interpolation selected in the last run, for parity checks against the

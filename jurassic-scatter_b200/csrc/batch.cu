@@ -7,6 +7,9 @@
 
 #include "kernels.cuh"
 #include "ega_kernel.cuh"
+#include "scatter.cuh"
+
+static int sca_alpha(double *alpha, int nalpha);
 
 static void batch_free_los(jsc_batch *b) {
   cudaFree(b->d_geo);
@@ -55,6 +58,17 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   cudaFree(b->d_los_off_b);
   cudaFree(b->d_geo_b);
   cudaFree(b->d_pts_b);
+  cudaFree(b->d_nsp);
+  cudaFree(b->d_sp_off);
+  cudaFree(b->d_sp);
+  cudaFree(b->d_sp_atm);
+  cudaFree(b->d_src);
+  cudaFree(b->d_theta2);
+  cudaFree(b->d_planck_sun);
+  jsc_batch_destroy(b->child);
+  jsc_batch_destroy(b->sun_child);
+  free(b->h_aero);
+  free(b->ctl);
   if (b->h_total) cudaFreeHost(b->h_total);
   for (int i = 0; i < 2 * JSC_T_N; i++)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
@@ -127,6 +141,12 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   if (!st) st = batch_alloc_los(b, max_seg > 0 ? max_seg : (int64_t)max_rays * 512);
   b->ega_variant = -1;
   for (int v = 0; v < 8; v++) b->ega_variant_ms[v] = -1;
+  b->depth = ctl->sca_n > 0 ? ctl->sca_mult : 0;
+  b->nalpha = JSC_NALPHA_REF;
+  sca_alpha(b->alpha, b->nalpha);
+  b->ctl = (ctl_t *)malloc(sizeof(ctl_t));
+  if (!b->ctl) st = st ? st : JSC_ERR_NOMEM;
+  else memcpy(b->ctl, ctl, sizeof(ctl_t));
   if (!st && cudaMallocHost((void **)&b->h_total, sizeof(int64_t)) != cudaSuccess) {
     jsc_set_error(JSC_ERR_NOMEM, "pinned host allocation");
     st = JSC_ERR_NOMEM;
@@ -138,6 +158,50 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
     return st;
   }
   *out = b;
+  return JSC_OK;
+}
+
+// Zenith angles of the secondary pencils: 0, a Fibonacci-spaced fan down to
+// the horizon, 1-degree steps from 83 to 90 degrees, the mirrored fan up,
+// and pi (src/scatter.c:695-715 for 28 pencils; any even count from 10 to
+// 28 gives increasing angles the same way).
+static int sca_alpha(double *alpha, int nalpha) {
+  if (nalpha < 10 || nalpha > JSC_NALPHA_REF || (nalpha & 1)) return JSC_ERR_ARG;
+  int n1 = 1, n2 = 2;
+  double midang = 83, up = 92, down = 81, step = 1 + 2;
+  alpha[0] = 0;
+  for (int ir = nalpha / 2 - 4; ir < nalpha / 2 + 4; ++ir) {
+    alpha[ir] = midang * M_PI / 180.;
+    midang++;
+  }
+  for (int ir = 0; ir < nalpha / 2 - 5; ++ir) {
+    alpha[nalpha / 2 + ir + 4] = up * M_PI / 180.;
+    alpha[nalpha / 2 - ir - 5] = down * M_PI / 180.;
+    up += step;
+    down -= step;
+    if (step < 13) {
+      step = (double)n1 + (double)n2;
+      n1 = n2;
+      n2 = (int)step;
+    }
+  }
+  alpha[nalpha - 1] = M_PI;
+  for (int i = 0; i + 1 < nalpha; i++)
+    if (!(alpha[i] < alpha[i + 1])) return JSC_ERR_ARG;
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_set_nalpha(jsc_batch *b, int nalpha) {
+  if (!b || sca_alpha(b->alpha, nalpha)) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_set_nalpha: %d secondary pencils (even, 10..%d)",
+                  nalpha, JSC_NALPHA_REF);
+    if (b) sca_alpha(b->alpha, b->nalpha);
+    return JSC_ERR_ARG;
+  }
+  b->nalpha = nalpha;
+  // child batches are sized per pencil count: rebuild on the next run
+  jsc_batch_destroy(b->child);
+  b->child = nullptr;
   return JSC_OK;
 }
 
@@ -228,10 +292,15 @@ extern "C" int jsc_batch_set_aero(jsc_batch *b, const aero_t *aero) {
     jsc_set_error(st, "jsc_batch_set_aero: device upload failed");
     return st;
   }
+  if (!b->h_aero && !(b->h_aero = (aero_t *)malloc(sizeof(aero_t)))) return JSC_ERR_NOMEM;
+  if (b->h_aero != aero) memcpy(b->h_aero, aero, sizeof(aero_t));
   b->aero_nl = nl;
   b->n_alti = jl;
   b->altimax = amax;
   b->altimin = amin;
+  // child batches (secondary and solar pencils) see the same layers
+  for (jsc_batch *c : {b->child, b->sun_child})
+    if (c && (st = jsc_batch_set_aero(c, aero))) return st;
   if (!b->d_nlos_b) {
     if ((st = jsc_dmalloc(&b->d_nlos_b, (size_t)b->max_rays))) return st;
     if ((st = jsc_dmalloc(&b->d_los_off_b, (size_t)b->max_rays + 1))) return st;
@@ -339,42 +408,10 @@ static void ev_record(jsc_batch *b, int k, int end, cudaStream_t s) {
   if (end) b->ran[k] = 1;
 }
 
-extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
-  if (!b) return JSC_ERR_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
+static void fill_ray_args(const jsc_batch *b, RayArgs &ra) {
   const jsc_model *m = b->m;
   const int nr = b->n_rays;
-  JSC_CUDA_TRY(cudaSetDevice(m->device));
-  (void)cudaGetLastError();  // launch checks below report this run's errors only
-  for (int k = 0; k < JSC_T_N; k++) b->ran[k] = 0;
-  JSC_CUDA_TRY(cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s));
-  JSC_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(unsigned long long), s));
-
-  AtmArgs aa;
-  aa.n_atm = b->n_atm;
-  aa.n_levels = b->n_levels;
-  aa.ng = b->cfg.ng;
-  aa.nw = b->cfg.nw;
-  aa.ig_h2o = m->dv.ig_h2o;
-  aa.off = b->d_atm_off;
-  aa.z = b->d_z;
-  aa.lon = b->d_lon;
-  aa.lat = b->d_lat;
-  aa.p_in = b->d_p_in;
-  aa.t = b->d_t;
-  aa.q = b->d_q;
-  aa.k = b->d_k;
-  aa.p = b->d_p;
-  aa.zmin = b->d_zmin;
-  aa.zmax = b->d_zmax;
-  aa.hydz = b->cfg.hydz;
-  ev_record(b, JSC_T_HYDRO, 0, s);
-  hydro_kernel<<<(b->n_atm + 127) / 128, 128, 0, s>>>(aa);
-  JSC_LAUNCH_CHECK();
-  ev_record(b, JSC_T_HYDRO, 1, s);
-  if (nr == 0) return JSC_OK;
-
-  RayArgs ra;
+  memset(&ra, 0, sizeof(ra));
   ra.n_rays = nr;
   ra.ng = b->cfg.ng;
   ra.nw = b->cfg.nw;
@@ -405,9 +442,246 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   ra.tsurf = b->d_tsurf;
   ra.tp = b->d_tp;
   ra.status = b->d_status;
-  ra.grid_np = 0;
-  ra.grid_p = ra.grid_t = nullptr;
-  ra.grid_nt = nullptr;
+}
+
+static int batch_run(jsc_batch *b, cudaStream_t s);
+
+// OR a child batch's device status into its parent's.
+static __global__ void status_or_kernel(unsigned *dst, const unsigned *src) { *dst |= *src; }
+
+// A child batch for the secondary (depth - 1) or solar (depth 0) pencils
+// of this batch's scattering points, with room for max_rays rays.
+static int ensure_child(jsc_batch *b, jsc_batch **pc, int max_rays, int depth) {
+  jsc_batch *c = *pc;
+  if (c && c->max_rays >= max_rays) return JSC_OK;
+  jsc_batch_destroy(c);
+  *pc = nullptr;
+  int st = jsc_batch_create(b->m, b->ctl, b->max_atm, b->max_levels, max_rays,
+                            (int64_t)max_rays * 128, &c);
+  if (st) return st;
+  c->cfg.hydz = -1;  // profiles arrive hydrostatically balanced
+  c->depth = depth;
+  c->nalpha = b->nalpha;
+  memcpy(c->alpha, b->alpha, sizeof(b->alpha));
+  c->ega_variant = b->ega_variant;
+  if ((st = jsc_batch_set_aero(c, b->h_aero))) {
+    jsc_batch_destroy(c);
+    return st;
+  }
+  *pc = c;
+  return JSC_OK;
+}
+
+// The child sees this batch's profiles, with the balanced pressures.
+static int copy_profiles(const jsc_batch *b, jsc_batch *c, cudaStream_t s) {
+  const size_t nl = (size_t)b->n_levels;
+  c->n_atm = b->n_atm;
+  c->n_levels = b->n_levels;
+#define D2D(dst, src, n) \
+  JSC_CUDA_TRY(cudaMemcpyAsync((dst), (src), (n) * sizeof(*(src)), cudaMemcpyDeviceToDevice, s))
+  D2D(c->d_atm_off, b->d_atm_off, (size_t)b->n_atm + 1);
+  D2D(c->d_z, b->d_z, nl);
+  D2D(c->d_lon, b->d_lon, nl);
+  D2D(c->d_lat, b->d_lat, nl);
+  D2D(c->d_p_in, b->d_p, nl);
+  D2D(c->d_t, b->d_t, nl);
+  if (b->cfg.ng > 0) D2D(c->d_q, b->d_q, nl * b->cfg.ng);
+  if (b->cfg.nw > 0) D2D(c->d_k, b->d_k, nl * b->cfg.nw);
+#undef D2D
+  return JSC_OK;
+}
+
+// Scattering points per ray and their list (src/forwardmodel.c:317-331).
+static int list_scattering_points(jsc_batch *b, cudaStream_t s) {
+  const int nr = b->n_rays;
+  int st;
+  if (!b->d_nsp) {
+    if ((st = jsc_dmalloc(&b->d_nsp, (size_t)b->max_rays))) return st;
+    if ((st = jsc_dmalloc(&b->d_sp_off, (size_t)b->max_rays + 1))) return st;
+  }
+  SpArgs sa;
+  sa.n_rays = nr;
+  sa.W = b->W;
+  sa.nlos = b->d_nlos;
+  sa.los_off = b->d_los_off;
+  sa.geo = b->d_geo;
+  sa.pts = b->d_pts;
+  sa.time = b->d_ray;
+  sa.ray_atm = b->d_ray_atm;
+  sa.nsp = b->d_nsp;
+  sa.sp_off = b->d_sp_off;
+  sa.sp = nullptr;
+  sa.sp_atm = nullptr;
+  sp_count_kernel<<<(nr + 127) / 128, 128, 0, s>>>(sa);
+  JSC_LAUNCH_CHECK();
+  scan_kernel<<<1, 1024, 0, s>>>(b->d_nsp, nr, b->d_sp_off);
+  JSC_LAUNCH_CHECK();
+  JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, b->d_sp_off + nr, sizeof(int64_t),
+                               cudaMemcpyDeviceToHost, s));
+  JSC_CUDA_TRY(cudaStreamSynchronize(s));
+  b->n_sp = *b->h_total;
+  if (b->n_sp > b->max_sp) {
+    cudaFree(b->d_sp);
+    cudaFree(b->d_sp_atm);
+    cudaFree(b->d_src);
+    b->d_sp = b->d_src = nullptr;
+    b->d_sp_atm = nullptr;
+    b->max_sp = 0;
+    const int64_t n = b->n_sp + b->n_sp / 4 + 256;
+    if ((st = jsc_dmalloc(&b->d_sp, (size_t)n * JSC_SP_REC))) return st;
+    if ((st = jsc_dmalloc(&b->d_sp_atm, (size_t)n))) return st;
+    if ((st = jsc_dmalloc(&b->d_src, (size_t)n * b->cfg.nd))) return st;
+    b->max_sp = n;
+  }
+  if (b->n_sp == 0) return JSC_OK;
+  sa.sp = b->d_sp;
+  sa.sp_atm = b->d_sp_atm;
+  sp_list_kernel<<<(nr + 127) / 128, 128, 0, s>>>(sa);
+  JSC_LAUNCH_CHECK();
+  return JSC_OK;
+}
+
+// Scattering points per chunk: the secondary pencils of a chunk run as one
+// child batch of chunk * nalpha rays.
+static const int64_t kScatterChunk = 8192;
+
+// Scattering source of every scattering point (srcfunc_sca,
+// src/scatter.c:643-662): thermal radiation from the secondary pencils,
+// then the solar term.
+static int scatter_sources(jsc_batch *b, cudaStream_t s) {
+  int st = list_scattering_points(b, s);
+  if (st || b->n_sp == 0) return st;
+  const int nd = b->cfg.nd, na = b->nalpha;
+  const int64_t chunk = b->n_sp < kScatterChunk ? b->n_sp : kScatterChunk;
+  if ((st = ensure_child(b, &b->child, (int)(chunk * na), b->depth - 1))) return st;
+  if ((st = ensure_child(b, &b->sun_child, (int)chunk, 0))) return st;
+  if (!b->d_planck_sun) {
+    double h[NDMAX];
+    for (int id = 0; id < nd; id++) h[id] = planck(JSC_TSUN, b->m->nu[id]);
+    if ((st = jsc_dmalloc(&b->d_planck_sun, (size_t)nd))) return st;
+    JSC_CUDA_TRY(cudaMemcpy(b->d_planck_sun, h, (size_t)nd * sizeof(double),
+                            cudaMemcpyHostToDevice));
+  }
+  if (b->n_theta2 < b->sun_child->max_rays) {
+    cudaFree(b->d_theta2);
+    b->d_theta2 = nullptr;
+    b->n_theta2 = 0;
+    if ((st = jsc_dmalloc(&b->d_theta2, (size_t)b->sun_child->max_rays))) return st;
+    b->n_theta2 = b->sun_child->max_rays;
+  }
+  if ((st = copy_profiles(b, b->child, s))) return st;
+  if ((st = copy_profiles(b, b->sun_child, s))) return st;
+
+  jsc_batch *c = b->child, *sc = b->sun_child;
+  const size_t shmem = ((size_t)JSC_NTH_SCA * nd + (size_t)na * nd + 4 * JSC_NTH_SCA +
+                        (JSC_INT_THREADS / 32) * JSC_INT_CH) * sizeof(double);
+  if (shmem > 48 * 1024)
+    JSC_CUDA_TRY(cudaFuncSetAttribute(sp_integral_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+  for (int64_t c0 = 0; c0 < b->n_sp; c0 += chunk) {
+    const int n = (int)((b->n_sp - c0) < chunk ? (b->n_sp - c0) : chunk);
+    // Secondary pencils (src/scatter.c:717-736).
+    SpawnArgs pa;
+    pa.n_pts = n;
+    pa.nalpha = na;
+    pa.sp = b->d_sp + c0 * JSC_SP_REC;
+    pa.sp_atm = b->d_sp_atm + c0;
+    memcpy(pa.alpha, b->alpha, sizeof(pa.alpha));
+    pa.ray_atm = c->d_ray_atm;
+    pa.ray = c->d_ray;
+    c->n_rays = n * na;
+    sp_spawn_kernel<<<(n * na + 127) / 128, 128, 0, s>>>(pa);
+    JSC_LAUNCH_CHECK();
+    if ((st = batch_run(c, s))) return st;
+    status_or_kernel<<<1, 1, 0, s>>>(b->d_status, c->d_status);
+    JSC_LAUNCH_CHECK();
+    // Source integral over the sphere (src/scatter.c:737-805).
+    IntegralArgs ia;
+    ia.n_pts = n;
+    ia.nalpha = na;
+    ia.nd = nd;
+    ia.nl = b->aero_nl;
+    ia.sp = pa.sp;
+    memcpy(ia.alpha, b->alpha, sizeof(ia.alpha));
+    ia.rad = c->d_rad;
+    ia.phase = b->d_phase;
+    ia.src = b->d_src + c0 * nd;
+    sp_integral_kernel<<<n, JSC_INT_THREADS, shmem, s>>>(ia);
+    JSC_LAUNCH_CHECK();
+    // Solar term (src/scatter.c:899-995).
+    SunArgs sn;
+    fill_ray_args(b, sn.ra);
+    sn.n_pts = n;
+    sn.sp = pa.sp;
+    sn.sp_atm = pa.sp_atm;
+    sn.n_alti = b->n_alti;
+    sn.altimax = b->altimax;
+    sn.altimin = b->altimin;
+    sn.alti = b->d_aero + 3 * NLMAX;
+    sn.ray_atm = sc->d_ray_atm;
+    sn.ray = sc->d_ray;
+    sn.theta2 = b->d_theta2;
+    sc->n_rays = n;
+    sun_kernel<<<(n + 127) / 128, 128, 0, s>>>(sn);
+    JSC_LAUNCH_CHECK();
+    if ((st = batch_run(sc, s))) return st;
+    status_or_kernel<<<1, 1, 0, s>>>(b->d_status, sc->d_status);
+    JSC_LAUNCH_CHECK();
+    SunAddArgs aa;
+    aa.n_pts = n;
+    aa.nd = nd;
+    aa.sp = pa.sp;
+    aa.theta2 = b->d_theta2;
+    aa.tau = sc->d_tau;
+    aa.phase = b->d_phase;
+    aa.planck_sun = b->d_planck_sun;
+    aa.src = b->d_src + c0 * nd;
+    sun_add_kernel<<<(n * nd + 127) / 128, 128, 0, s>>>(aa);
+    JSC_LAUNCH_CHECK();
+  }
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
+  if (!b) return JSC_ERR_ARG;
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  (void)cudaGetLastError();  // launch checks below report this run's errors only
+  return batch_run(b, (cudaStream_t)stream);
+}
+
+static int batch_run(jsc_batch *b, cudaStream_t s) {
+  const jsc_model *m = b->m;
+  const int nr = b->n_rays;
+  for (int k = 0; k < JSC_T_N; k++) b->ran[k] = 0;
+  JSC_CUDA_TRY(cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s));
+  JSC_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(unsigned long long), s));
+
+  AtmArgs aa;
+  aa.n_atm = b->n_atm;
+  aa.n_levels = b->n_levels;
+  aa.ng = b->cfg.ng;
+  aa.nw = b->cfg.nw;
+  aa.ig_h2o = m->dv.ig_h2o;
+  aa.off = b->d_atm_off;
+  aa.z = b->d_z;
+  aa.lon = b->d_lon;
+  aa.lat = b->d_lat;
+  aa.p_in = b->d_p_in;
+  aa.t = b->d_t;
+  aa.q = b->d_q;
+  aa.k = b->d_k;
+  aa.p = b->d_p;
+  aa.zmin = b->d_zmin;
+  aa.zmax = b->d_zmax;
+  aa.hydz = b->cfg.hydz;
+  ev_record(b, JSC_T_HYDRO, 0, s);
+  hydro_kernel<<<(b->n_atm + 127) / 128, 128, 0, s>>>(aa);
+  JSC_LAUNCH_CHECK();
+  ev_record(b, JSC_T_HYDRO, 1, s);
+  if (nr == 0) return JSC_OK;
+
+  RayArgs ra;
+  fill_ray_args(b, ra);
   if (m->n_grid == 1) {
     int gnp = 0;
     JSC_CUDA_TRY(cudaMemcpy(&gnp, m->d_grid_np, sizeof(int), cudaMemcpyDeviceToHost));
@@ -416,7 +690,6 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
     ra.grid_nt = m->d_grid_nt;
     ra.grid_t = m->d_grid_t;
   }
-
   const bool refine = b->cfg.sca_n > 0;
   if (refine && !b->d_aero) {
     jsc_set_error(JSC_ERR_ARG, "SCA_N > 0 needs jsc_batch_set_aero before jsc_batch_run");
@@ -512,6 +785,16 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   }
   ev_record(b, JSC_T_RAYTRACE, 1, s);
 
+  // Scattering source at every scattering point (srcfunc_sca), from the
+  // child batches of secondary and solar pencils.
+  const bool scattering = b->depth > 0;
+  if (scattering) {
+    ev_record(b, JSC_T_SCATTER, 0, s);
+    int st = scatter_sources(b, s);
+    if (st) return st;
+    ev_record(b, JSC_T_SCATTER, 1, s);
+  }
+
   EgaArgs ea;
   ea.m = m->dv;
   ea.cfg = b->cfg;
@@ -535,6 +818,8 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   ea.digest = b->digest ? b->d_digest : nullptr;
   ea.beta = b->d_beta;
   ea.aero_nl = b->aero_nl;
+  ea.src_sca = (scattering && b->n_sp > 0) ? b->d_src : nullptr;
+  ea.sp_off = (scattering && b->n_sp > 0) ? b->d_sp_off : nullptr;
   b->last_ega = ea;
   ev_record(b, JSC_T_EGA, 0, s);
   int st = launch_ega(ea, nr, ndp, m->ng, b->ega_variant, s);
@@ -684,6 +969,7 @@ extern "C" double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel) {
   if (!b || !b->timing || !kernel) return -1;
   int k = -1;
   if (!strcmp(kernel, "hydrostatic")) k = JSC_T_HYDRO;
+  else if (!strcmp(kernel, "scatter")) k = JSC_T_SCATTER;
   else if (!strcmp(kernel, "raytrace")) k = JSC_T_RAYTRACE;
   else if (!strcmp(kernel, "ega_rt")) k = JSC_T_EGA;
   if (k < 0 || !b->ran[k]) return -1;

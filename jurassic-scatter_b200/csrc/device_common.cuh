@@ -154,6 +154,15 @@ __device__ __forceinline__ int search_row(const jsc_node *row, int n, double x, 
   return lo;
 }
 
+// The exact interval search of ega_node's slow path, kept out of line: the
+// fast path is inlined for every (emitter, node) of the unrolled EGA loop,
+// the searches are called rarely and would otherwise multiply the code size
+// (instruction-fetch stalls).
+template <bool U>
+__device__ __noinline__ int find_interval(const jsc_node *row, int n, bool strict, double x, int h) {
+  return strict ? search_row<U>(row, n, x, h) : bisect_row<U>(row, n, x);
+}
+
 // LIN on float table entries with the slope already in float, as the
 // reference evaluates it: y0 + slope * (x - x0), promoted to double.
 __device__ __forceinline__ double lin_node(float x0, float y0, float slope, double x) {
@@ -183,7 +192,7 @@ __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, j
   const float x1f = __double2float_rd(x1);
   // bracket for x1 on eps: (e[k] <= x1 or k == 0) and (x1 < e[k+1] or k == last)
   if (!(strict && (!(a.y > x1f) || k == 0) && (b.y > x1f || k == last) && x1 == x1)) {
-    k = strict ? search_row<false>(row, n, x1, k) : bisect_row<false>(row, n, x1);
+    k = find_interval<false>(row, n, strict, x1, k);
     a = __ldg(reinterpret_cast<const float4 *>(row + k));
     b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
   }
@@ -191,7 +200,7 @@ __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, j
   const float x2f = __double2float_rd(x2);
   int j = k;
   if (!(strict && (!(a.x > x2f) || k == 0) && (b.x > x2f || k == last) && x2 == x2)) {
-    j = strict ? search_row<true>(row, n, x2, k) : bisect_row<true>(row, n, x2);
+    j = find_interval<true>(row, n, strict, x2, k);
     if (j != k) a = __ldg(reinterpret_cast<const float4 *>(row + j));
   }
   if (DIG) *dig = (*dig * 1000003ull + (unsigned long long)k) * 1000003ull + (unsigned long long)j;

@@ -45,6 +45,8 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
   unsigned n_ega = 0;
   const int np = A.nlos[r];
   const double *__restrict__ rec = A.pts + (size_t)A.los_off[r] * A.W;
+  // scattering source of this ray's next scattering point
+  const double *__restrict__ ssrc = A.src_sca ? A.src_sca + (size_t)A.sp_off[r] * nd + d : nullptr;
 
   for (int ip = 0; ip < np; ip++, rec += A.W) {
     const double P = rec[REC_P], T = rec[REC_T], DS = rec[REC_DS];
@@ -103,10 +105,24 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
     const double beta = continua(m, A.cfg, cc, nu, has_w ? rec[REC_K + w] : 0.0, P, T, DS,
                                  rec[REC_QH2O], rec + REC_K + m.nw);
     const double src = pb[itp] + ps[itp] * (T - planck_temp(itp));
-    if (tau_gas > 0) {
+    const double af = rec[REC_AF];
+    if (ssrc && af > 0) {
+      // scattering point: gas, continuum and aerosol extinction, thermal
+      // source mixed with the scattering source by the single-scattering
+      // albedo of the layer (src/forwardmodel.c:317-363)
+      if (tau_gas > 0) {
+        const int ia = (int)rec[REC_AI];
+        const double be = A.beta[ia * nd + d], bs = A.beta[A.aero_nl * nd + ia * nd + d];
+        const double bext = (-1.) * log(tau_gas) / DS + beta + af * be;
+        const double eps = 1 - exp(-1 * bext * DS);
+        const double src_all = ((bext - af * bs) * src + af * bs * *ssrc) / bext;
+        rad += tau * eps * src_all;
+        tau *= exp(-1. * bext * DS);
+      }
+      ssrc += nd;
+    } else if (tau_gas > 0) {
       // clear air, or aerosol/cloud extinction without a scattering source
       // (src/forwardmodel.c:365-389)
-      const double af = rec[REC_AF];
       double eps;
       if (A.cfg.sca_n == 0 || af == 0) {
         eps = 1 - tau_gas * exp(-1. * beta * DS);

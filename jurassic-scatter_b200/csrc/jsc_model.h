@@ -52,10 +52,17 @@ struct EgaArgs {
   unsigned long long *digest;  // optional [n_rays][nd] EGA index checksums
   const double *beta;          // aerosol beta_e/beta_s/beta_a [3][nl][nd]
   int aero_nl;
+  // Scattering source at the scattering points (LOS points with aerosol
+  // factor > 0) when the batch scatters: [n_sp][nd], points of ray r from
+  // sp_off[r] on, in LOS order.  Null: extinction only.
+  const double *src_sca;
+  const int64_t *sp_off;
 };
 
 // Kernel timers of a batch.
-enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_N };
+enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_SCATTER, JSC_T_N };
+
+#define JSC_NALPHA_REF 28  // secondary pencils per scattering point (src/scatter.c:673)
 
 struct jsc_batch {
   jsc_model *m;
@@ -84,6 +91,26 @@ struct jsc_batch {
   int64_t *d_los_off_b;
   double *d_geo_b, *d_pts_b;
   int64_t max_seg_b;
+  aero_t *h_aero;           // host copy for child batches
+
+  // Scattering (depth > 0): the scattering order of this batch's rays
+  // (ctl->sca_mult for the caller's batch, one less for each generation of
+  // secondary pencils), the secondary pencils per point and their zenith
+  // angles, the scattering points and their source, and the child batches
+  // that run the secondary and the solar pencils.
+  int depth, nalpha;
+  double alpha[32];
+  int *d_nsp;               // [max_rays]
+  int64_t *d_sp_off;        // [max_rays+1]
+  double *d_sp;             // [max_sp][JSC_SP_REC]
+  int *d_sp_atm;            // [max_sp]
+  double *d_src;            // [max_sp][nd]
+  int64_t max_sp, n_sp;
+  double *d_theta2;         // [n_theta2] solar scattering angles
+  int n_theta2;
+  double *d_planck_sun;     // [nd]
+  jsc_batch *child, *sun_child;
+  ctl_t *ctl;               // copy for child batches
 
   // Line of sight.
   int *d_nlos;

@@ -139,12 +139,28 @@ __device__ __forceinline__ void emit_point(const RayArgs &A, const Profile &a,
   }
 }
 
+// Observer and view point of one ray.
+struct RayIn {
+  double obsz, obslon, obslat, vpz, vplon, vplat;
+};
+
+// What the end-tracking march reports: the surface temperature it would
+// store (-999 when the ray leaves at the top), and the geometry (z, lon,
+// lat) of the last two LOS points.
+struct RayEnd {
+  double tsurf;
+  double g[2][3];
+};
+
 // Ray march of one ray (src/lineofsight.c:5-190 without the aerosol layer
-// refinement).  COUNT pass: returns the number of LOS points.  STORE pass:
-// writes the points at los_off[r], the tangent point and surface temperature.
-template <bool STORE>
-__device__ int trace_ray(const RayArgs &A, int r) {
-  const int ai = A.ray_atm[r];
+// refinement) through profile ai.  MODE 0 (count): returns the number of LOS
+// points.  MODE 1 (store): writes the points at los_off[r], the tangent
+// point and surface temperature of ray r.  MODE 2 (ends): counts like
+// MODE 0 and reports the last two points and the surface temperature in
+// *end.
+template <int MODE>
+__device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayEnd *end) {
+  constexpr bool STORE = MODE == 1;
   const int lo = A.atm_off[ai];
   Profile a;
   a.n = A.atm_off[ai + 1] - lo;
@@ -155,15 +171,16 @@ __device__ int trace_ray(const RayArgs &A, int r) {
   a.q = A.q + lo;
   a.k = A.k + lo;
   const double zmin = A.zmin[ai], zmax = A.zmax[ai];
-  const double obsz = A.obsz[r], vpz = A.vpz[r];
+  const double obsz = in.obsz, vpz = in.vpz;
   int64_t base = 0;
   if (STORE) {
     base = A.los_off[r];
     A.tp[r] = vpz;
-    A.tp[A.n_rays + r] = A.vplon[r];
-    A.tp[2 * A.n_rays + r] = A.vplat[r];
+    A.tp[A.n_rays + r] = in.vplon;
+    A.tp[2 * A.n_rays + r] = in.vplat;
     A.tsurf[r] = -999;
   }
+  if (MODE == 2) end->tsurf = -999;
   if (obsz < zmin) {
     atomicOr(A.status, JSC_DEV_ERR_OBSERVER);
     return 0;
@@ -171,8 +188,8 @@ __device__ int trace_ray(const RayArgs &A, int r) {
   if (vpz > zmax - 0.001) return 0;
 
   double xobs[3], xvp[3], ex0[3], ex1[3], x[3], xh[3], ng[3];
-  jsc_geo2cart(obsz, A.obslon[r], A.obslat[r], xobs);
-  jsc_geo2cart(vpz, A.vplon[r], A.vplat[r], xvp);
+  jsc_geo2cart(obsz, in.obslon, in.obslat, xobs);
+  jsc_geo2cart(vpz, in.vplon, in.vplat, xvp);
   for (int i = 0; i < 3; i++) ex0[i] = xvp[i] - xobs[i];
   double norm = sqrt(ex0[0] * ex0[0] + ex0[1] * ex0[1] + ex0[2] * ex0[2]);
   for (int i = 0; i < 3; i++) ex0[i] /= norm;
@@ -193,6 +210,7 @@ __device__ int trace_ray(const RayArgs &A, int r) {
 
   int np = 0, stop = 0;
   double zprev = 0, lonprev = 0, latprev = 0, rprev = 0, rprev2 = 0, dprev = 0;
+  double ends[3][3] = {};  // MODE 2: the last three points, newest last
   while (1) {
     double ds = A.rayds;
     if (A.raydz > 0) {
@@ -249,6 +267,13 @@ __device__ int trace_ray(const RayArgs &A, int r) {
       emit_point<true>(A, a, base + np, pz, plon, plat, pp, pt, ipz, pz, raw, dsm);
     }
     np++;
+    if (MODE == 2) {
+      for (int j = 0; j < 2; j++)
+        for (int c = 0; c < 3; c++) ends[j][c] = ends[j + 1][c];
+      ends[2][0] = pz;
+      ends[2][1] = plon;
+      ends[2][2] = plat;
+    }
     rprev2 = rprev;
     rprev = raw;
     dprev = dsm;
@@ -257,6 +282,7 @@ __device__ int trace_ray(const RayArgs &A, int r) {
     latprev = plat;
     if (stop) {
       if (STORE) A.tsurf[r] = (stop == 2 ? t : -999);
+      if (MODE == 2) end->tsurf = (stop == 2 ? t : -999);
       break;
     }
 
@@ -287,7 +313,15 @@ __device__ int trace_ray(const RayArgs &A, int r) {
   }
 
   // Drop a last point that follows a too-short step (src/lineofsight.c:170-171).
-  if (np >= 3 && rprev2 < 1e-3) np--;
+  bool dropped = false;
+  if (np >= 3 && rprev2 < 1e-3) {
+    np--;
+    dropped = true;
+  }
+  if (MODE == 2) {
+    for (int j = 0; j < 2; j++)
+      for (int c = 0; c < 3; c++) end->g[j][c] = ends[j + (dropped ? 0 : 1)][c];
+  }
 
   if (STORE) {
     // Tangent point (src/lineofsight.c:411-452) from the stored geometry.
@@ -331,6 +365,12 @@ __device__ int trace_ray(const RayArgs &A, int r) {
     A.tp[2 * A.n_rays + r] = tplat;
   }
   return np;
+}
+
+template <bool STORE>
+__device__ __forceinline__ int trace_ray(const RayArgs &A, int r) {
+  const RayIn in = {A.obsz[r], A.obslon[r], A.obslat[r], A.vpz[r], A.vplon[r], A.vplat[r]};
+  return trace_core<STORE ? 1 : 0>(A, A.ray_atm[r], r, in, nullptr);
 }
 
 template <bool STORE>

@@ -207,6 +207,7 @@ static int noalloc_run(jsc_model *m, const ctl_t *ctl, const jsc_batch_input *in
     JSC_LAUNCH_CHECK();
 
     EgaArgs ea;
+    memset(&ea, 0, sizeof(ea));  // no scattering source, no digests
     ea.m = m->dv;
     jsc_run_cfg &cf = ea.cfg;
     memset(&cf, 0, sizeof(cf));

@@ -155,6 +155,10 @@ class Batch:
         """Aerosol/cloud layers (an AeroT) for runs with ctl.sca_n > 0."""
         L.check(L.load().jsc_batch_set_aero(self.h, C.byref(aero)), "jsc_batch_set_aero")
 
+    def set_nalpha(self, nalpha):
+        """Secondary pencils per scattering point (even, 10..28; 28 default)."""
+        L.check(L.load().jsc_batch_set_nalpha(self.h, int(nalpha)), "jsc_batch_set_nalpha")
+
     def set_timing(self, on=True):
         L.load().jsc_batch_set_timing(self.h, 1 if on else 0)
 
@@ -179,10 +183,13 @@ class Batch:
             pass
 
 
-def formod_batch(ctl, inp, device=0, model=None, digest=False, aero=None):
+def formod_batch(ctl, inp, device=0, model=None, digest=False, aero=None, nalpha=None,
+                 timing=False):
     """One-shot batch forward model: returns dict of rad/tau/tp*/nlos (and
     the per-(ray, channel) EGA index digests when digest=True).  aero: an
-    AeroT with the layers and optical properties when ctl.sca_n > 0."""
+    AeroT with the layers and optical properties when ctl.sca_n > 0;
+    nalpha: secondary pencils per scattering point; timing: adds the
+    per-stage milliseconds as out["ms"]."""
     own = model is None
     m = Model(ctl, device) if own else model
     nl = len(inp["z"])
@@ -192,9 +199,15 @@ def formod_batch(ctl, inp, device=0, model=None, digest=False, aero=None):
             b.set_aero(aero)
         if digest:
             b.set_digest(True)
+        if nalpha is not None:
+            b.set_nalpha(nalpha)
+        if timing:
+            b.set_timing(True)
         b.upload(inp)
         b.run()
         out = b.download()
+        if timing:
+            out["ms"] = {k: b.kernel_ms(k) for k in ("hydrostatic", "raytrace", "scatter", "ega_rt")}
         if digest:
             out["digest"] = b.index_digest()
         return out

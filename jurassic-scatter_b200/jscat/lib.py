@@ -19,7 +19,7 @@ EXPORTS = [
     "jsc_formod_batch", "jsc_batch_set_timing", "jsc_batch_kernel_ms",
     "jsc_batch_counters", "jsc_batch_set_digest", "jsc_batch_index_digest",
     "jsc_batch_autotune", "jsc_batch_variant", "jsc_batch_variant_ms",
-    "jsc_batch_set_aero", "jsc_formod_batch_noalloc",
+    "jsc_batch_set_aero", "jsc_formod_batch_noalloc", "jsc_batch_set_nalpha",
 ]
 
 
@@ -93,6 +93,7 @@ def load():
         "jsc_batch_variant": (i, [vp, P(i), P(i), P(i)]),
         "jsc_batch_variant_ms": (d, [vp, i]),
         "jsc_batch_set_aero": (i, [vp, P(S.AeroT)]),
+        "jsc_batch_set_nalpha": (i, [vp, i]),
         "jsc_formod_batch_noalloc": (i, [vp, P(S.CtlT), P(BatchInput), P(BatchOutput), vp]),
     }
     for name, (res, args) in sig.items():

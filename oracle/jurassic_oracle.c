@@ -912,14 +912,26 @@ static void o_sca_alpha(double *alpha, int nalpha) {
   alpha[nalpha - 1] = M_PI;
 }
 
+/* Secondary pencils per scattering point: the reference's 28, or an even
+ * count from 10 to 28 with the same angle construction (for checking the
+ * GPU path's pencil-count option). */
+static int g_nalpha = 28;
+
+int oracle_set_nalpha(int nalpha) {
+  if (nalpha < 10 || nalpha > 28 || (nalpha & 1)) return JSC_ERR_ARG;
+  g_nalpha = nalpha;
+  return 0;
+}
+
 /* Thermal single scattering in 1-D atmospheres (src/scatter.c:666-807):
  * 28 secondary pencils at fixed zenith angles, then the phase-function
  * weighted integral over 180 x 180 directions. */
 static int o_srcfunc_sca_1d(const ctl_t *ctl, const atm_t *atm, const aero_t *aero,
                             const double *x, const double *dx, int il, double *src_sca,
                             int scattering) {
-  enum { NALPHA = 28, NPHI = 180, NTHETA2 = 180 };
-  double alpha[NALPHA], dnorth[3], ek[3], lx[3], ly[3], lz[3], sx[3], sy[3], sz[3],
+  enum { NPHI = 180, NTHETA2 = 180 };
+  const int NALPHA = g_nalpha;
+  double alpha[28], dnorth[3], ek[3], lx[3], ly[3], lz[3], sx[3], sy[3], sz[3],
          theta[NTHETA], wsum[NDMAX], xv[3], mlz[3];
   obs_t *obs2 = (obs_t *)calloc(1, sizeof(obs_t));
   int st = 0;

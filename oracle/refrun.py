@@ -63,6 +63,9 @@ def _child(job):
     P = C.POINTER
     port = job.get("port", False)
     fm = lib.oracle_formod if port else lib.formod
+    if port and job.get("nalpha"):
+        if lib.oracle_set_nalpha(int(job["nalpha"])):
+            raise RuntimeError("oracle_set_nalpha(%r) refused" % job["nalpha"])
     fm.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT)]
     fm.restype = C.c_int if port else None
     if not port:
@@ -176,16 +179,17 @@ def reference_aero(ctl_kw, aerofile, cwd, timeout=600):
 
 
 def run_port(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False, los=False,
-             timeout=1800):
+             timeout=1800, nalpha=None):
     """Same as run() with the C restatement (oracle/jurassic_oracle.c)
     instead of the reference build; with los=True it also returns the
-    per-(ray, channel) EGA index digests."""
+    per-(ray, channel) EGA index digests.  nalpha: secondary pencils per
+    scattering point (the reference's 28 by default)."""
     return run(ctl_kw, atms, ray_atm, geom, aero=aero, threads=threads, warmup=warmup,
-               los=los, lib=PORT_LIB, timeout=timeout, port=True)
+               los=los, lib=PORT_LIB, timeout=timeout, port=True, nalpha=nalpha)
 
 
 def run(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False,
-        los=False, lib=None, timeout=1800, port=False):
+        los=False, lib=None, timeout=1800, port=False, nalpha=None):
     """Reference formod over profiles atms (list of dicts) and rays.
     Returns rad/tau [n_rays][nd], tpz/tplon/tplat, seconds (wall time of
     the formod calls after the optional warm-up call), and with los=True
@@ -195,7 +199,8 @@ def run(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False,
     import tempfile
     job = {"ctl": ctl_kw, "atms": atms, "ray_atm": np.asarray(ray_atm),
            "geom": geom, "aero": None if aero is None else bytes(aero),
-           "threads": threads, "warmup": warmup, "los": los, "port": port}
+           "threads": threads, "warmup": warmup, "los": los, "port": port,
+           "nalpha": nalpha}
     if lib:
         job["lib"] = lib
     return _spawn(job, timeout)

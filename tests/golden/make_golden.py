@@ -113,6 +113,15 @@ def main():
         ref = refrun.run(ctlkw, [atm], ra, geom, aero=aero, los=True)
         port = refrun.run_port(ctlkw, [atm], ra, geom, aero=aero, los=True)
         save_aero("aerosol_ext_" + ext, ctlkw, atm, geom, ref, aero, port)
+    for name, sec in (("night", 0.0), ("day", 43200.0)):
+        ctlkw, atm, geom, aerofile = aerosol_case(workdir, 1)
+        geom["time"] = np.full(len(geom["obsz"]), sec)
+        aero = refrun.reference_aero(ctlkw, aerofile, os.path.dirname(aerofile))
+        ra = np.zeros(len(geom["obsz"]), int)
+        ref = refrun.run(ctlkw, [atm], ra, geom, aero=aero, los=True)
+        port = refrun.run_port(ctlkw, [atm], ra, geom, aero=aero)
+        assert np.max(np.abs(port["rad"] - ref["rad"]) / np.abs(ref["rad"])) < 1e-12
+        save_aero("aerosol_sca1_" + name, ctlkw, atm, geom, ref, aero)
     print("fixtures written to", HERE)
 
 
