@@ -140,7 +140,7 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   st = st ? st : jsc_dmalloc(&b->d_counters, 2);
   if (!st) st = batch_alloc_los(b, max_seg > 0 ? max_seg : (int64_t)max_rays * 512);
   b->ega_variant = -1;
-  for (int v = 0; v < 8; v++) b->ega_variant_ms[v] = -1;
+  for (int v = 0; v < 16; v++) b->ega_variant_ms[v] = -1;
   b->depth = ctl->sca_n > 0 ? ctl->sca_mult : 0;
   b->nalpha = JSC_NALPHA_REF;
   sca_alpha(b->alpha, b->nalpha);
@@ -381,12 +381,16 @@ extern "C" int jsc_batch_upload(jsc_batch *b, const jsc_batch_input *in,
 }
 
 // Launch variants of ega_rt_kernel: (threads per block, minimum resident
-// blocks per SM).  The second number sets the register budget, i.e. the
-// trade between occupancy and spills; jsc_batch_autotune picks one.
-struct EgaVariant { int blk, minb; };
-static const EgaVariant kEgaVariants[] = {{128, 4}, {128, 6}, {128, 8}, {256, 3}, {256, 4}};
-static const int kNumEgaVariants = 5;
-static const int kEgaDefault = 1;
+// blocks per SM, emitter loop rolled).  The second number sets the register
+// budget, i.e. the trade between occupancy and spills; the rolled loop
+// trades registers and instruction-cache footprint for local-memory path
+// state.  jsc_batch_autotune picks one.
+struct EgaVariant { int blk, minb, roll; };
+static const EgaVariant kEgaVariants[] = {{128, 4, 0}, {128, 6, 0}, {128, 8, 0}, {256, 3, 0},
+                                          {256, 4, 0}, {128, 8, 1}, {128, 12, 1}, {256, 4, 1},
+                                          {256, 6, 1}};
+static const int kNumEgaVariants = 9;
+static const int kEgaDefault = JSC_EGA_DEFAULT_VARIANT;
 
 static int launch_ega(const EgaArgs &ea, int nr, int ndp, int ng, int variant,
                       cudaStream_t s) {

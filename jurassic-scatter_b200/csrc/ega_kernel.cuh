@@ -11,7 +11,7 @@
 // registers (GMAX >= ng, the emitter loop is unrolled so the lookups of
 // different emitters overlap); LOS records are read by all threads of a
 // ray (broadcast loads).
-template <int GMAX, bool DIG, int BLK, int MINB>
+template <int GMAX, bool DIG, int BLK, int MINB, bool ROLL>
 __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
   const jsc_dev_model &m = A.m;
   const int nd = m.nd, ng = m.ng;
@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
 
   double tp[GMAX];
   int hint[GMAX];
-#pragma unroll(GMAX <= 8 ? GMAX : 1)
+#pragma unroll((GMAX <= 8 && !ROLL) ? GMAX : 1)
   for (int g = 0; g < GMAX; g++) {
     tp[g] = 1;
     hint[g] = 0;
@@ -54,8 +54,9 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
     int code = (int)rec[REC_GRID];
     double tau_gas = 1;
     // unrolled up to 8 emitters (state in registers, lookups of different
-    // emitters overlap); larger counts keep the state in local memory
-#pragma unroll(GMAX <= 8 ? GMAX : 1)
+    // emitters overlap) unless ROLL; larger counts and ROLL keep the state in
+    // local memory and the code small
+#pragma unroll((GMAX <= 8 && !ROLL) ? GMAX : 1)
     for (int g = 0; g < GMAX; g++) {
       if (g >= ng) break;
       double eps = 0;
@@ -155,11 +156,15 @@ template <int G, bool DIG>
 static void ega_launch_variant(const EgaArgs &ea, unsigned g128, unsigned g256, int v,
                                cudaStream_t s) {
   switch (v) {
-    case 0: ega_rt_kernel<G, DIG, 128, 4><<<g128, 128, 0, s>>>(ea); break;
-    case 2: ega_rt_kernel<G, DIG, 128, 8><<<g128, 128, 0, s>>>(ea); break;
-    case 3: ega_rt_kernel<G, DIG, 256, 3><<<g256, 256, 0, s>>>(ea); break;
-    case 4: ega_rt_kernel<G, DIG, 256, 4><<<g256, 256, 0, s>>>(ea); break;
-    default: ega_rt_kernel<G, DIG, 128, 6><<<g128, 128, 0, s>>>(ea); break;
+    case 0: ega_rt_kernel<G, DIG, 128, 4, false><<<g128, 128, 0, s>>>(ea); break;
+    case 2: ega_rt_kernel<G, DIG, 128, 8, false><<<g128, 128, 0, s>>>(ea); break;
+    case 3: ega_rt_kernel<G, DIG, 256, 3, false><<<g256, 256, 0, s>>>(ea); break;
+    case 4: ega_rt_kernel<G, DIG, 256, 4, false><<<g256, 256, 0, s>>>(ea); break;
+    case 5: ega_rt_kernel<G, DIG, 128, 8, true><<<g128, 128, 0, s>>>(ea); break;
+    case 6: ega_rt_kernel<G, DIG, 128, 12, true><<<g128, 128, 0, s>>>(ea); break;
+    case 7: ega_rt_kernel<G, DIG, 256, 4, true><<<g256, 256, 0, s>>>(ea); break;
+    case 8: ega_rt_kernel<G, DIG, 256, 6, true><<<g256, 256, 0, s>>>(ea); break;
+    default: ega_rt_kernel<G, DIG, 128, 6, false><<<g128, 128, 0, s>>>(ea); break;
   }
 }
 
@@ -169,10 +174,12 @@ void jsc_ega_launch_g4(const EgaArgs &, unsigned, unsigned, int, bool, cudaStrea
 void jsc_ega_launch_g8(const EgaArgs &, unsigned, unsigned, int, bool, cudaStream_t);
 void jsc_ega_launch_gmax(const EgaArgs &, unsigned, unsigned, int, bool, cudaStream_t);
 
-// Index digests run the default variant only.
+// Index digests run the default variant (6: 128 threads, 12 blocks per SM,
+// rolled emitter loop) only.
+#define JSC_EGA_DEFAULT_VARIANT 6
 #define JSC_EGA_LAUNCHER(NAME, G)                                                      \
   void NAME(const EgaArgs &ea, unsigned g128, unsigned g256, int v, bool dig,          \
             cudaStream_t s) {                                                          \
-    if (dig) ega_launch_variant<G, true>(ea, g128, g256, 1, s);                        \
+    if (dig) ega_launch_variant<G, true>(ea, g128, g256, JSC_EGA_DEFAULT_VARIANT, s);  \
     else ega_launch_variant<G, false>(ea, g128, g256, v, s);                           \
   }

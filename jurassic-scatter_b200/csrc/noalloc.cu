@@ -246,12 +246,14 @@ static int noalloc_run(jsc_model *m, const ctl_t *ctl, const jsc_batch_input *in
     const int64_t threads = (int64_t)nr * ndp;
     const unsigned g128 = (unsigned)((threads + 127) / 128);
     const unsigned g256 = (unsigned)((threads + 255) / 256);
-    // Launch variant 1 (128 threads, 6 blocks per SM): the default of
-    // jsc_batch_run, so results match jsc_formod_batch bit for bit.
-    if (ng <= 2) jsc_ega_launch_g2(ea, g128, g256, 1, false, s);
-    else if (ng <= 4) jsc_ega_launch_g4(ea, g128, g256, 1, false, s);
-    else if (ng <= 8) jsc_ega_launch_g8(ea, g128, g256, 1, false, s);
-    else jsc_ega_launch_gmax(ea, g128, g256, 1, false, s);
+    // The default launch variant of jsc_batch_run (every variant computes
+    // the same operations in the same order; they differ in registers and
+    // unrolling only).
+    const int v = JSC_EGA_DEFAULT_VARIANT;
+    if (ng <= 2) jsc_ega_launch_g2(ea, g128, g256, v, false, s);
+    else if (ng <= 4) jsc_ega_launch_g4(ea, g128, g256, v, false, s);
+    else if (ng <= 8) jsc_ega_launch_g8(ea, g128, g256, v, false, s);
+    else jsc_ega_launch_gmax(ea, g128, g256, v, false, s);
     JSC_LAUNCH_CHECK();
 
     if (out->rad) NDCPY(out->rad, d_rad, (size_t)nr * nd, s);

@@ -95,6 +95,16 @@ def save_aero(name, ctlkw, atm, geom, ref, aero_bytes, port=None):
         **{"geom_" + k: v for k, v in geom.items()}, **extra)
 
 
+def aero_fixture(workdir, name, layer_files, nus):
+    """aero_t (as bytes) of a layer file on a channel grid, from the
+    reference's read_aero + get_opt_prop (Mie), for benchmark inputs."""
+    ctlkw = dict(emitters=synth.CFG0_EMITTERS, nus=nus, tblbase="-", sca_n=1, sca_mult=1)
+    aerofile = layer_files(os.path.join(workdir, "aero"))
+    aero = refrun.reference_aero(ctlkw, aerofile, os.path.dirname(aerofile))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), nus=np.asarray(nus),
+                        aero=np.frombuffer(aero, dtype=np.uint8))
+
+
 def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
     ctlkw, atm, geom = synth.clear_limb_case(workdir)
@@ -122,6 +132,8 @@ def main():
         port = refrun.run_port(ctlkw, [atm], ra, geom, aero=aero)
         assert np.max(np.abs(port["rad"] - ref["rad"]) / np.abs(ref["rad"])) < 1e-12
         save_aero("aerosol_sca1_" + name, ctlkw, atm, geom, ref, aero)
+    aero_fixture(workdir, "aero_sulfate16", synth.sulfate_layer_files, list(synth.CFG2_NU))
+    aero_fixture(workdir, "aero_ice8", synth.ice_layer_files, list(synth.CFG2_NU[::2]))
     print("fixtures written to", HERE)
 
 
