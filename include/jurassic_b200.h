@@ -289,7 +289,7 @@ int jsc_formod_batch(jsc_model *m, const ctl_t *ctl, const jsc_batch_input *in,
  * whole device).  The model (its tables) must exist already.
  *
  * Limits: ctl->sca_n must be 0 (clear air); the inputs, outputs and
- * (4 + 8 + nw + ng) doubles per LOS point must fit the scratch, e.g.
+ * (12 + nw + ng) doubles per LOS point must fit the scratch, e.g.
  * about 390,000 LOS points for 8 emitters and one window.  A larger input
  * returns JSC_ERR_ARG with the sizes in jsc_last_error_message(), before
  * any LOS record is written.
@@ -321,6 +321,12 @@ double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel);
  * jsc_batch_variant reports the choice. */
 int jsc_batch_autotune(jsc_batch *b, void *stream);
 int jsc_batch_variant(const jsc_batch *b, int *variant, int *block, int *min_blocks);
+
+/* Select the EGA launch variant by hand (-1: the default).  Variants 0-8
+ * run a thread per (ray, channel) with every emitter's path state; 9-13 a
+ * lane per (ray, channel, emitter) after a separate continuum/Planck pass.
+ * All variants compute the same operations in the same order. */
+int jsc_batch_set_variant(jsc_batch *b, int variant);
 double jsc_batch_variant_ms(const jsc_batch *b, int variant);
 
 /* Aerosol/cloud layers and optical properties for runs with ctl->sca_n > 0
@@ -337,12 +343,14 @@ int jsc_batch_set_nalpha(jsc_batch *b, int nalpha);
 
 /* Per-(ray, channel) checksum of every emissivity-table index the EGA
  * interpolation selected in the last run, for parity checks against the
- * reference's indices: for each LOS point and emitter with a full
- * interpolation, fold d = d*1000003 + v over the (p, T) bracket code
+ * reference's indices.  Per emitter g, D_g folds d = d*1000003 + v over the
+ * LOS points with a full interpolation: the (p, T) bracket code
  * ipr*961 + it0*31 + it1 and then, for the (p, T) nodes (ipr,it0),
  * (ipr,it0+1), (ipr+1,it1), (ipr+1,it1+1), the interval found for the
  * path emissivity (intpol_tbl_u) and the one found for the extended column
- * (intpol_tbl_eps).  Enable before jsc_batch_run; out is [n_rays][nd]. */
+ * (intpol_tbl_eps); the checksum folds D_0, D_1, ... the same way.  Enable
+ * before jsc_batch_run (the run then uses the default launch variant of
+ * the selected kernel family); out is [n_rays][nd]. */
 int jsc_batch_set_digest(jsc_batch *b, int on);
 int jsc_batch_index_digest(jsc_batch *b, uint64_t *out);
 
@@ -350,6 +358,66 @@ int jsc_batch_index_digest(jsc_batch *b, uint64_t *out);
  * (point, channel, emitter) EGA interpolations actually evaluated. */
 int jsc_batch_counters(const jsc_batch *b, int64_t *n_points,
                        int64_t *n_ega);
+
+/* ------------------------------------------------------------------------
+ * Scattering-source surrogate (no counterpart in the reference: it stands
+ * in for srcfunc_sca, src/scatter.c:643-1041, at the scattering points of
+ * a batch).  A 4-layer MLP, width 128, tanh, maps 8 features of a
+ * scattering point (altitude, cosine of the LOS chord's zenith angle,
+ * temperature, log pressure, cosine of the solar zenith angle, cosine of
+ * the solar scattering angle, layer index, 0) to the log of the scattering
+ * source of each channel.  Trained on the GPU (FP32 forward/backward, Adam)
+ * on samples of the plain source; inference runs BF16 weights on the
+ * tensor cores with FP32 accumulation.
+ * ------------------------------------------------------------------------ */
+typedef struct jsc_surrogate jsc_surrogate;
+
+/* A network with nd (1..64) outputs and seeded initial weights. */
+int jsc_surrogate_create(int nd, int device, uint64_t seed, jsc_surrogate **out);
+void jsc_surrogate_destroy(jsc_surrogate *s);
+
+/* Parameters as one FP32 vector: W0 [128][8], b0 [128], W1 [128][128], b1,
+ * W2 [128][128], b2, W3 [nd][128], b3 [nd]. */
+int jsc_surrogate_param_count(const jsc_surrogate *s);
+int jsc_surrogate_get_params(const jsc_surrogate *s, float *out);
+int jsc_surrogate_set_params(jsc_surrogate *s, const float *in);
+
+/* Loss (mean over the n rows of the squared error summed over outputs) and
+ * its gradient with respect to every parameter (layout of get_params), for
+ * network inputs x [n][8] and targets t [n][nd] as given (no
+ * standardisation); the FP32 training kernels. */
+int jsc_surrogate_loss_grad(jsc_surrogate *s, const float *x, const float *t, int n,
+                            float *loss, float *grads);
+
+/* Train on n samples: raw features X [n][8] (as jsc_batch_scatter_samples
+ * returns them) and plain sources src [n][nd].  Standardises features and
+ * log sources, records the feature envelope, runs epochs of Adam on
+ * shuffled minibatches with a cosine-decayed learning rate; loss_per_epoch
+ * (may be NULL) receives the last minibatch loss of each epoch. */
+int jsc_surrogate_train(jsc_surrogate *s, const float *X, const double *src, int64_t n,
+                        int epochs, int batch, float lr, uint64_t seed,
+                        float *loss_per_epoch);
+
+/* Sources [n][nd] of n raw feature rows. */
+int jsc_surrogate_predict(jsc_surrogate *s, const float *feat, int n, double *src);
+
+/* Features and plain scattering sources of the last run's scattering
+ * points (training data); n receives the point count, arrays may be NULL
+ * to query it. */
+int jsc_batch_scatter_samples(jsc_batch *b, float *feat, double *src, int64_t max, int64_t *n);
+
+/* Use the surrogate (NULL: never) for the batch's scattering sources.
+ * Points whose features leave the training envelope take the plain path;
+ * every check_stride-th point inside it (0: none) is computed both ways, and
+ * if one deviates from the plain source by more than tol_rel (relative) the
+ * whole batch is recomputed with the plain path. */
+int jsc_batch_set_surrogate(jsc_batch *b, jsc_surrogate *s, double tol_rel, int check_stride);
+
+/* Surrogate counts of the last run: scattering points, fallbacks, checked
+ * points, largest relative deviation found by the check, and whether the
+ * surrogate's sources were used (0 after a rejection). */
+int jsc_batch_surrogate_stats(const jsc_batch *b, int64_t *points, int64_t *fallback,
+                              int64_t *checked, double *max_rel_err, int *used);
 
 #ifdef __cplusplus
 }

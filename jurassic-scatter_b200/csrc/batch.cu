@@ -7,14 +7,18 @@
 
 #include "kernels.cuh"
 #include "ega_kernel.cuh"
+#include "ega_lane.cuh"
 #include "scatter.cuh"
+#include "surrogate.h"
 
 static int sca_alpha(double *alpha, int nalpha);
 
 static void batch_free_los(jsc_batch *b) {
   cudaFree(b->d_geo);
   cudaFree(b->d_pts);
-  b->d_geo = b->d_pts = nullptr;
+  cudaFree(b->d_ctm);
+  cudaFree(b->d_srcp);
+  b->d_geo = b->d_pts = b->d_ctm = b->d_srcp = nullptr;
 }
 
 static int batch_alloc_los(jsc_batch *b, int64_t max_seg) {
@@ -22,6 +26,8 @@ static int batch_alloc_los(jsc_batch *b, int64_t max_seg) {
   int st;
   if ((st = jsc_dmalloc(&b->d_geo, (size_t)max_seg * 4))) return st;
   if ((st = jsc_dmalloc(&b->d_pts, (size_t)max_seg * b->W))) return st;
+  if ((st = jsc_dmalloc(&b->d_ctm, (size_t)max_seg * b->cfg.nd))) return st;
+  if ((st = jsc_dmalloc(&b->d_srcp, (size_t)max_seg * b->cfg.nd))) return st;
   b->max_seg = max_seg;
   return JSC_OK;
 }
@@ -67,6 +73,12 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   cudaFree(b->d_planck_sun);
   jsc_batch_destroy(b->child);
   jsc_batch_destroy(b->sun_child);
+  cudaFree(b->d_feat);
+  cudaFree(b->d_mark);
+  cudaFree(b->d_idx);
+  cudaFree(b->d_sp_sub);
+  cudaFree(b->d_atm_sub);
+  cudaFree(b->d_src_sub);
   free(b->h_aero);
   free(b->ctl);
   if (b->h_total) cudaFreeHost(b->h_total);
@@ -380,17 +392,28 @@ extern "C" int jsc_batch_upload(jsc_batch *b, const jsc_batch_input *in,
   return JSC_OK;
 }
 
-// Launch variants of ega_rt_kernel: (threads per block, minimum resident
-// blocks per SM, emitter loop rolled).  The second number sets the register
-// budget, i.e. the trade between occupancy and spills; the rolled loop
-// trades registers and instruction-cache footprint for local-memory path
-// state.  jsc_batch_autotune picks one.
-struct EgaVariant { int blk, minb, roll; };
-static const EgaVariant kEgaVariants[] = {{128, 4, 0}, {128, 6, 0}, {128, 8, 0}, {256, 3, 0},
-                                          {256, 4, 0}, {128, 8, 1}, {128, 12, 1}, {256, 4, 1},
-                                          {256, 6, 1}};
-static const int kNumEgaVariants = 9;
-static const int kEgaDefault = JSC_EGA_DEFAULT_VARIANT;
+// Launch variants of the EGA + radiative-transfer step.  0-8: ega_rt_kernel,
+// a thread per (ray, channel) with all emitters' path state: (threads per
+// block, minimum resident blocks per SM, emitter loop rolled); the second
+// number sets the register budget, i.e. the trade between occupancy and
+// spills, the rolled loop trades registers and instruction-cache footprint
+// for local-memory path state.  9-13: ega_lane_kernel, a lane per
+// (ray, channel, emitter), after ctm_src_kernel.  jsc_batch_autotune picks
+// one.
+struct EgaVariant { int blk, minb, roll, lane; };
+static const EgaVariant kEgaVariants[] = {
+    {128, 4, 0, 0}, {128, 6, 0, 0}, {128, 8, 0, 0}, {256, 3, 0, 0}, {256, 4, 0, 0},
+    {128, 8, 1, 0}, {128, 12, 1, 0}, {256, 4, 1, 0}, {256, 6, 1, 0},
+    {128, 12, 0, 1}, {128, 8, 0, 1}, {256, 4, 0, 1}, {256, 5, 0, 1}, {512, 2, 0, 1}};
+static const int kNumEgaVariants = 14;
+static const int kLaneBase = 9;
+static const int kEgaDefault = JSC_EGA_DEFAULT_VARIANT;  // fastest measured (batched clear air)
+// Index digests run the default variant of the selected kernel family.
+
+static bool lane_variant(int variant) {
+  const int v = (variant >= 0 && variant < kNumEgaVariants) ? variant : kEgaDefault;
+  return kEgaVariants[v].lane != 0;
+}
 
 static int launch_ega(const EgaArgs &ea, int nr, int ndp, int ng, int variant,
                       cudaStream_t s) {
@@ -399,6 +422,13 @@ static int launch_ega(const EgaArgs &ea, int nr, int ndp, int ng, int variant,
   const unsigned g256 = (unsigned)((threads + 255) / 256);
   const int v = (variant >= 0 && variant < kNumEgaVariants) ? variant : kEgaDefault;
   const bool dig = ea.digest != nullptr;  // index digests: default variant only
+  if (kEgaVariants[v].lane) {
+    const int lv = dig ? 0 : v - kLaneBase;
+    if (ng <= 4) jsc_ega_lane_launch_s(ea, lv, dig, s);
+    else jsc_ega_lane_launch_l(ea, lv, dig, s);
+    JSC_LAUNCH_CHECK();
+    return JSC_OK;
+  }
   if (ng <= 2) jsc_ega_launch_g2(ea, g128, g256, v, dig, s);
   else if (ng <= 4) jsc_ega_launch_g4(ea, g128, g256, v, dig, s);
   else if (ng <= 8) jsc_ega_launch_g8(ea, g128, g256, v, dig, s);
@@ -552,11 +582,14 @@ static const int64_t kScatterChunk = 8192;
 // Scattering source of every scattering point (srcfunc_sca,
 // src/scatter.c:643-662): thermal radiation from the secondary pencils,
 // then the solar term.
-static int scatter_sources(jsc_batch *b, cudaStream_t s) {
-  int st = list_scattering_points(b, s);
-  if (st || b->n_sp == 0) return st;
+// The plain scattering source (srcfunc_sca) of n point records sp
+// (profiles sp_atm) into src [n][nd].
+static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int64_t n_pts,
+                         double *src, cudaStream_t s) {
+  int st = JSC_OK;
+  if (n_pts <= 0) return JSC_OK;
   const int nd = b->cfg.nd, na = b->nalpha;
-  const int64_t chunk = b->n_sp < kScatterChunk ? b->n_sp : kScatterChunk;
+  const int64_t chunk = n_pts < kScatterChunk ? n_pts : kScatterChunk;
   if ((st = ensure_child(b, &b->child, (int)(chunk * na), b->depth - 1))) return st;
   if ((st = ensure_child(b, &b->sun_child, (int)chunk, 0))) return st;
   if (!b->d_planck_sun) {
@@ -582,14 +615,14 @@ static int scatter_sources(jsc_batch *b, cudaStream_t s) {
   if (shmem > 48 * 1024)
     JSC_CUDA_TRY(cudaFuncSetAttribute(sp_integral_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-  for (int64_t c0 = 0; c0 < b->n_sp; c0 += chunk) {
-    const int n = (int)((b->n_sp - c0) < chunk ? (b->n_sp - c0) : chunk);
+  for (int64_t c0 = 0; c0 < n_pts; c0 += chunk) {
+    const int n = (int)((n_pts - c0) < chunk ? (n_pts - c0) : chunk);
     // Secondary pencils (src/scatter.c:717-736).
     SpawnArgs pa;
     pa.n_pts = n;
     pa.nalpha = na;
-    pa.sp = b->d_sp + c0 * JSC_SP_REC;
-    pa.sp_atm = b->d_sp_atm + c0;
+    pa.sp = sp + c0 * JSC_SP_REC;
+    pa.sp_atm = sp_atm + c0;
     memcpy(pa.alpha, b->alpha, sizeof(pa.alpha));
     pa.ray_atm = c->d_ray_atm;
     pa.ray = c->d_ray;
@@ -609,7 +642,7 @@ static int scatter_sources(jsc_batch *b, cudaStream_t s) {
     memcpy(ia.alpha, b->alpha, sizeof(ia.alpha));
     ia.rad = c->d_rad;
     ia.phase = b->d_phase;
-    ia.src = b->d_src + c0 * nd;
+    ia.src = src + c0 * nd;
     sp_integral_kernel<<<n, JSC_INT_THREADS, shmem, s>>>(ia);
     JSC_LAUNCH_CHECK();
     // Solar term (src/scatter.c:899-995).
@@ -639,10 +672,165 @@ static int scatter_sources(jsc_batch *b, cudaStream_t s) {
     aa.tau = sc->d_tau;
     aa.phase = b->d_phase;
     aa.planck_sun = b->d_planck_sun;
-    aa.src = b->d_src + c0 * nd;
+    aa.src = src + c0 * nd;
     sun_add_kernel<<<(n * nd + 127) / 128, 128, 0, s>>>(aa);
     JSC_LAUNCH_CHECK();
   }
+  return JSC_OK;
+}
+
+// Marks of the surrogate pass: 0 surrogate only, 1 outside the envelope
+// (plain), 2 inside and sampled for the accuracy check (both).
+static __global__ void sur_mark_kernel(int n, const float *feat, SurEnvelope env, int stride,
+                                       int *mark) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  bool in = true;
+  for (int c = 0; c < SUR_NF; c++) {
+    const float v = feat[(size_t)k * SUR_NF + c];
+    if (!(v >= env.lo[c] && v <= env.hi[c])) in = false;
+  }
+  mark[k] = !in ? 1 : ((stride > 0 && k % stride == 0) ? 2 : 0);
+}
+
+// Compact the marked points: idx[] of marks != 0 in order (one block).
+static __global__ void sur_compact_kernel(int n, const int *mark, int *idx, int *count) {
+  __shared__ int base;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  for (int k0 = 0; k0 < n; k0 += blockDim.x) {
+    const int k = k0 + threadIdx.x;
+    const int f = (k < n && mark[k] != 0) ? 1 : 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    __shared__ int wsum[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) wsum[w] = __popc(bal);
+    __syncthreads();
+    int off = 0;
+    for (int i = 0; i < w; i++) off += wsum[i];
+    if (f) idx[base + off + __popc(bal & ((1u << lane) - 1))] = k;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); i++) tot += wsum[i];
+      base += tot;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *count = base;
+}
+
+static __global__ void sur_gather_kernel(int m, const int *idx, const double *sp, const int *sp_atm,
+                                         double *sp_sub, int *atm_sub) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int k = idx[i];
+  for (int c = 0; c < JSC_SP_REC; c++) sp_sub[(size_t)i * JSC_SP_REC + c] = sp[(size_t)k * JSC_SP_REC + c];
+  atm_sub[i] = sp_atm[k];
+}
+
+// Fallback points take the plain source; checked points compare the
+// surrogate's source with it (largest relative deviation, as float bits).
+static __global__ void sur_merge_kernel(int m, int nd, const int *idx, const int *mark,
+                                        const double *src_sub, double *src, unsigned *maxerr) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m * nd) return;
+  const int i = t / nd, d = t - i * nd, k = idx[i];
+  const double plain = src_sub[(size_t)i * nd + d];
+  double *dst = src + (size_t)k * nd + d;
+  if (mark[k] == 1) {
+    *dst = plain;
+  } else {
+    const float e = (float)(fabs(*dst - plain) / fmax(fabs(plain), 1e-300));
+    atomicMax(maxerr, __float_as_uint(e == e ? e : 3.0e38f));
+  }
+}
+
+// Scattering source of every scattering point (srcfunc_sca,
+// src/scatter.c:643-662): the plain path (secondary and solar pencils), or,
+// with a trained surrogate attached, the surrogate for points inside its
+// envelope and the plain path for the rest and for a sample of the inside
+// points, which checks the surrogate; if a checked point deviates by more
+// than the tolerance the whole batch takes the plain path.
+static int scatter_sources(jsc_batch *b, cudaStream_t s) {
+  int st = list_scattering_points(b, s);
+  if (st || b->n_sp == 0) return st;
+  const int nd = b->cfg.nd;
+  const int n = (int)b->n_sp;
+  b->sur_points = b->n_sp;
+  b->sur_fallback = b->sur_checked = 0;
+  b->sur_maxerr = 0;
+  b->sur_used = 0;
+  if (!(b->sur && b->sur_on && jsc_sur_trained(b->sur) && jsc_sur_nout(b->sur) == nd))
+    return plain_sources(b, b->d_sp, b->d_sp_atm, b->n_sp, b->d_src, s);
+  if (b->sur_cap < b->n_sp) {
+    cudaFree(b->d_feat);
+    cudaFree(b->d_mark);
+    cudaFree(b->d_idx);
+    cudaFree(b->d_sp_sub);
+    cudaFree(b->d_atm_sub);
+    cudaFree(b->d_src_sub);
+    b->d_feat = nullptr;
+    b->d_mark = b->d_idx = b->d_atm_sub = nullptr;
+    b->d_sp_sub = b->d_src_sub = nullptr;
+    b->sur_cap = 0;
+    const int64_t cap = b->max_sp;
+    if ((st = jsc_dmalloc(&b->d_feat, (size_t)cap * SUR_NF))) return st;
+    if ((st = jsc_dmalloc(&b->d_mark, (size_t)cap))) return st;
+    if ((st = jsc_dmalloc(&b->d_idx, (size_t)cap + 1))) return st;
+    if ((st = jsc_dmalloc(&b->d_sp_sub, (size_t)cap * JSC_SP_REC))) return st;
+    if ((st = jsc_dmalloc(&b->d_atm_sub, (size_t)cap))) return st;
+    if ((st = jsc_dmalloc(&b->d_src_sub, (size_t)cap * nd))) return st;
+    b->sur_cap = cap;
+  }
+  if ((st = jsc_sur_features(n, b->d_sp, b->d_feat, s))) return st;
+  SurEnvelope env;
+  jsc_sur_envelope(b->sur, env.lo, env.hi);
+  sur_mark_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, b->d_feat, env, b->sur_stride, b->d_mark);
+  JSC_LAUNCH_CHECK();
+  if ((st = jsc_sur_infer(b->sur, n, b->d_feat, b->d_src, nd, s))) return st;
+  sur_compact_kernel<<<1, 1024, 0, s>>>(n, b->d_mark, b->d_idx, b->d_idx + b->sur_cap);
+  JSC_LAUNCH_CHECK();
+  int m = 0;
+  JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, b->d_idx + b->sur_cap, sizeof(int),
+                               cudaMemcpyDeviceToHost, s));
+  JSC_CUDA_TRY(cudaStreamSynchronize(s));
+  m = *(int *)b->h_total;
+  if (m > 0) {
+    sur_gather_kernel<<<(m + 127) / 128, 128, 0, s>>>(m, b->d_idx, b->d_sp, b->d_sp_atm,
+                                                      b->d_sp_sub, b->d_atm_sub);
+    JSC_LAUNCH_CHECK();
+    if ((st = plain_sources(b, b->d_sp_sub, b->d_atm_sub, m, b->d_src_sub, s))) return st;
+    unsigned *d_err = (unsigned *)b->d_idx + b->sur_cap;  // reuse the count word
+    JSC_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
+    sur_merge_kernel<<<(m * nd + 127) / 128, 128, 0, s>>>(m, nd, b->d_idx, b->d_mark,
+                                                          b->d_src_sub, b->d_src, d_err);
+    JSC_LAUNCH_CHECK();
+    unsigned eb = 0;
+    JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    JSC_CUDA_TRY(cudaStreamSynchronize(s));
+    eb = *(unsigned *)b->h_total;
+    float e;
+    memcpy(&e, &eb, sizeof(e));
+    b->sur_maxerr = e;
+  }
+  // marks: count fallback and checked points on the host side of the copy
+  {
+    int *hm = (int *)malloc((size_t)n * sizeof(int));
+    if (!hm) return JSC_ERR_NOMEM;
+    JSC_CUDA_TRY(cudaMemcpy(hm, b->d_mark, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < n; k++) {
+      if (hm[k] == 1) b->sur_fallback++;
+      else if (hm[k] == 2) b->sur_checked++;
+    }
+    free(hm);
+  }
+  if (b->sur_maxerr > b->sur_tol) {
+    // a checked point missed the tolerance: the whole batch takes the plain path
+    b->sur_rejected++;
+    return plain_sources(b, b->d_sp, b->d_sp_atm, b->n_sp, b->d_src, s);
+  }
+  b->sur_used = 1;
   return JSC_OK;
 }
 
@@ -724,6 +912,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
       int st = batch_alloc_los(b, *b->h_total + *b->h_total / 4 + 1024);
       if (st) return st;
     }
+    b->n_points = *b->h_total;
     ra.geo = b->d_geo;
     ra.pts = b->d_pts;
     ra.max_seg = b->max_seg;
@@ -781,6 +970,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
       int st = batch_alloc_los(b, *b->h_total + *b->h_total / 4 + 1024);
       if (st) return st;
     }
+    b->n_points = *b->h_total;
     fa.geo = b->d_geo;
     fa.pts = b->d_pts;
     fa.max_seg = b->max_seg;
@@ -824,6 +1014,23 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   ea.aero_nl = b->aero_nl;
   ea.src_sca = (scattering && b->n_sp > 0) ? b->d_src : nullptr;
   ea.sp_off = (scattering && b->n_sp > 0) ? b->d_sp_off : nullptr;
+  ea.beta_ctm = b->d_ctm;
+  ea.src_pl = b->d_srcp;
+  if (lane_variant(b->ega_variant)) {
+    // continuum extinction and Planck source per (LOS point, channel)
+    CtmArgs ca;
+    ca.m = m->dv;
+    ca.cfg = b->cfg;
+    ca.n_points = b->n_points;
+    ca.W = b->W;
+    ca.pts = b->d_pts;
+    ca.beta = b->d_ctm;
+    ca.src = b->d_srcp;
+    ev_record(b, JSC_T_CTM, 0, s);
+    jsc_ctm_src_launch(ca, s);
+    JSC_LAUNCH_CHECK();
+    ev_record(b, JSC_T_CTM, 1, s);
+  }
   b->last_ega = ea;
   ev_record(b, JSC_T_EGA, 0, s);
   int st = launch_ega(ea, nr, ndp, m->ng, b->ega_variant, s);
@@ -913,6 +1120,7 @@ extern "C" int jsc_batch_index_digest(jsc_batch *b, uint64_t *out) {
 extern "C" int jsc_batch_autotune(jsc_batch *b, void *stream) {
   if (!b || b->n_rays < 1) return JSC_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
+  b->ega_variant = kLaneBase;  // a lane variant also fills the continuum arrays
   int st = jsc_batch_run(b, stream);  // LOS records for the timing runs
   if (st) return st;
   EgaArgs ea = b->last_ega;
@@ -950,6 +1158,16 @@ extern "C" int jsc_batch_autotune(jsc_batch *b, void *stream) {
   return JSC_OK;
 }
 
+extern "C" int jsc_batch_set_variant(jsc_batch *b, int variant) {
+  if (!b || variant < -1 || variant >= kNumEgaVariants) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_set_variant: variant %d outside -1..%d", variant,
+                  kNumEgaVariants - 1);
+    return JSC_ERR_ARG;
+  }
+  b->ega_variant = variant;
+  return JSC_OK;
+}
+
 extern "C" double jsc_batch_variant_ms(const jsc_batch *b, int variant) {
   if (!b || variant < 0 || variant >= kNumEgaVariants) return -1;
   return b->ega_variant_ms[variant];
@@ -974,6 +1192,7 @@ extern "C" double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel) {
   int k = -1;
   if (!strcmp(kernel, "hydrostatic")) k = JSC_T_HYDRO;
   else if (!strcmp(kernel, "scatter")) k = JSC_T_SCATTER;
+  else if (!strcmp(kernel, "continua")) k = JSC_T_CTM;
   else if (!strcmp(kernel, "raytrace")) k = JSC_T_RAYTRACE;
   else if (!strcmp(kernel, "ega_rt")) k = JSC_T_EGA;
   if (k < 0 || !b->ran[k]) return -1;
@@ -991,4 +1210,54 @@ extern "C" int jsc_batch_counters(const jsc_batch *b, int64_t *n_points,
   if (n_points) *n_points = (int64_t)c[0];
   if (n_ega) *n_ega = (int64_t)c[1];
   return JSC_OK;
+}
+
+extern "C" int jsc_batch_set_surrogate(jsc_batch *b, jsc_surrogate *s, double tol_rel,
+                                       int check_stride) {
+  if (!b || (s && (jsc_sur_nout(s) != b->cfg.nd || tol_rel <= 0 || check_stride < 0))) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_set_surrogate: channel count, tolerance or stride");
+    return JSC_ERR_ARG;
+  }
+  b->sur = s;
+  b->sur_on = s != nullptr;
+  b->sur_tol = (float)tol_rel;
+  b->sur_stride = check_stride;
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_surrogate_stats(const jsc_batch *b, int64_t *points, int64_t *fallback,
+                                         int64_t *checked, double *max_rel_err, int *used) {
+  if (!b) return JSC_ERR_ARG;
+  if (points) *points = b->sur_points;
+  if (fallback) *fallback = b->sur_fallback;
+  if (checked) *checked = b->sur_checked;
+  if (max_rel_err) *max_rel_err = b->sur_maxerr;
+  if (used) *used = b->sur_used;
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_scatter_samples(jsc_batch *b, float *feat, double *src, int64_t max,
+                                         int64_t *n) {
+  if (!b || !n) return JSC_ERR_ARG;
+  *n = b->n_sp;
+  if (!feat || !src || b->n_sp == 0) return JSC_OK;
+  if (b->n_sp > max) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_scatter_samples: %lld points, room for %lld",
+                  (long long)b->n_sp, (long long)max);
+    return JSC_ERR_ARG;
+  }
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  JSC_CUDA_TRY(cudaDeviceSynchronize());  // the last run may be on any stream
+  float *d_f = nullptr;
+  int st = jsc_dmalloc(&d_f, (size_t)b->n_sp * SUR_NF);
+  if (st) return st;
+  st = jsc_sur_features((int)b->n_sp, b->d_sp, d_f, 0);
+  if (!st && cudaMemcpy(feat, d_f, (size_t)b->n_sp * SUR_NF * sizeof(float),
+                        cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = JSC_ERR_CUDA;
+  if (!st && cudaMemcpy(src, b->d_src, (size_t)b->n_sp * b->cfg.nd * sizeof(double),
+                        cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = JSC_ERR_CUDA;
+  cudaFree(d_f);
+  return st;
 }

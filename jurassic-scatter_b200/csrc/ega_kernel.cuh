@@ -41,7 +41,9 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
     hint[g] = 0;
   }
   double rad = 0, tau = 1;
-  unsigned long long dig = 0;
+  unsigned long long dig[DIG ? GMAX : 1];  // per-emitter index digests
+#pragma unroll
+  for (int g = 0; g < (DIG ? GMAX : 1); g++) dig[g] = 0;
   unsigned n_ega = 0;
   const int np = A.nlos[r];
   const double *__restrict__ rec = A.pts + (size_t)A.los_off[r] * A.W;
@@ -81,12 +83,13 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
           if ((r00.nf & 0xffff) >= 2 && (r01.nf & 0xffff) >= 2 &&
               (r10.nf & 0xffff) >= 2 && (r11.nf & 0xffff) >= 2) {
             const double x1 = 1 - tpg, useg = rec[REC_K + m.nw + g];
-            if (DIG) dig = dig * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
+            unsigned long long *dg = &dig[DIG ? g : 0];
+            if (DIG) *dg = *dg * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
             int j00, jx;
-            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, hint[g], &j00, &dig);
-            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, hint[g], &jx, &dig);
-            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, hint[g], &jx, &dig);
-            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, hint[g], &jx, &dig);
+            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, hint[g], &j00, dg);
+            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, hint[g], &jx, dg);
+            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, hint[g], &jx, dg);
+            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, hint[g], &jx, dg);
             hint[g] = j00;
             const double *gp = m.grid_p + (size_t)gid * TBLNPMAX;
             const double *gt = m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX;
@@ -143,7 +146,12 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
   }
   A.rad[(size_t)r * nd + d] = rad;
   A.tau[(size_t)r * nd + d] = tau;
-  if (DIG) A.digest[(size_t)r * nd + d] = dig;
+  if (DIG) {
+    // fold of the per-emitter digests in emitter order
+    unsigned long long dd = 0;
+    for (int g = 0; g < ng && g < GMAX; g++) dd = dd * 1000003ull + dig[g];
+    A.digest[(size_t)r * nd + d] = dd;
+  }
   const unsigned mask = __activemask();
   const unsigned tot = __reduce_add_sync(mask, n_ega);
   if ((threadIdx.x & 31) == __ffs(mask) - 1) atomicAdd(&A.counters[1], (unsigned long long)tot);
@@ -174,8 +182,8 @@ void jsc_ega_launch_g4(const EgaArgs &, unsigned, unsigned, int, bool, cudaStrea
 void jsc_ega_launch_g8(const EgaArgs &, unsigned, unsigned, int, bool, cudaStream_t);
 void jsc_ega_launch_gmax(const EgaArgs &, unsigned, unsigned, int, bool, cudaStream_t);
 
-// Index digests run the default variant (6: 128 threads, 12 blocks per SM,
-// rolled emitter loop) only.
+// Index digests run variant 6 (128 threads, 12 blocks per SM, rolled
+// emitter loop), the default of this kernel family.
 #define JSC_EGA_DEFAULT_VARIANT 6
 #define JSC_EGA_LAUNCHER(NAME, G)                                                      \
   void NAME(const EgaArgs &ea, unsigned g128, unsigned g256, int v, bool dig,          \

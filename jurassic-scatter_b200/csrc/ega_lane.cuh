@@ -1,0 +1,197 @@
+// The EGA + radiative-transfer kernel with lanes over (channel, emitter),
+// and the per-(LOS point, channel) continuum and Planck kernel it reads.
+//
+// ctm_src_kernel   one thread per (LOS point, channel): continuum extinction
+//                  (src/forwardmodel.c:120-152) and Planck source
+//                  (:788-793), written [point][channel].
+// ega_lane_kernel  a group of GP lanes per (ray, channel), one lane per
+//                  emitter: each lane carries its emitter's path
+//                  transmittance along the ray and evaluates its EGA
+//                  (src/forwardmodel.c:409-502); the group multiplies the
+//                  segment transmittances in emitter order (shuffles) and
+//                  every lane of the group runs the same radiative transfer
+//                  step (:302-399); lane 0 writes the result.
+//
+// One emitter per lane keeps the path state in registers (no local
+// arrays), the loop body small and the number of independent table
+// gathers in flight per SM high; the continua, whose transcendental
+// functions cost more than the EGA itself, run once per (point, channel)
+// in a separate, fully parallel launch.
+#pragma once
+#include "device_common.cuh"
+
+struct CtmArgs {
+  jsc_dev_model m;
+  jsc_run_cfg cfg;
+  int64_t n_points;
+  int W;
+  const double *pts;
+  double *beta, *src;  // [n_points][nd]
+};
+
+static __global__ void __launch_bounds__(256) ctm_src_kernel(CtmArgs A) {
+  const int nd = A.m.nd;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.n_points * nd) return;
+  const int64_t pt = t / nd;
+  const int d = (int)(t - pt * nd);
+  const double *rec = A.pts + pt * A.W;
+  const double P = rec[REC_P], T = rec[REC_T], DS = rec[REC_DS];
+  const int w = A.m.window[d];
+  A.beta[t] = continua(A.m, A.cfg, A.m.ctm[d], A.m.nu[d], w < A.m.nw ? rec[REC_K + w] : 0.0, P,
+                       T, DS, rec[REC_QH2O], rec + REC_K + A.m.nw);
+  const int itp = (int)rec[REC_PLK];
+  A.src[t] = planck_src(A.m, d, itp, T);
+}
+
+template <int GP, bool DIG, int BLK, int MINB>
+__global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
+  const jsc_dev_model &m = A.m;
+  const int nd = m.nd, ng = m.ng;
+  const int64_t tid = (int64_t)blockIdx.x * BLK + threadIdx.x;
+  const int64_t pc = tid / GP;  // (ray, channel) pair of this lane's group
+  const int r = (int)(pc / nd);
+  const int d = (int)(pc - (int64_t)r * nd);
+  if (r >= A.n_rays) return;  // whole groups leave together
+  const int g = (int)(threadIdx.x & (GP - 1));
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned gbase = lane & ~(unsigned)(GP - 1);
+  const unsigned gmask = GP == 32 ? 0xffffffffu : (((1u << GP) - 1u) << gbase);
+
+  const bool has_g = g < ng;
+  const int gid = has_g ? m.tab_grid[d * ng + g] : -1;
+  const bool ok = gid >= 0;  // the table of (channel, emitter) exists
+  const jsc_row *__restrict__ rows_dg = m.rows + (size_t)(has_g ? g : 0) * nd + d;
+  const size_t rs = (size_t)ng * nd;  // stride of one (ip, it) slot
+  const double *__restrict__ gp = m.grid_p + (size_t)(ok ? gid : 0) * TBLNPMAX;
+  const double *__restrict__ gt = m.grid_t + (size_t)(ok ? gid : 0) * TBLNPMAX * TBLNTMAX;
+
+  double tp = 1, rad = 0, tau = 1;
+  int hint = 0;
+  unsigned long long dig = 0;
+  unsigned n_ega = 0;
+  const int np = A.nlos[r];
+  const int64_t off = A.los_off[r];
+  const double *__restrict__ rec = A.pts + off * A.W;
+  const double *__restrict__ bc = A.beta_ctm + off * nd + d;
+  const double *__restrict__ sp = A.src_pl + off * nd + d;
+  const double *__restrict__ ssrc = A.src_sca ? A.src_sca + (size_t)A.sp_off[r] * nd + d : nullptr;
+
+  for (int ip = 0; ip < np; ip++, rec += A.W, bc += nd, sp += nd) {
+    const double P = rec[REC_P], T = rec[REC_T], DS = rec[REC_DS];
+    double eps = 0;
+    if (ok) {
+      if (tp < 1e-9) {
+        eps = 1;
+      } else {
+        const int code = A.single_grid
+                             ? (int)rec[REC_GRID]
+                             : grid_code(m.grid_np[gid], gp, m.grid_nt + (size_t)gid * TBLNPMAX, gt, P, T);
+        if (code & (1 << 16)) {
+          const int ipr = (code >> 10) & 63, it0 = (code >> 5) & 31, it1 = code & 31;
+          const jsc_row r00 = rows_dg[(size_t)(ipr * TBLNTMAX + it0) * rs];
+          const jsc_row r01 = rows_dg[(size_t)(ipr * TBLNTMAX + it0 + 1) * rs];
+          const jsc_row r10 = rows_dg[(size_t)((ipr + 1) * TBLNTMAX + it1) * rs];
+          const jsc_row r11 = rows_dg[(size_t)((ipr + 1) * TBLNTMAX + it1 + 1) * rs];
+          if ((r00.nf & 0xffff) >= 2 && (r01.nf & 0xffff) >= 2 && (r10.nf & 0xffff) >= 2 &&
+              (r11.nf & 0xffff) >= 2) {
+            const double x1 = 1 - tp, useg = rec[REC_K + m.nw + g];
+            if (DIG) dig = dig * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
+            int j00, jx;
+            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, hint, &j00, &dig);
+            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, hint, &jx, &dig);
+            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, hint, &jx, &dig);
+            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, hint, &jx, &dig);
+            hint = j00;
+            double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
+                                            gt[ipr * TBLNTMAX + it0 + 1], e01, T));
+            const double eb = jsc_clamp01(jsc_lin(gt[(ipr + 1) * TBLNTMAX + it1], e10,
+                                                  gt[(ipr + 1) * TBLNTMAX + it1 + 1], e11, T));
+            ea = jsc_clamp01(jsc_lin(gp[ipr], ea, gp[ipr + 1], eb, P));
+            eps = 1 - (1 - ea) / tp;
+            n_ega++;
+          }
+        }
+      }
+    }
+    tp = tp * (1 - eps);
+    // Segment transmittance: the product over emitters in emitter order,
+    // as the reference accumulates it (lanes past ng hold eps = 0).
+    const double f = 1 - eps;
+    double tau_gas = __shfl_sync(gmask, f, gbase);
+    for (int j = 1; j < ng; j++) tau_gas *= __shfl_sync(gmask, f, gbase + j);
+
+    const double beta = *bc, src = *sp;
+    const double af = rec[REC_AF];
+    if (ssrc && af > 0) {
+      // scattering point (src/forwardmodel.c:317-363)
+      if (tau_gas > 0) {
+        const int ia = (int)rec[REC_AI];
+        const double be = A.beta[ia * nd + d], bs = A.beta[A.aero_nl * nd + ia * nd + d];
+        const double bext = (-1.) * log(tau_gas) / DS + beta + af * be;
+        const double e = 1 - exp(-1 * bext * DS);
+        const double src_all = ((bext - af * bs) * src + af * bs * *ssrc) / bext;
+        rad += tau * e * src_all;
+        tau *= exp(-1. * bext * DS);
+      }
+      ssrc += nd;
+    } else if (tau_gas > 0) {
+      // clear air, or aerosol/cloud extinction (src/forwardmodel.c:365-389)
+      double e;
+      if (A.cfg.sca_n == 0 || af == 0) {
+        e = 1 - tau_gas * exp(-1. * beta * DS);
+      } else {
+        const int ia = (int)rec[REC_AI];
+        const double bx = A.beta[(A.cfg.sca_ext_beta_a ? 2 : 0) * A.aero_nl * nd + ia * nd + d];
+        e = 1 - tau_gas * exp(-1. * (beta + af * bx) * DS);
+      }
+      rad += src * e * tau;
+      tau *= (1 - e);
+    }
+  }
+  if (DIG) {
+    // per-channel digest: fold of the per-emitter digests in emitter order
+    unsigned long long dd = 0;
+    for (int j = 0; j < ng; j++) dd = dd * 1000003ull + __shfl_sync(gmask, dig, gbase + j);
+    dig = dd;
+  }
+  if (g == 0) {
+    const double ts = A.tsurf[r];
+    if (ts > 0) {
+      const int its = planck_index(ts);
+      rad += planck_src(m, d, its, ts) * tau;
+    }
+    A.rad[(size_t)r * nd + d] = rad;
+    A.tau[(size_t)r * nd + d] = tau;
+    if (DIG) A.digest[(size_t)r * nd + d] = dig;
+  }
+  const unsigned mask = __activemask();
+  const unsigned tot = __reduce_add_sync(mask, n_ega);
+  if (lane == (unsigned)(__ffs(mask) - 1)) atomicAdd(&A.counters[1], (unsigned long long)tot);
+}
+
+// Launch variants of ega_lane_kernel: (threads per block, minimum resident
+// blocks per SM).  Index digests run variant 0 only.
+template <int GP>
+static void ega_lane_variant(const EgaArgs &ea, int v, bool dig, cudaStream_t s) {
+  const int64_t threads = (int64_t)ea.n_rays * ea.m.nd * GP;
+  if (dig) {
+    ega_lane_kernel<GP, true, 128, 12><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(ea);
+    return;
+  }
+  constexpr bool DIG = false;
+  switch (v) {
+    case 1: ega_lane_kernel<GP, DIG, 128, 8><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(ea); break;
+    case 2: ega_lane_kernel<GP, DIG, 256, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(ea); break;
+    case 3: ega_lane_kernel<GP, DIG, 256, 5><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(ea); break;
+    case 4: ega_lane_kernel<GP, DIG, 512, 2><<<(unsigned)((threads + 511) / 512), 512, 0, s>>>(ea); break;
+    default: ega_lane_kernel<GP, DIG, 128, 12><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(ea); break;
+  }
+}
+
+// Launchers (ega_lane_s.cu: up to 4 emitters, ega_lane_l.cu: more and the
+// continuum kernel): lanes per group from the emitter count.
+void jsc_ega_lane_launch_s(const EgaArgs &ea, int v, bool dig, cudaStream_t s);
+void jsc_ega_lane_launch_l(const EgaArgs &ea, int v, bool dig, cudaStream_t s);
+void jsc_ctm_src_launch(const CtmArgs &ca, cudaStream_t s);
+#define JSC_LANE_VARIANTS 5

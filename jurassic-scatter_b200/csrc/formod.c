@@ -99,9 +99,9 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
     jsc_set_error(JSC_ERR_UNSUPPORTED, "field-of-view convolution (FOV=%s)", ctl->fov);
     return JSC_ERR_UNSUPPORTED;
   }
-  if (ctl->sca_n > 0) {
-    jsc_set_error(JSC_ERR_UNSUPPORTED, "aerosol/cloud models (SCA_N=%d)", ctl->sca_n);
-    return JSC_ERR_UNSUPPORTED;
+  if (ctl->sca_n > 0 && !aero) {
+    jsc_set_error(JSC_ERR_ARG, "formod: SCA_N=%d needs the aerosol/cloud data", ctl->sca_n);
+    return JSC_ERR_ARG;
   }
 
   /* Observation mask (src/forwardmodel.c:25-28). */
@@ -171,7 +171,10 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
       out.tpz = tp;
       out.tplon = tp + nr;
       out.tplat = tp + 2 * nr;
-      st = jsc_batch_upload(g_batch, &in, NULL);
+      /* Aerosol/cloud layers and optical properties (read_aero +
+       * get_opt_prop of the caller, or of this call for retrievals). */
+      if (ctl->sca_n > 0) st = jsc_batch_set_aero(g_batch, aero);
+      if (!st) st = jsc_batch_upload(g_batch, &in, NULL);
       if (!st) st = jsc_batch_run(g_batch, NULL);
       if (!st) st = jsc_batch_download(g_batch, &out, NULL);
       if (!st) {

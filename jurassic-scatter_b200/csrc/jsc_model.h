@@ -57,10 +57,13 @@ struct EgaArgs {
   // sp_off[r] on, in LOS order.  Null: extinction only.
   const double *src_sca;
   const int64_t *sp_off;
+  // Continuum extinction and Planck source per (LOS point, channel),
+  // [n_points][nd] (read by the lane kernel).
+  const double *beta_ctm, *src_pl;
 };
 
 // Kernel timers of a batch.
-enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_SCATTER, JSC_T_N };
+enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_SCATTER, JSC_T_CTM, JSC_T_N };
 
 #define JSC_NALPHA_REF 28  // secondary pencils per scattering point (src/scatter.c:673)
 
@@ -112,11 +115,27 @@ struct jsc_batch {
   jsc_batch *child, *sun_child;
   ctl_t *ctl;               // copy for child batches
 
+  // Scattering-source surrogate (caller's batch only): the network, the
+  // relative tolerance of the sampled check and its stride, per-point
+  // features and marks, the plain-path subset, and the last run's counts.
+  struct jsc_surrogate *sur;
+  int sur_on, sur_stride;
+  float sur_tol;
+  int64_t sur_cap;
+  float *d_feat;
+  int *d_mark, *d_idx, *d_atm_sub;
+  double *d_sp_sub, *d_src_sub;
+  int64_t sur_points, sur_fallback, sur_checked, sur_rejected;
+  float sur_maxerr;
+  int sur_used;
+
   // Line of sight.
   int *d_nlos;
   int64_t *d_los_off;       // [max_rays+1]
   double *d_geo;            // [max_seg][4]: z lon lat raw-ds
   double *d_pts;            // [max_seg][W]: p t ds qh2o k[nw] u[ng]
+  double *d_ctm, *d_srcp;   // [max_seg][nd]: continuum extinction, Planck source
+  int64_t n_points;         // LOS points of the current run
   double *d_tsurf;          // [max_rays]
   double *d_tp;             // [3][max_rays]
 

@@ -20,13 +20,14 @@
 #pragma once
 #include "kernels.cuh"
 
-#define JSC_SP_REC 8      // doubles per scattering point record
+#define JSC_SP_REC 10     // doubles per scattering point record
 #define JSC_NPHI_SCA 180  // azimuth steps of the source integral
 #define JSC_NTH_SCA 180   // polar steps of the source integral
 #define JSC_NALPHA_MAX 32 // secondary pencils per scattering point
 
-// Scattering point record (doubles): x[3], dx[3], layer, time.
-enum { SP_X = 0, SP_DX = 3, SP_IL = 6, SP_TIME = 7 };
+// Scattering point record (doubles): x[3], dx[3], layer, time, pressure,
+// temperature.
+enum { SP_X = 0, SP_DX = 3, SP_IL = 6, SP_TIME = 7, SP_P = 8, SP_T = 9 };
 
 // Orthonormal basis with ez along dz and ey in the plane of dy and dz
 // (bascoord, src/scatter.c:6-52).
@@ -124,6 +125,8 @@ static __global__ void sp_list_kernel(SpArgs A) {
     }
     o[SP_IL] = rc[REC_AI];
     o[SP_TIME] = A.time[r];
+    o[SP_P] = rc[REC_P];
+    o[SP_T] = rc[REC_T];
     A.sp_atm[k] = A.ray_atm[r];
     k++;
   }

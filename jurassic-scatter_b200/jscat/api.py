@@ -157,6 +157,38 @@ class Batch:
         """Aerosol/cloud layers (an AeroT) for runs with ctl.sca_n > 0."""
         L.check(L.load().jsc_batch_set_aero(self.h, C.byref(aero)), "jsc_batch_set_aero")
 
+    def scatter_samples(self):
+        """Features [n][8] and plain scattering sources [n][nd] of the last
+        run's scattering points."""
+        lib = L.load()
+        n = C.c_int64()
+        L.check(lib.jsc_batch_scatter_samples(self.h, None, None, 0, C.byref(n)),
+                "jsc_batch_scatter_samples")
+        feat = np.empty((n.value, Surrogate.NF), np.float32)
+        src = np.empty((n.value, self.nd))
+        if n.value:
+            L.check(lib.jsc_batch_scatter_samples(self.h, _fptr(feat), _dptr(src), n.value,
+                                                  C.byref(n)), "jsc_batch_scatter_samples")
+        return feat, src
+
+    def set_surrogate(self, sur, tol_rel=0.05, check_stride=64):
+        L.check(L.load().jsc_batch_set_surrogate(self.h, sur.h if sur is not None else None,
+                                                 float(tol_rel), int(check_stride)),
+                "jsc_batch_set_surrogate")
+
+    def surrogate_stats(self):
+        p, f, c, u = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int()
+        e = C.c_double()
+        L.check(L.load().jsc_batch_surrogate_stats(self.h, C.byref(p), C.byref(f), C.byref(c),
+                                                   C.byref(e), C.byref(u)),
+                "jsc_batch_surrogate_stats")
+        return {"points": p.value, "fallback": f.value, "checked": c.value,
+                "max_rel_err": e.value, "used": bool(u.value)}
+
+    def set_variant(self, variant):
+        """EGA launch variant (-1: default); see jsc_batch_set_variant."""
+        L.check(L.load().jsc_batch_set_variant(self.h, int(variant)), "jsc_batch_set_variant")
+
     def set_nalpha(self, nalpha):
         """Secondary pencils per scattering point (even, 10..28; 28 default)."""
         L.check(L.load().jsc_batch_set_nalpha(self.h, int(nalpha)), "jsc_batch_set_nalpha")
@@ -186,7 +218,7 @@ class Batch:
 
 
 def formod_batch(ctl, inp, device=0, model=None, digest=False, aero=None, nalpha=None,
-                 timing=False):
+                 timing=False, variant=None):
     """One-shot batch forward model: returns dict of rad/tau/tp*/nlos (and
     the per-(ray, channel) EGA index digests when digest=True).  aero: an
     AeroT with the layers and optical properties when ctl.sca_n > 0;
@@ -203,13 +235,16 @@ def formod_batch(ctl, inp, device=0, model=None, digest=False, aero=None, nalpha
             b.set_digest(True)
         if nalpha is not None:
             b.set_nalpha(nalpha)
+        if variant is not None:
+            b.set_variant(variant)
         if timing:
             b.set_timing(True)
         b.upload(inp)
         b.run()
         out = b.download()
         if timing:
-            out["ms"] = {k: b.kernel_ms(k) for k in ("hydrostatic", "raytrace", "scatter", "ega_rt")}
+            out["ms"] = {k: b.kernel_ms(k) for k in ("hydrostatic", "raytrace", "scatter",
+                                                     "continua", "ega_rt")}
         if digest:
             out["digest"] = b.index_digest()
         return out
@@ -248,6 +283,88 @@ def formod_batch_noalloc(ctl, inp, model, stream=None):
                                               C.byref(bo), stream),
             "jsc_formod_batch_noalloc")
     return out
+
+
+_F = C.POINTER(C.c_float)
+
+
+def _fptr(a):
+    return a.ctypes.data_as(_F)
+
+
+class Surrogate:
+    """Scattering-source surrogate (jsc_surrogate_*): a 4-layer MLP trained
+    on the GPU on plain-path samples, BF16 tensor-core inference."""
+
+    NF = 8
+
+    def __init__(self, nd, device=0, seed=1):
+        self.nd = nd
+        self.h = C.c_void_p()
+        L.check(L.load().jsc_surrogate_create(int(nd), int(device), int(seed), C.byref(self.h)),
+                "jsc_surrogate_create")
+
+    @property
+    def n_params(self):
+        return L.load().jsc_surrogate_param_count(self.h)
+
+    def get_params(self):
+        out = np.empty(self.n_params, np.float32)
+        L.check(L.load().jsc_surrogate_get_params(self.h, _fptr(out)), "jsc_surrogate_get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        L.check(L.load().jsc_surrogate_set_params(self.h, _fptr(p)), "jsc_surrogate_set_params")
+
+    def layers(self, flat):
+        """Split a flat parameter vector into [(W0, b0), ..., (W3, b3)]."""
+        shapes = [(128, self.NF), (128, 128), (128, 128), (self.nd, 128)]
+        out, o = [], 0
+        for r, c in shapes:
+            w = flat[o:o + r * c].reshape(r, c)
+            o += r * c
+            b = flat[o:o + r]
+            o += r
+            out.append((w, b))
+        return out
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = C.c_float()
+        g = np.empty(self.n_params, np.float32)
+        L.check(L.load().jsc_surrogate_loss_grad(self.h, _fptr(x), _fptr(t), len(x),
+                                                 C.byref(loss), _fptr(g)),
+                "jsc_surrogate_loss_grad")
+        return loss.value, g
+
+    def train(self, feat, src, epochs=20, batch=4096, lr=2e-3, seed=7):
+        feat = np.ascontiguousarray(feat, dtype=np.float32)
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        losses = np.zeros(epochs, np.float32)
+        L.check(L.load().jsc_surrogate_train(self.h, _fptr(feat), _dptr(src), len(feat), int(epochs),
+                                             int(batch), float(lr), int(seed), _fptr(losses)),
+                "jsc_surrogate_train")
+        return losses
+
+    def predict(self, feat):
+        feat = np.ascontiguousarray(feat, dtype=np.float32)
+        out = np.empty((len(feat), self.nd))
+        L.check(L.load().jsc_surrogate_predict(self.h, _fptr(feat), len(feat), _dptr(out)),
+                "jsc_surrogate_predict")
+        return out
+
+    def close(self):
+        if self.h:
+            L.load().jsc_surrogate_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def launch_count():

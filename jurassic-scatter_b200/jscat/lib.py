@@ -20,6 +20,10 @@ EXPORTS = [
     "jsc_batch_counters", "jsc_batch_set_digest", "jsc_batch_index_digest",
     "jsc_batch_autotune", "jsc_batch_variant", "jsc_batch_variant_ms",
     "jsc_batch_set_aero", "jsc_formod_batch_noalloc", "jsc_batch_set_nalpha",
+    "jsc_batch_set_variant", "jsc_surrogate_create", "jsc_surrogate_destroy",
+    "jsc_surrogate_param_count", "jsc_surrogate_get_params", "jsc_surrogate_set_params",
+    "jsc_surrogate_loss_grad", "jsc_surrogate_train", "jsc_surrogate_predict",
+    "jsc_batch_scatter_samples", "jsc_batch_set_surrogate", "jsc_batch_surrogate_stats",
 ]
 
 
@@ -94,6 +98,21 @@ def load():
         "jsc_batch_variant_ms": (d, [vp, i]),
         "jsc_batch_set_aero": (i, [vp, P(S.AeroT)]),
         "jsc_batch_set_nalpha": (i, [vp, i]),
+        "jsc_batch_set_variant": (i, [vp, i]),
+        "jsc_surrogate_create": (i, [i, i, C.c_uint64, P(vp)]),
+        "jsc_surrogate_destroy": (None, [vp]),
+        "jsc_surrogate_param_count": (i, [vp]),
+        "jsc_surrogate_get_params": (i, [vp, P(C.c_float)]),
+        "jsc_surrogate_set_params": (i, [vp, P(C.c_float)]),
+        "jsc_surrogate_loss_grad": (i, [vp, P(C.c_float), P(C.c_float), i, P(C.c_float),
+                                        P(C.c_float)]),
+        "jsc_surrogate_train": (i, [vp, P(C.c_float), P(d), C.c_int64, i, i, C.c_float,
+                                    C.c_uint64, P(C.c_float)]),
+        "jsc_surrogate_predict": (i, [vp, P(C.c_float), i, P(d)]),
+        "jsc_batch_scatter_samples": (i, [vp, P(C.c_float), P(d), C.c_int64, P(C.c_int64)]),
+        "jsc_batch_set_surrogate": (i, [vp, vp, d, i]),
+        "jsc_batch_surrogate_stats": (i, [vp, P(C.c_int64), P(C.c_int64), P(C.c_int64), P(d),
+                                          P(i)]),
         "jsc_formod_batch_noalloc": (i, [vp, P(S.CtlT), P(BatchInput), P(BatchOutput), vp]),
     }
     for name, (res, args) in sig.items():

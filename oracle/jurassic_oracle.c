@@ -716,17 +716,17 @@ static double o_tbl_u(const otab_t *tb, int ip, int it, double eps, uint64_t *di
 
 #define CLAMP01(e) MAX(MIN((e), 1), 0)
 
-/* src/forwardmodel.c:409-502.  digs (optional, [nd]) accumulate, per
- * channel, every table index the interpolation selects. */
+/* src/forwardmodel.c:409-502.  digs (optional, [nd][ng]) accumulate, per
+ * channel and emitter, every table index the interpolation selects. */
 static void o_intpol_tbl(const ctl_t *ctl, const olos_t *los, int ip,
                          double tau_path[NGMAX][NDMAX], double *tau_seg, uint64_t *digs) {
   if (ip <= 0)
     for (int ig = 0; ig < ctl->ng; ig++)
       for (int id = 0; id < ctl->nd; id++) tau_path[ig][id] = 1;
   for (int id = 0; id < ctl->nd; id++) {
-    uint64_t *dig = digs ? &digs[id] : NULL;
     tau_seg[id] = 1;
     for (int ig = 0; ig < ctl->ng; ig++) {
+      uint64_t *dig = digs ? &digs[id * ctl->ng + ig] : NULL;
       const otab_t *tb = &g_tab[id * ctl->ng + ig];
       double eps;
       if (tb->np < 2)
@@ -1055,6 +1055,8 @@ static int o_pencil(const ctl_t *ctl, const atm_t *atm, obs_t *obs, const aero_t
   double beta[NDMAX], src[NDMAX], tau_seg[NDMAX], src_sca[NDMAX], x[3], x0[3], x1[3], dx[3];
   double (*tau_path)[NDMAX] = malloc(sizeof(double) * NGMAX * NDMAX);
   olos_t *los = los_new();
+  /* per (channel, emitter) index digests, folded per channel at the end */
+  uint64_t *gdig = dig ? (uint64_t *)calloc((size_t)NDMAX * NGMAX, sizeof(uint64_t)) : NULL;
   int st = o_raytrace(ctl, atm, obs, aero, los, ir);
   const int beta_a = strcmp(ctl->sca_ext, "beta_a") == 0;
   if (nlos) *nlos = los->np;
@@ -1063,7 +1065,7 @@ static int o_pencil(const ctl_t *ctl, const atm_t *atm, obs_t *obs, const aero_t
     obs->tau[id][ir] = 1;
   }
   for (int ip = 0; ip < los->np && !st; ip++) {
-    o_intpol_tbl(ctl, los, ip, tau_path, tau_seg, dig);
+    o_intpol_tbl(ctl, los, ip, tau_path, tau_seg, gdig);
     o_continua(ctl, los, ip, beta);
     o_srcfunc_planck(ctl, los->t[ip], src);
     const double af = los->aerofac[ip];
@@ -1107,6 +1109,13 @@ static int o_pencil(const ctl_t *ctl, const atm_t *atm, obs_t *obs, const aero_t
     o_srcfunc_planck(ctl, los->tsurf, src);
     for (int id = 0; id < ctl->nd; id++) obs->rad[id][ir] += src[id] * obs->tau[id][ir];
   }
+  if (dig) {
+    for (int id = 0; id < ctl->nd; id++) {
+      dig[id] = 0;
+      for (int ig = 0; ig < ctl->ng; ig++) dig[id] = dig[id] * 1000003u + gdig[id * ctl->ng + ig];
+    }
+    free(gdig);
+  }
   los_free(los);
   free(tau_path);
   return st;
@@ -1147,10 +1156,11 @@ int oracle_formod(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
 }
 
 /* LOS point counts per ray and EGA index checksums per (ray, channel):
- * digest[ir*nd+id] = fold over LOS points, then emitters, of the (p, T)
- * bracket code ipr*961+it0*31+it1 followed by the eps->u and u->eps
- * interval indices of the four (p, T) nodes in the order (ipr,it0),
- * (ipr,it0+1), (ipr+1,it1), (ipr+1,it1+1); fold: d = d*1000003 + v.
+ * digest[ir*nd+id] = fold over emitters of D_g, where D_g folds, over the
+ * LOS points with a full interpolation of emitter g, the (p, T) bracket
+ * code ipr*961+it0*31+it1 followed by the eps->u and u->eps interval
+ * indices of the four (p, T) nodes in the order (ipr,it0), (ipr,it0+1),
+ * (ipr+1,it1), (ipr+1,it1+1); fold: d = d*1000003 + v.
  * The radiances are computed as by oracle_formod. */
 int oracle_diagnostics(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, int *nlos,
                        uint64_t *digest) {

@@ -1,0 +1,41 @@
+"""FP64 numpy restatement of the scattering-source surrogate network, for
+checking the GPU training kernels.  TEST INFRASTRUCTURE ONLY: imported by
+tests/, never by the product.
+
+Network: x[NF] -> tanh(W0 x + b0) -> tanh(W1 . + b1) -> tanh(W2 . + b2)
+-> W3 . + b3 = y[nout]; weights W_l are [out][in] row-major.  Loss: mean
+over the batch of the sum over outputs of (y - t)^2.
+"""
+import numpy as np
+
+
+def forward(params, x):
+    """params: [(W0, b0), ..., (W3, b3)]; x: [n][NF].  Returns the
+    activations of every layer (input first) and the output."""
+    acts = [x]
+    h = x
+    for li, (w, b) in enumerate(params):
+        z = h @ w.T + b
+        h = np.tanh(z) if li < len(params) - 1 else z
+        acts.append(h)
+    return acts
+
+
+def loss_and_grads(params, x, t):
+    """Loss and gradients (same structure as params) for one batch."""
+    x = np.asarray(x, dtype=np.float64)
+    t = np.asarray(t, dtype=np.float64)
+    p64 = [(np.asarray(w, np.float64), np.asarray(b, np.float64)) for w, b in params]
+    acts = forward(p64, x)
+    n = x.shape[0]
+    y = acts[-1]
+    loss = np.sum((y - t) ** 2) / n
+    dh = 2.0 * (y - t) / n
+    grads = [None] * len(p64)
+    for li in range(len(p64) - 1, -1, -1):
+        w, _ = p64[li]
+        if li < len(p64) - 1:
+            dh = dh * (1.0 - acts[li + 1] ** 2)  # tanh'
+        grads[li] = (dh.T @ acts[li], dh.sum(axis=0))
+        dh = dh @ w
+    return loss, grads

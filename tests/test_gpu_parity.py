@@ -54,26 +54,33 @@ def test_clear_limb_dropin_formod(workdir):
     np.testing.assert_allclose(S.arr(obs.tpz)[:nr], g["tpz"], rtol=1e-9, atol=1e-9)
 
 
-def test_clear_limb_batch_indices(workdir):
+# EGA kernel families: -1 the default (a thread per (ray, channel)), 9 a
+# lane per (ray, channel, emitter)
+VARIANTS = [-1, 9]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_clear_limb_batch_indices(workdir, variant):
     from jscat import structs as S, synth, api
     g = _load("clear_limb")
     ctlkw, atm, geom = synth.clear_limb_case(workdir)
     ctl = S.make_ctl(**ctlkw)
     out = api.formod_batch(ctl, synth.batch_from([atm], np.zeros(len(geom["obsz"]), np.int32), geom),
-                           digest=True)
+                           digest=True, variant=variant)
     np.testing.assert_array_equal(out["nlos"], g["nlos"])
     np.testing.assert_array_equal(out["digest"], g["digest"])
     assert max_rel(out["rad"], g["rad"]) <= REL_TOL
 
 
-def test_mixed_batch(workdir):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_mixed_batch(workdir, variant):
     from jscat import synth, api, structs as S
     from make_golden_shim import mixed_case
     g = _load("mixed_batch")
     ctlkw, atms, ray_atm, geom = mixed_case(workdir)
     _check_tables(g, ctlkw)
     ctl = S.make_ctl(**ctlkw)
-    out = api.formod_batch(ctl, synth.batch_from(atms, ray_atm, geom), digest=True)
+    out = api.formod_batch(ctl, synth.batch_from(atms, ray_atm, geom), digest=True, variant=variant)
     np.testing.assert_array_equal(out["nlos"], g["nlos"])
     np.testing.assert_array_equal(out["digest"], g["digest"])
     assert bt_error(out["rad"], g["rad"], ctlkw["nus"]) <= BT_TOL_K
@@ -82,8 +89,9 @@ def test_mixed_batch(workdir):
     np.testing.assert_allclose(out["tpz"], g["tpz"], rtol=1e-9, atol=1e-9)
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("ext", ["beta_a", "beta_e"])
-def test_aerosol_extinction(workdir, ext):
+def test_aerosol_extinction(workdir, ext, variant):
     """Aerosol layer with extinction only (SCA_MULT=0): layer-edge LOS
     refinement (add_aerosol_layers) and the aerosol RT branch."""
     from jscat import synth, api, structs as S
@@ -94,7 +102,7 @@ def test_aerosol_extinction(workdir, ext):
     aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
     ctl = S.make_ctl(**ctlkw)
     out = api.formod_batch(ctl, synth.batch_from([atm], np.zeros(len(geom["obsz"]), np.int32), geom),
-                           digest=True, aero=aero)
+                           digest=True, aero=aero, variant=variant)
     np.testing.assert_array_equal(out["nlos"], g["nlos"])
     np.testing.assert_array_equal(out["digest"], g["digest"])
     assert bt_error(out["rad"], g["rad"], ctlkw["nus"]) <= BT_TOL_K
@@ -102,8 +110,9 @@ def test_aerosol_extinction(workdir, ext):
     assert max_rel(out["tau"], g["tau"]) <= REL_TOL
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("when", ["night", "day"])
-def test_aerosol_single_scattering(workdir, when):
+def test_aerosol_single_scattering(workdir, when, variant):
     """Single scattering (SCA_MULT=1) on the sulfate-like layer: secondary
     pencils, source integral and, by day, the solar term (srcfunc_sca_1d
     and srcfunc_sca_sun), against the reference's own outputs.  The
@@ -120,7 +129,7 @@ def test_aerosol_single_scattering(workdir, when):
     aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
     ctl = S.make_ctl(**ctlkw)
     out = api.formod_batch(ctl, synth.batch_from([atm], np.zeros(len(geom["obsz"]), np.int32), geom),
-                           aero=aero)
+                           aero=aero, variant=variant)
     np.testing.assert_array_equal(out["nlos"], g["nlos"])
     assert bt_error(out["rad"], g["rad"], ctlkw["nus"]) <= BT_TOL_K
     assert max_rel(out["rad"], g["rad"]) <= REL_TOL
@@ -128,3 +137,22 @@ def test_aerosol_single_scattering(workdir, when):
     d_ref = g["rad"] - ge["rad"]
     d_gpu = out["rad"] - ge["rad"]
     assert np.max(np.abs(d_gpu - d_ref)) <= 1e-6 * np.max(np.abs(d_ref))
+
+
+def test_dropin_formod_single_scattering(workdir):
+    """The drop-in formod() on the reference's structs with an aerosol layer
+    and SCA_MULT=1 (daytime: thermal and solar scattering source)."""
+    from jscat import structs as S, synth, api
+    from make_golden_shim import aerosol_case
+    g = _load("aerosol_sca1_day")
+    ctlkw, atm, geom, aerofile = aerosol_case(workdir, 1)
+    ctl = S.make_ctl(**ctlkw)
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm["k"])
+    n = len(geom["obsz"])
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"],
+                     geom["obslon"], geom["vplon"], np.full(n, 43200.0))
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    api.formod(ctl, a, obs, aero)
+    rad = S.arr(obs.rad)[:ctl.nd, :n].T
+    assert bt_error(rad, g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(rad, g["rad"]) <= REL_TOL

@@ -1,0 +1,114 @@
+"""Scattering-source surrogate on the GPU: training gradients against the
+FP64 numpy restatement (oracle/mlp_ref.py), training on plain-path samples,
+radiances with the surrogate against the plain path, envelope fallback and
+rejection by the sampled check."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from helpers import bt_error
+
+pytestmark = pytest.mark.gpu
+
+
+def test_training_gradients_match_cpu():
+    from jscat import api
+    from oracle import mlp_ref
+    rng = np.random.default_rng(5)
+    s = api.Surrogate(nd=6, seed=11)
+    try:
+        p = s.get_params()
+        p = (p + rng.normal(0, 0.05, p.shape)).astype(np.float32)  # nonzero biases too
+        s.set_params(p)
+        x = rng.normal(0, 1, (200, 8)).astype(np.float32)
+        t = rng.normal(0, 1, (200, 6)).astype(np.float32)
+        loss, g = s.loss_grad(x, t)
+        ref_loss, ref_g = mlp_ref.loss_and_grads(s.layers(p.astype(np.float64)), x, t)
+        assert abs(loss - ref_loss) <= 1e-4 * abs(ref_loss)
+        flat = np.concatenate([np.concatenate([gw.ravel(), gb]) for gw, gb in ref_g])
+        # FP32 kernels against FP64: relative to the largest gradient
+        assert np.max(np.abs(g - flat)) <= 2e-4 * np.max(np.abs(flat))
+    finally:
+        s.close()
+
+
+def _sca_case(workdir, n_rays, times):
+    from jscat import synth, structs as S
+    from make_golden_shim import aerosol_case
+    g = dict(np.load(GOLDEN + "/aerosol_sca1_day.npz"))
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    ctlkw, atm, geom, _ = aerosol_case(workdir, 1, n_rays=n_rays)
+    geom["time"] = np.resize(np.asarray(times, dtype=np.float64), n_rays)
+    return ctlkw, atm, geom, aero
+
+
+def test_surrogate_trains_and_replaces_plain_source(workdir):
+    from jscat import api, synth, structs as S
+    # training data: plain sources of limb rays at several times of day
+    ctlkw, atm, geom, aero = _sca_case(workdir, 96, np.linspace(0, 86400, 7))
+    ctl = S.make_ctl(**ctlkw)
+    m = api.Model(ctl)
+    inp = synth.batch_from([atm], np.zeros(96, np.int32), geom)
+    b = api.Batch(m, ctl, 1, len(inp["z"]), 96)
+    sur = api.Surrogate(ctl.nd, seed=3)
+    try:
+        b.set_aero(aero)
+        b.set_nalpha(10)
+        b.upload(inp)
+        b.run()
+        plain = b.download()
+        feat, src = b.scatter_samples()
+        assert len(feat) > 500 and np.all(src > 0)
+        losses = sur.train(feat, src, epochs=60, batch=256, lr=3e-3)
+        assert losses[-1] < 0.5 * losses[0]
+        # surrogate path, everything inside the envelope, sampled check on
+        b.set_surrogate(sur, tol_rel=0.5, check_stride=16)
+        b.run()
+        out = b.download()
+        st = b.surrogate_stats()
+        assert st["used"] and st["fallback"] == 0 and st["checked"] > 0
+        assert st["max_rel_err"] < 0.5
+        assert bt_error(out["rad"], plain["rad"], ctlkw["nus"]) <= 0.05
+        # a tolerance the surrogate cannot meet: the batch falls back whole
+        b.set_surrogate(sur, tol_rel=1e-9, check_stride=1)
+        b.run()
+        out2 = b.download()
+        st2 = b.surrogate_stats()
+        assert not st2["used"]
+        np.testing.assert_array_equal(out2["rad"], plain["rad"])
+    finally:
+        sur.close()
+        b.close()
+        m.close()
+
+
+def test_surrogate_envelope_fallback(workdir):
+    """Points outside the training envelope (here: every point, the network
+    was trained on features of another layer index) take the plain path and
+    reproduce it exactly."""
+    from jscat import api, synth, structs as S
+    ctlkw, atm, geom, aero = _sca_case(workdir, 24, [43200.0])
+    ctl = S.make_ctl(**ctlkw)
+    m = api.Model(ctl)
+    inp = synth.batch_from([atm], np.zeros(24, np.int32), geom)
+    b = api.Batch(m, ctl, 1, len(inp["z"]), 24)
+    sur = api.Surrogate(ctl.nd, seed=3)
+    try:
+        b.set_aero(aero)
+        b.set_nalpha(10)
+        b.upload(inp)
+        b.run()
+        plain = b.download()
+        feat, src = b.scatter_samples()
+        feat[:, 6] += 5.0  # train on a shifted layer index: real points fall outside
+        sur.train(feat, src, epochs=2, batch=64, lr=1e-3)
+        b.set_surrogate(sur, tol_rel=0.5, check_stride=0)
+        b.run()
+        out = b.download()
+        st = b.surrogate_stats()
+        assert st["fallback"] == st["points"] > 0
+        np.testing.assert_array_equal(out["rad"], plain["rad"])
+    finally:
+        sur.close()
+        b.close()
+        m.close()
