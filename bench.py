@@ -14,6 +14,12 @@ e2e:   same, through the C-ABI with host buffers: every step copies the
 Inputs (5.9 GB of table intervals, ~4 GB of LOS records) exceed the 126 MB
 L2, so no flush is needed between steps.
 
+scattering (extra key of the same line): the plain single-scattering
+forward model against the surrogate-accelerated one on 20,000 limb rays
+through a sulfate-like layer (16 channels, 20 secondary pencils per
+scattering point); the surrogate is trained on the GPU on plain-path
+sources before it is timed.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
 import argparse
@@ -45,6 +51,11 @@ def parse():
     ap.add_argument("--cpu-rays", type=int, default=600,
                     help="rays of the bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sca-rays", type=int, default=20_000,
+                    help="rays of the scattering (plain vs surrogate) workload; 0 skips it")
+    ap.add_argument("--sca-epochs", type=int, default=40)
+    ap.add_argument("--requests", type=int, default=512,
+                    help="requests of the mixed-size request batch; 0 skips it")
     return ap.parse_args()
 
 
@@ -122,6 +133,301 @@ def algorithmic_bytes(n_ega, n_points, n_rays, nd, ng):
     per LOS point and channel the Planck bracket (8 B); per LOS point p, T
     and u[g] (16 + 8 G B); per ray and channel rad + tau out (8 B)."""
     return 128 * n_ega + 8 * n_points * nd + (16 + 8 * ng) * n_points + 8 * n_rays * nd
+
+
+SCA_WORKLOAD = ("single scattering on a sulfate-like layer at 15-20 km: limb rays TH U[8, 30] km, "
+                "times of day U[0, 86400] s, 16 channels 780-1250 cm-1, 2 emitters, 20 secondary "
+                "pencils per scattering point")
+
+
+def scattering_case(n, seed):
+    from jscat import synth, structs as S
+    workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
+    g = np.load(os.path.join(REPO, "tests", "golden", "aero_sulfate16.npz"))
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    nus = [float(v) for v in g["nus"]]
+    rng = np.random.default_rng(seed)
+    atm = synth.atmosphere(synth.CFG0_EMITTERS, rng)
+    geom = synth.limb_geometry(rng.uniform(8.0, 30.0, n))
+    geom["time"] = rng.uniform(0.0, 86400.0, n)
+    base = synth.write_tables(workdir, synth.CFG0_EMITTERS, nus, 20261203)
+    ctlkw = dict(emitters=synth.CFG0_EMITTERS, nus=nus, tblbase=base, hydz=0.0, sca_n=1,
+                 sca_mult=1, sca_ext="beta_a")
+    return ctlkw, atm, geom, aero
+
+
+def scattering_bench(args, local, torch, oracle_sample=True):
+    """Plain scattering forward model against the surrogate-accelerated one
+    on the scattering workload (single GPU): the surrogate is trained on
+    plain-path sources of three seeded batches (the timed one included),
+    then both paths are timed with CUDA events; BT errors are taken
+    against the plain GPU path on every ray and against the C oracle
+    (oracle/jurassic_oracle.c, same 20 pencils) on a ray sample."""
+    from jscat import api, structs as S, synth
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    from helpers import bt_error
+    n = args.sca_rays
+    ctlkw, atm, geom, aero = scattering_case(n, 1)
+    ctl = S.make_ctl(**ctlkw)
+    nd = ctl.nd
+    inp = synth.batch_from([atm], np.zeros(n, np.int32), geom)
+    model = api.Model(ctl, device=local)
+    b = api.Batch(model, ctl, 1, len(inp["z"]), n)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(steps):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            b.run(stream=sp)
+        e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    b.set_aero(aero)
+    b.set_nalpha(20)
+    b.upload(inp, stream=sp)
+    b.run(stream=sp)                       # warm-up, also the first training batch
+    stream.synchronize()
+    feats, srcs = [], []
+    f, s_ = b.scatter_samples()
+    feats.append(f)
+    srcs.append(s_)
+    plain_ms = timed(1)
+    plain = b.download(stream=sp)
+    for seed in (2, 3):                    # two more batches of training samples
+        c2, a2, g2, _ = scattering_case(n, seed)
+        b.upload(synth.batch_from([a2], np.zeros(n, np.int32), g2), stream=sp)
+        b.run(stream=sp)
+        stream.synchronize()
+        f, s_ = b.scatter_samples()
+        feats.append(f)
+        srcs.append(s_)
+    X, Y = np.concatenate(feats), np.concatenate(srcs)
+    sur = api.Surrogate(nd, device=local, seed=5)
+    t0 = time.perf_counter()
+    losses = sur.train(X, Y, epochs=args.sca_epochs, batch=4096, lr=3e-3)
+    train_s = time.perf_counter() - t0
+    b.upload(inp, stream=sp)
+    b.set_surrogate(sur, tol_rel=0.01, check_stride=256)
+    for _ in range(3):
+        b.run(stream=sp)
+    sur_ms = timed(5)
+    out = b.download(stream=sp)
+    st = b.surrogate_stats()
+    res = {"workload": SCA_WORKLOAD, "rays": n, "channels": nd, "scattering_points": st["points"],
+           "plain": {"value": n * nd / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
+                     "steps": 1, "warmup": 1},
+           "surrogate": {"value": n * nd / (sur_ms / 1e3), "unit": UNIT, "ms_per_step": sur_ms,
+                         "steps": 5, "warmup": 3, "speedup_vs_plain": plain_ms / sur_ms,
+                         "bt_err_k_vs_plain": bt_error(out["rad"], plain["rad"], ctlkw["nus"]),
+                         "used": st["used"], "fallback_points": st["fallback"],
+                         "checked_points": st["checked"],
+                         "max_albedo_weighted_src_err_checked": st["max_rel_err"], "check_tolerance": 0.01,
+                         "network": "4 layers, width 128, tanh; BF16 weights, FP32 accumulation "
+                                    "(mma.sync m16n8k16)"},
+           "training": {"samples": int(len(X)), "epochs": args.sca_epochs, "seconds": train_s,
+                        "final_loss": float(losses[-1]),
+                        "kernels": "hand-written FP32 SGEMM forward/backward, Adam"}}
+    if oracle_sample:
+        try:
+            from oracle import refrun
+            k = 6
+            sub = {kk: v[:k] for kk, v in geom.items()}
+            t0 = time.perf_counter()
+            ref = refrun.run_port(ctlkw, [atm], np.zeros(k, int), sub, aero=bytes(aero),
+                                  threads=os.cpu_count(), nalpha=20, timeout=1800)
+            res["oracle_sample"] = {
+                "rays": k, "kind": "port", "seconds": time.perf_counter() - t0,
+                "bt_err_k_plain": bt_error(plain["rad"][:k], ref["rad"], ctlkw["nus"]),
+                "bt_err_k_surrogate": bt_error(out["rad"][:k], ref["rad"], ctlkw["nus"])}
+        except Exception as exc:  # reported, never required
+            res["oracle_sample"] = {"error": str(exc)[:200]}
+    b.close()
+    model.close()
+    res["_surrogate"] = sur
+    return res
+
+
+MIX_WORKLOAD = ("independent forward-model requests, rays log-uniform in [50, 5000], 50 % clear "
+                "air (8 emitters, 4/8/16/32/64 of the 64 channels 700-1400 cm-1, limb and nadir) "
+                "and 50 % aerosol (sulfate layer, 2 emitters, the 16 channels 780-1250 cm-1, "
+                "limb, single scattering)")
+
+RAY_CAP, ATM_CAP = 16384, 64   # rays and profiles per packed batch
+
+
+def _pack(reqs):
+    """One batch input from a list of (atm, geom) requests: profiles in
+    order, rays of request i on profile i."""
+    from jscat import synth
+    atms = [r["atm"] for r in reqs]
+    ray_atm = np.concatenate([np.full(len(r["geom"]["obsz"]), i, np.int32)
+                              for i, r in enumerate(reqs)])
+    geom = {k: np.concatenate([r["geom"][k] for r in reqs]) for k in reqs[0]["geom"]}
+    return synth.batch_from(atms, ray_atm, geom)
+
+
+def _pad(inp, n_atm, n_rays, lev):
+    """Pad a packed input to the captured shape: copies of profile 0 and of
+    ray 0 (their results are discarded)."""
+    out = {}
+    na = len(inp["atm_off"]) - 1
+    nr = len(inp["ray_atm"])
+    add_l = (n_atm - na) * lev
+    for k in ("z", "lon", "lat", "p", "t"):
+        out[k] = np.concatenate([inp[k], np.tile(inp[k][:lev], n_atm - na)])
+    for k in ("q", "k"):
+        out[k] = np.concatenate([inp[k], np.tile(inp[k][:, :lev], (1, n_atm - na))], axis=1)
+    out["atm_off"] = np.arange(n_atm + 1, dtype=np.int32) * lev
+    out["ray_atm"] = np.concatenate([inp["ray_atm"], np.zeros(n_rays - nr, np.int32)])
+    for k in ("time", "obsz", "obslon", "obslat", "vpz", "vplon", "vplat"):
+        out[k] = np.concatenate([inp[k], np.full(n_rays - nr, inp[k][0])])
+    assert len(out["z"]) == n_atm * lev and add_l >= 0
+    return out
+
+
+def mixed_bench(args, local, torch, sur=None):
+    """Mixed-size request batch: requests are admitted in arrival order into
+    packed batches per model (up to RAY_CAP rays and ATM_CAP profiles);
+    clear-air batches replay a CUDA graph captured once per model (fixed
+    capacity, padded), aerosol batches run the scattering path with the
+    surrogate (per-point fallback to the plain path).  All requests arrive
+    at t = 0; a request's latency is the end of its batch on the device
+    (CUDA events).  Depth-2 requests are not generated: the reference's
+    multiple scattering returns NaN whenever a scattering point sits on a
+    layer edge, which its own refinement makes the common case."""
+    from jscat import api, structs as S, synth
+    workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
+    rng = np.random.default_rng(20261203)
+    nreq = args.requests
+    reqs = []
+    for i in range(nreq):
+        n = int(round(np.exp(rng.uniform(np.log(50), np.log(5000)))))
+        aerosol = rng.uniform() < 0.5
+        # aerosol requests: the scattering workload's profile family (the
+        # surrogate's training distribution); clear air: the batched one
+        atm = (synth.atmosphere(synth.CFG0_EMITTERS, rng) if aerosol else
+               synth.atmosphere(synth.CFG1_EMITTERS, rng, t_sigma=5.0, vmr_sigma=0.2))
+        if aerosol:
+            geom = synth.limb_geometry(rng.uniform(8.0, 30.0, n))
+            nd = 16
+        else:
+            nl = n // 2
+            g1 = synth.limb_geometry(rng.uniform(5.0, 60.0, nl))
+            g2 = synth.nadir_geometry(rng.uniform(0.0, 60.0, n - nl))
+            geom = {k: np.concatenate([g1[k], g2[k]]) for k in g1}
+            nd = int(rng.choice([4, 8, 16, 32, 64]))
+        geom["time"] = rng.uniform(0.0, 86400.0, n)
+        reqs.append({"i": i, "n": n, "aerosol": aerosol, "nd": nd, "atm": atm, "geom": geom})
+    lev = len(reqs[0]["atm"]["z"])
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+
+    def pin(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+
+    # models, graphs (clear air) and the scattering batch (aerosol)
+    g = np.load(os.path.join(REPO, "tests", "golden", "aero_sulfate16.npz"))
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    runners, models = {}, []
+    for nd in sorted({r["nd"] for r in reqs if not r["aerosol"]}):
+        nus = list(synth.CFG1_NU[::64 // nd])
+        base = synth.write_tables(workdir, synth.CFG1_EMITTERS, nus, 20261203)
+        ctl = S.make_ctl(emitters=synth.CFG1_EMITTERS, nus=nus, tblbase=base, hydz=0.0)
+        m = api.Model(ctl, device=local)
+        models.append(m)
+        first = [r for r in reqs if not r["aerosol"] and r["nd"] == nd][:1]
+        shape = _pad(_pack(first), ATM_CAP, RAY_CAP, lev)
+        runners[nd] = api.GraphBatch(m, ctl, shape, sp, pin, max_seg=RAY_CAP * 420)
+    a_nus = [float(v) for v in g["nus"]]
+    a_base = synth.write_tables(workdir, synth.CFG0_EMITTERS, a_nus, 20261203)
+    a_ctl = S.make_ctl(emitters=synth.CFG0_EMITTERS, nus=a_nus, tblbase=a_base, hydz=0.0,
+                       sca_n=1, sca_mult=1, sca_ext="beta_a")
+    a_model = api.Model(a_ctl, device=local)
+    models.append(a_model)
+    a_batch = api.Batch(a_model, a_ctl, ATM_CAP, ATM_CAP * lev, RAY_CAP)
+    a_batch.set_aero(aero)
+    a_batch.set_nalpha(20)
+    if sur is not None:
+        a_batch.set_surrogate(sur, tol_rel=0.01, check_stride=256)
+
+    # admission: arrival order, per model key, up to the caps
+    batches, open_b = [], {}
+    for r in reqs:
+        key = ("aero",) if r["aerosol"] else ("clear", r["nd"])
+        cur = open_b.get(key)
+        if cur is None or cur["rays"] + r["n"] > RAY_CAP or len(cur["reqs"]) >= ATM_CAP:
+            cur = {"key": key, "reqs": [], "rays": 0}
+            open_b[key] = cur
+            batches.append(cur)
+        cur["reqs"].append(r)
+        cur["rays"] += r["n"]
+    packed = [(b_, _pack(b_["reqs"])) for b_ in batches]
+    ev0 = torch.cuda.Event(enable_timing=True)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in packed]
+    outs = {}
+    l0 = api.launch_count()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for (b_, inp), ev in zip(packed, evs):
+        if b_["key"][0] == "clear":
+            gr = runners[b_["key"][1]]
+            gr.launch(_pad(inp, ATM_CAP, RAY_CAP, lev))
+            ev.record(stream)
+            stream.synchronize()        # the staging arrays are reused by the next batch
+            gr.status()
+            outs[id(b_)] = gr.out["rad"][:b_["rays"]].copy()
+        else:
+            a_batch.upload(inp, stream=sp)
+            a_batch.run(stream=sp)
+            res = a_batch.download(stream=sp)
+            ev.record(stream)
+            outs[id(b_)] = res["rad"]
+    stream.synchronize()
+    launches = api.launch_count() - l0
+    lat, units = [], 0
+    for (b_, _), ev in zip(packed, evs):
+        t = ev0.elapsed_time(ev)
+        for r in b_["reqs"]:
+            lat.append(t)
+            units += r["n"] * r["nd"]
+    make = max(lat)
+    # accuracy: aerosol batches against the plain path, clear against the
+    # ordinary (non-graph) batch path
+    errs = {}
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    from helpers import bt_error
+    a_b = next((bb for bb, _ in packed if bb["key"][0] == "aero"), None)
+    if a_b is not None:
+        a_batch.set_surrogate(None)
+        a_batch.upload(_pack(a_b["reqs"]), stream=sp)
+        a_batch.run(stream=sp)
+        plain = a_batch.download(stream=sp)
+        errs["aerosol_surrogate_vs_plain_k"] = bt_error(outs[id(a_b)], plain["rad"], a_nus)
+    c_b = next((bb for bb, _ in packed if bb["key"][0] == "clear"), None)
+    if c_b is not None:
+        nd = c_b["key"][1]
+        nus = list(synth.CFG1_NU[::64 // nd])
+        base = synth.write_tables(workdir, synth.CFG1_EMITTERS, nus, 20261203)
+        ctl = S.make_ctl(emitters=synth.CFG1_EMITTERS, nus=nus, tblbase=base, hydz=0.0)
+        ref = api.formod_batch(ctl, _pack(c_b["reqs"]), device=local)
+        errs["clear_graph_vs_batch_k"] = bt_error(outs[id(c_b)], ref["rad"], nus)
+    for gr in runners.values():
+        gr.close()
+    a_batch.close()
+    for m in models:
+        m.close()
+    return {"workload": MIX_WORKLOAD, "requests": nreq, "batches": len(packed),
+            "graph_batches": sum(1 for bb, _ in packed if bb["key"][0] == "clear"),
+            "value": units / (make / 1e3), "unit": UNIT, "makespan_ms": make,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "gpu_launches": int(launches), "bt_err": errs,
+            "admission": "arrival order, per model, <= %d rays and %d profiles per batch; "
+                         "clear-air batches replay a CUDA graph (padded to capacity)"
+                         % (RAY_CAP, ATM_CAP)}
 
 
 def cpu_baseline(ctlkw, atms, ray_atm, geom, n_sample):
@@ -318,10 +624,25 @@ def main():
             line["bt_err_k_vs_reference"] = bt_error(res["rad"][sel], ref["rad"], ctlkw["nus"])
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
-    if rank == 0:
-        print(json.dumps(line))
     batch.close()
     model.close()
+    sur = None
+    if rank == 0 and world == 1 and args.sca_rays > 0:
+        try:
+            line["scattering"] = scattering_bench(args, local, torch,
+                                                  oracle_sample=not args.no_cpu_baseline)
+            sur = line["scattering"].pop("_surrogate")
+        except Exception as exc:  # reported beside the headline, never required
+            line["scattering"] = {"error": str(exc)[:300]}
+    if rank == 0 and world == 1 and args.requests > 0:
+        try:
+            line["mixed_requests"] = mixed_bench(args, local, torch, sur)
+        except Exception as exc:
+            line["mixed_requests"] = {"error": str(exc)[:300]}
+    if sur is not None:
+        sur.close()
+    if rank == 0:
+        print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
 

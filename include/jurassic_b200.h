@@ -322,6 +322,30 @@ double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel);
 int jsc_batch_autotune(jsc_batch *b, void *stream);
 int jsc_batch_variant(const jsc_batch *b, int *variant, int *block, int *min_blocks);
 
+/* Fixed-capacity runs (on != 0): jsc_batch_run then never reads back from
+ * the device (LOS buffers hold the capacity given at jsc_batch_create, a
+ * longer line of sight sets JSC_ERR_NLOS in the status), so upload + run +
+ * download can be captured into a CUDA graph.  Depth 0 only (clear air or
+ * aerosol extinction, ctl->sca_mult = 0). */
+int jsc_batch_set_fixed(jsc_batch *b, int on);
+
+/* Enqueue the result copies (and the device status word) without waiting;
+ * jsc_batch_async_status maps the status once the stream has passed them.
+ * Requires fixed-capacity mode; host buffers should be pinned. */
+int jsc_batch_download_async(jsc_batch *b, const jsc_batch_output *out, void *stream);
+int jsc_batch_async_status(const jsc_batch *b);
+
+/* Capture upload(in) + run + download_async(out) of a fixed-capacity batch
+ * on stream (not the default stream) into a CUDA graph; in/out must point
+ * to pinned host arrays, which later launches read and write again.
+ * jsc_batch_graph_launch re-checks the inputs those arrays hold (profile
+ * offsets and ray profiles, as jsc_batch_upload) and replays the graph;
+ * synchronise the stream, then read the outputs and
+ * jsc_batch_async_status. */
+int jsc_batch_graph_capture(jsc_batch *b, const jsc_batch_input *in,
+                            const jsc_batch_output *out, void *stream);
+int jsc_batch_graph_launch(jsc_batch *b, void *stream);
+
 /* Select the EGA launch variant by hand (-1: the default).  Variants 0-8
  * run a thread per (ray, channel) with every emitter's path state; 9-13 a
  * lane per (ray, channel, emitter) after a separate continuum/Planck pass.
@@ -365,7 +389,8 @@ int jsc_batch_counters(const jsc_batch *b, int64_t *n_points,
  * a batch).  A 4-layer MLP, width 128, tanh, maps 8 features of a
  * scattering point (altitude, cosine of the LOS chord's zenith angle,
  * temperature, log pressure, cosine of the solar zenith angle, cosine of
- * the solar scattering angle, layer index, 0) to the log of the scattering
+ * the solar scattering angle, layer index, solar elevation above the
+ * geometric horizon) to the log of the scattering
  * source of each channel.  Trained on the GPU (FP32 forward/backward, Adam)
  * on samples of the plain source; inference runs BF16 weights on the
  * tensor cores with FP32 accumulation.
@@ -408,14 +433,18 @@ int jsc_batch_scatter_samples(jsc_batch *b, float *feat, double *src, int64_t ma
 
 /* Use the surrogate (NULL: never) for the batch's scattering sources.
  * Points whose features leave the training envelope take the plain path;
- * every check_stride-th point inside it (0: none) is computed both ways, and
- * if one deviates from the plain source by more than tol_rel (relative) the
- * whole batch is recomputed with the plain path. */
+ * every check_stride-th point inside it (0: none) is computed both ways,
+ * and if for one of them omega * |S_surrogate - S_plain| / S_plain exceeds
+ * tol_rel the whole batch is recomputed with the plain path.  omega = the
+ * layer's single-scattering albedo beta_s / beta_e bounds the weight of the
+ * scattering source in the segment source (src/forwardmodel.c:344-349), so
+ * the measure bounds the relative error of the segment source. */
 int jsc_batch_set_surrogate(jsc_batch *b, jsc_surrogate *s, double tol_rel, int check_stride);
 
 /* Surrogate counts of the last run: scattering points, fallbacks, checked
  * points, largest relative deviation found by the check, and whether the
- * surrogate's sources were used (0 after a rejection). */
+ * surrogate's sources were used (0 after a rejection); the deviation is
+ * the albedo-weighted one of jsc_batch_set_surrogate. */
 int jsc_batch_surrogate_stats(const jsc_batch *b, int64_t *points, int64_t *fallback,
                               int64_t *checked, double *max_rel_err, int *used);
 

@@ -81,6 +81,8 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   cudaFree(b->d_src_sub);
   free(b->h_aero);
   free(b->ctl);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->h_status) cudaFreeHost(b->h_status);
   if (b->h_total) cudaFreeHost(b->h_total);
   for (int i = 0; i < 2 * JSC_T_N; i++)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
@@ -480,6 +482,16 @@ static void fill_ray_args(const jsc_batch *b, RayArgs &ra) {
 
 static int batch_run(jsc_batch *b, cudaStream_t s);
 
+// Fixed-capacity runs: rays whose line of sight did not fit (the storing
+// pass flagged them) keep only the points inside the buffer, so that no
+// later kernel reads past it.
+static __global__ void clamp_los_kernel(int *nlos, const int64_t *off, int n, int64_t cap) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t room = cap - off[r];
+  if (room < nlos[r]) nlos[r] = room > 0 ? (int)room : 0;
+}
+
 // OR a child batch's device status into its parent's.
 static __global__ void status_or_kernel(unsigned *dst, const unsigned *src) { *dst |= *src; }
 
@@ -730,8 +742,13 @@ static __global__ void sur_gather_kernel(int m, const int *idx, const double *sp
 }
 
 // Fallback points take the plain source; checked points compare the
-// surrogate's source with it (largest relative deviation, as float bits).
+// surrogate's source with it.  The source enters the radiance through the
+// segment source ((bext - af bs) B + af bs S) / bext
+// (src/forwardmodel.c:344-349), where af bs / bext <= bs / be, the layer's
+// single-scattering albedo; the check measures omega |dS| / S, which bounds
+// the relative error of the segment source (largest value, as float bits).
 static __global__ void sur_merge_kernel(int m, int nd, const int *idx, const int *mark,
+                                        const double *sp, const double *beta, int nl,
                                         const double *src_sub, double *src, unsigned *maxerr) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= m * nd) return;
@@ -741,7 +758,10 @@ static __global__ void sur_merge_kernel(int m, int nd, const int *idx, const int
   if (mark[k] == 1) {
     *dst = plain;
   } else {
-    const float e = (float)(fabs(*dst - plain) / fmax(fabs(plain), 1e-300));
+    const int il = (int)sp[(size_t)k * JSC_SP_REC + SP_IL];
+    const double be = beta[(size_t)il * nd + d], bs = beta[(size_t)(nl + il) * nd + d];
+    const double omega = be > 0 ? fmin(fmax(bs / be, 0.0), 1.0) : 1.0;
+    const float e = (float)(omega * fabs(*dst - plain) / fmax(fabs(plain), 1e-300));
     atomicMax(maxerr, __float_as_uint(e == e ? e : 3.0e38f));
   }
 }
@@ -803,8 +823,9 @@ static int scatter_sources(jsc_batch *b, cudaStream_t s) {
     if ((st = plain_sources(b, b->d_sp_sub, b->d_atm_sub, m, b->d_src_sub, s))) return st;
     unsigned *d_err = (unsigned *)b->d_idx + b->sur_cap;  // reuse the count word
     JSC_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
-    sur_merge_kernel<<<(m * nd + 127) / 128, 128, 0, s>>>(m, nd, b->d_idx, b->d_mark,
-                                                          b->d_src_sub, b->d_src, d_err);
+    sur_merge_kernel<<<(m * nd + 127) / 128, 128, 0, s>>>(m, nd, b->d_idx, b->d_mark, b->d_sp,
+                                                          b->d_beta, b->aero_nl, b->d_src_sub,
+                                                          b->d_src, d_err);
     JSC_LAUNCH_CHECK();
     unsigned eb = 0;
     JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
@@ -875,9 +896,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   RayArgs ra;
   fill_ray_args(b, ra);
   if (m->n_grid == 1) {
-    int gnp = 0;
-    JSC_CUDA_TRY(cudaMemcpy(&gnp, m->d_grid_np, sizeof(int), cudaMemcpyDeviceToHost));
-    ra.grid_np = gnp;
+    ra.grid_np = m->grid_np0;
     ra.grid_p = m->d_grid_p;
     ra.grid_nt = m->d_grid_nt;
     ra.grid_t = m->d_grid_t;
@@ -896,9 +915,21 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   scan_kernel<<<1, 1024, 0, s>>>(ra.nlos, nr, (int64_t *)ra.los_off);
   JSC_LAUNCH_CHECK();
   // The LOS buffer is sized from the counting pass (one small copy).
-  JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, ra.los_off + nr, sizeof(int64_t),
-                               cudaMemcpyDeviceToHost, s));
-  JSC_CUDA_TRY(cudaStreamSynchronize(s));
+  if (b->fixed) {
+    // Fixed capacity (graph capture): no read-back, the buffers hold
+    // max_seg points and the storing passes flag an overflow.
+    *b->h_total = 0;
+  } else {
+    JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, ra.los_off + nr, sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, s));
+    JSC_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (b->fixed && (b->depth > 0 || (refine && b->max_seg_b < b->max_seg))) {
+    jsc_set_error(JSC_ERR_UNSUPPORTED,
+                  "fixed-capacity runs cover clear air and aerosol extinction; the base LOS "
+                  "buffer is sized by jsc_batch_set_fixed");
+    return JSC_ERR_UNSUPPORTED;
+  }
   if (refine) {
     if (*b->h_total > b->max_seg_b) {
       int st = batch_alloc_los_b(b, *b->h_total + *b->h_total / 4 + 1024);
@@ -912,7 +943,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
       int st = batch_alloc_los(b, *b->h_total + *b->h_total / 4 + 1024);
       if (st) return st;
     }
-    b->n_points = *b->h_total;
+    b->n_points = b->fixed ? b->max_seg : *b->h_total;
     ra.geo = b->d_geo;
     ra.pts = b->d_pts;
     ra.max_seg = b->max_seg;
@@ -920,6 +951,11 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   raytrace_kernel<true><<<(nr + 127) / 128, 128, 0, s>>>(ra);
   JSC_LAUNCH_CHECK();
   if (refine) {
+    if (b->fixed) {  // keep the refinement's reads inside the base buffer
+      clamp_los_kernel<<<(nr + 127) / 128, 128, 0, s>>>(b->d_nlos_b, b->d_los_off_b, nr,
+                                                         b->max_seg_b);
+      JSC_LAUNCH_CHECK();
+    }
     // Layer-edge points, chord steps and aerosol factors
     // (add_aerosol_layers, src/lineofsight.c:193-372).
     RefineArgs fa;
@@ -963,18 +999,26 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     JSC_LAUNCH_CHECK();
     scan_kernel<<<1, 1024, 0, s>>>(b->d_nlos, nr, b->d_los_off);
     JSC_LAUNCH_CHECK();
-    JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, b->d_los_off + nr, sizeof(int64_t),
-                                 cudaMemcpyDeviceToHost, s));
-    JSC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (b->fixed) {
+      *b->h_total = 0;
+    } else {
+      JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, b->d_los_off + nr, sizeof(int64_t),
+                                   cudaMemcpyDeviceToHost, s));
+      JSC_CUDA_TRY(cudaStreamSynchronize(s));
+    }
     if (*b->h_total > b->max_seg) {
       int st = batch_alloc_los(b, *b->h_total + *b->h_total / 4 + 1024);
       if (st) return st;
     }
-    b->n_points = *b->h_total;
+    b->n_points = b->fixed ? b->max_seg : *b->h_total;
     fa.geo = b->d_geo;
     fa.pts = b->d_pts;
     fa.max_seg = b->max_seg;
     refine_kernel<true><<<(nr + 127) / 128, 128, 0, s>>>(fa);
+    JSC_LAUNCH_CHECK();
+  }
+  if (b->fixed) {
+    clamp_los_kernel<<<(nr + 127) / 128, 128, 0, s>>>(b->d_nlos, b->d_los_off, nr, b->max_seg);
     JSC_LAUNCH_CHECK();
   }
   ev_record(b, JSC_T_RAYTRACE, 1, s);
@@ -1260,4 +1304,133 @@ extern "C" int jsc_batch_scatter_samples(jsc_batch *b, float *feat, double *src,
     st = JSC_ERR_CUDA;
   cudaFree(d_f);
   return st;
+}
+
+extern "C" int jsc_batch_set_fixed(jsc_batch *b, int on) {
+  if (!b) return JSC_ERR_ARG;
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  if (on) {
+    if (b->depth > 0) {
+      jsc_set_error(JSC_ERR_UNSUPPORTED, "fixed-capacity runs cover depth 0 (no scattering source)");
+      return JSC_ERR_UNSUPPORTED;
+    }
+    int st;
+    if (b->cfg.sca_n > 0 && b->max_seg_b < b->max_seg &&
+        (st = batch_alloc_los_b(b, b->max_seg)))
+      return st;
+    if (!b->h_status && cudaMallocHost((void **)&b->h_status, sizeof(unsigned)) != cudaSuccess) {
+      jsc_set_error(JSC_ERR_NOMEM, "pinned host allocation");
+      return JSC_ERR_NOMEM;
+    }
+    *b->h_status = 0;
+  }
+  b->fixed = on != 0;
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_download_async(jsc_batch *b, const jsc_batch_output *out,
+                                        void *stream) {
+  if (!b || !out || !b->h_status) return JSC_ERR_ARG;
+  const int nr = b->n_rays, nd = b->cfg.nd;
+  if (nr > 0) {
+    if (out->rad) DCPY(out->rad, b->d_rad, (size_t)nr * nd, stream);
+    if (out->tau) DCPY(out->tau, b->d_tau, (size_t)nr * nd, stream);
+    if (out->tpz) DCPY(out->tpz, b->d_tp, nr, stream);
+    if (out->tplon) DCPY(out->tplon, b->d_tp + nr, nr, stream);
+    if (out->tplat) DCPY(out->tplat, b->d_tp + 2 * (size_t)nr, nr, stream);
+    if (out->nlos) DCPY(out->nlos, b->d_nlos, nr, stream);
+  }
+  DCPY(b->h_status, b->d_status, 1, stream);
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_async_status(const jsc_batch *b) {
+  if (!b || !b->h_status) return JSC_ERR_ARG;
+  return map_status(*b->h_status);
+}
+
+// Host checks of the indices the kernels follow (as in jsc_batch_upload).
+static int check_input(const jsc_batch *b, const jsc_batch_input *in) {
+  if (in->n_atm < 1 || in->n_atm > b->max_atm || in->n_levels < 2 ||
+      in->n_levels > b->max_levels || in->n_rays < 0 || in->n_rays > b->max_rays ||
+      in->atm_off[0] != 0 || in->atm_off[in->n_atm] != in->n_levels) {
+    jsc_set_error(JSC_ERR_ARG, "batch input exceeds the batch capacity or has bad offsets");
+    return JSC_ERR_ARG;
+  }
+  for (int a = 0; a < in->n_atm; a++)
+    if (in->atm_off[a + 1] - in->atm_off[a] < 2) {
+      jsc_set_error(JSC_ERR_ARG, "profile %d has fewer than 2 levels", a);
+      return JSC_ERR_ARG;
+    }
+  for (int r = 0; r < in->n_rays; r++)
+    if (in->ray_atm[r] < 0 || in->ray_atm[r] >= in->n_atm) {
+      jsc_set_error(JSC_ERR_ARG, "ray %d names profile %d of %d", r, in->ray_atm[r], in->n_atm);
+      return JSC_ERR_ARG;
+    }
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_graph_capture(jsc_batch *b, const jsc_batch_input *in,
+                                       const jsc_batch_output *out, void *stream) {
+  if (!b || !in || !out || !stream || !b->fixed) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_graph_capture: needs a fixed-capacity batch and a "
+                               "non-default stream");
+    return JSC_ERR_ARG;
+  }
+  int st = check_input(b, in);
+  if (st) return st;
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  b->graph_ready = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  (void)cudaGetLastError();
+  JSC_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  st = jsc_batch_upload(b, in, stream);
+  if (!st) st = batch_run(b, s);
+  if (!st) st = jsc_batch_download_async(b, out, stream);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (!st && e != cudaSuccess) {
+    jsc_set_error(JSC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    st = JSC_ERR_CUDA;
+  }
+  if (!st) {
+    size_t nn = 0;
+    b->graph_kernels = 0;
+    if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+      cudaGraphNode_t *nodes = (cudaGraphNode_t *)malloc(nn * sizeof(cudaGraphNode_t));
+      if (nodes && cudaGraphGetNodes(g, nodes, &nn) == cudaSuccess)
+        for (size_t i = 0; i < nn; i++) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+            b->graph_kernels++;
+        }
+      free(nodes);
+    }
+    e = cudaGraphInstantiate(&b->gexec, g, 0);
+    if (e != cudaSuccess) {
+      jsc_set_error(JSC_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+      st = JSC_ERR_CUDA;
+      b->gexec = nullptr;
+    }
+  }
+  if (g) cudaGraphDestroy(g);
+  if (st) return st;
+  b->gin = *in;
+  b->graph_ready = 1;
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_graph_launch(jsc_batch *b, void *stream) {
+  if (!b || !b->graph_ready) return JSC_ERR_ARG;
+  // the graph copies from the captured host arrays: check what they hold now
+  int st = check_input(b, &b->gin);
+  if (st) return st;
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  JSC_CUDA_TRY(cudaGraphLaunch(b->gexec, (cudaStream_t)stream));
+  for (int i = 0; i < b->graph_kernels; i++) jsc_count_launch();
+  return JSC_OK;
 }

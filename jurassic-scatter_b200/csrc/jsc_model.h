@@ -9,6 +9,7 @@ struct jsc_model {
   int device;
   int ng, nd, nw;
   int n_grid;
+  int grid_np0;  // pressure levels of grid 0 (host copy)
   int64_t n_nodes;
   size_t table_bytes;
   double nu[NDMAX];
@@ -128,6 +129,14 @@ struct jsc_batch {
   int64_t sur_points, sur_fallback, sur_checked, sur_rejected;
   float sur_maxerr;
   int sur_used;
+
+  // Fixed-capacity mode (no host read-backs; graph capture) and the
+  // captured upload + run + download graph.
+  int fixed;
+  unsigned *h_status;       // pinned: status word of the last asynchronous download
+  cudaGraphExec_t gexec;
+  jsc_batch_input gin;      // host inputs the graph copies from
+  int graph_ready, graph_kernels;
 
   // Line of sight.
   int *d_nlos;

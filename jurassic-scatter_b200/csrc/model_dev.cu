@@ -177,6 +177,7 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
   if ((st = jsc_dmalloc(&m->d_nodes, (size_t)niv))) return st;
   m->n_nodes = niv;
   m->n_grid = ngrid;
+  m->grid_np0 = g_np.empty() ? 0 : g_np[0];
 
   if (niv > 0) {
     float *du = nullptr, *de = nullptr;

@@ -13,7 +13,8 @@
 // Features of a scattering point (sur_features_kernel): altitude, cosine
 // of the LOS chord's zenith angle, temperature, log pressure, cosine of the
 // solar zenith angle, cosine of the angle between the (unrefracted) solar
-// direction and the chord, layer index.  They are standardised with the
+// direction and the chord, layer index, and the sun's elevation above the
+// point's geometric horizon [deg] (where the solar term switches off).  They are standardised with the
 // training set's mean and spread; a point whose raw features leave the
 // training set's range (widened by 2 % of it) is outside the envelope and
 // takes the plain path.
@@ -54,7 +55,9 @@ static __global__ void sur_features_kernel(int n, const double *sp, float *feat)
   f[4] = (float)cz;
   f[5] = (float)cth;
   f[6] = (float)o[SP_IL];
-  f[7] = 0.f;
+  // elevation above the geometric horizon: 90 - sza + dip, dip = acos(RE / (RE + z))
+  const double zz = z > 0 ? z : 0.0;
+  f[7] = (float)(90.0 - sza + acos(JSC_RE / (JSC_RE + zz)) * 180 / M_PI);
 }
 
 // ------------------------------------------------------- FP32 training --
@@ -65,7 +68,9 @@ static __global__ void sur_features_kernel(int n, const double *sp, float *feat)
 
 // C[M][N] (ldc) = op(A) op(B) (+ bias[n]) with op(A)(m,k) = TA ? A[k*lda+m]
 // : A[m*lda+k] and op(B)(k,n) = TB ? B[n*ldb+k] : B[k*ldb+n].  256 threads,
-// a 64 x 64 tile per block, 4 x 4 outputs per thread.
+// a 64 x 64 tile per block, 4 x 4 outputs per thread.  With gridDim.z > 1
+// the K range is split over blockIdx.z and the partial products are added
+// atomically into C (zeroed by the caller; no bias).
 template <bool TA, bool TB>
 static __global__ void __launch_bounds__(256)
 sgemm_kernel(int M, int N, int K, const float *A, int lda, const float *B, int ldb, float *C,
@@ -74,17 +79,19 @@ sgemm_kernel(int M, int N, int K, const float *A, int lda, const float *B, int l
   __shared__ float Bs[TG_K][TG_N + 4];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int m0 = blockIdx.y * TG_M, n0 = blockIdx.x * TG_N;
+  const int kchunk = (K + (int)gridDim.z - 1) / (int)gridDim.z;
+  const int kb = (int)blockIdx.z * kchunk, ke = min(K, kb + kchunk);
   float acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += TG_K) {
+  for (int k0 = kb; k0 < ke; k0 += TG_K) {
     for (int i = threadIdx.x; i < TG_K * TG_M; i += 256) {
       const int kk = i / TG_M, mm = i - kk * TG_M;
       const int m = m0 + mm, k = k0 + kk;
-      As[kk][mm] = (m < M && k < K) ? (TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k]) : 0.f;
+      As[kk][mm] = (m < M && k < ke) ? (TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k]) : 0.f;
     }
     for (int i = threadIdx.x; i < TG_K * TG_N; i += 256) {
       const int kk = i / TG_N, nn = i - kk * TG_N;
       const int n = n0 + nn, k = k0 + kk;
-      Bs[kk][nn] = (n < N && k < K) ? (TB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n]) : 0.f;
+      Bs[kk][nn] = (n < N && k < ke) ? (TB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n]) : 0.f;
     }
     __syncthreads();
 #pragma unroll
@@ -107,14 +114,20 @@ sgemm_kernel(int M, int N, int K, const float *A, int lda, const float *B, int l
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const int m = m0 + ty * 4 + i, n = n0 + tx * 4 + j;
-      if (m < M && n < N) C[(size_t)m * ldc + n] = acc[i][j] + (bias ? bias[n] : 0.f);
+      if (m < M && n < N) {
+        if (gridDim.z > 1) atomicAdd(&C[(size_t)m * ldc + n], acc[i][j]);
+        else C[(size_t)m * ldc + n] = acc[i][j] + (bias ? bias[n] : 0.f);
+      }
     }
 }
 
+// ksplit > 1: split-K (C zeroed here, bias ignored) for products with a
+// long K and a small output (the weight gradients: K = batch).
 template <bool TA, bool TB>
 static void sgemm(int M, int N, int K, const float *A, int lda, const float *B, int ldb, float *C,
-                  int ldc, const float *bias, cudaStream_t s) {
-  dim3 grid((N + TG_N - 1) / TG_N, (M + TG_M - 1) / TG_M);
+                  int ldc, const float *bias, cudaStream_t s, int ksplit = 1) {
+  dim3 grid((N + TG_N - 1) / TG_N, (M + TG_M - 1) / TG_M, ksplit);
+  if (ksplit > 1) cudaMemsetAsync(C, 0, (size_t)M * ldc * sizeof(float), s);
   sgemm_kernel<TA, TB><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, bias);
 }
 
@@ -149,19 +162,21 @@ static __global__ void mse_kernel(int64_t cnt, int n, const float *y, const floa
   if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
-// db[o] = sum over the batch of dZ[:, o]
+// db[o] = sum over the batch of dZ[:, o]: block (32 columns) x (8 row
+// lanes), coalesced over the columns.
 static __global__ void colsum_kernel(int n, int cols, const float *dz, float *db) {
-  const int o = blockIdx.x;
+  const int o = blockIdx.x * 32 + (threadIdx.x & 31), r0 = threadIdx.x >> 5;
   float sacc = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) sacc += dz[(size_t)i * cols + o];
-  __shared__ float red[256];
-  red[threadIdx.x] = sacc;
+  if (o < cols)
+    for (int i = r0; i < n; i += 8) sacc += dz[(size_t)i * cols + o];
+  __shared__ float red[8][32];
+  red[r0][threadIdx.x & 31] = sacc;
   __syncthreads();
-  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
-    if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
-    __syncthreads();
+  if (r0 == 0 && o < cols) {
+    float t = 0;
+    for (int j = 0; j < 8; j++) t += red[j][threadIdx.x];
+    db[o] = t;
   }
-  if (threadIdx.x == 0) db[o] = red[0];
 }
 
 static __global__ void adam_kernel(int64_t n, float *p, const float *g, float *m, float *v,
@@ -387,7 +402,8 @@ struct jsc_surrogate {
   float *d_h[5];            // activations per layer, [max_batch][width]
   float *d_dh[2];           // two ping-pong gradient buffers [max_batch][SUR_W]
   float *d_xb, *d_tb, *d_part;
-  int *d_idx;
+  int *d_idx;               // [max_batch] (gradient checks)
+  int *d_perm;              // [n_train] per-epoch permutation
   float *d_X, *d_T;         // device copy of the training set
   int64_t n_train;
 };
@@ -426,6 +442,7 @@ extern "C" void jsc_surrogate_destroy(jsc_surrogate *s) {
   cudaFree(s->d_ys);
   cudaFree(s->d_X);
   cudaFree(s->d_T);
+  cudaFree(s->d_perm);
   free_train(s);
   free(s);
 }
@@ -574,9 +591,12 @@ static int forward_backward(jsc_surrogate *s, int n, cudaStream_t st, float *los
   float *dcur = dy, *dnext = s->d_dh[1];
   for (int l = 3; l >= 0; l--) {
     // dW = dZ^T H_l, db = colsum(dZ)
+    const int tiles = ((s->out[l] + TG_M - 1) / TG_M) * ((s->in[l] + TG_N - 1) / TG_N);
+    int ksplit = 296 / tiles;  // about two blocks per SM
+    if (ksplit > n / 64) ksplit = n / 64 > 0 ? n / 64 : 1;
     sgemm<true, false>(s->out[l], s->in[l], n, dcur, s->out[l], s->d_h[l], s->in[l],
-                       s->d_g[l][0], s->in[l], nullptr, st);
-    colsum_kernel<<<s->out[l], 256, 0, st>>>(n, s->out[l], dcur, s->d_g[l][1]);
+                       s->d_g[l][0], s->in[l], nullptr, st, ksplit > 1 ? ksplit : 1);
+    colsum_kernel<<<(s->out[l] + 31) / 32, 256, 0, st>>>(n, s->out[l], dcur, s->d_g[l][1]);
     if (l > 0) {
       // dH_l = dZ W_l, then dZ_{l-1} = dH_l (1 - H_l^2)
       sgemm<false, false>(n, s->in[l], s->out[l], dcur, s->out[l], s->d_p[l][0], s->in[l], dnext,
@@ -676,9 +696,12 @@ extern "C" int jsc_surrogate_train(jsc_surrogate *s, const float *X, const doubl
   int st = JSC_OK;
   cudaFree(s->d_X);
   cudaFree(s->d_T);
+  cudaFree(s->d_perm);
   s->d_X = s->d_T = nullptr;
+  s->d_perm = nullptr;
   st = st ? st : jsc_dmalloc(&s->d_X, (size_t)n * SUR_NF);
   st = st ? st : jsc_dmalloc(&s->d_T, (size_t)n * nd);
+  st = st ? st : jsc_dmalloc(&s->d_perm, (size_t)n);
   if (!st && (cudaMemcpy(s->d_X, X, (size_t)n * SUR_NF * sizeof(float), cudaMemcpyHostToDevice) ||
               cudaMemcpy(s->d_T, T, (size_t)n * nd * sizeof(float), cudaMemcpyHostToDevice) ||
               cudaMemcpy(s->d_ym, s->h_ym, nd * sizeof(float), cudaMemcpyHostToDevice) ||
@@ -709,13 +732,15 @@ extern "C" int jsc_surrogate_train(jsc_surrogate *s, const float *X, const doubl
     double ep_loss = 0;
     int64_t ep_n = 0;
     const float lr_ep = lr * (float)(0.5 * (1 + cos(M_PI * ep / epochs)));  // cosine decay
+    // one upload of the epoch's permutation; the minibatch steps then run
+    // back to back on the stream without host synchronisation
+    if (cudaMemcpy(s->d_perm, perm, (size_t)n * sizeof(int), cudaMemcpyHostToDevice)) {
+      st = JSC_ERR_CUDA;
+      break;
+    }
     for (int64_t b0 = 0; b0 + batch <= n && !st; b0 += batch) {
-      if (cudaMemcpy(s->d_idx, perm + b0, batch * sizeof(int), cudaMemcpyHostToDevice)) {
-        st = JSC_ERR_CUDA;
-        break;
-      }
-      gather_kernel<<<batch, 32>>>(batch, nd, s->d_idx, s->d_X, s->d_T, d_xm, d_xs, s->d_h[0],
-                                   s->d_tb);
+      gather_kernel<<<batch, 32>>>(batch, nd, s->d_perm + b0, s->d_X, s->d_T, d_xm, d_xs,
+                                   s->d_h[0], s->d_tb);
       const bool last = b0 + 2 * batch > n;
       float l = 0;
       st = forward_backward(s, batch, 0, last ? &l : nullptr);

@@ -285,6 +285,63 @@ def formod_batch_noalloc(ctl, inp, model, stream=None):
     return out
 
 
+class GraphBatch:
+    """A fixed-capacity batch whose upload + run + download is captured once
+    into a CUDA graph for one input shape (n_atm, n_levels, n_rays).
+    run(inp) copies inp into the pinned staging arrays the graph reads,
+    replays it and returns the outputs.  pin(a) must return a pinned copy
+    of a numpy array (e.g. through torch's pin_memory)."""
+
+    _KEYS = ("z", "lon", "lat", "p", "t", "q", "k", "time", "obsz", "obslon", "obslat",
+             "vpz", "vplon", "vplat")
+
+    def __init__(self, model, ctl, inp, stream, pin, max_seg=0, aero=None):
+        lib = L.load()
+        self.nd = ctl.nd
+        self.stream = stream
+        n_atm = len(inp["atm_off"]) - 1
+        self.batch = Batch(model, ctl, n_atm, len(inp["z"]), len(inp["ray_atm"]), max_seg)
+        if aero is not None:
+            self.batch.set_aero(aero)
+        L.check(lib.jsc_batch_set_fixed(self.batch.h, 1), "jsc_batch_set_fixed")
+        self.host = {k: pin(np.ascontiguousarray(inp[k], dtype=np.float64)) for k in self._KEYS}
+        self.host["atm_off"] = pin(np.ascontiguousarray(inp["atm_off"], dtype=np.int32))
+        self.host["ray_atm"] = pin(np.ascontiguousarray(inp["ray_atm"], dtype=np.int32))
+        nr = len(inp["ray_atm"])
+        self.out = {"rad": pin(np.zeros((nr, self.nd))), "tau": pin(np.zeros((nr, self.nd))),
+                    "tpz": pin(np.zeros(nr)), "tplon": pin(np.zeros(nr)), "tplat": pin(np.zeros(nr)),
+                    "nlos": pin(np.zeros(nr, np.int32))}
+        bi = L.BatchInput()
+        bi.n_atm = n_atm
+        bi.n_levels = len(inp["z"])
+        bi.n_rays = nr
+        bi.atm_off = _iptr(self.host["atm_off"])
+        bi.ray_atm = _iptr(self.host["ray_atm"])
+        for k in self._KEYS:
+            setattr(bi, k, _dptr(self.host[k]))
+        bo = L.BatchOutput()
+        for k in ("rad", "tau", "tpz", "tplon", "tplat"):
+            setattr(bo, k, _dptr(self.out[k]))
+        bo.nlos = _iptr(self.out["nlos"])
+        self._keep = (bi, bo)
+        L.check(lib.jsc_batch_graph_capture(self.batch.h, C.byref(bi), C.byref(bo), stream),
+                "jsc_batch_graph_capture")
+
+    def launch(self, inp=None):
+        """Copy inp (same shapes) into the staging arrays and replay; the
+        caller synchronises the stream before reading self.out."""
+        if inp is not None:
+            for k in self._KEYS + ("atm_off", "ray_atm"):
+                self.host[k][...] = inp[k]
+        L.check(L.load().jsc_batch_graph_launch(self.batch.h, self.stream), "jsc_batch_graph_launch")
+
+    def status(self):
+        L.check(L.load().jsc_batch_async_status(self.batch.h), "jsc_batch_async_status")
+
+    def close(self):
+        self.batch.close()
+
+
 _F = C.POINTER(C.c_float)
 
 

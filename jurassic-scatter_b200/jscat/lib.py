@@ -24,6 +24,8 @@ EXPORTS = [
     "jsc_surrogate_param_count", "jsc_surrogate_get_params", "jsc_surrogate_set_params",
     "jsc_surrogate_loss_grad", "jsc_surrogate_train", "jsc_surrogate_predict",
     "jsc_batch_scatter_samples", "jsc_batch_set_surrogate", "jsc_batch_surrogate_stats",
+    "jsc_batch_set_fixed", "jsc_batch_download_async", "jsc_batch_async_status",
+    "jsc_batch_graph_capture", "jsc_batch_graph_launch",
 ]
 
 
@@ -99,6 +101,11 @@ def load():
         "jsc_batch_set_aero": (i, [vp, P(S.AeroT)]),
         "jsc_batch_set_nalpha": (i, [vp, i]),
         "jsc_batch_set_variant": (i, [vp, i]),
+        "jsc_batch_set_fixed": (i, [vp, i]),
+        "jsc_batch_download_async": (i, [vp, P(BatchOutput), vp]),
+        "jsc_batch_async_status": (i, [vp]),
+        "jsc_batch_graph_capture": (i, [vp, P(BatchInput), P(BatchOutput), vp]),
+        "jsc_batch_graph_launch": (i, [vp, vp]),
         "jsc_surrogate_create": (i, [i, i, C.c_uint64, P(vp)]),
         "jsc_surrogate_destroy": (None, [vp]),
         "jsc_surrogate_param_count": (i, [vp]),

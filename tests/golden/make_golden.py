@@ -95,6 +95,23 @@ def save_aero(name, ctlkw, atm, geom, ref, aero_bytes, port=None):
         **{"geom_" + k: v for k, v in geom.items()}, **extra)
 
 
+def double_scattering_fixture(workdir):
+    """SCA_MULT=2 on one limb ray (tangent height 16.37 km, noon) through
+    the sulfate layer, 2 channels.  The reference returns NaN here (a
+    zero-length chord at a layer-edge point of a second-order pencil, 0/0 in
+    formod_continua); the fixture pins that behaviour.  Slow: about 47 min
+    of reference CPU time (28 pencils per scattering point, two orders)."""
+    nus = [synth.CFG2_NU[i] for i in (0, 10)]
+    ctlkw, atm, geom, aerofile = aerosol_case(workdir, 2, n_rays=1, nus=nus)
+    geom = synth.limb_geometry(np.array([16.37]))
+    geom["time"] = np.full(1, 43200.0)
+    aero = refrun.reference_aero(ctlkw, aerofile, os.path.dirname(aerofile))
+    ref = refrun.run(ctlkw, [atm], np.zeros(1, int), geom, aero=aero, timeout=7200, los=True)
+    np.savez_compressed(os.path.join(HERE, "aerosol_sca2.npz"), rad=ref["rad"], tau=ref["tau"],
+                        nlos=ref["nlos"], nus=np.asarray(nus),
+                        **{"geom_" + k: v for k, v in geom.items()})
+
+
 def aero_fixture(workdir, name, layer_files, nus):
     """aero_t (as bytes) of a layer file on a channel grid, from the
     reference's read_aero + get_opt_prop (Mie), for benchmark inputs."""
@@ -133,6 +150,8 @@ def main():
         assert np.max(np.abs(port["rad"] - ref["rad"]) / np.abs(ref["rad"])) < 1e-12
         save_aero("aerosol_sca1_" + name, ctlkw, atm, geom, ref, aero)
     aero_fixture(workdir, "aero_sulfate16", synth.sulfate_layer_files, list(synth.CFG2_NU))
+    if os.environ.get("JSC_SLOW_FIXTURES"):
+        double_scattering_fixture(workdir)
     aero_fixture(workdir, "aero_ice8", synth.ice_layer_files, list(synth.CFG2_NU[::2]))
     print("fixtures written to", HERE)
 

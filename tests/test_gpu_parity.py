@@ -156,3 +156,42 @@ def test_dropin_formod_single_scattering(workdir):
     rad = S.arr(obs.rad)[:ctl.nd, :n].T
     assert bt_error(rad, g["rad"], ctlkw["nus"]) <= BT_TOL_K
     assert max_rel(rad, g["rad"]) <= REL_TOL
+
+
+def test_double_scattering_matches_reference_nan(workdir):
+    """SCA_MULT=2: the reference returns NaN for this limb ray (second-order
+    pencils starting on layer-edge points get a zero-length chord and 0/0
+    in the continua); the GPU path follows the same arithmetic and returns
+    NaN in the same channels, with the same LOS point count."""
+    from jscat import synth, api, structs as S
+    from make_golden_shim import aerosol_case
+    g = _load("aerosol_sca2")
+    ga = _load("aerosol_sca1_day")
+    nus = [float(v) for v in g["nus"]]
+    ctlkw, atm, _, _ = aerosol_case(workdir, 2, n_rays=1, nus=nus)
+    geom = _geom(g)
+    aero_full = S.AeroT.from_buffer_copy(ga["aero"].tobytes())
+    aero = _aero_for(aero_full, ga, nus)
+    ctl = S.make_ctl(**ctlkw)
+    out = api.formod_batch(ctl, synth.batch_from([atm], np.zeros(1, np.int32), geom), aero=aero)
+    np.testing.assert_array_equal(out["nlos"], g["nlos"])
+    np.testing.assert_array_equal(np.isnan(out["rad"]), np.isnan(g["rad"]))
+
+
+def _aero_for(aero, g, nus):
+    """The sulfate layer's optical properties on the channels nus (taken from
+    the 4-channel fixture's aero_t, whose channels include them)."""
+    import ctypes as C
+    from jscat import synth
+    have = [synth.CFG2_NU[i] for i in (0, 5, 10, 15)]
+    idx = [have.index(v) for v in nus]
+    from jscat import structs as S
+    out = S.AeroT.from_buffer_copy(bytes(aero))
+    for il in range(aero.nl):
+        for j, i in enumerate(idx):
+            out.beta_e[il][j] = aero.beta_e[il][i]
+            out.beta_s[il][j] = aero.beta_s[il][i]
+            out.beta_a[il][j] = aero.beta_a[il][i]
+            for a in range(181):
+                out.p[il][j][a] = aero.p[il][i][a]
+    return out
