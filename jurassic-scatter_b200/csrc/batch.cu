@@ -154,7 +154,7 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   st = st ? st : jsc_dmalloc(&b->d_counters, 2);
   if (!st) st = batch_alloc_los(b, max_seg > 0 ? max_seg : (int64_t)max_rays * 512);
   b->ega_variant = -1;
-  for (int v = 0; v < 16; v++) b->ega_variant_ms[v] = -1;
+  for (int v = 0; v < 32; v++) b->ega_variant_ms[v] = -1;
   b->depth = ctl->sca_n > 0 ? ctl->sca_mult : 0;
   b->nalpha = JSC_NALPHA_REF;
   sca_alpha(b->alpha, b->nalpha);
@@ -408,6 +408,7 @@ static const EgaVariant kEgaVariants[] = {
     {128, 8, 1, 0}, {128, 12, 1, 0}, {256, 4, 1, 0}, {256, 6, 1, 0},
     {128, 12, 0, 1}, {128, 8, 0, 1}, {256, 4, 0, 1}, {256, 5, 0, 1}, {512, 2, 0, 1}};
 static const int kNumEgaVariants = 14;
+static_assert(kNumEgaVariants <= 32, "ega_variant_ms holds 32 timings");
 static const int kLaneBase = 9;
 static const int kEgaDefault = JSC_EGA_DEFAULT_VARIANT;  // fastest measured (batched clear air)
 // Index digests run the default variant of the selected kernel family.

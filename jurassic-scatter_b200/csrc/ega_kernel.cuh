@@ -33,12 +33,20 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
   for (int g = 0; g < ng && g < GMAX; g++)
     if (m.tab_grid[d * ng + g] >= 0) okmask |= 1u << g;
 
-  double tp[GMAX];
-  int hint[GMAX];
+  // Path transmittance and interval hints per emitter: registers
+  // (unrolled) or local memory (rolled).  (State in shared memory measured
+  // slower: the allocation shrinks the L1 the table gathers hit.)
+  double tp_l[GMAX];
+  // four 16-bit interval hints per emitter, one per (p, T) corner row:
+  // rows one pressure level apart sit several intervals apart on the
+  // column-density grid, so a shared hint sends three of them searching
+  unsigned long long hint_l[GMAX];
+#define JSC_TP(g) (tp_l[g])
+#define JSC_HINT(g) (hint_l[g])
 #pragma unroll((GMAX <= 8 && !ROLL) ? GMAX : 1)
   for (int g = 0; g < GMAX; g++) {
-    tp[g] = 1;
-    hint[g] = 0;
+    JSC_TP(g) = 1;
+    JSC_HINT(g) = 0;
   }
   double rad = 0, tau = 1;
   unsigned long long dig[DIG ? GMAX : 1];  // per-emitter index digests
@@ -62,7 +70,7 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
     for (int g = 0; g < GMAX; g++) {
       if (g >= ng) break;
       double eps = 0;
-      const double tpg = tp[g];
+      const double tpg = JSC_TP(g);
       if (!((okmask >> g) & 1u)) {
         eps = 0;
       } else if (tpg < 1e-9) {
@@ -85,12 +93,16 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
             const double x1 = 1 - tpg, useg = rec[REC_K + m.nw + g];
             unsigned long long *dg = &dig[DIG ? g : 0];
             if (DIG) *dg = *dg * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
-            int j00, jx;
-            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, hint[g], &j00, dg);
-            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, hint[g], &jx, dg);
-            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, hint[g], &jx, dg);
-            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, hint[g], &jx, dg);
-            hint[g] = j00;
+            int j00;
+            const unsigned long long hp = JSC_HINT(g);
+            int j01, j10, j11;
+            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(hp & 0xffff), &j00, dg);
+            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((hp >> 16) & 0xffff), &j01, dg);
+            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((hp >> 32) & 0xffff), &j10, dg);
+            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(hp >> 48), &j11, dg);
+            JSC_HINT(g) = (unsigned long long)(j00 & 0xffff) | ((unsigned long long)(j01 & 0xffff) << 16) |
+                          ((unsigned long long)(j10 & 0xffff) << 32) |
+                          ((unsigned long long)(j11 & 0xffff) << 48);
             const double *gp = m.grid_p + (size_t)gid * TBLNPMAX;
             const double *gt = m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX;
             double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
@@ -103,7 +115,7 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
           }
         }
       }
-      tp[g] = tpg * (1 - eps);
+      JSC_TP(g) = tpg * (1 - eps);
       tau_gas *= (1 - eps);
     }
     const double beta = continua(m, A.cfg, cc, nu, has_w ? rec[REC_K + w] : 0.0, P, T, DS,
@@ -139,6 +151,8 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
       tau *= (1 - eps);
     }
   }
+#undef JSC_TP
+#undef JSC_HINT
   const double ts = A.tsurf[r];
   if (ts > 0) {
     const int its = planck_index(ts);

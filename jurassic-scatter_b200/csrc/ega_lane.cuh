@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
   const double *__restrict__ gt = m.grid_t + (size_t)(ok ? gid : 0) * TBLNPMAX * TBLNTMAX;
 
   double tp = 1, rad = 0, tau = 1;
-  int hint = 0;
+  unsigned long long hint = 0;  // 16-bit interval hint per (p, T) corner row
   unsigned long long dig = 0;
   unsigned n_ega = 0;
   const int np = A.nlos[r];
@@ -97,12 +97,13 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
               (r11.nf & 0xffff) >= 2) {
             const double x1 = 1 - tp, useg = rec[REC_K + m.nw + g];
             if (DIG) dig = dig * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
-            int j00, jx;
-            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, hint, &j00, &dig);
-            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, hint, &jx, &dig);
-            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, hint, &jx, &dig);
-            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, hint, &jx, &dig);
-            hint = j00;
+            int j00, j01, j10, j11;
+            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(hint & 0xffff), &j00, &dig);
+            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((hint >> 16) & 0xffff), &j01, &dig);
+            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((hint >> 32) & 0xffff), &j10, &dig);
+            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(hint >> 48), &j11, &dig);
+            hint = (unsigned long long)(j00 & 0xffff) | ((unsigned long long)(j01 & 0xffff) << 16) |
+                   ((unsigned long long)(j10 & 0xffff) << 32) | ((unsigned long long)(j11 & 0xffff) << 48);
             double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
                                             gt[ipr * TBLNTMAX + it0 + 1], e01, T));
             const double eb = jsc_clamp01(jsc_lin(gt[(ipr + 1) * TBLNTMAX + it1], e10,

@@ -159,7 +159,7 @@ struct jsc_batch {
   int timing;
   int ega_variant;          // launch variant of ega_rt (autotuned), -1 = default
   EgaArgs last_ega;         // arguments of the last ega_rt launch
-  float ega_variant_ms[16];  // autotuner timings
+  float ega_variant_ms[32];  // autotuner timings (room for every variant)
   cudaEvent_t ev[2 * JSC_T_N];
   int ran[JSC_T_N];
 };

@@ -147,7 +147,7 @@ class Batch:
         lib = L.load()
         L.check(lib.jsc_batch_variant(self.h, C.byref(v), C.byref(b), C.byref(mb)),
                 "jsc_batch_variant")
-        ms = [lib.jsc_batch_variant_ms(self.h, i) for i in range(16)]
+        ms = [lib.jsc_batch_variant_ms(self.h, i) for i in range(32)]
         while ms and ms[-1] < 0:  # variants past the last one report -1
             ms.pop()
         return {"variant": v.value, "block": b.value, "min_blocks": mb.value,
