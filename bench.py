@@ -127,6 +127,9 @@ def make_workload(n_rays, seed_offset=0):
     return ctlkw, atms, ray_atm, geom
 
 
+TRAFFIC_PER_EGA = 283.4e9 / 1.854e9  # ncu dram__bytes read+write per EGA evaluation
+
+
 def algorithmic_bytes(n_ega, n_points, n_rays, nd, ng):
     """Bytes one ega_rt launch must touch per the roofline model: per EGA
     evaluation 4 (p,T) nodes x 2 lookups x bracketing (u,eps) pair = 128 B;
@@ -591,10 +594,10 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     achieved = B / (ega / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(REPO, "profiles", "ega_rt_traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("bytes_per_launch")
+    # DRAM bytes (read + write) per launch: ncu's dram__bytes of one 20k-ray
+    # launch of this workload (283.4 GB for 1.854e9 EGA evaluations, see
+    # profiles/ega_rt_clear_batched.md) scaled by the EGA evaluations here
+    traffic = TRAFFIC_PER_EGA * n_ega
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
