@@ -163,6 +163,26 @@ __device__ __noinline__ int find_interval(const jsc_node *row, int n, bool stric
   return strict ? search_row<U>(row, n, x, h) : bisect_row<U>(row, n, x);
 }
 
+// Interval hints of the four (p, T) corner rows, packed 16 bits each in
+// the order (ipr, it0), (ipr, it0+1), (ipr+1, it1), (ipr+1, it1+1) of a
+// packed bracket code; remap_hints moves them from the corners of code
+// `from` to those of code `to`, taking for every new row the old row of the
+// same pressure level (else the nearest level) and the nearest temperature.
+__device__ __forceinline__ unsigned long long remap_hints(unsigned long long h, int from, int to) {
+  const int pi = (from >> 10) & 63, p0 = (from >> 5) & 31, p1 = from & 31;
+  const int ni = (to >> 10) & 63, n0 = (to >> 5) & 31, n1 = to & 31;
+  unsigned long long out = 0;
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const int L = ni + (c >> 1), t = (c >> 1 ? n1 : n0) + (c & 1);
+    int src;
+    if (L <= pi) src = t <= p0 ? 0 : 1;
+    else src = t <= p1 ? 2 : 3;
+    out |= ((h >> (16 * src)) & 0xffffull) << (16 * c);
+  }
+  return out;
+}
+
 // LIN on float table entries with the slope already in float, as the
 // reference evaluates it: y0 + slope * (x - x0), promoted to double.
 __device__ __forceinline__ double lin_node(float x0, float y0, float slope, double x) {
@@ -175,13 +195,15 @@ __device__ __forceinline__ double lin_node(float x0, float y0, float slope, doub
 // column, look the emissivity up again, clamp to [0, 1].
 //
 // Fast path: the row is strictly increasing, the interval [h, h+1] of the
-// previous point still brackets x1 and the extended column stays in the
-// same interval -- then the two nodes h, h+1 (one 32-byte sector) answer
-// both lookups.  Otherwise the exact searches above find the intervals.
+// hint still brackets x1 and the extended column falls in the interval
+// k + dj guessed from the previous point's distance -- then one or two
+// node pairs answer both lookups.  Otherwise the exact searches above find
+// the intervals, starting from the guesses.  *kout and *jout receive the
+// intervals (they do not depend on the guesses).
 template <bool DIG>
 __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, jsc_row rd,
-                                           double x1, double useg, int hint, int *jout,
-                                           unsigned long long *dig) {
+                                           double x1, double useg, int hint, int dj, int *kout,
+                                           int *jout, unsigned long long *dig) {
   const int n = rd.nf & 0xffff;
   const bool strict = (rd.nf >> 16) & JSC_ROW_STRICT;
   const jsc_node *row = nodes + rd.off;
@@ -198,12 +220,19 @@ __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, j
   }
   const double x2 = lin_node(a.y, a.x, a.z, x1) + useg;
   const float x2f = __double2float_rd(x2);
-  int j = k;
-  if (!(strict && (!(a.x > x2f) || k == 0) && (b.x > x2f || k == last) && x2 == x2)) {
-    j = find_interval<true>(row, n, strict, x2, k);
-    if (j != k) a = __ldg(reinterpret_cast<const float4 *>(row + j));
+  int j = k + (dj > 0 ? dj : 0);
+  if (j > last) j = last;
+  if (j != k) {
+    a = __ldg(reinterpret_cast<const float4 *>(row + j));
+    b = __ldg(reinterpret_cast<const float4 *>(row + j + 1));
+  }
+  if (!(strict && (!(a.x > x2f) || j == 0) && (b.x > x2f || j == last) && x2 == x2)) {
+    const int j0 = j;
+    j = find_interval<true>(row, n, strict, x2, j0);
+    if (j != j0) a = __ldg(reinterpret_cast<const float4 *>(row + j));
   }
   if (DIG) *dig = (*dig * 1000003ull + (unsigned long long)k) * 1000003ull + (unsigned long long)j;
+  *kout = k;
   *jout = j;
   return jsc_clamp01(lin_node(a.x, a.y, a.w, x2));
 }

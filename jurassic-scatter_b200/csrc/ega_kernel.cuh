@@ -41,12 +41,18 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
   // rows one pressure level apart sit several intervals apart on the
   // column-density grid, so a shared hint sends three of them searching
   unsigned long long hint_l[GMAX];
+  // per emitter: the (p, T) bracket code the hints belong to, and the
+  // forward distances j - k of the four rows (8 bits each)
+  int hcode_l[GMAX];
+  unsigned dj_l[GMAX];
 #define JSC_TP(g) (tp_l[g])
 #define JSC_HINT(g) (hint_l[g])
 #pragma unroll((GMAX <= 8 && !ROLL) ? GMAX : 1)
   for (int g = 0; g < GMAX; g++) {
     JSC_TP(g) = 1;
     JSC_HINT(g) = 0;
+    hcode_l[g] = -1;
+    dj_l[g] = 0;
   }
   double rad = 0, tau = 1;
   unsigned long long dig[DIG ? GMAX : 1];  // per-emitter index digests
@@ -93,16 +99,25 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
             const double x1 = 1 - tpg, useg = rec[REC_K + m.nw + g];
             unsigned long long *dg = &dig[DIG ? g : 0];
             if (DIG) *dg = *dg * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
-            int j00;
-            const unsigned long long hp = JSC_HINT(g);
-            int j01, j10, j11;
-            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(hp & 0xffff), &j00, dg);
-            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((hp >> 16) & 0xffff), &j01, dg);
-            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((hp >> 32) & 0xffff), &j10, dg);
-            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(hp >> 48), &j11, dg);
+            unsigned long long hp = JSC_HINT(g);
+            const int hc = hcode_l[g];
+            if (hc >= 0 && hc != code) hp = remap_hints(hp, hc, code);
+            const unsigned dj = dj_l[g];
+            int k00, k01, k10, k11, j00, j01, j10, j11;
+            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(hp & 0xffff),
+                                             (int)(dj & 0xff), &k00, &j00, dg);
+            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((hp >> 16) & 0xffff),
+                                             (int)((dj >> 8) & 0xff), &k01, &j01, dg);
+            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((hp >> 32) & 0xffff),
+                                             (int)((dj >> 16) & 0xff), &k10, &j10, dg);
+            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(hp >> 48),
+                                             (int)(dj >> 24), &k11, &j11, dg);
             JSC_HINT(g) = (unsigned long long)(j00 & 0xffff) | ((unsigned long long)(j01 & 0xffff) << 16) |
                           ((unsigned long long)(j10 & 0xffff) << 32) |
                           ((unsigned long long)(j11 & 0xffff) << 48);
+            hcode_l[g] = code;
+            dj_l[g] = (unsigned)min(j00 - k00, 255) | ((unsigned)min(j01 - k01, 255) << 8) |
+                      ((unsigned)min(j10 - k10, 255) << 16) | ((unsigned)min(j11 - k11, 255) << 24);
             const double *gp = m.grid_p + (size_t)gid * TBLNPMAX;
             const double *gt = m.grid_t + (size_t)gid * TBLNPMAX * TBLNTMAX;
             double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,

@@ -68,6 +68,8 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
 
   double tp = 1, rad = 0, tau = 1;
   unsigned long long hint = 0;  // 16-bit interval hint per (p, T) corner row
+  int hcode = -1;               // the bracket code the hints belong to
+  unsigned djp = 0;             // forward distances j - k of the rows, 8 bits each
   unsigned long long dig = 0;
   unsigned n_ega = 0;
   const int np = A.nlos[r];
@@ -97,13 +99,21 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
               (r11.nf & 0xffff) >= 2) {
             const double x1 = 1 - tp, useg = rec[REC_K + m.nw + g];
             if (DIG) dig = dig * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
-            int j00, j01, j10, j11;
-            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(hint & 0xffff), &j00, &dig);
-            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((hint >> 16) & 0xffff), &j01, &dig);
-            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((hint >> 32) & 0xffff), &j10, &dig);
-            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(hint >> 48), &j11, &dig);
+            if (hcode >= 0 && hcode != code) hint = remap_hints(hint, hcode, code);
+            int k00, k01, k10, k11, j00, j01, j10, j11;
+            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(hint & 0xffff),
+                                             (int)(djp & 0xff), &k00, &j00, &dig);
+            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((hint >> 16) & 0xffff),
+                                             (int)((djp >> 8) & 0xff), &k01, &j01, &dig);
+            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((hint >> 32) & 0xffff),
+                                             (int)((djp >> 16) & 0xff), &k10, &j10, &dig);
+            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(hint >> 48),
+                                             (int)(djp >> 24), &k11, &j11, &dig);
             hint = (unsigned long long)(j00 & 0xffff) | ((unsigned long long)(j01 & 0xffff) << 16) |
                    ((unsigned long long)(j10 & 0xffff) << 32) | ((unsigned long long)(j11 & 0xffff) << 48);
+            hcode = code;
+            djp = (unsigned)min(j00 - k00, 255) | ((unsigned)min(j01 - k01, 255) << 8) |
+                  ((unsigned)min(j10 - k10, 255) << 16) | ((unsigned)min(j11 - k11, 255) << 24);
             double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
                                             gt[ipr * TBLNTMAX + it0 + 1], e01, T));
             const double eb = jsc_clamp01(jsc_lin(gt[(ipr + 1) * TBLNTMAX + it1], e10,
