@@ -595,8 +595,8 @@ def main():
         peak, peak_src = 6650.0, "fallback"
     achieved = B / (ega / 1e3) / 1e9
     # DRAM bytes (read + write) per launch: ncu's dram__bytes of one 20k-ray
-    # launch of this workload (283.4 GB for 1.854e9 EGA evaluations, see
-    # profiles/ega_rt_clear_batched.md) scaled by the EGA evaluations here
+    # launch of this workload (283.4 GB for 1.854e9 EGA evaluations, rolled
+    # variant, 128 threads x 12 blocks/SM) scaled by the EGA evaluations here
     traffic = TRAFFIC_PER_EGA * n_ega
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
