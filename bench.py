@@ -127,7 +127,11 @@ def make_workload(n_rays, seed_offset=0):
     return ctlkw, atms, ray_atm, geom
 
 
-TRAFFIC_PER_EGA = 283.4e9 / 1.854e9  # ncu dram__bytes read+write per EGA evaluation
+# ncu dram__bytes (read + write) per EGA evaluation of one 20k-ray launch of
+# this workload (1.854e9 evaluations), per kernel family: a thread per
+# (ray, channel) (variants 0-8: 277.5 + 81.3 GB) and a lane per (ray,
+# channel, emitter) (variants 9-13: 66.2 + 0.7 GB)
+TRAFFIC_PER_EGA = {"thread": 358.8e9 / 1.854e9, "lane": 66.9e9 / 1.854e9}
 
 
 def algorithmic_bytes(n_ega, n_points, n_rays, nd, ng):
@@ -594,10 +598,10 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     achieved = B / (ega / 1e3) / 1e9
-    # DRAM bytes (read + write) per launch: ncu's dram__bytes of one 20k-ray
-    # launch of this workload (283.4 GB for 1.854e9 EGA evaluations, rolled
-    # variant, 128 threads x 12 blocks/SM) scaled by the EGA evaluations here
-    traffic = TRAFFIC_PER_EGA * n_ega
+    # DRAM bytes per launch: the captured bytes per EGA evaluation of the
+    # chosen kernel family, scaled by the EGA evaluations here
+    family = "lane" if tuned.get("variant", 0) >= 9 else "thread"
+    traffic = TRAFFIC_PER_EGA[family] * n_ega
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
