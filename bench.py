@@ -219,11 +219,27 @@ def scattering_bench(args, local, torch, oracle_sample=True):
     train_s = time.perf_counter() - t0
     b.upload(inp, stream=sp)
     b.set_surrogate(sur, tol_rel=0.01, check_stride=256)
+    b.set_timing(True)
     for _ in range(3):
         b.run(stream=sp)
     sur_ms = timed(5)
+    inf_ms = b.kernel_ms("surrogate")
     out = b.download(stream=sp)
     st = b.surrogate_stats()
+    # the same step on the legacy mma.sync path, for comparison
+    sur.set_tensor_path(False)
+    b.run(stream=sp)
+    sur_ms_mma = timed(3)
+    inf_ms_mma = b.kernel_ms("surrogate")
+    sur.set_tensor_path(True)
+    # tensor-pipe work of one inference: 2 x (16x128 + 2 x 128x128 + 128 x nd16) per point
+    nd16 = (nd + 15) // 16 * 16
+    mlp_flop = 2.0 * st["points"] * (16 * 128 + 2 * 128 * 128 + 128 * nd16)
+    peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        tc_peak, tc_src = json.load(open(peaks_path))["bf16_tflops"], "measured"
+    else:
+        tc_peak, tc_src = 1590.0, "fallback"
     res = {"workload": SCA_WORKLOAD, "rays": n, "channels": nd, "scattering_points": st["points"],
            "plain": {"value": n * nd / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                      "steps": 1, "warmup": 1},
@@ -234,7 +250,16 @@ def scattering_bench(args, local, torch, oracle_sample=True):
                          "checked_points": st["checked"],
                          "max_albedo_weighted_src_err_checked": st["max_rel_err"], "check_tolerance": 0.01,
                          "network": "4 layers, width 128, tanh; BF16 weights, FP32 accumulation "
-                                    "(mma.sync m16n8k16)"},
+                                    "(tcgen05.mma, accumulators in tensor memory)",
+                         "inference_ms": inf_ms,
+                         "inference_tensor": {"bound": "tensor", "achieved": mlp_flop / (inf_ms / 1e3) / 1e12,
+                                              "peak": tc_peak, "unit": "TFLOP/s",
+                                              "frac": mlp_flop / (inf_ms / 1e3) / 1e12 / tc_peak,
+                                              "peak_source": tc_src,
+                                              "note": "one launch per step, timed up to the read-back "
+                                                      "of its wait status; the feature pass, envelope "
+                                                      "marks and sampled plain check are outside it"},
+                         "mma_sync_path": {"ms_per_step": sur_ms_mma, "inference_ms": inf_ms_mma}},
            "training": {"samples": int(len(X)), "epochs": args.sca_epochs, "seconds": train_s,
                         "final_loss": float(losses[-1]),
                         "kernels": "hand-written FP32 SGEMM forward/backward, Adam"}}

@@ -310,7 +310,9 @@ int jsc_formod_batch_noalloc(jsc_model *m, const ctl_t *ctl,
 
 /* Per-kernel timing of the last jsc_batch_run (CUDA events on its stream).
  * kernel: "hydrostatic", "raytrace", "scatter" (scattering sources: the
- * secondary and solar pencils and the source integrals), "ega_rt".  Returns milliseconds, or a
+ * secondary and solar pencils and the source integrals, or the surrogate
+ * path), "surrogate" (the network's inference inside it), "continua" (the
+ * lane variants' pre-pass), "ega_rt".  Returns milliseconds, or a
  * negative value when timing is off or the kernel did not run. */
 void jsc_batch_set_timing(jsc_batch *b, int on);
 double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel);
@@ -425,6 +427,11 @@ int jsc_surrogate_train(jsc_surrogate *s, const float *X, const double *src, int
 
 /* Sources [n][nd] of n raw feature rows. */
 int jsc_surrogate_predict(jsc_surrogate *s, const float *feat, int n, double *src);
+
+/* Inference path: 1 (default) tcgen05 (BF16 operands in shared memory,
+ * FP32 accumulators in tensor memory, 128 points per tile), 0 BF16
+ * mma.sync.  Both use the same rounded weights. */
+int jsc_surrogate_set_tensor_path(jsc_surrogate *s, int tcgen05);
 
 /* Features and plain scattering sources of the last run's scattering
  * points (training data); n receives the point count, arrays may be NULL

@@ -24,10 +24,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 C_SRCS = ["model_host.c", "formod.c"]
 CU_SRCS = ["model_dev.cu", "batch.cu", "ega_g2.cu", "ega_g4.cu", "ega_g8.cu",
-           "ega_gmax.cu", "ega_lane_s.cu", "ega_lane_l.cu", "noalloc.cu", "surrogate.cu"]
+           "ega_gmax.cu", "ega_lane_s.cu", "ega_lane_l.cu", "noalloc.cu", "surrogate.cu",
+           "surrogate_tc.cu"]
 HEADERS = ["jsc_internal.h", "physics.h", "ckd_tables.h", "jsc_model.h",
            "cuda_util.cuh", "device_common.cuh", "kernels.cuh", "ega_kernel.cuh",
-           "ega_lane.cuh", "scatter.cuh", "surrogate.h"]
+           "ega_lane.cuh", "scatter.cuh", "surrogate.h", "surrogate_tc.h"]
 
 INC = ["-I" + os.path.join(REPO, "include"), "-I" + CSRC]
 CFLAGS = ["-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-std=gnu11",

@@ -809,7 +809,9 @@ static int scatter_sources(jsc_batch *b, cudaStream_t s) {
   jsc_sur_envelope(b->sur, env.lo, env.hi);
   sur_mark_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, b->d_feat, env, b->sur_stride, b->d_mark);
   JSC_LAUNCH_CHECK();
+  ev_record(b, JSC_T_SUR, 0, s);
   if ((st = jsc_sur_infer(b->sur, n, b->d_feat, b->d_src, nd, s))) return st;
+  ev_record(b, JSC_T_SUR, 1, s);
   sur_compact_kernel<<<1, 1024, 0, s>>>(n, b->d_mark, b->d_idx, b->d_idx + b->sur_cap);
   JSC_LAUNCH_CHECK();
   int m = 0;
@@ -1238,6 +1240,7 @@ extern "C" double jsc_batch_kernel_ms(const jsc_batch *b, const char *kernel) {
   if (!strcmp(kernel, "hydrostatic")) k = JSC_T_HYDRO;
   else if (!strcmp(kernel, "scatter")) k = JSC_T_SCATTER;
   else if (!strcmp(kernel, "continua")) k = JSC_T_CTM;
+  else if (!strcmp(kernel, "surrogate")) k = JSC_T_SUR;
   else if (!strcmp(kernel, "raytrace")) k = JSC_T_RAYTRACE;
   else if (!strcmp(kernel, "ega_rt")) k = JSC_T_EGA;
   if (k < 0 || !b->ran[k]) return -1;

@@ -64,7 +64,7 @@ struct EgaArgs {
 };
 
 // Kernel timers of a batch.
-enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_SCATTER, JSC_T_CTM, JSC_T_N };
+enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_SCATTER, JSC_T_CTM, JSC_T_SUR, JSC_T_N };
 
 #define JSC_NALPHA_REF 28  // secondary pencils per scattering point (src/scatter.c:673)
 

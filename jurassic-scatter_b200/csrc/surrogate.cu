@@ -26,6 +26,7 @@
 
 #include "scatter.cuh"
 #include "surrogate.h"
+#include "surrogate_tc.h"
 
 // ------------------------------------------------------------ features --
 
@@ -391,7 +392,11 @@ struct jsc_surrogate {
   float *d_g[4][2];         // gradients
   float *d_m[4][2], *d_v[4][2];  // Adam moments
   int64_t adam_t;
-  unsigned char *d_image;   // bf16 inference image
+  unsigned char *d_image;   // bf16 inference image (mma.sync path)
+  int tc;                   // 1: tcgen05 inference path
+  unsigned char *d_tc_image;
+  int tc_packed;
+  unsigned *d_tc_status;    // the tcgen05 kernel's wait status
   float xm[SUR_NF], xs[SUR_NF];
   float lo[SUR_NF], hi[SUR_NF];  // envelope of raw features
   float *d_ym, *d_ys;       // [nout] target standardisation
@@ -418,7 +423,7 @@ extern "C" int jsc_surrogate_param_count(const jsc_surrogate *s) {
 static void free_train(jsc_surrogate *s) {
   for (int i = 0; i < 5; i++) cudaFree(s->d_h[i]), s->d_h[i] = nullptr;
   for (int i = 0; i < 2; i++) cudaFree(s->d_dh[i]), s->d_dh[i] = nullptr;
-  cudaFree(s->d_xb);
+  // d_xb is the first activation buffer d_h[0], freed above
   cudaFree(s->d_tb);
   cudaFree(s->d_part);
   cudaFree(s->d_idx);
@@ -438,6 +443,8 @@ extern "C" void jsc_surrogate_destroy(jsc_surrogate *s) {
       cudaFree(s->d_v[l][j]);
     }
   cudaFree(s->d_image);
+  cudaFree(s->d_tc_image);
+  cudaFree(s->d_tc_status);
   cudaFree(s->d_ym);
   cudaFree(s->d_ys);
   cudaFree(s->d_X);
@@ -467,6 +474,7 @@ extern "C" int jsc_surrogate_create(int nd, int device, uint64_t seed, jsc_surro
   s->device = device;
   s->nout = nd;
   s->noutp = (nd + 7) / 8 * 8;
+  s->tc = 1;  // tcgen05 inference by default
   const int in[4] = {SUR_NF, SUR_W, SUR_W, SUR_W}, outw[4] = {SUR_W, SUR_W, SUR_W, nd};
   int st = JSC_OK;
   uint64_t rs = seed;
@@ -550,6 +558,7 @@ extern "C" int jsc_surrogate_set_params(jsc_surrogate *s, const float *in) {
     o += nb;
   }
   s->packed = 0;
+  s->tc_packed = 0;
   return JSC_OK;
 }
 
@@ -773,6 +782,7 @@ extern "C" int jsc_surrogate_train(jsc_surrogate *s, const float *X, const doubl
   if (st) return st;
   s->trained = 1;
   s->packed = 0;
+  s->tc_packed = 0;
   return JSC_OK;
 }
 
@@ -795,9 +805,63 @@ int jsc_sur_features(int n, const double *sp, float *feat, cudaStream_t st) {
   return JSC_OK;
 }
 
+static int infer_tc(jsc_surrogate *s, int n, const float *feat, double *src, int nd,
+                    cudaStream_t st) {
+  int e;
+  if (!s->d_tc_image) {
+    if ((e = jsc_dmalloc(&s->d_tc_image, (size_t)jsc_sur_tc_image_bytes(s->nout)))) return e;
+    if ((e = jsc_dmalloc(&s->d_tc_status, 1))) return e;
+  }
+  if (!s->tc_packed) {
+    const float *w[4] = {s->d_p[0][0], s->d_p[1][0], s->d_p[2][0], s->d_p[3][0]};
+    const float *b[4] = {s->d_p[0][1], s->d_p[1][1], s->d_p[2][1], s->d_p[3][1]};
+    jsc_count_launch();
+    if ((e = jsc_sur_tc_pack(s->nout, w, b, s->d_tc_image, st))) {
+      jsc_set_error(JSC_ERR_CUDA, "tcgen05 weight packing: %s", cudaGetErrorString((cudaError_t)e));
+      return JSC_ERR_CUDA;
+    }
+    s->tc_packed = 1;
+  }
+  TcInferArgs a;
+  a.n = n;
+  a.nout = s->nout;
+  a.nd = nd;
+  a.feat = feat;
+  a.image = s->d_tc_image;
+  for (int c = 0; c < SUR_NF; c++) {
+    a.xm[c] = s->xm[c];
+    a.xs[c] = s->xs[c];
+  }
+  a.ym = s->d_ym;
+  a.ys = s->d_ys;
+  a.src = src;
+  a.status = s->d_tc_status;
+  JSC_CUDA_TRY(cudaMemsetAsync(s->d_tc_status, 0, sizeof(unsigned), st));
+  jsc_count_launch();
+  if ((e = jsc_sur_tc_infer(a, st))) {
+    jsc_set_error(JSC_ERR_CUDA, "tcgen05 inference launch: %s", cudaGetErrorString((cudaError_t)e));
+    return JSC_ERR_CUDA;
+  }
+  unsigned hs = 0;
+  JSC_CUDA_TRY(cudaMemcpyAsync(&hs, s->d_tc_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  JSC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (hs) {
+    jsc_set_error(JSC_ERR_WATCHDOG, "tcgen05 inference: an MMA completion wait gave up");
+    return JSC_ERR_WATCHDOG;
+  }
+  return JSC_OK;
+}
+
+extern "C" int jsc_surrogate_set_tensor_path(jsc_surrogate *s, int tcgen05) {
+  if (!s) return JSC_ERR_ARG;
+  s->tc = tcgen05 != 0;
+  return JSC_OK;
+}
+
 int jsc_sur_infer(jsc_surrogate *s, int n, const float *feat, double *src, int nd,
                   cudaStream_t st) {
   if (n <= 0) return JSC_OK;
+  if (s->tc) return infer_tc(s, n, feat, src, nd, st);
   int e = pack(s, st);
   if (e) return e;
   SurInferArgs a;

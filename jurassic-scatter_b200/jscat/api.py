@@ -405,6 +405,11 @@ class Surrogate:
                 "jsc_surrogate_train")
         return losses
 
+    def set_tensor_path(self, tcgen05):
+        """Inference on the tcgen05 path (True) or mma.sync (False)."""
+        L.check(L.load().jsc_surrogate_set_tensor_path(self.h, 1 if tcgen05 else 0),
+                "jsc_surrogate_set_tensor_path")
+
     def predict(self, feat):
         feat = np.ascontiguousarray(feat, dtype=np.float32)
         out = np.empty((len(feat), self.nd))

@@ -25,7 +25,7 @@ EXPORTS = [
     "jsc_surrogate_loss_grad", "jsc_surrogate_train", "jsc_surrogate_predict",
     "jsc_batch_scatter_samples", "jsc_batch_set_surrogate", "jsc_batch_surrogate_stats",
     "jsc_batch_set_fixed", "jsc_batch_download_async", "jsc_batch_async_status",
-    "jsc_batch_graph_capture", "jsc_batch_graph_launch",
+    "jsc_batch_graph_capture", "jsc_batch_graph_launch", "jsc_surrogate_set_tensor_path",
 ]
 
 
@@ -116,6 +116,7 @@ def load():
         "jsc_surrogate_train": (i, [vp, P(C.c_float), P(d), C.c_int64, i, i, C.c_float,
                                     C.c_uint64, P(C.c_float)]),
         "jsc_surrogate_predict": (i, [vp, P(C.c_float), i, P(d)]),
+        "jsc_surrogate_set_tensor_path": (i, [vp, i]),
         "jsc_batch_scatter_samples": (i, [vp, P(C.c_float), P(d), C.c_int64, P(C.c_int64)]),
         "jsc_batch_set_surrogate": (i, [vp, vp, d, i]),
         "jsc_batch_surrogate_stats": (i, [vp, P(C.c_int64), P(C.c_int64), P(C.c_int64), P(d),

@@ -112,3 +112,26 @@ def test_surrogate_envelope_fallback(workdir):
         sur.close()
         b.close()
         m.close()
+
+
+@pytest.mark.parametrize("nd", [4, 16, 40])
+def test_tcgen05_inference_matches_mma_sync(nd):
+    """The tcgen05 inference path (TMEM accumulators) and the mma.sync path
+    run the same BF16 weights on the same features: their sources agree to
+    the FP32 accumulation order."""
+    from jscat import api
+    rng = np.random.default_rng(9)
+    s = api.Surrogate(nd=nd, seed=2)
+    try:
+        n = 300  # three 128-point tiles, the last one partial
+        feat = rng.normal(0, 1, (n, 8)).astype(np.float32)
+        src = np.exp(rng.normal(-3, 0.3, (n, nd)))
+        s.train(feat, src, epochs=2, batch=64, lr=1e-3)  # sets the standardisation
+        s.set_tensor_path(False)
+        a = s.predict(feat)
+        s.set_tensor_path(True)
+        b = s.predict(feat)
+        assert np.all(np.isfinite(b))
+        assert np.max(np.abs(np.log(b) - np.log(a))) < 2e-3
+    finally:
+        s.close()
