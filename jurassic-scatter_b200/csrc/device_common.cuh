@@ -185,6 +185,12 @@ __device__ __forceinline__ unsigned long long remap_hints(unsigned long long h, 
 
 // LIN on float table entries with the slope already in float, as the
 // reference evaluates it: y0 + slope * (x - x0), promoted to double.
+// Slope of the interval from (x0, y0) to (x1, y1) as LIN evaluates it on
+// float table entries: (y1 - y0) / (x1 - x0) in IEEE single precision.
+__device__ __forceinline__ float float_slope(float y0, float x0, float y1, float x1) {
+  return __fdiv_rn(__fsub_rn(y1, y0), __fsub_rn(x1, x0));
+}
+
 __device__ __forceinline__ double lin_node(float x0, float y0, float slope, double x) {
   return (double)y0 + (double)slope * (x - (double)x0);
 }
@@ -197,7 +203,7 @@ __device__ __forceinline__ double lin_node(float x0, float y0, float slope, doub
 // Fast path: the row is strictly increasing, the interval [h, h+1] of the
 // hint still brackets x1 and the extended column falls in the interval
 // k + dj guessed from the previous point's distance -- then one or two
-// node pairs answer both lookups.  Otherwise the exact searches above find
+// node pairs (8 bytes a node) answer both lookups.  Otherwise the exact searches above find
 // the intervals, starting from the guesses.  *kout and *jout receive the
 // intervals (they do not depend on the guesses).
 template <bool DIG>
@@ -209,31 +215,34 @@ __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, j
   const jsc_node *row = nodes + rd.off;
   const int last = n - 2;
   int k = hint < 0 ? 0 : (hint > last ? last : hint);
-  float4 a = __ldg(reinterpret_cast<const float4 *>(row + k));
-  float4 b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
+  float2 a = __ldg(reinterpret_cast<const float2 *>(row + k));      // (u, eps)[k]
+  float2 b = __ldg(reinterpret_cast<const float2 *>(row + k + 1));  // (u, eps)[k+1]
   const float x1f = __double2float_rd(x1);
   // bracket for x1 on eps: (e[k] <= x1 or k == 0) and (x1 < e[k+1] or k == last)
   if (!(strict && (!(a.y > x1f) || k == 0) && (b.y > x1f || k == last) && x1 == x1)) {
     k = find_interval<false>(row, n, strict, x1, k);
-    a = __ldg(reinterpret_cast<const float4 *>(row + k));
-    b = __ldg(reinterpret_cast<const float4 *>(row + k + 1));
+    a = __ldg(reinterpret_cast<const float2 *>(row + k));
+    b = __ldg(reinterpret_cast<const float2 *>(row + k + 1));
   }
-  const double x2 = lin_node(a.y, a.x, a.z, x1) + useg;
+  const double x2 = lin_node(a.y, a.x, float_slope(a.x, a.y, b.x, b.y), x1) + useg;
   const float x2f = __double2float_rd(x2);
   int j = k + (dj > 0 ? dj : 0);
   if (j > last) j = last;
   if (j != k) {
-    a = __ldg(reinterpret_cast<const float4 *>(row + j));
-    b = __ldg(reinterpret_cast<const float4 *>(row + j + 1));
+    a = __ldg(reinterpret_cast<const float2 *>(row + j));
+    b = __ldg(reinterpret_cast<const float2 *>(row + j + 1));
   }
   if (!(strict && (!(a.x > x2f) || j == 0) && (b.x > x2f || j == last) && x2 == x2)) {
     const int j0 = j;
     j = find_interval<true>(row, n, strict, x2, j0);
-    if (j != j0) a = __ldg(reinterpret_cast<const float4 *>(row + j));
+    if (j != j0) {
+      a = __ldg(reinterpret_cast<const float2 *>(row + j));
+      b = __ldg(reinterpret_cast<const float2 *>(row + j + 1));
+    }
   }
   if (DIG) *dig = (*dig * 1000003ull + (unsigned long long)k) * 1000003ull + (unsigned long long)j;
   *kout = k;
   *jout = j;
-  return jsc_clamp01(lin_node(a.x, a.y, a.w, x2));
+  return jsc_clamp01(lin_node(a.x, a.y, float_slope(a.y, a.x, b.y, b.x), x2));
 }
 

@@ -127,15 +127,14 @@ void jsc_set_error(int status, const char *fmt, ...);
  * Device layout of a model (device pointers; passed by value to kernels).
  * ------------------------------------------------------------------------ */
 
-/* One point k of an emissivity-table row with the slopes of the interval
- * [k, k+1] (zero at the last point).  The reference's LIN on float table
- * entries evaluates (y1-y0)/(x1-x0) in single precision
- * (src/forwardmodel.c:519-541 with the LIN macro of src/jurassic.h:72), so
- * the slopes are stored as the float values it computes. */
-typedef struct JSC_ALIGN(16) {
+/* One point k of an emissivity-table row: column density and emissivity
+ * as the table stores them (float).  The reference's LIN on float table
+ * entries evaluates the slope (y1-y0)/(x1-x0) in single precision
+ * (src/forwardmodel.c:519-541 with the LIN macro of src/jurassic.h:72);
+ * the kernels compute it from the two nodes of an interval with the same
+ * IEEE single-precision operations. */
+typedef struct JSC_ALIGN(8) {
   float u, e;
-  float s_ue;       /* (u1-u0)/(e1-e0): eps -> u  (intpol_tbl_u) */
-  float s_eu;       /* (e1-e0)/(u1-u0): u -> eps  (intpol_tbl_eps) */
 } jsc_node;
 
 /* Row descriptor: first node of the row and n | flags << 16, where n is

@@ -3,10 +3,9 @@
 // Device layout (all in HBM, read-only during a forward model):
 //  * (p, T) grids, deduplicated across tables (most table sets share one);
 //  * a row descriptor per (p level, T, emitter, channel) slot;
-//  * one 16-byte node per table point: u, eps and both slopes of the
-//    interval to the next point, computed on the device with the same IEEE
-//    single-precision operations the reference's LIN evaluates at run time,
-//    so a lookup reads two neighbouring nodes (one 32-byte sector);
+//  * one 8-byte node per table point (u, eps): a lookup reads the two
+//    nodes of its interval and computes the slope with the same IEEE
+//    single-precision operations the reference's LIN evaluates;
 //  * Planck source tables with slopes, continuum coefficients per channel.
 #include <stdio.h>
 #include <stdlib.h>
@@ -38,13 +37,6 @@ __global__ void build_nodes_kernel(const jsc_row *rows, const int64_t *row_pt,
       jsc_node v;
       v.u = u[pt + k];
       v.e = e[pt + k];
-      v.s_ue = 0.0f;
-      v.s_eu = 0.0f;
-      if (k + 1 < n) {
-        const float u1 = u[pt + k + 1], e1 = e[pt + k + 1];
-        v.s_ue = __fdiv_rn(__fsub_rn(u1, v.u), __fsub_rn(e1, v.e));
-        v.s_eu = __fdiv_rn(__fsub_rn(e1, v.e), __fsub_rn(u1, v.u));
-      }
       nodes[off + k] = v;
     }
   }
