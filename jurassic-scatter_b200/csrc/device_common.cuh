@@ -183,14 +183,14 @@ __device__ __forceinline__ unsigned long long remap_hints(unsigned long long h, 
   return out;
 }
 
-// LIN on float table entries with the slope already in float, as the
-// reference evaluates it: y0 + slope * (x - x0), promoted to double.
 // Slope of the interval from (x0, y0) to (x1, y1) as LIN evaluates it on
 // float table entries: (y1 - y0) / (x1 - x0) in IEEE single precision.
 __device__ __forceinline__ float float_slope(float y0, float x0, float y1, float x1) {
   return __fdiv_rn(__fsub_rn(y1, y0), __fsub_rn(x1, x0));
 }
 
+// LIN on float table entries with the slope already in float, as the
+// reference evaluates it: y0 + slope * (x - x0), promoted to double.
 __device__ __forceinline__ double lin_node(float x0, float y0, float slope, double x) {
   return (double)y0 + (double)slope * (x - (double)x0);
 }
