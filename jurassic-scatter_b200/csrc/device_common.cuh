@@ -195,6 +195,56 @@ __device__ __forceinline__ double lin_node(float x0, float y0, float slope, doub
   return (double)y0 + (double)slope * (x - (double)x0);
 }
 
+// Key of a node read as float2 (u, eps).
+template <bool U>
+__device__ __forceinline__ float key2(float2 v) { return U ? v.x : v.y; }
+
+// Near miss of an interval guess on a strictly increasing row: the guess i
+// (nodes *a = i, *b = i+1) failed the bracket test for xf = RD(x), x not
+// NaN.  Tries the two intervals on the side where x lies with independent
+// loads (one round of latency); on success moves *k, *a, *b there and
+// returns true.  The accepted interval passes the same bracket test as the
+// exact search's result, so it is that result (the bracket is unique on a
+// strictly increasing row).
+template <bool U>
+__device__ __forceinline__ bool near_interval(const jsc_node *row, int last, float xf, int *k,
+                                              float2 *a, float2 *b) {
+  const int i = *k;
+  if (key2<U>(*a) > xf) {  // below the interval (then i > 0)
+    const float2 m1 = __ldg(reinterpret_cast<const float2 *>(row + i - 1));
+    const float2 m2 = i >= 2 ? __ldg(reinterpret_cast<const float2 *>(row + i - 2)) : m1;
+    if (!(key2<U>(m1) > xf) || i == 1) {
+      *b = *a;
+      *a = m1;
+      *k = i - 1;
+      return true;
+    }
+    if (!(key2<U>(m2) > xf) || i == 2) {  // i >= 2 here
+      *b = m1;
+      *a = m2;
+      *k = i - 2;
+      return true;
+    }
+    return false;
+  }
+  // at or above the upper key (then i < last)
+  const float2 p2 = __ldg(reinterpret_cast<const float2 *>(row + i + 2));
+  const float2 p3 = i + 2 <= last ? __ldg(reinterpret_cast<const float2 *>(row + i + 3)) : p2;
+  if (key2<U>(p2) > xf || i + 1 == last) {
+    *a = *b;
+    *b = p2;
+    *k = i + 1;
+    return true;
+  }
+  if (key2<U>(p3) > xf || i + 2 == last) {  // i + 2 <= last here
+    *a = p2;
+    *b = p3;
+    *k = i + 2;
+    return true;
+  }
+  return false;
+}
+
 // Emissivity of the extended path at one (p, T) node of a table
 // (intpol_tbl_u then intpol_tbl_eps, src/forwardmodel.c:460-474): invert
 // the path emissivity x1 to a column density on the row, add the segment's
@@ -203,9 +253,10 @@ __device__ __forceinline__ double lin_node(float x0, float y0, float slope, doub
 // Fast path: the row is strictly increasing, the interval [h, h+1] of the
 // hint still brackets x1 and the extended column falls in the interval
 // k + dj guessed from the previous point's distance -- then one or two
-// node pairs (8 bytes a node) answer both lookups.  Otherwise the exact searches above find
-// the intervals, starting from the guesses.  *kout and *jout receive the
-// intervals (they do not depend on the guesses).
+// node pairs (8 bytes a node) answer both lookups.  A guess off by one or
+// two intervals is corrected by near_interval; otherwise the exact
+// searches above find the intervals, starting from the guesses.  *kout and
+// *jout receive the intervals (they do not depend on the guesses).
 template <bool DIG>
 __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, jsc_row rd,
                                            double x1, double useg, int hint, int dj, int *kout,
@@ -219,7 +270,8 @@ __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, j
   float2 b = __ldg(reinterpret_cast<const float2 *>(row + k + 1));  // (u, eps)[k+1]
   const float x1f = __double2float_rd(x1);
   // bracket for x1 on eps: (e[k] <= x1 or k == 0) and (x1 < e[k+1] or k == last)
-  if (!(strict && (!(a.y > x1f) || k == 0) && (b.y > x1f || k == last) && x1 == x1)) {
+  if (!(strict && (!(a.y > x1f) || k == 0) && (b.y > x1f || k == last) && x1 == x1) &&
+      !(strict && x1 == x1 && near_interval<false>(row, last, x1f, &k, &a, &b))) {
     k = find_interval<false>(row, n, strict, x1, k);
     a = __ldg(reinterpret_cast<const float2 *>(row + k));
     b = __ldg(reinterpret_cast<const float2 *>(row + k + 1));
@@ -232,7 +284,8 @@ __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, j
     a = __ldg(reinterpret_cast<const float2 *>(row + j));
     b = __ldg(reinterpret_cast<const float2 *>(row + j + 1));
   }
-  if (!(strict && (!(a.x > x2f) || j == 0) && (b.x > x2f || j == last) && x2 == x2)) {
+  if (!(strict && (!(a.x > x2f) || j == 0) && (b.x > x2f || j == last) && x2 == x2) &&
+      !(strict && x2 == x2 && near_interval<true>(row, last, x2f, &j, &a, &b))) {
     const int j0 = j;
     j = find_interval<true>(row, n, strict, x2, j0);
     if (j != j0) {
