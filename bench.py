@@ -128,10 +128,10 @@ def make_workload(n_rays, seed_offset=0):
 
 
 # ncu dram__bytes (read + write) per EGA evaluation of one 20k-ray launch of
-# this workload (1.854e9 evaluations), per kernel family: a thread per
-# (ray, channel) (variants 0-8: 277.5 + 81.3 GB) and a lane per (ray,
-# channel, emitter) (variants 9-13: 66.2 + 0.7 GB)
-TRAFFIC_PER_EGA = {"thread": 358.8e9 / 1.854e9, "lane": 66.9e9 / 1.854e9}
+# this workload (1.8536e9 evaluations), per kernel family: a thread per
+# (ray, channel) (variant 6: 194.5 + 74.3 GB) and a lane per (ray,
+# channel, emitter) (variant 13: 27.8 + 0.6 GB)
+TRAFFIC_PER_EGA = {"thread": 268.8e9 / 1.8536e9, "lane": 28.4e9 / 1.8536e9}
 
 
 def algorithmic_bytes(n_ega, n_points, n_rays, nd, ng):
