@@ -348,7 +348,8 @@ int jsc_batch_graph_capture(jsc_batch *b, const jsc_batch_input *in,
                             const jsc_batch_output *out, void *stream);
 int jsc_batch_graph_launch(jsc_batch *b, void *stream);
 
-/* Select the EGA launch variant by hand (-1: the default).  Variants 0-8
+/* Select the EGA launch variant by hand (-1: the default, variant 6 for
+ * clear air and 10 for runs with aerosol/cloud layers).  Variants 0-8
  * run a thread per (ray, channel) with every emitter's path state; 9-13 a
  * lane per (ray, channel, emitter) after a separate continuum/Planck pass.
  * All variants compute the same operations in the same order. */

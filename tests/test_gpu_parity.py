@@ -54,9 +54,10 @@ def test_clear_limb_dropin_formod(workdir):
     np.testing.assert_allclose(S.arr(obs.tpz)[:nr], g["tpz"], rtol=1e-9, atol=1e-9)
 
 
-# EGA kernel families: -1 the default (a thread per (ray, channel)), 9 a
-# lane per (ray, channel, emitter)
-VARIANTS = [-1, 9]
+# EGA kernel families: -1 the default (variant 6 for clear air, 10 with
+# aerosol/cloud layers), 6 a thread per (ray, channel), 9 a lane per (ray,
+# channel, emitter)
+VARIANTS = [-1, 6, 9]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
