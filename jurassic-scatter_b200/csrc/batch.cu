@@ -1012,7 +1012,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     fa.geo = b->d_geo;
     fa.pts = b->d_pts;
     fa.max_seg = b->max_seg;
-    refine_kernel<false><<<(nr + 127) / 128, 128, 0, s>>>(fa);
+    refine_count_kernel<<<(nr + 127) / 128, 128, 0, s>>>(fa);
     JSC_LAUNCH_CHECK();
     scan_kernel<<<1, 1024, 0, s>>>(b->d_nlos, nr, b->d_los_off);
     JSC_LAUNCH_CHECK();
@@ -1031,7 +1031,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     fa.geo = b->d_geo;
     fa.pts = b->d_pts;
     fa.max_seg = b->max_seg;
-    refine_kernel<true><<<(nr + 127) / 128, 128, 0, s>>>(fa);
+    refine_store_kernel<<<(unsigned)(((int64_t)nr * 32 + 127) / 128), 128, 0, s>>>(fa);
     JSC_LAUNCH_CHECK();
   }
   if (b->fixed) {

@@ -6,7 +6,8 @@
 //                     (src/lineofsight.c:5-190); a counting pass sizes the
 //                     line of sight, a storing pass writes the LOS records.
 //   scan_kernel       exclusive prefix sum of LOS points per ray.
-//   refine_kernel     aerosol/cloud layer-edge refinement of the LOS.
+//   refine_count_kernel, refine_store_kernel
+//                     aerosol/cloud layer-edge refinement of the LOS.
 //   (ega_rt_kernel, the EGA + continua + Planck + radiative-transfer
 //   kernel, is in ega_kernel.cuh.)
 //
@@ -427,19 +428,66 @@ __device__ __forceinline__ void refine_cross(const RefineArgs &A, const Profile 
   for (int g = 0; g < A.ng; g++) po[REC_K + A.nw + g] = atm_lin(a.q + (size_t)g * a.stride, a, ipz, zz);
 }
 
-// Extra LOS points at the layer edges and through the transition layers,
-// chord step lengths, column densities, layer index and scaling factor per
-// point (add_aerosol_layers, src/lineofsight.c:193-372).  COUNT pass sizes
-// the refined LOS, STORE pass writes it.
-template <bool STORE>
-__global__ void __launch_bounds__(128) refine_kernel(RefineArgs A) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= A.n_rays) return;
-  const int nb = A.nlos_b[r];
-  if (nb == 0) {
-    if (!STORE) A.nlos[r] = 0;
-    return;
+// Chord step length, column densities, (p, T) bracket, Planck index and
+// aerosol layer/factor of refined point i (the per-point part of
+// add_aerosol_layers, src/lineofsight.c:300-372).  xp, xc, xn: Cartesian
+// positions of points i-1, i, i+1 (xp unused at i = 0, xn at i = o-1).
+__device__ __forceinline__ void refine_point(const RefineArgs &A, int64_t base, int o, int i,
+                                             const double *xp, const double *xc,
+                                             const double *xn) {
+  double ds;
+  if (o == 1) {
+    ds = 0;
+  } else if (i == 0) {
+    ds = 0.5 * sqrt((xc[0] - xn[0]) * (xc[0] - xn[0]) + (xc[1] - xn[1]) * (xc[1] - xn[1]) +
+                    (xc[2] - xn[2]) * (xc[2] - xn[2]));
+  } else if (i == o - 1) {
+    ds = 0.5 * sqrt((xc[0] - xp[0]) * (xc[0] - xp[0]) + (xc[1] - xp[1]) * (xc[1] - xp[1]) +
+                    (xc[2] - xp[2]) * (xc[2] - xp[2]));
+  } else {
+    ds = 0.5 * (sqrt((xp[0] - xc[0]) * (xp[0] - xc[0]) + (xp[1] - xc[1]) * (xp[1] - xc[1]) +
+                     (xp[2] - xc[2]) * (xp[2] - xc[2])) +
+                sqrt((xc[0] - xn[0]) * (xc[0] - xn[0]) + (xc[1] - xn[1]) * (xc[1] - xn[1]) +
+                     (xc[2] - xn[2]) * (xc[2] - xn[2])));
   }
+  double *go = A.geo + base * 4;
+  double *rec = A.pts + (base + i) * A.W;
+  const double p = rec[REC_P], t = rec[REC_T], z = go[(size_t)i * 4];
+  rec[REC_DS] = ds;
+  go[(size_t)i * 4 + 3] = ds;
+  for (int g = 0; g < A.ng; g++) {
+    const double q = rec[REC_K + A.nw + g];
+    rec[REC_K + A.nw + g] = 10 * q * p / (JSC_KBOLTZ * t) * ds;
+  }
+  rec[REC_GRID] = A.grid_p ? (double)grid_code(A.grid_np, A.grid_p, A.grid_nt, A.grid_t, p, t) : -1.0;
+  rec[REC_PLK] = (double)planck_index(t);
+  // At i = 0 the reference compares z[-1]; the first point, at the top
+  // of the atmosphere and outside every layer, stands in for it.
+  const double zprev = go[(size_t)(i > 0 ? i - 1 : 0) * 4];
+  int aeroi = -999;
+  double aerofac = 0.;
+  if ((zprev < A.altimax || z < A.altimax) && (zprev > A.altimin || z > A.altimin)) {
+    for (int il = 0; il < A.nl; il++) {
+      if (z <= A.top[il] && z >= A.bottom[il]) {
+        aeroi = il;
+        aerofac = 1.;
+      }
+      if (A.trans[il] > A.transs && z <= (A.top[il] + A.trans[il]) && z > A.top[il]) {
+        aeroi = il;
+        aerofac = (A.top[il] + A.trans[il] - z) / A.trans[il];
+      }
+      if (A.trans[il] > A.transs && z < A.bottom[il] && z >= (A.bottom[il] - A.trans[il])) {
+        aeroi = il;
+        aerofac = fabs(A.bottom[il] - A.trans[il] - z) / A.trans[il];
+      }
+    }
+  }
+  rec[REC_AF] = aerofac;
+  rec[REC_AI] = (double)aeroi;
+}
+
+// Profile of ray r's atmosphere.
+__device__ __forceinline__ Profile refine_profile(const RefineArgs &A, int r) {
   const int ai = A.ray_atm[r];
   const int lo = A.atm_off[ai];
   Profile a;
@@ -450,113 +498,143 @@ __global__ void __launch_bounds__(128) refine_kernel(RefineArgs A) {
   a.t = A.t + lo;
   a.q = A.q + lo;
   a.k = A.k + lo;
+  return a;
+}
+
+// STORE pass of the layer-edge refinement with a warp per ray (the COUNT
+// pass is refine_count_kernel): lanes take 32 raw points at a time, a
+// warp scan of their output counts (crossing points of the segment before
+// the point, then the point) places them in the order the serial pass
+// writes them, the raw records are copied with coalesced loads, then lanes
+// take 32 refined points at a time for refine_point, with the neighbours'
+// Cartesian positions passed by shuffles.  Same outputs as the serial pass,
+// including its overflow status.
+static __global__ void __launch_bounds__(128) refine_store_kernel(RefineArgs A) {
+  const int r = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  const unsigned full = 0xffffffffu;
+  if (r >= A.n_rays) return;  // whole warps leave together
+  const int nb = A.nlos_b[r];
+  if (nb == 0) return;
+  const Profile a = refine_profile(A, r);
   const double *gb = A.geo_b + A.off_b[r] * 4, *pb = A.pts_b + A.off_b[r] * A.W;
-  const int64_t base = STORE ? A.off[r] : 0;
-  const int nmax = STORE ? A.nlos[r] : NLOS + 1;
+  const int64_t base = A.off[r];
+  const int nmax = A.nlos[r];
+  const int W = A.W;
   int o = 0;
-  bool over = false;
-#define JSC_PUT_BASE(ip)                                                     \
-  do {                                                                       \
-    if (o >= nmax || base + o >= A.max_seg) { over = true; break; }          \
-    if (STORE) {                                                             \
-      double *go = A.geo + (base + o) * 4, *po = A.pts + (base + o) * A.W;   \
-      const double *gs = gb + (size_t)(ip) * 4, *ps = pb + (size_t)(ip) * A.W; \
-      go[0] = gs[0]; go[1] = gs[1]; go[2] = gs[2];                           \
-      for (int c = 0; c < A.W; c++) po[c] = ps[c];                           \
-    }                                                                        \
-    o++;                                                                     \
-  } while (0)
-  JSC_PUT_BASE(0);
-  for (int ip = 1; ip < nb && !over; ip++) {
-    const double zp = gb[(size_t)(ip - 1) * 4], zc = gb[(size_t)ip * 4];
-    if ((zp < A.altimax || zc < A.altimax) && (zp > A.altimin || zc > A.altimin)) {
-      for (int il = 0; il < A.n_alti && !over; il++) {
-        const double z1 = A.alti[il], z2 = A.alti[A.n_alti - il - 1];
-        if (zp > z1 && zc < z1) {
-          if (o >= nmax || base + o >= A.max_seg) { over = true; break; }
-          if (STORE) refine_cross(A, a, gb, ip, z1, A.geo + (base + o) * 4, A.pts + (base + o) * A.W);
-          o++;
-        }
-        if (zp < z2 && zc > z2) {
-          if (o >= nmax || base + o >= A.max_seg) { over = true; break; }
-          if (STORE) refine_cross(A, a, gb, ip, z2, A.geo + (base + o) * 4, A.pts + (base + o) * A.W);
-          o++;
-        }
+  for (int c0 = 0; c0 < nb; c0 += 32) {
+    const int ip = c0 + lane;
+    int cnt = 0;
+    double zp = 0, zc = 0;
+    bool win = false;
+    if (ip < nb) {
+      cnt = 1;
+      if (ip >= 1) {
+        zp = gb[(size_t)(ip - 1) * 4];
+        zc = gb[(size_t)ip * 4];
+        win = (zp < A.altimax || zc < A.altimax) && (zp > A.altimin || zc > A.altimin);
+        if (win)
+          for (int il = 0; il < A.n_alti; il++) {
+            const double z1 = A.alti[il], z2 = A.alti[A.n_alti - il - 1];
+            cnt += (zp > z1 && zc < z1) + (zp < z2 && zc > z2);
+          }
       }
     }
-    if (!over) JSC_PUT_BASE(ip);
+    int incl = cnt;
+    for (int d = 1; d < 32; d <<= 1) {
+      const int v = __shfl_up_sync(full, incl, d);
+      if (lane >= d) incl += v;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    if (o + total > nmax || base + o + total > A.max_seg) {
+      if (lane == 0) atomicOr(A.status, JSC_DEV_ERR_NLOS);
+      return;
+    }
+    int slot = o + incl - cnt;  // first output slot of this lane
+    if (ip < nb) {
+      if (win)
+        for (int il = 0; il < A.n_alti; il++) {
+          const double z1 = A.alti[il], z2 = A.alti[A.n_alti - il - 1];
+          if (zp > z1 && zc < z1) {
+            refine_cross(A, a, gb, ip, z1, A.geo + (base + slot) * 4, A.pts + (base + slot) * W);
+            slot++;
+          }
+          if (zp < z2 && zc > z2) {
+            refine_cross(A, a, gb, ip, z2, A.geo + (base + slot) * 4, A.pts + (base + slot) * W);
+            slot++;
+          }
+        }
+      double *go = A.geo + (base + slot) * 4;
+      const double *gs = gb + (size_t)ip * 4;
+      go[0] = gs[0];
+      go[1] = gs[1];
+      go[2] = gs[2];
+    }
+    // raw records of the chunk's points, copied element by element
+    const int m = min(32, nb - c0);
+    const int ne = m * W;
+    for (int e0 = 0; e0 < ne; e0 += 32) {
+      const int e = e0 + lane;
+      const int pp = e < ne ? e / W : 0;
+      const int sl = __shfl_sync(full, slot, pp);
+      if (e < ne) A.pts[(base + sl) * W + (e - pp * W)] = pb[(size_t)c0 * W + e];
+    }
+    o += total;
   }
-#undef JSC_PUT_BASE
-  if (over || o > NLOS) {
-    atomicOr(A.status, JSC_DEV_ERR_NLOS);
-    if (!STORE) A.nlos[r] = 0;
+  if (o > NLOS) {
+    if (lane == 0) atomicOr(A.status, JSC_DEV_ERR_NLOS);
     return;
   }
-  if (!STORE) {
-    A.nlos[r] = o;
-    return;
-  }
-  // Chord step lengths, column densities, layer index and factor.
-  double xp[3], xc[3], xn[3];
-  double *go = A.geo + base * 4;
-  jsc_geo2cart(go[0], go[1], go[2], xc);
-  if (o > 1) jsc_geo2cart(go[4], go[5], go[6], xn);
-  for (int i = 0; i < o; i++) {
-    double ds;
-    if (o == 1) {
-      ds = 0;
-    } else if (i == 0) {
-      ds = 0.5 * sqrt((xc[0] - xn[0]) * (xc[0] - xn[0]) + (xc[1] - xn[1]) * (xc[1] - xn[1]) +
-                      (xc[2] - xn[2]) * (xc[2] - xn[2]));
-    } else if (i == o - 1) {
-      ds = 0.5 * sqrt((xc[0] - xp[0]) * (xc[0] - xp[0]) + (xc[1] - xp[1]) * (xc[1] - xp[1]) +
-                      (xc[2] - xp[2]) * (xc[2] - xp[2]));
-    } else {
-      ds = 0.5 * (sqrt((xp[0] - xc[0]) * (xp[0] - xc[0]) + (xp[1] - xc[1]) * (xp[1] - xc[1]) +
-                       (xp[2] - xc[2]) * (xp[2] - xc[2])) +
-                  sqrt((xc[0] - xn[0]) * (xc[0] - xn[0]) + (xc[1] - xn[1]) * (xc[1] - xn[1]) +
-                       (xc[2] - xn[2]) * (xc[2] - xn[2])));
-    }
-    double *rec = A.pts + (base + i) * A.W;
-    const double p = rec[REC_P], t = rec[REC_T], z = go[(size_t)i * 4];
-    rec[REC_DS] = ds;
-    go[(size_t)i * 4 + 3] = ds;
-    for (int g = 0; g < A.ng; g++) {
-      const double q = rec[REC_K + A.nw + g];
-      rec[REC_K + A.nw + g] = 10 * q * p / (JSC_KBOLTZ * t) * ds;
-    }
-    rec[REC_GRID] = A.grid_p ? (double)grid_code(A.grid_np, A.grid_p, A.grid_nt, A.grid_t, p, t) : -1.0;
-    rec[REC_PLK] = (double)planck_index(t);
-    // At i = 0 the reference compares z[-1]; the first point, at the top
-    // of the atmosphere and outside every layer, stands in for it.
-    const double zprev = go[(size_t)(i > 0 ? i - 1 : 0) * 4];
-    int aeroi = -999;
-    double aerofac = 0.;
-    if ((zprev < A.altimax || z < A.altimax) && (zprev > A.altimin || z > A.altimin)) {
-      for (int il = 0; il < A.nl; il++) {
-        if (z <= A.top[il] && z >= A.bottom[il]) {
-          aeroi = il;
-          aerofac = 1.;
-        }
-        if (A.trans[il] > A.transs && z <= (A.top[il] + A.trans[il]) && z > A.top[il]) {
-          aeroi = il;
-          aerofac = (A.top[il] + A.trans[il] - z) / A.trans[il];
-        }
-        if (A.trans[il] > A.transs && z < A.bottom[il] && z >= (A.bottom[il] - A.trans[il])) {
-          aeroi = il;
-          aerofac = fabs(A.bottom[il] - A.trans[il] - z) / A.trans[il];
-        }
-      }
-    }
-    rec[REC_AF] = aerofac;
-    rec[REC_AI] = (double)aeroi;
+  __syncwarp();  // the points written above, for every lane
+  const double *go = A.geo + base * 4;
+  double carry[3] = {0, 0, 0};  // position of the point before the chunk
+  for (int i0 = 0; i0 < o; i0 += 32) {
+    const int i = i0 + lane;
+    double xc[3] = {0, 0, 0}, xp[3], xn[3];
+    if (i < o) jsc_geo2cart(go[(size_t)i * 4], go[(size_t)i * 4 + 1], go[(size_t)i * 4 + 2], xc);
     for (int c = 0; c < 3; c++) {
-      xp[c] = xc[c];
-      xc[c] = xn[c];
+      const double up = __shfl_up_sync(full, xc[c], 1);
+      const double dn = __shfl_down_sync(full, xc[c], 1);
+      xp[c] = lane == 0 ? carry[c] : up;
+      xn[c] = dn;
+      carry[c] = __shfl_sync(full, xc[c], 31);
     }
-    if (i + 2 < o) jsc_geo2cart(go[(size_t)(i + 2) * 4], go[(size_t)(i + 2) * 4 + 1],
-                                go[(size_t)(i + 2) * 4 + 2], xn);
+    if (lane == 31 && i + 1 < o)
+      jsc_geo2cart(go[(size_t)(i + 1) * 4], go[(size_t)(i + 1) * 4 + 1],
+                   go[(size_t)(i + 1) * 4 + 2], xn);
+    if (i < o) refine_point(A, base, o, i, xp, xc, xn);
   }
+}
+
+// COUNT pass of the layer-edge refinement (add_aerosol_layers,
+// src/lineofsight.c:193-372): the number of refined LOS points of each ray,
+// the raw points plus the points where a segment crosses a layer edge or a
+// transition-layer level; refine_store_kernel writes them.
+static __global__ void __launch_bounds__(128) refine_count_kernel(RefineArgs A) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.n_rays) return;
+  const int nb = A.nlos_b[r];
+  if (nb == 0) {
+    A.nlos[r] = 0;
+    return;
+  }
+  const double *gb = A.geo_b + A.off_b[r] * 4;
+  int o = 1;
+  for (int ip = 1; ip < nb; ip++) {
+    const double zp = gb[(size_t)(ip - 1) * 4], zc = gb[(size_t)ip * 4];
+    if ((zp < A.altimax || zc < A.altimax) && (zp > A.altimin || zc > A.altimin))
+      for (int il = 0; il < A.n_alti; il++) {
+        const double z1 = A.alti[il], z2 = A.alti[A.n_alti - il - 1];
+        o += (zp > z1 && zc < z1) + (zp < z2 && zc > z2);
+      }
+    o++;
+  }
+  if (o > NLOS || o > A.max_seg) {
+    atomicOr(A.status, JSC_DEV_ERR_NLOS);
+    A.nlos[r] = 0;
+    return;
+  }
+  A.nlos[r] = o;
 }
 
 // Exclusive scan of nlos into off[0..n] by one block.
