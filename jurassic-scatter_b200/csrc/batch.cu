@@ -638,7 +638,8 @@ static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int6
 
   jsc_batch *c = b->child, *sc = b->sun_child;
   const size_t shmem = ((size_t)JSC_NTH_SCA * nd + (size_t)na * nd + 4 * JSC_NTH_SCA +
-                        (JSC_INT_THREADS / 32) * JSC_INT_CH) * sizeof(double);
+                        (JSC_INT_THREADS / 32) * JSC_INT_CH + (size_t)na * JSC_INT_CH) *
+                       sizeof(double);
   if (shmem > 48 * 1024)
     JSC_CUDA_TRY(cudaFuncSetAttribute(sp_integral_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));

@@ -197,6 +197,7 @@ sp_integral_kernel(IntegralArgs A) {
   double *rd = wt + (size_t)JSC_NTH_SCA * nd;        // [na][nd]
   double *trig = rd + (size_t)na * nd;               // sin/cos of theta2 and phi
   double *red = trig + 4 * JSC_NTH_SCA;              // [JSC_INT_THREADS / 32][JSC_INT_CH]
+  double *slp = red + (JSC_INT_THREADS / 32) * JSC_INT_CH;  // [na - 1][JSC_INT_CH]
   const double *o = A.sp + (size_t)k * JSC_SP_REC;
   const int il = (int)o[SP_IL];
   for (int i = threadIdx.x; i < JSC_NTH_SCA; i += blockDim.x) {
@@ -240,6 +241,15 @@ sp_integral_kernel(IntegralArgs A) {
   const int ndir = JSC_NTH_SCA * JSC_NPHI_SCA;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int c0 = 0; c0 < nd; c0 += JSC_INT_CH) {
+    // slopes (r1 - r0) / (a1 - a0) of the pass's channels per alpha
+    // interval, the quotient jsc_lin evaluates first
+    for (int i = threadIdx.x; i < (na - 1) * JSC_INT_CH; i += blockDim.x) {
+      const int lo = i / JSC_INT_CH, c = i - lo * JSC_INT_CH;
+      if (c0 + c < nd)
+        slp[i] = (rd[(size_t)(lo + 1) * nd + c0 + c] - rd[(size_t)lo * nd + c0 + c]) /
+                 (A.alpha[lo + 1] - A.alpha[lo]);
+    }
+    __syncthreads();
     double acc[JSC_INT_CH];
 #pragma unroll
     for (int c = 0; c < JSC_INT_CH; c++) acc[c] = 0;
@@ -256,12 +266,12 @@ sp_integral_kernel(IntegralArgs A) {
         const int mid = (hi + lo) >> 1;
         if (A.alpha[mid] > alpha2) hi = mid; else lo = mid;
       }
-      const double a0 = A.alpha[lo], a1 = A.alpha[lo + 1];
+      const double da = alpha2 - A.alpha[lo];
       const double *w = wt + (size_t)it * nd + c0;
-      const double *r0 = rd + (size_t)lo * nd + c0, *r1 = r0 + nd;
+      const double *r0 = rd + (size_t)lo * nd + c0, *s0 = slp + lo * JSC_INT_CH;
 #pragma unroll
       for (int c = 0; c < JSC_INT_CH; c++)
-        if (c0 + c < nd) acc[c] += w[c] * jsc_lin(a0, r0[c], a1, r1[c], alpha2);
+        if (c0 + c < nd) acc[c] += w[c] * (r0[c] + s0[c] * da);  // jsc_lin, slope precomputed
     }
     // block reduction per channel
 #pragma unroll
