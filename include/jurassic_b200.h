@@ -202,8 +202,57 @@ void jsc_set_exit_on_error(int on);
 /* Message describing the last error on this thread. */
 const char *jsc_last_error_message(void);
 
-/* Release the model and batch that formod() caches between calls. */
+/* Release the model and batches that formod() and jsc_kernel() cache
+ * between calls. */
 void jsc_release_cache(void);
+
+/* ------------------------------------------------------------------------
+ * Jacobians (the retrieval's caller of the forward model).
+ * ------------------------------------------------------------------------ */
+
+/* Quantity codes of state-vector elements (IDXP..IDXSS, src/jurassic.h:
+ * 203-221). */
+#define JSC_IDXP 0
+#define JSC_IDXT 1
+#define JSC_IDXQ(ig) (2 + (ig))
+#define JSC_IDXK(ctl, iw) (2 + (ctl)->ng + (iw))
+#define JSC_IDXNN(ctl) (2 + (ctl)->ng + (ctl)->nw + 1)
+#define JSC_IDXRR(ctl) (2 + (ctl)->ng + (ctl)->nw + 2)
+#define JSC_IDXSS(ctl) (2 + (ctl)->ng + (ctl)->nw + 3)
+
+/* State vector of atm and aero (atm2x, src/atmosphere.c:5-97): pressure,
+ * temperature, volume mixing ratios and extinction at the levels inside
+ * each quantity's ctl->ret*_zmin..zmax, then the aerosol parameters
+ * selected by ctl->retnn/retrr/retss.  x, iqa (quantity codes) and ipa
+ * (level, -1 for aerosol parameters) may be NULL.  Returns the length. */
+size_t jsc_atm2x(const ctl_t *ctl, const atm_t *atm, const aero_t *aero, double *x,
+                 int *iqa, int *ipa);
+
+/* Inverse of jsc_atm2x (x2atm, src/retrievalmodel.c:1103-1163). */
+void jsc_x2atm(const ctl_t *ctl, const double *x, atm_t *atm, aero_t *aero);
+
+/* Measurement vector: the finite entries of obs->rad, ray-major
+ * (obs2y, src/retrievalmodel.c:379-403).  y, ida, ira may be NULL.
+ * Returns the length. */
+size_t jsc_obs2y(const ctl_t *ctl, const obs_t *obs, double *y, int *ida, int *ira);
+
+/* Replaces kernel (src/retrievalmodel.c:201-298): the Jacobian
+ * k[i * tda + j] = (y_j[i] - y[i]) / h_j of the measurement vector with
+ * respect to the state vector, by finite differences with the reference's
+ * perturbation sizes h_j (1 % of p and VMR with floors 1e-7 and 1e-15,
+ * 1 K, 1e-4 km^-1 for extinction).  The undisturbed forward model and all
+ * n disturbed ones run as ONE batch on the GPU (n + 1 profiles, each traced
+ * by every ray of obs) instead of n + 1 calls.  Like the reference, it
+ * first does formod(ctl, atm, obs, aero) on the caller's data (hydrostatic
+ * balance in atm->p, radiances in obs), and each disturbed profile gets
+ * its own hydrostatic balance.  m, n: the matrix size, which must equal
+ * jsc_obs2y's count after that forward model and jsc_atm2x's length (a
+ * gsl_matrix maps as k->data, k->size1, k->size2, k->tda).  Aerosol
+ * parameters in the state vector (retnn/retrr/retss) return
+ * JSC_ERR_UNSUPPORTED: every column would need its own optical
+ * properties. */
+int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size_t m,
+               size_t n, size_t tda);
 
 /* Number of CUDA kernels this library has launched since load. */
 uint64_t jsc_launch_count(void);

@@ -24,6 +24,9 @@ static pthread_mutex_t g_lock = PTHREAD_MUTEX_INITIALIZER;
 static jsc_model *g_model;
 static jsc_batch *g_batch;
 static ctl_t *g_key;          /* ctl the cache was built for */
+/* Batch of jsc_kernel (undisturbed + disturbed profiles) and its capacity. */
+static jsc_batch *g_jbatch;
+static int g_jcap_atm, g_jcap_lev, g_jcap_rays;
 
 void jsc_set_exit_on_error(int on) { g_exit_on_error = on; }
 int jsc_last_status(void) { return g_last_status; }
@@ -63,13 +66,17 @@ static int ensure_cache(const ctl_t *ctl) {
   int st;
   if (g_key && !same_tables(g_key, ctl)) {
     jsc_batch_destroy(g_batch);
+    jsc_batch_destroy(g_jbatch);
     jsc_model_destroy(g_model);
     g_batch = NULL;
+    g_jbatch = NULL;
     g_model = NULL;
   }
-  if (g_batch && g_key && !same_switches(g_key, ctl)) {
+  if (g_key && !same_switches(g_key, ctl)) {
     jsc_batch_destroy(g_batch);
+    jsc_batch_destroy(g_jbatch);
     g_batch = NULL;
+    g_jbatch = NULL;
   }
   if (!g_key) {
     g_key = (ctl_t *)malloc(sizeof(ctl_t));
@@ -219,14 +226,349 @@ void formod(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
   }
 }
 
-/* Release the cached model and batch (tests and long-running hosts). */
+/* Release the cached model and batches (tests and long-running hosts). */
 void jsc_release_cache(void) {
   pthread_mutex_lock(&g_lock);
   jsc_batch_destroy(g_batch);
+  jsc_batch_destroy(g_jbatch);
   jsc_model_destroy(g_model);
   g_batch = NULL;
+  g_jbatch = NULL;
   g_model = NULL;
   free(g_key);
   g_key = NULL;
   pthread_mutex_unlock(&g_lock);
+}
+
+/* ---------------------------------------------------------------- kernel -- */
+
+/* Elements of one quantity at the levels inside [zmin, zmax]
+ * (atm2x_help, src/atmosphere.c:72-97). */
+static void atm2x_help(const atm_t *atm, double zmin, double zmax, const double *value,
+                       int idx, double *x, int *iqa, int *ipa, size_t *n) {
+  for (int ip = 0; ip < atm->np; ip++)
+    if (atm->z[ip] >= zmin && atm->z[ip] <= zmax) {
+      if (x) x[*n] = value[ip];
+      if (iqa) iqa[*n] = idx;
+      if (ipa) ipa[*n] = ip;
+      (*n)++;
+    }
+}
+
+static void atm2x_aero(double v, int idx, double *x, int *iqa, int *ipa, size_t *n) {
+  if (x) x[*n] = v;
+  if (iqa) iqa[*n] = idx;
+  if (ipa) ipa[*n] = -1;
+  (*n)++;
+}
+
+size_t jsc_atm2x(const ctl_t *ctl, const atm_t *atm, const aero_t *aero, double *x,
+                 int *iqa, int *ipa) {
+  size_t n = 0;
+  atm2x_help(atm, ctl->retp_zmin, ctl->retp_zmax, atm->p, JSC_IDXP, x, iqa, ipa, &n);
+  atm2x_help(atm, ctl->rett_zmin, ctl->rett_zmax, atm->t, JSC_IDXT, x, iqa, ipa, &n);
+  for (int ig = 0; ig < ctl->ng; ig++)
+    atm2x_help(atm, ctl->retq_zmin[ig], ctl->retq_zmax[ig], atm->q[ig], JSC_IDXQ(ig), x, iqa,
+               ipa, &n);
+  for (int iw = 0; iw < ctl->nw; iw++)
+    atm2x_help(atm, ctl->retk_zmin[iw], ctl->retk_zmax[iw], atm->k[iw], JSC_IDXK(ctl, iw), x,
+               iqa, ipa, &n);
+  if (ctl->retnn) atm2x_aero(aero ? aero->nn[0] : 0, JSC_IDXNN(ctl), x, iqa, ipa, &n);
+  if (ctl->retrr) atm2x_aero(aero ? aero->rr[0] : 0, JSC_IDXRR(ctl), x, iqa, ipa, &n);
+  if (ctl->retss) atm2x_aero(aero ? aero->ss[0] : 0, JSC_IDXSS(ctl), x, iqa, ipa, &n);
+  return n;
+}
+
+/* x2atm_help, src/retrievalmodel.c:1147-1163. */
+static void x2atm_help(atm_t *atm, double zmin, double zmax, double *value, const double *x,
+                       size_t *n) {
+  for (int ip = 0; ip < atm->np; ip++)
+    if (atm->z[ip] >= zmin && atm->z[ip] <= zmax) value[ip] = x[(*n)++];
+}
+
+void jsc_x2atm(const ctl_t *ctl, const double *x, atm_t *atm, aero_t *aero) {
+  size_t n = 0;
+  x2atm_help(atm, ctl->retp_zmin, ctl->retp_zmax, atm->p, x, &n);
+  x2atm_help(atm, ctl->rett_zmin, ctl->rett_zmax, atm->t, x, &n);
+  for (int ig = 0; ig < ctl->ng; ig++)
+    x2atm_help(atm, ctl->retq_zmin[ig], ctl->retq_zmax[ig], atm->q[ig], x, &n);
+  for (int iw = 0; iw < ctl->nw; iw++)
+    x2atm_help(atm, ctl->retk_zmin[iw], ctl->retk_zmax[iw], atm->k[iw], x, &n);
+  if (ctl->retnn) {
+    if (aero) aero->nn[0] = x[n];
+    n++;
+  }
+  if (ctl->retrr) {
+    if (aero) aero->rr[0] = x[n];
+    n++;
+  }
+  if (ctl->retss) {
+    if (aero) aero->ss[0] = x[n];
+    n++;
+  }
+}
+
+size_t jsc_obs2y(const ctl_t *ctl, const obs_t *obs, double *y, int *ida, int *ira) {
+  size_t m = 0;
+  for (int ir = 0; ir < obs->nr; ir++)
+    for (int id = 0; id < ctl->nd; id++)
+      if (isfinite(obs->rad[id][ir])) {
+        if (y) y[m] = obs->rad[id][ir];
+        if (ida) ida[m] = id;
+        if (ira) ira[m] = ir;
+        m++;
+      }
+  return m;
+}
+
+/* GSL_MAX as the reference evaluates it. */
+static double gmax(double a, double b) { return a > b ? a : b; }
+
+/* Perturbation size of a state-vector element of quantity iqa and value x
+ * (src/retrievalmodel.c:241-273); -999 where the reference has none. */
+static double perturbation(const ctl_t *ctl, int iqa, double x) {
+  double h = -999;
+  if (iqa == JSC_IDXP) h = gmax(fabs(0.01 * x), 1e-7);
+  if (iqa == JSC_IDXT) h = 1;
+  if (iqa >= JSC_IDXQ(0) && iqa < JSC_IDXQ(ctl->ng)) h = gmax(fabs(0.01 * x), 1e-15);
+  if (iqa >= JSC_IDXK(ctl, 0) && iqa < JSC_IDXK(ctl, ctl->nw)) h = 1e-4;
+  return h;
+}
+
+/* Pointer to the profile value a state-vector element of quantity iqa sets
+ * at level ip of a packed profile set (p, t, q [ng][nl], k [nw][nl]). */
+static double *element(const ctl_t *ctl, int iqa, int ip, double *p, double *t, double *q,
+                       double *k, size_t nl) {
+  if (iqa == JSC_IDXP) return p + ip;
+  if (iqa == JSC_IDXT) return t + ip;
+  if (iqa >= JSC_IDXQ(0) && iqa < JSC_IDXQ(ctl->ng)) return q + (size_t)(iqa - JSC_IDXQ(0)) * nl + ip;
+  return k + (size_t)(iqa - JSC_IDXK(ctl, 0)) * nl + ip;
+}
+
+/* Jacobian batch with room for natm profiles of np levels and nrays rays. */
+static int ensure_jbatch(const ctl_t *ctl, int natm, int nlev, int nrays) {
+  if (g_jbatch && natm <= g_jcap_atm && nlev <= g_jcap_lev && nrays <= g_jcap_rays)
+    return JSC_OK;
+  jsc_batch_destroy(g_jbatch);
+  g_jbatch = NULL;
+  ctl_t c2;
+  memcpy(&c2, ctl, sizeof(ctl_t));
+  c2.hydz = -999;  /* hydrostatic balance is applied per profile on the host */
+  int st = jsc_batch_create(g_model, &c2, natm, nlev, nrays, 0, &g_jbatch);
+  if (st) return st;
+  g_jcap_atm = natm;
+  g_jcap_lev = nlev;
+  g_jcap_rays = nrays;
+  return JSC_OK;
+}
+
+/* Radiance of ray ir, channel id of a batch output as formod leaves it in
+ * obs->rad (brightness temperature when ctl->write_bbt). */
+static double out_rad(const ctl_t *ctl, const double *rad, size_t ray, int id) {
+  const double v = rad[ray * ctl->nd + id];
+  return ctl->write_bbt ? brightness(v, ctl->nu[id]) : v;
+}
+
+int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size_t m,
+               size_t n, size_t tda) {
+  const int nd = ctl->nd, nr = obs->nr, np = atm->np, ng = ctl->ng, nw = ctl->nw;
+  if (nd < 1 || nd > NDMAX || ng < 0 || ng > NGMAX || nw < 0 || nw > NWMAX ||
+      nr < 0 || nr > NRMAX || np < 2 || np > NPMAX) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: invalid sizes (nd=%d ng=%d nw=%d nr=%d np=%d)",
+                  nd, ng, nw, nr, np);
+    return JSC_ERR_ARG;
+  }
+  if (ctl->fov[0] != '-') {
+    jsc_set_error(JSC_ERR_UNSUPPORTED, "field-of-view convolution (FOV=%s)", ctl->fov);
+    return JSC_ERR_UNSUPPORTED;
+  }
+  if (ctl->retnn || ctl->retrr || ctl->retss) {
+    jsc_set_error(JSC_ERR_UNSUPPORTED,
+                  "jsc_kernel: aerosol parameters in the state vector (RETNN/RETRR/RETSS)");
+    return JSC_ERR_UNSUPPORTED;
+  }
+  if (ctl->sca_n > 0 && !aero) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: SCA_N=%d needs the aerosol/cloud data", ctl->sca_n);
+    return JSC_ERR_ARG;
+  }
+  if ((m > 0 && n > 0 && !k) || tda < n) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: no matrix, or row stride %zu below %zu columns",
+                  tda, n);
+    return JSC_ERR_ARG;
+  }
+
+  /* Hydrostatic balance on the caller's atmosphere, as formod does. */
+  const int ig_h2o = jsc_find_emitter(ctl, "H2O");
+  jsc_hydrostatic(ctl->hydz, np, atm->z, atm->lon, atm->lat, atm->t,
+                  ig_h2o >= 0 ? atm->q[ig_h2o] : NULL, atm->p);
+  const size_t n0 = jsc_atm2x(ctl, atm, aero, NULL, NULL, NULL);
+  if (n0 != n) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: the state vector has %zu elements, k %zu columns",
+                  n0, n);
+    return JSC_ERR_ARG;
+  }
+  const size_t natm = n + 1, nl = natm * (size_t)np, nrays = natm * (size_t)nr;
+  if (nl > 0x7fffffff || nrays > 0x7fffffff) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: %zu profiles x %d rays exceed the batch limits",
+                  natm, nr);
+    return JSC_ERR_ARG;
+  }
+
+  int st = JSC_OK;
+  double *x0 = (double *)malloc((n + 1) * sizeof(double));
+  double *h = (double *)malloc((n + 1) * sizeof(double));
+  int *iqa = (int *)malloc((n + 1) * sizeof(int)), *ipa = (int *)malloc((n + 1) * sizeof(int));
+  unsigned char *mask = (unsigned char *)malloc((size_t)nd * (nr > 0 ? nr : 1));
+  /* packed profiles: z lon lat p t [nl], q [ng][nl], k [nw][nl] */
+  double *prof = (double *)malloc(nl * (5 + (size_t)ng + nw) * sizeof(double));
+  int *atm_off = (int *)malloc((natm + 1) * sizeof(int));
+  /* rays: time obsz obslon obslat vpz vplon vplat [nrays]; outputs */
+  double *rays = (double *)malloc(nrays * 7 * sizeof(double) + 1);
+  int *ray_atm = (int *)malloc(nrays * sizeof(int) + 1);
+  double *res = (double *)malloc((nrays * (2 * (size_t)nd + 3) + 2 * m + 1) * sizeof(double));
+  if (!x0 || !h || !iqa || !ipa || !mask || !prof || !atm_off || !rays || !ray_atm || !res) {
+    st = JSC_ERR_NOMEM;
+    goto done;
+  }
+  for (int id = 0; id < nd; id++)
+    for (int ir = 0; ir < nr; ir++) mask[(size_t)id * nr + ir] = !isfinite(obs->rad[id][ir]);
+  jsc_atm2x(ctl, atm, aero, x0, iqa, ipa);
+  for (size_t j = 0; j < n; j++) {
+    h[j] = perturbation(ctl, iqa[j], x0[j]);
+    if (h[j] <= 0) {
+      jsc_set_error(JSC_ERR_ARG, "jsc_kernel: cannot set perturbation size");
+      st = JSC_ERR_ARG;
+      goto done;
+    }
+  }
+
+  {
+    double *z = prof, *lon = z + nl, *lat = lon + nl, *p = lat + nl, *t = p + nl;
+    double *q = t + nl, *kx = q + (size_t)ng * nl;
+    for (size_t a = 0; a < natm; a++) {
+      const size_t o = a * np;
+      atm_off[a] = (int)o;
+      memcpy(z + o, atm->z, np * sizeof(double));
+      memcpy(lon + o, atm->lon, np * sizeof(double));
+      memcpy(lat + o, atm->lat, np * sizeof(double));
+      memcpy(p + o, atm->p, np * sizeof(double));
+      memcpy(t + o, atm->t, np * sizeof(double));
+      for (int ig = 0; ig < ng; ig++) memcpy(q + (size_t)ig * nl + o, atm->q[ig], np * sizeof(double));
+      for (int iw = 0; iw < nw; iw++) memcpy(kx + (size_t)iw * nl + o, atm->k[iw], np * sizeof(double));
+      if (a == 0) continue;
+      /* disturbed profile a: element a-1 of the state vector + h, then the
+       * hydrostatic balance formod applies to it */
+      const size_t j = a - 1;
+      *element(ctl, iqa[j], ipa[j], p + o, t + o, q + o, kx + o, nl) = x0[j] + h[j];
+      jsc_hydrostatic(ctl->hydz, np, z + o, lon + o, lat + o, t + o,
+                      ig_h2o >= 0 ? q + (size_t)ig_h2o * nl + o : NULL, p + o);
+    }
+    atm_off[natm] = (int)nl;
+    for (size_t a = 0; a < natm; a++)
+      for (int ir = 0; ir < nr; ir++) {
+        const size_t r = a * nr + ir;
+        ray_atm[r] = (int)a;
+        rays[r] = obs->time[ir];
+        rays[nrays + r] = obs->obsz[ir];
+        rays[2 * nrays + r] = obs->obslon[ir];
+        rays[3 * nrays + r] = obs->obslat[ir];
+        rays[4 * nrays + r] = obs->vpz[ir];
+        rays[5 * nrays + r] = obs->vplon[ir];
+        rays[6 * nrays + r] = obs->vplat[ir];
+      }
+    jsc_batch_input in;
+    memset(&in, 0, sizeof(in));
+    in.n_atm = (int)natm;
+    in.n_levels = (int)nl;
+    in.atm_off = atm_off;
+    in.z = z;
+    in.lon = lon;
+    in.lat = lat;
+    in.p = p;
+    in.t = t;
+    in.q = q;
+    in.k = kx;
+    in.n_rays = (int)nrays;
+    in.ray_atm = ray_atm;
+    in.time = rays;
+    in.obsz = rays + nrays;
+    in.obslon = rays + 2 * nrays;
+    in.obslat = rays + 3 * nrays;
+    in.vpz = rays + 4 * nrays;
+    in.vplon = rays + 5 * nrays;
+    in.vplat = rays + 6 * nrays;
+    double *rad = res, *tau = rad + nrays * nd, *tp = tau + nrays * nd;
+    jsc_batch_output out;
+    memset(&out, 0, sizeof(out));
+    out.rad = rad;
+    out.tau = tau;
+    out.tpz = tp;
+    out.tplon = tp + nrays;
+    out.tplat = tp + 2 * nrays;
+    if (nr > 0) {
+      pthread_mutex_lock(&g_lock);
+      st = ensure_cache(ctl);
+      if (!st) st = ensure_jbatch(ctl, (int)natm, (int)nl, (int)nrays);
+      if (!st && ctl->sca_n > 0) st = jsc_batch_set_aero(g_jbatch, aero);
+      if (!st) st = jsc_batch_upload(g_jbatch, &in, NULL);
+      if (!st) st = jsc_batch_run(g_jbatch, NULL);
+      if (!st) st = jsc_batch_download(g_jbatch, &out, NULL);
+      pthread_mutex_unlock(&g_lock);
+    }
+    if (st) goto done;
+
+    /* The undisturbed forward model into obs (formod's outputs). */
+    for (int ir = 0; ir < nr; ir++) {
+      obs->tpz[ir] = tp[ir];
+      obs->tplon[ir] = tp[nrays + ir];
+      obs->tplat[ir] = tp[2 * nrays + ir];
+      for (int id = 0; id < nd; id++) {
+        obs->rad[id][ir] = mask[(size_t)id * nr + ir] ? NAN : out_rad(ctl, rad, ir, id);
+        obs->tau[id][ir] = tau[(size_t)ir * nd + id];
+      }
+    }
+    double *y0 = tp + 3 * nrays, *y1 = y0 + m;
+    const size_t m0 = jsc_obs2y(ctl, obs, NULL, NULL, NULL);
+    if (m0 != m) {
+      jsc_set_error(JSC_ERR_ARG, "jsc_kernel: %zu finite radiances, k has %zu rows", m0, m);
+      st = JSC_ERR_ARG;
+      goto done;
+    }
+    jsc_obs2y(ctl, obs, y0, NULL, NULL);
+    /* Disturbed columns: the measurement vector of each disturbed forward
+     * model (obs2y of a copy of obs, whose non-finite entries stay masked). */
+    for (size_t j = 0; j < n; j++) {
+      const size_t r0 = (j + 1) * nr;
+      size_t c = 0;
+      for (int ir = 0; ir < nr; ir++)
+        for (int id = 0; id < nd; id++) {
+          if (!isfinite(obs->rad[id][ir])) continue;
+          const double v = out_rad(ctl, rad, r0 + ir, id);
+          if (!isfinite(v)) continue;
+          if (c < m) y1[c] = v;
+          c++;
+        }
+      if (c != m) {
+        jsc_set_error(JSC_ERR_ARG,
+                      "jsc_kernel: disturbed forward model %zu has %zu finite radiances, "
+                      "the undisturbed one %zu", j, c, m);
+        st = JSC_ERR_ARG;
+        goto done;
+      }
+      for (size_t i = 0; i < m; i++) k[i * tda + j] = (y1[i] - y0[i]) / h[j];
+    }
+  }
+
+done:
+  free(x0);
+  free(h);
+  free(iqa);
+  free(ipa);
+  free(mask);
+  free(prof);
+  free(atm_off);
+  free(rays);
+  free(ray_atm);
+  free(res);
+  return st;
 }

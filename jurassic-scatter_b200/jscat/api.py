@@ -35,6 +35,54 @@ def formod(ctl, atm, obs, aero=None, exit_on_error=False):
     L.check(lib.jsc_last_status(), "formod")
 
 
+def atm2x(ctl, atm, aero=None):
+    """State vector, quantity codes and levels (jsc_atm2x)."""
+    lib = L.load()
+    aero = S.AeroT() if aero is None else aero
+    n = lib.jsc_atm2x(C.byref(ctl), C.byref(atm), C.byref(aero), None, None, None)
+    x = np.zeros(n)
+    iqa = np.zeros(n, np.int32)
+    ipa = np.zeros(n, np.int32)
+    if n:
+        lib.jsc_atm2x(C.byref(ctl), C.byref(atm), C.byref(aero), _dptr(x), _iptr(iqa),
+                      _iptr(ipa))
+    return x, iqa, ipa
+
+
+def x2atm(ctl, x, atm, aero=None):
+    """Write a state vector back into atm (and aero) (jsc_x2atm)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    L.load().jsc_x2atm(C.byref(ctl), _dptr(x), C.byref(atm),
+                       C.byref(S.AeroT() if aero is None else aero))
+
+
+def obs2y(ctl, obs):
+    """Measurement vector and its channel and ray indices (jsc_obs2y)."""
+    lib = L.load()
+    m = lib.jsc_obs2y(C.byref(ctl), C.byref(obs), None, None, None)
+    y = np.zeros(m)
+    ida = np.zeros(m, np.int32)
+    ira = np.zeros(m, np.int32)
+    if m:
+        lib.jsc_obs2y(C.byref(ctl), C.byref(obs), _dptr(y), _iptr(ida), _iptr(ira))
+    return y, ida, ira
+
+
+def kernel(ctl, atm, obs, aero=None):
+    """Jacobian [m][n] of the measurement vector by finite differences,
+    undisturbed and disturbed forward models in one GPU batch (jsc_kernel,
+    the reference's kernel()).  Like the reference it also leaves formod's
+    results in atm (hydrostatic pressure) and obs (radiances)."""
+    lib = L.load()
+    aero = S.AeroT() if aero is None else aero
+    m = lib.jsc_obs2y(C.byref(ctl), C.byref(obs), None, None, None)
+    n = lib.jsc_atm2x(C.byref(ctl), C.byref(atm), C.byref(aero), None, None, None)
+    k = np.zeros((m, n))
+    L.check(lib.jsc_kernel(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero),
+                           _dptr(k) if k.size else None, m, n, n), "jsc_kernel")
+    return k
+
+
 def brightness(rad, nu):
     return L.load().brightness(float(rad), float(nu))
 

@@ -26,6 +26,7 @@ EXPORTS = [
     "jsc_batch_scatter_samples", "jsc_batch_set_surrogate", "jsc_batch_surrogate_stats",
     "jsc_batch_set_fixed", "jsc_batch_download_async", "jsc_batch_async_status",
     "jsc_batch_graph_capture", "jsc_batch_graph_launch", "jsc_surrogate_set_tensor_path",
+    "jsc_atm2x", "jsc_x2atm", "jsc_obs2y", "jsc_kernel",
 ]
 
 
@@ -78,6 +79,11 @@ def load():
         "jsc_status_string": (C.c_char_p, [i]),
         "jsc_last_status": (i, []),
         "jsc_set_exit_on_error": (None, [i]),
+        "jsc_atm2x": (C.c_size_t, [P(S.CtlT), P(S.AtmT), P(S.AeroT), vp, vp, vp]),
+        "jsc_x2atm": (None, [P(S.CtlT), vp, P(S.AtmT), P(S.AeroT)]),
+        "jsc_obs2y": (C.c_size_t, [P(S.CtlT), P(S.ObsT), vp, vp, vp]),
+        "jsc_kernel": (i, [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT), vp, C.c_size_t,
+                           C.c_size_t, C.c_size_t]),
         "jsc_last_error_message": (C.c_char_p, []),
         "jsc_release_cache": (None, []),
         "jsc_launch_count": (C.c_uint64, []),

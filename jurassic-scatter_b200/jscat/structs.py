@@ -174,6 +174,9 @@ def make_ctl(emitters, nus, tblbase, **kw):
         elif k == "window":
             for i, w in enumerate(v):
                 ctl.window[i] = int(w)
+        elif k in ("retq_zmin", "retq_zmax", "retk_zmin", "retk_zmax"):
+            for i, w in enumerate(v):
+                getattr(ctl, k)[i] = float(w)
         else:
             setattr(ctl, k, v)
     return ctl

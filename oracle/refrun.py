@@ -151,6 +151,138 @@ def _child(job):
     return out
 
 
+REF_RET_LIB = os.path.join(HERE, "_ref", "libjurassic_ref_ret.so")
+
+
+class GslMatrix(C.Structure):
+    """gsl_matrix of the bundled GSL 1.15 (gsl/gsl_matrix_double.h)."""
+    _fields_ = [("size1", C.c_size_t), ("size2", C.c_size_t), ("tda", C.c_size_t),
+                ("data", C.POINTER(C.c_double)), ("block", C.c_void_p), ("owner", C.c_int)]
+
+
+class GslVector(C.Structure):
+    """gsl_vector of the bundled GSL 1.15 (gsl/gsl_vector_double.h)."""
+    _fields_ = [("size", C.c_size_t), ("stride", C.c_size_t),
+                ("data", C.POINTER(C.c_double)), ("block", C.c_void_p), ("owner", C.c_int)]
+
+
+def kernel_available():
+    return os.path.exists(REF_RET_LIB)
+
+
+def _kernel_child(job):
+    """The reference's kernel() (src/retrievalmodel.c:201-298) on one
+    profile and the rays of geom; obs->rad starts at 0 with NaN where
+    job["mask"] is set.  Also returns the state vector (atm2x after the
+    call, i.e. with the hydrostatic pressures), its quantity and level
+    indices, and the undisturbed radiances kernel() leaves in obs."""
+    _silence()
+    lib = C.CDLL(REF_RET_LIB)
+    P = C.POINTER
+    lib.gsl_matrix_alloc.restype = P(GslMatrix)
+    lib.gsl_matrix_alloc.argtypes = [C.c_size_t, C.c_size_t]
+    lib.gsl_vector_alloc.restype = P(GslVector)
+    lib.gsl_vector_alloc.argtypes = [C.c_size_t]
+    lib.atm2x.restype = C.c_size_t
+    lib.atm2x.argtypes = [P(S.CtlT), P(S.AtmT), P(S.AeroT), C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.obs2y.restype = C.c_size_t
+    lib.obs2y.argtypes = [P(S.CtlT), P(S.ObsT), C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.kernel.restype = None
+    lib.kernel.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT), P(GslMatrix)]
+    ctl = S.make_ctl(**job["ctl"])
+    atm = _atm_struct(job["atm"])
+    g = job["geom"]
+    obs = S.make_obs(g["obsz"], g["obslat"], g["vpz"], g["vplat"], g["obslon"], g["vplon"],
+                     g["time"])
+    nr, nd = obs.nr, ctl.nd
+    rad = S.arr(obs.rad)
+    mask = job.get("mask")
+    if mask is not None:
+        for ir in range(nr):
+            for id_ in range(nd):
+                if mask[ir][id_]:
+                    rad[id_, ir] = np.nan
+    aero = S.AeroT()
+    m = lib.obs2y(C.byref(ctl), C.byref(obs), None, None, None)
+    n = lib.atm2x(C.byref(ctl), C.byref(atm), C.byref(aero), None, None, None)
+    k = lib.gsl_matrix_alloc(m, n)
+    t0 = time.perf_counter()
+    lib.kernel(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero), k)
+    seconds = time.perf_counter() - t0
+    km = k.contents
+    K = np.ctypeslib.as_array(km.data, shape=(m * km.tda,)).reshape(m, km.tda)[:, :n].copy()
+    x = lib.gsl_vector_alloc(n)
+    iqa = (C.c_int * max(n, 1))()
+    ipa = (C.c_int * max(n, 1))()
+    lib.atm2x(C.byref(ctl), C.byref(atm), C.byref(aero), x, iqa, ipa)
+    xv = x.contents
+    x0 = np.array([xv.data[i * xv.stride] for i in range(n)])
+    return {"k": K, "x0": x0, "iqa": np.array(iqa[:n]), "ipa": np.array(ipa[:n]),
+            "rad": S.arr(obs.rad)[:nd, :nr].T.copy(), "p": S.arr(atm.p)[:atm.np].copy(),
+            "seconds": seconds}
+
+
+def _state_vector_child(job):
+    """The reference's atm2x, x2atm and obs2y (src/atmosphere.c:5-97,
+    src/retrievalmodel.c:379-403,1103-1163) on one profile: the state
+    vector, then x2atm of x * scale + shift, then the measurement vector of
+    an obs_t whose radiances are job["rad"] ([nr][nd], NaN = masked)."""
+    _silence()
+    lib = C.CDLL(REF_RET_LIB)
+    P = C.POINTER
+    lib.gsl_vector_alloc.restype = P(GslVector)
+    lib.gsl_vector_alloc.argtypes = [C.c_size_t]
+    lib.atm2x.restype = C.c_size_t
+    lib.atm2x.argtypes = [P(S.CtlT), P(S.AtmT), P(S.AeroT), C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.x2atm.restype = None
+    lib.x2atm.argtypes = [P(S.CtlT), P(GslVector), P(S.AtmT), P(S.AeroT)]
+    lib.obs2y.restype = C.c_size_t
+    lib.obs2y.argtypes = [P(S.CtlT), P(S.ObsT), C.c_void_p, C.c_void_p, C.c_void_p]
+    ctl = S.make_ctl(**job["ctl"])
+    atm = _atm_struct(job["atm"])
+    aero = S.AeroT()
+    n = lib.atm2x(C.byref(ctl), C.byref(atm), C.byref(aero), None, None, None)
+    x = lib.gsl_vector_alloc(max(n, 1))
+    iqa = (C.c_int * max(n, 1))()
+    ipa = (C.c_int * max(n, 1))()
+    lib.atm2x(C.byref(ctl), C.byref(atm), C.byref(aero), x, iqa, ipa)
+    xv = x.contents
+    x0 = np.array([xv.data[i * xv.stride] for i in range(n)])
+    for i in range(n):
+        xv.data[i * xv.stride] = x0[i] * job["scale"] + job["shift"]
+    lib.x2atm(C.byref(ctl), x, C.byref(atm), C.byref(aero))
+    na = atm.np
+    out = {"x0": x0, "iqa": np.array(iqa[:n]), "ipa": np.array(ipa[:n]),
+           "p": S.arr(atm.p)[:na].copy(), "t": S.arr(atm.t)[:na].copy(),
+           "q": S.arr(atm.q)[:ctl.ng, :na].copy(), "k": S.arr(atm.k)[:ctl.nw, :na].copy()}
+    rad = np.asarray(job["rad"])
+    obs = S.ObsT()
+    obs.nr = rad.shape[0]
+    S.arr(obs.rad)[:ctl.nd, :obs.nr] = rad.T
+    m = lib.obs2y(C.byref(ctl), C.byref(obs), None, None, None)
+    y = lib.gsl_vector_alloc(max(m, 1))
+    ida = (C.c_int * max(m, 1))()
+    ira = (C.c_int * max(m, 1))()
+    lib.obs2y(C.byref(ctl), C.byref(obs), y, ida, ira)
+    yv = y.contents
+    out.update(y=np.array([yv.data[i * yv.stride] for i in range(m)]),
+               ida=np.array(ida[:m]), ira=np.array(ira[:m]))
+    return out
+
+
+def reference_state_vector(ctl_kw, atm, rad, scale=1.0, shift=0.0, timeout=600):
+    """atm2x / x2atm / obs2y of the reference (see _state_vector_child)."""
+    return _spawn({"sv_job": True, "ctl": ctl_kw, "atm": atm, "rad": np.asarray(rad),
+                   "scale": scale, "shift": shift}, timeout)
+
+
+def reference_kernel(ctl_kw, atm, geom, mask=None, timeout=3600):
+    """Jacobian of the reference's kernel() for one profile (dict) and the
+    rays of geom; mask [n_rays][nd] marks observations set to NaN."""
+    return _spawn({"kernel_job": True, "ctl": ctl_kw, "atm": atm, "geom": geom,
+                   "mask": None if mask is None else np.asarray(mask, bool)}, timeout)
+
+
 PORT_LIB = os.path.join(HERE, "build", "libjscat_oracle.so")
 
 
@@ -229,6 +361,10 @@ if __name__ == "__main__":
         _job = pickle.load(f)
     if _job.get("aero_job"):
         _out = _aero_child(_job)
+    elif _job.get("kernel_job"):
+        _out = _kernel_child(_job)
+    elif _job.get("sv_job"):
+        _out = _state_vector_child(_job)
     else:
         if _job.get("aero") is not None:
             _job["aero"] = S.AeroT.from_buffer_copy(_job["aero"])

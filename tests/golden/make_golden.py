@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [jacobian]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -122,8 +122,48 @@ def aero_fixture(workdir, name, layer_files, nus):
                         aero=np.frombuffer(aero, dtype=np.uint8))
 
 
+# Retrieval settings of the Jacobian fixtures: temperature, both VMRs and
+# the window extinction over parts of the profile, and pressure at levels
+# whose disturbance the hydrostatic balance of the disturbed forward model
+# undoes (zero columns, as in the reference).
+JACOBIAN_RET = dict(rett_zmin=5.0, rett_zmax=40.0, retq_zmin=[20.0, 5.0], retq_zmax=[30.0, 25.0],
+                    retk_zmin=[10.0], retk_zmax=[15.0], retp_zmin=30.0, retp_zmax=35.0)
+
+
+def jacobian_case(workdir, bt=False):
+    """The clear limb case with the retrieval settings above (radiances,
+    two observations masked and one ray fully masked), or with brightness
+    temperatures, temperature only and every fourth ray (bt=True)."""
+    ctlkw, atm, geom = synth.clear_limb_case(workdir)
+    if bt:
+        ctlkw = dict(ctlkw, write_bbt=1, rett_zmin=10.0, rett_zmax=30.0)
+        geom = {k: v[::4] for k, v in geom.items()}
+        mask = np.zeros((len(geom["obsz"]), len(ctlkw["nus"])), bool)
+    else:
+        ctlkw = dict(ctlkw, **JACOBIAN_RET)
+        mask = np.zeros((len(geom["obsz"]), len(ctlkw["nus"])), bool)
+        mask[3, 1] = mask[40, 2] = True
+        mask[10, :] = True
+    return ctlkw, atm, geom, mask
+
+
+def jacobian_fixture(workdir, name, bt):
+    """Jacobian of the reference's own kernel() (oracle/_ref/libjurassic_ref_ret.so)."""
+    ctlkw, atm, geom, mask = jacobian_case(workdir, bt)
+    ref = refrun.reference_kernel(reference_ctl(ctlkw), atm, geom, mask=mask)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"), k=ref["k"], x0=ref["x0"], iqa=ref["iqa"],
+        ipa=ref["ipa"], rad=ref["rad"], p=ref["p"], mask=mask,
+        table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
+        **{"geom_" + k: v for k, v in geom.items()})
+
+
 def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
+    if sys.argv[1:] == ["jacobian"]:
+        jacobian_fixture(workdir, "jacobian_limb", False)
+        jacobian_fixture(workdir, "jacobian_limb_bt", True)
+        return
     ctlkw, atm, geom = synth.clear_limb_case(workdir)
     ra = np.zeros(len(geom["obsz"]), int)
     ref = refrun.run(reference_ctl(ctlkw), [atm], ra, geom, los=True)
@@ -153,6 +193,8 @@ def main():
     if os.environ.get("JSC_SLOW_FIXTURES"):
         double_scattering_fixture(workdir)
     aero_fixture(workdir, "aero_ice8", synth.ice_layer_files, list(synth.CFG2_NU[::2]))
+    jacobian_fixture(workdir, "jacobian_limb", False)
+    jacobian_fixture(workdir, "jacobian_limb_bt", True)
     print("fixtures written to", HERE)
 
 

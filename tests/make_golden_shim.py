@@ -3,4 +3,4 @@ import os
 import sys
 
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
-from make_golden import aerosol_case, mixed_case, tables_digest  # noqa: E402,F401
+from make_golden import aerosol_case, jacobian_case, mixed_case, tables_digest  # noqa: E402,F401
