@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--sca-epochs", type=int, default=40)
     ap.add_argument("--requests", type=int, default=512,
                     help="requests of the mixed-size request batch; 0 skips it")
+    ap.add_argument("--jacobians", type=int, default=5,
+                    help="timed Jacobians of the retrieval workload; 0 skips it")
     return ap.parse_args()
 
 
@@ -462,6 +464,66 @@ def mixed_bench(args, local, torch, sur=None):
                          % (RAY_CAP, ATM_CAP)}
 
 
+# Retrieval state vector of the Jacobian workload: temperature 5-60 km,
+# CO2 10-50 km, H2O 5-40 km, window extinction 5-30 km (1-km levels).
+JACOBIAN_RET = dict(rett_zmin=5.0, rett_zmax=60.0, retq_zmin=[10.0, 5.0], retq_zmax=[50.0, 40.0],
+                    retk_zmin=[5.0], retk_zmax=[30.0])
+
+
+def jacobian_bench(args, torch, cpu=True):
+    """Finite-difference Jacobian of a limb scan (the retrieval's kernel(),
+    src/retrievalmodel.c:201-298): 61 limb rays 5-35 km, 4 channels, 2
+    emitters, 159 state-vector elements, so 160 forward models per
+    Jacobian, run by jsc_kernel as one batch.  Timed end to end through
+    the public call (host structs in, host matrix out), after warm-up; the
+    reference's own kernel() (n + 1 formod calls on the host cores) is timed
+    on the same case."""
+    from jscat import api, structs as S, synth
+    workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
+    ctlkw, atm, geom = synth.clear_limb_case(workdir)
+    ctlkw = dict(ctlkw, **JACOBIAN_RET)
+
+    def structs():
+        ctl = S.make_ctl(**ctlkw)
+        a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm.get("k"))
+        obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"],
+                         geom["obslon"], geom["vplon"], geom["time"])
+        return ctl, a, obs
+
+    for _ in range(3):
+        k = api.kernel(*structs())
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.jacobians):
+        ctl, a, obs = structs()
+        t0 = time.perf_counter()
+        k = api.kernel(ctl, a, obs)
+        times.append(time.perf_counter() - t0)
+    m, n = k.shape
+    ms = 1e3 * float(np.median(times))
+    res = {"workload": "Jacobian of a limb scan: 61 rays 5-35 km, 4 channels, 2 emitters; "
+                       "state vector T 5-60 km, CO2 10-50 km, H2O 5-40 km, extinction 5-30 km",
+           "rows": m, "columns": n, "forward_models_per_jacobian": n + 1,
+           "ms_per_jacobian": ms, "jacobians": len(times),
+           "value": (n + 1) * len(geom["obsz"]) * len(ctlkw["nus"]) / (ms / 1e3),
+           "unit": UNIT, "timing": "host wall clock around jsc_kernel (inputs and matrix in host memory)"}
+    if cpu:
+        from oracle import refrun
+        if refrun.kernel_available():
+            # SCA_MULT=0: clear-air arithmetic without the reference's read
+            # of the uninitialised los->aerofac (as in cpu_baseline)
+            ref = refrun.reference_kernel(dict(ctlkw, sca_mult=0), atm, geom)
+            scale = np.max(np.abs(ref["k"]), axis=0)
+            err = np.abs(k - ref["k"]) / np.where(scale > 0, scale, 1.0)
+            res["cpu_baseline"] = {
+                "value": (n + 1) * len(geom["obsz"]) * len(ctlkw["nus"]) / ref["seconds"],
+                "unit": UNIT, "ms_per_jacobian": 1e3 * ref["seconds"],
+                "cores": os.cpu_count() or 1, "kind": "reference",
+                "sample": "one Jacobian of the same case by the reference's kernel()"}
+            res["max_err_vs_reference_rel_to_column_max"] = float(err.max())
+    return res
+
+
 def cpu_baseline(ctlkw, atms, ray_atm, geom, n_sample):
     """The reference's OpenMP formod on a bounded sample of the workload
     (whole profiles, first n_sample rays), all host cores, after a warm-up
@@ -673,6 +735,11 @@ def main():
             line["mixed_requests"] = {"error": str(exc)[:300]}
     if sur is not None:
         sur.close()
+    if rank == 0 and world == 1 and args.jacobians > 0:
+        try:
+            line["jacobian"] = jacobian_bench(args, torch, cpu=not args.no_cpu_baseline)
+        except Exception as exc:
+            line["jacobian"] = {"error": str(exc)[:300]}
     if rank == 0:
         print(json.dumps(line))
     if dist:
