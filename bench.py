@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--requests", type=int, default=512,
                     help="requests of the mixed-size request batch; 0 skips it")
     ap.add_argument("--jacobians", type=int, default=5,
-                    help="timed Jacobians of the retrieval workload; 0 skips it")
+                    help="timed Jacobians / optical-property calls; 0 skips both sections")
     return ap.parse_args()
 
 
@@ -524,6 +524,51 @@ def jacobian_bench(args, torch, cpu=True):
     return res
 
 
+def optprop_bench(args, torch, cpu=True):
+    """Aerosol/cloud optical properties (get_opt_prop, src/scatter.c:330-512)
+    of the benchmark's layers: jsc_get_opt_prop (Mie series on the GPU, 170
+    radius nodes x channels per mode) timed end to end through the public
+    call after warm-up, beside the reference's own get_opt_prop on the host
+    (single-threaded, as the reference runs it)."""
+    from jscat import api, structs as S, synth
+    workdir = os.path.join(os.environ.get("JSC_WORKDIR", "/tmp/jsc"), "aero")
+    cases = (("sulfate layer, 16 channels", synth.sulfate_layer_files, list(synth.CFG2_NU), 1),
+             ("ice-cloud layer, 8 channels", synth.ice_layer_files, list(synth.CFG2_NU[::2]), 1),
+             ("two layers, two Mie modes + database, 8 channels", synth.layered_aero_files,
+              list(synth.CFG2_NU[::2]), 3))
+    res = []
+    for name, files, nus, sca_n in cases:
+        f = files(workdir)
+        ctl = S.make_ctl(synth.CFG0_EMITTERS, nus, "-", sca_n=sca_n)
+        times = []
+        for rep in range(3 + max(args.jacobians, 3)):
+            aero = api.read_aero(ctl, f)
+            t0 = time.perf_counter()
+            api.get_opt_prop(ctl, aero)
+            if rep >= 3:
+                times.append(time.perf_counter() - t0)
+        row = {"case": name, "ms": 1e3 * float(np.median(times)), "channels": len(nus),
+               "modes": sca_n}
+        if cpu:
+            from oracle import refrun
+            ctlkw = dict(emitters=synth.CFG0_EMITTERS, nus=nus, tblbase="-", sca_n=sca_n,
+                         sca_mult=1)
+            ref = refrun.reference_aero(ctlkw, f, os.path.dirname(f), timed=True)
+            ra = S.AeroT.from_buffer_copy(ref["aero"])
+            nl, nd = ra.nl, len(nus)
+            got = np.concatenate([S.arr(aero.beta_e)[:nl, :nd].ravel(),
+                                  S.arr(aero.p)[:nl, :nd].ravel()])
+            want = np.concatenate([S.arr(ra.beta_e)[:nl, :nd].ravel(),
+                                   S.arr(ra.p)[:nl, :nd].ravel()])
+            row["reference_cpu_ms"] = 1e3 * ref["seconds"]
+            row["max_rel_err_vs_reference"] = float(np.max(np.abs(got - want) /
+                                                           np.maximum(np.abs(want), 1e-300)))
+        res.append(row)
+    return {"workload": "get_opt_prop of the benchmark's aerosol/cloud layers", "cases": res,
+            "timing": "host wall clock around jsc_get_opt_prop (aero_t in host memory)",
+            "cpu_baseline_kind": "reference (1 core)"}
+
+
 def cpu_baseline(ctlkw, atms, ray_atm, geom, n_sample):
     """The reference's OpenMP formod on a bounded sample of the workload
     (whole profiles, first n_sample rays), all host cores, after a warm-up
@@ -740,6 +785,10 @@ def main():
             line["jacobian"] = jacobian_bench(args, torch, cpu=not args.no_cpu_baseline)
         except Exception as exc:
             line["jacobian"] = {"error": str(exc)[:300]}
+        try:
+            line["optical_properties"] = optprop_bench(args, torch, cpu=not args.no_cpu_baseline)
+        except Exception as exc:
+            line["optical_properties"] = {"error": str(exc)[:300]}
     if rank == 0:
         print(json.dumps(line))
     if dist:

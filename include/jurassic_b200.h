@@ -207,6 +207,28 @@ const char *jsc_last_error_message(void);
 void jsc_release_cache(void);
 
 /* ------------------------------------------------------------------------
+ * Aerosol/cloud optical properties.
+ * ------------------------------------------------------------------------ */
+
+/* Replaces read_aero (src/scatter.c:584-640): the modes of an aerosol
+ * file (top, bottom, transition [km], type MIE/Ext/Const, property file,
+ * and nn [cm^-3], rr [micron], ss for log-normal Mie modes) into
+ * aero->nm and the *_mod / type / filepath / nn / rr / ss fields; the count
+ * must equal ctl->sca_n.  dirname may be NULL. */
+int jsc_read_aero(const char *dirname, const char *filename, const ctl_t *ctl, aero_t *aero);
+
+/* Replaces get_opt_prop (src/scatter.c:330-437): groups the modes into
+ * layers (aero->nl, nmod, top, bottom, trans) and fills beta_e, beta_s,
+ * beta_a and the phase function p per layer and channel.  MIE modes
+ * integrate the Bohren-Huffman Mie series over a log-normal size
+ * distribution with 170 Gauss-Hermite radius nodes (opt_prop_mie_log); all
+ * Mie series of the call run on the GPU in one launch, the size integral
+ * sums them in the reference's order.  Ext modes take the nearest-
+ * wavenumber record of their database file (opt_prop_external).  The GPU
+ * is JURASSIC_GPU_DEVICE (default 0). */
+int jsc_get_opt_prop(const ctl_t *ctl, aero_t *aero);
+
+/* ------------------------------------------------------------------------
  * Jacobians (the retrieval's caller of the forward model).
  * ------------------------------------------------------------------------ */
 

@@ -12,10 +12,6 @@
 #include "jsc_internal.h"
 #include "physics.h"
 
-/* Aerosol optical properties for RETNN/RETRR/RETSS retrievals come from the
- * program's own get_opt_prop (the reference's scatter.o) when it is linked. */
-extern void get_opt_prop(ctl_t *ctl, aero_t *aero) __attribute__((weak));
-
 static int g_exit_on_error = 1;
 static __thread int g_last_status = JSC_OK;
 static pthread_mutex_t g_lock = PTHREAD_MUTEX_INITIALIZER;
@@ -125,14 +121,11 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
                     ig_h2o >= 0 ? atm->q[ig_h2o] : NULL, atm->p);
   }
 
-  /* Optical properties for aerosol retrievals (src/forwardmodel.c:34-36). */
-  if (ctl->retnn || ctl->retrr || ctl->retss) {
-    if (!get_opt_prop) {
-      free(mask);
-      jsc_set_error(JSC_ERR_UNSUPPORTED, "RETNN/RETRR/RETSS need get_opt_prop");
-      return JSC_ERR_UNSUPPORTED;
-    }
-    get_opt_prop(ctl, aero);
+  /* Optical properties for aerosol retrievals (src/forwardmodel.c:34-36),
+   * with the Mie series on the GPU. */
+  if ((ctl->retnn || ctl->retrr || ctl->retss) && (st = jsc_get_opt_prop(ctl, aero))) {
+    free(mask);
+    return st;
   }
 
   pthread_mutex_lock(&g_lock);

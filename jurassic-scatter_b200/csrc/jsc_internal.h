@@ -123,6 +123,12 @@ int jsc_find_emitter(const ctl_t *ctl, const char *name);
 /* Error reporting shared by C and CUDA parts. */
 void jsc_set_error(int status, const char *fmt, ...);
 
+/* Mie efficiencies and phase functions of n (size parameter, refractive
+ * index) tasks on GPU `device` (mie.cu): out[i][0] = Q_ext,
+ * out[i][1] = Q_sca, out[i][2 + j] = phase function at j degrees. */
+int jsc_mie_eval(int device, int n, const double *x, const double *nr, const double *ni,
+                 double *out);
+
 /* ------------------------------------------------------------------------
  * Device layout of a model (device pointers; passed by value to kernels).
  * ------------------------------------------------------------------------ */

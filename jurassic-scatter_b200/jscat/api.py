@@ -35,6 +35,22 @@ def formod(ctl, atm, obs, aero=None, exit_on_error=False):
     L.check(lib.jsc_last_status(), "formod")
 
 
+def read_aero(ctl, filename, dirname=None):
+    """aero_t with the modes of an aerosol file (jsc_read_aero)."""
+    aero = S.AeroT()
+    L.check(L.load().jsc_read_aero(None if dirname is None else dirname.encode(),
+                                   filename.encode(), C.byref(ctl), C.byref(aero)),
+            "jsc_read_aero")
+    return aero
+
+
+def get_opt_prop(ctl, aero):
+    """Layers and optical properties of aero's modes, Mie series on the GPU
+    (jsc_get_opt_prop)."""
+    L.check(L.load().jsc_get_opt_prop(C.byref(ctl), C.byref(aero)), "jsc_get_opt_prop")
+    return aero
+
+
 def atm2x(ctl, atm, aero=None):
     """State vector, quantity codes and levels (jsc_atm2x)."""
     lib = L.load()

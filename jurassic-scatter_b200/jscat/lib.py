@@ -26,7 +26,7 @@ EXPORTS = [
     "jsc_batch_scatter_samples", "jsc_batch_set_surrogate", "jsc_batch_surrogate_stats",
     "jsc_batch_set_fixed", "jsc_batch_download_async", "jsc_batch_async_status",
     "jsc_batch_graph_capture", "jsc_batch_graph_launch", "jsc_surrogate_set_tensor_path",
-    "jsc_atm2x", "jsc_x2atm", "jsc_obs2y", "jsc_kernel",
+    "jsc_atm2x", "jsc_x2atm", "jsc_obs2y", "jsc_kernel", "jsc_read_aero", "jsc_get_opt_prop",
 ]
 
 
@@ -79,6 +79,8 @@ def load():
         "jsc_status_string": (C.c_char_p, [i]),
         "jsc_last_status": (i, []),
         "jsc_set_exit_on_error": (None, [i]),
+        "jsc_read_aero": (i, [C.c_char_p, C.c_char_p, P(S.CtlT), P(S.AeroT)]),
+        "jsc_get_opt_prop": (i, [P(S.CtlT), P(S.AeroT)]),
         "jsc_atm2x": (C.c_size_t, [P(S.CtlT), P(S.AtmT), P(S.AeroT), vp, vp, vp]),
         "jsc_x2atm": (None, [P(S.CtlT), vp, P(S.AtmT), P(S.AeroT)]),
         "jsc_obs2y": (C.c_size_t, [P(S.CtlT), P(S.ObsT), vp, vp, vp]),

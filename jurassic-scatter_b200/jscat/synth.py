@@ -264,13 +264,56 @@ def write_refractive_index(path, fn, lo=600.0, hi=1500.0, step=1.0):
 
 def write_aero_file(path, layers):
     """Aerosol model file: top bottom transition type refractive-index-file
-    concentration radius width (one line per log-normal mode)."""
+    concentration radius width (one line per mode; MIE unless a layer
+    tuple carries the type as an eighth element)."""
     with open(path, "w") as f:
         f.write("# $1 = top [km]\n# $2 = bottom [km]\n# $3 = transition [km]\n"
                 "# $4 = type\n# $5 = refractive index file\n# $6 = N [cm-3]\n"
                 "# $7 = median radius [um]\n# $8 = width\n\n")
         for lay in layers:
-            f.write("%g %g %g MIE %s %g %g %g\n" % lay)
+            kind = lay[7] if len(lay) > 7 else "MIE"
+            f.write("%g %g %g %s %s %g %g %g\n" % (lay[:3] + (kind,) + lay[3:7]))
+
+
+def write_optical_database(path, nus):
+    """External optical-property database (opt_prop_external's format): per
+    line nu, extinction and scattering [1/km] and the phase function at
+    NTHETA angles (a normalised Henyey-Greenstein shape whose asymmetry
+    varies with nu)."""
+    th = np.radians(np.arange(181.0))
+    with open(path, "w") as f:
+        for nu in nus:
+            g = 0.3 + 0.4 * (nu - 700.0) / 700.0
+            hg = (1 - g * g) / (1 + g * g - 2 * g * np.cos(th)) ** 1.5
+            ext = 1e-3 * (1.0 + 0.5 * np.sin(nu / 90.0))
+            sca = 0.6 * ext
+            f.write("%.4f %.8e %.8e %s\n" % (nu, ext, sca, " ".join("%.8e" % v for v in hg)))
+
+
+def layered_aero_files(directory):
+    """aero.tab with two layers and three modes: a sulfate-like layer at
+    15-20 km with two log-normal Mie modes (0.1 um and 0.4 um), and a
+    9-11 km layer from an external optical-property database."""
+    os.makedirs(directory, exist_ok=True)
+    ri = os.path.join(directory, "sulfate_ri.dat")
+    write_refractive_index(ri, sulfate_refractive_index)
+    db = os.path.join(directory, "optical_db.dat")
+    write_optical_database(db, np.arange(700.0, 1401.0, 50.0))
+    aero = os.path.join(directory, "aero_layers.tab")
+    write_aero_file(aero, [(20.0, 15.0, 0.1, ri, 10.0, 0.1, 1.5),
+                           (20.0, 15.0, 0.1, ri, 2.0, 0.4, 1.3),
+                           (11.0, 9.0, 0.1, db, 0.0, 0.0, 0.0, "Ext")])
+    return aero
+
+
+def external_aero_files(directory):
+    """aero.tab with one layer from the external database only."""
+    os.makedirs(directory, exist_ok=True)
+    db = os.path.join(directory, "optical_db.dat")
+    write_optical_database(db, np.arange(700.0, 1401.0, 50.0))
+    aero = os.path.join(directory, "aero_external.tab")
+    write_aero_file(aero, [(11.0, 9.0, 0.1, db, 0.0, 0.0, 0.0, "Ext")])
+    return aero
 
 
 def sulfate_layer_files(directory):

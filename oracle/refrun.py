@@ -300,14 +300,20 @@ def _aero_child(job):
     aero = S.AeroT()
     os.chdir(job["cwd"])
     lib.read_aero(None, job["aerofile"].encode(), C.byref(ctl), C.byref(aero))
+    t0 = time.perf_counter()
     lib.get_opt_prop(C.byref(ctl), C.byref(aero))
+    seconds = time.perf_counter() - t0
+    if job.get("timed"):
+        return {"aero": bytes(aero), "seconds": seconds}
     return bytes(aero)
 
 
-def reference_aero(ctl_kw, aerofile, cwd, timeout=600):
+def reference_aero(ctl_kw, aerofile, cwd, timeout=600, timed=False):
     """aero_t (as bytes) from the reference's read_aero + get_opt_prop
-    (Mie optical properties, src/scatter.c:330-508,583-639), run in cwd."""
-    return _spawn({"aero_job": True, "ctl": ctl_kw, "aerofile": aerofile, "cwd": cwd}, timeout)
+    (Mie optical properties, src/scatter.c:330-508,583-639), run in cwd;
+    with timed=True a dict with the bytes and get_opt_prop's seconds."""
+    return _spawn({"aero_job": True, "ctl": ctl_kw, "aerofile": aerofile, "cwd": cwd,
+                   "timed": timed}, timeout)
 
 
 def run_port(ctl_kw, atms, ray_atm, geom, aero=None, threads=None, warmup=False, los=False,

@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [jacobian]
+    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -112,10 +112,11 @@ def double_scattering_fixture(workdir):
                         **{"geom_" + k: v for k, v in geom.items()})
 
 
-def aero_fixture(workdir, name, layer_files, nus):
+def aero_fixture(workdir, name, layer_files, nus, sca_n=1):
     """aero_t (as bytes) of a layer file on a channel grid, from the
-    reference's read_aero + get_opt_prop (Mie), for benchmark inputs."""
-    ctlkw = dict(emitters=synth.CFG0_EMITTERS, nus=nus, tblbase="-", sca_n=1, sca_mult=1)
+    reference's read_aero + get_opt_prop (Mie), for benchmark inputs and
+    the optical-property parity tests."""
+    ctlkw = dict(emitters=synth.CFG0_EMITTERS, nus=nus, tblbase="-", sca_n=sca_n, sca_mult=1)
     aerofile = layer_files(os.path.join(workdir, "aero"))
     aero = refrun.reference_aero(ctlkw, aerofile, os.path.dirname(aerofile))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), nus=np.asarray(nus),
@@ -164,6 +165,10 @@ def main():
         jacobian_fixture(workdir, "jacobian_limb", False)
         jacobian_fixture(workdir, "jacobian_limb_bt", True)
         return
+    if sys.argv[1:] == ["aero"]:
+        aero_fixture(workdir, "aero_layers8", synth.layered_aero_files, list(synth.CFG2_NU[::2]),
+                     sca_n=3)
+        return
     ctlkw, atm, geom = synth.clear_limb_case(workdir)
     ra = np.zeros(len(geom["obsz"]), int)
     ref = refrun.run(reference_ctl(ctlkw), [atm], ra, geom, los=True)
@@ -193,6 +198,8 @@ def main():
     if os.environ.get("JSC_SLOW_FIXTURES"):
         double_scattering_fixture(workdir)
     aero_fixture(workdir, "aero_ice8", synth.ice_layer_files, list(synth.CFG2_NU[::2]))
+    aero_fixture(workdir, "aero_layers8", synth.layered_aero_files, list(synth.CFG2_NU[::2]),
+                     sca_n=3)
     jacobian_fixture(workdir, "jacobian_limb", False)
     jacobian_fixture(workdir, "jacobian_limb_bt", True)
     print("fixtures written to", HERE)
