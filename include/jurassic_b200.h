@@ -158,8 +158,10 @@ typedef struct {
  * obs->rad, applies hydrostatic balance to atm->p (ctl->hydz >= 0), traces
  * every ray, evaluates EGA transmittances, continua, Planck source and
  * radiative transfer on the GPU (single/multiple scattering when
- * ctl->sca_mult > 0 and ctl->sca_n > 0), converts to brightness temperature
- * when ctl->write_bbt, and restores the mask.  Writes obs->rad, obs->tau and
+ * ctl->sca_mult > 0 and ctl->sca_n > 0), convolves with the field-of-view
+ * shape of ctl->fov unless it is "-" (formod_fov, src/forwardmodel.c:
+ * 156-220), converts to brightness temperature when ctl->write_bbt, and
+ * restores the mask.  Writes obs->rad, obs->tau and
  * obs->tpz/tplon/tplat.  Errors follow the reference's ERRMSG convention
  * (message, exit(EXIT_FAILURE)) unless jsc_set_exit_on_error(0). */
 void formod(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero);

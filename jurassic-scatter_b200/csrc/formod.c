@@ -89,6 +89,104 @@ static int ensure_cache(const ctl_t *ctl) {
   return JSC_OK;
 }
 
+/* Field-of-view shape of the last FOV file read (read_shape,
+ * src/forwardmodel.c:577-606): offsets dz [km] and weights. */
+static pthread_mutex_t g_fov_lock = PTHREAD_MUTEX_INITIALIZER;
+static char g_fov_file[LEN];
+static double g_fov_dz[NSHAPE + 1], g_fov_w[NSHAPE + 1];
+static int g_fov_n;
+
+static int fov_shape(const char *file) {
+  if (g_fov_n > 0 && !strcmp(g_fov_file, file)) return JSC_OK;
+  FILE *in = fopen(file, "r");
+  if (!in) {
+    jsc_set_error(JSC_ERR_FILE, "cannot open field-of-view file %s", file);
+    return JSC_ERR_FILE;
+  }
+  char *line = (char *)malloc(LEN);
+  int n = 0, st = JSC_OK;
+  if (!line) st = JSC_ERR_NOMEM;
+  while (!st && fgets(line, LEN, in))
+    if (sscanf(line, "%lg %lg", &g_fov_dz[n], &g_fov_w[n]) == 2)
+      if (++n > NSHAPE) {
+        jsc_set_error(JSC_ERR_ARG, "too many points in %s", file);
+        st = JSC_ERR_ARG;
+      }
+  fclose(in);
+  free(line);
+  if (!st && n < 1) {
+    jsc_set_error(JSC_ERR_FILE, "could not read any data from %s", file);
+    st = JSC_ERR_FILE;
+  }
+  g_fov_n = st ? 0 : n;
+  if (!st) snprintf(g_fov_file, LEN, "%s", file);
+  return st;
+}
+
+/* Field-of-view convolution of the pencil-beam results (formod_fov,
+ * src/forwardmodel.c:156-220): per ray, the radiance and transmittance
+ * profiles over tangent height of the up to NFOV rays on either side with
+ * the same observation time, interpolated at tangent height + dz of every
+ * shape point and averaged with the shape's weights. */
+static int fov_convolve(const ctl_t *ctl, obs_t *obs) {
+  pthread_mutex_lock(&g_fov_lock);
+  int st = fov_shape(ctl->fov);
+  const int nd = ctl->nd, nr = obs->nr, nf = 2 * NFOV + 1;
+  double *rad = NULL, *tau = NULL, *buf = NULL;
+  if (!st) {
+    rad = (double *)malloc(2 * (size_t)nd * nr * sizeof(double) + 1);
+    buf = (double *)malloc((size_t)nf * (2 * nd + 1) * sizeof(double));
+    if (!rad || !buf) st = JSC_ERR_NOMEM;
+  }
+  if (!st) {
+    tau = rad + (size_t)nd * nr;
+    /* the profiles come from the unconvolved results */
+    for (int id = 0; id < nd; id++) {
+      memcpy(rad + (size_t)id * nr, obs->rad[id], nr * sizeof(double));
+      memcpy(tau + (size_t)id * nr, obs->tau[id], nr * sizeof(double));
+    }
+    double *z = buf, *pr = z + nf, *pt = pr + (size_t)nd * nf;
+    for (int ir = 0; ir < nr && !st; ir++) {
+      int nz = 0;
+      const int lo = ir - NFOV > 0 ? ir - NFOV : 0, hi = ir + 1 + NFOV < nr ? ir + 1 + NFOV : nr;
+      for (int ir2 = lo; ir2 < hi; ir2++)
+        if (obs->time[ir2] == obs->time[ir]) {
+          z[nz] = obs->tpz[ir2];
+          for (int id = 0; id < nd; id++) {
+            pr[(size_t)id * nf + nz] = rad[(size_t)id * nr + ir2];
+            pt[(size_t)id * nf + nz] = tau[(size_t)id * nr + ir2];
+          }
+          nz++;
+        }
+      if (nz < 2) {
+        jsc_set_error(JSC_ERR_ARG, "cannot apply FOV convolution to ray %d", ir);
+        st = JSC_ERR_ARG;
+        break;
+      }
+      double wsum = 0;
+      for (int id = 0; id < nd; id++) obs->rad[id][ir] = obs->tau[id][ir] = 0;
+      for (int i = 0; i < g_fov_n; i++) {
+        const double zf = obs->tpz[ir] + g_fov_dz[i];
+        const int k = jsc_locate(z, nz, zf);
+        for (int id = 0; id < nd; id++) {
+          const double *r = pr + (size_t)id * nf, *t = pt + (size_t)id * nf;
+          obs->rad[id][ir] += g_fov_w[i] * jsc_lin(z[k], r[k], z[k + 1], r[k + 1], zf);
+          obs->tau[id][ir] += g_fov_w[i] * jsc_lin(z[k], t[k], z[k + 1], t[k + 1], zf);
+        }
+        wsum += g_fov_w[i];
+      }
+      for (int id = 0; id < nd; id++) {
+        obs->rad[id][ir] /= wsum;
+        obs->tau[id][ir] /= wsum;
+      }
+    }
+  }
+  pthread_mutex_unlock(&g_fov_lock);
+  free(rad);
+  free(buf);
+  return st;
+}
+
 static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
   const int nd = ctl->nd, nr = obs->nr, np = atm->np, ng = ctl->ng, nw = ctl->nw;
   int st = JSC_OK;
@@ -97,10 +195,6 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
     jsc_set_error(JSC_ERR_ARG, "formod: invalid sizes (nd=%d ng=%d nw=%d nr=%d np=%d)",
                   nd, ng, nw, nr, np);
     return JSC_ERR_ARG;
-  }
-  if (ctl->fov[0] != '-') {
-    jsc_set_error(JSC_ERR_UNSUPPORTED, "field-of-view convolution (FOV=%s)", ctl->fov);
-    return JSC_ERR_UNSUPPORTED;
   }
   if (ctl->sca_n > 0 && !aero) {
     jsc_set_error(JSC_ERR_ARG, "formod: SCA_N=%d needs the aerosol/cloud data", ctl->sca_n);
@@ -194,6 +288,8 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
   pthread_mutex_unlock(&g_lock);
   free(buf);
 
+  /* Field-of-view convolution (src/forwardmodel.c:102). */
+  if (!st && ctl->fov[0] != '-') st = fov_convolve(ctl, obs);
   if (!st) {
     /* Brightness temperature (src/forwardmodel.c:106-109). */
     if (ctl->write_bbt)
@@ -371,10 +467,6 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
                   nd, ng, nw, nr, np);
     return JSC_ERR_ARG;
   }
-  if (ctl->fov[0] != '-') {
-    jsc_set_error(JSC_ERR_UNSUPPORTED, "field-of-view convolution (FOV=%s)", ctl->fov);
-    return JSC_ERR_UNSUPPORTED;
-  }
   if (ctl->retnn || ctl->retrr || ctl->retss) {
     jsc_set_error(JSC_ERR_UNSUPPORTED,
                   "jsc_kernel: aerosol parameters in the state vector (RETNN/RETRR/RETSS)");
@@ -419,7 +511,9 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
   double *rays = (double *)malloc(nrays * 7 * sizeof(double) + 1);
   int *ray_atm = (int *)malloc(nrays * sizeof(int) + 1);
   double *res = (double *)malloc((nrays * (2 * (size_t)nd + 3) + 2 * m + 1) * sizeof(double));
-  if (!x0 || !h || !iqa || !ipa || !mask || !prof || !atm_off || !rays || !ray_atm || !res) {
+  obs_t *fobs = ctl->fov[0] != '-' ? (obs_t *)malloc(sizeof(obs_t)) : NULL;
+  if (!x0 || !h || !iqa || !ipa || !mask || !prof || !atm_off || !rays || !ray_atm || !res ||
+      (ctl->fov[0] != '-' && !fobs)) {
     st = JSC_ERR_NOMEM;
     goto done;
   }
@@ -510,16 +604,25 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
     }
     if (st) goto done;
 
-    /* The undisturbed forward model into obs (formod's outputs). */
+    /* The undisturbed forward model into obs (formod's outputs: field-of-
+     * view convolution, brightness temperature, mask). */
+    const int fov = ctl->fov[0] != '-';
     for (int ir = 0; ir < nr; ir++) {
       obs->tpz[ir] = tp[ir];
       obs->tplon[ir] = tp[nrays + ir];
       obs->tplat[ir] = tp[2 * nrays + ir];
       for (int id = 0; id < nd; id++) {
-        obs->rad[id][ir] = mask[(size_t)id * nr + ir] ? NAN : out_rad(ctl, rad, ir, id);
+        obs->rad[id][ir] = rad[(size_t)ir * nd + id];
         obs->tau[id][ir] = tau[(size_t)ir * nd + id];
       }
     }
+    if (fov && (st = fov_convolve(ctl, obs))) goto done;
+    for (int ir = 0; ir < nr; ir++)
+      for (int id = 0; id < nd; id++) {
+        const double v = obs->rad[id][ir];
+        obs->rad[id][ir] = mask[(size_t)id * nr + ir] ? NAN
+                           : ctl->write_bbt ? brightness(v, ctl->nu[id]) : v;
+      }
     double *y0 = tp + 3 * nrays, *y1 = y0 + m;
     const size_t m0 = jsc_obs2y(ctl, obs, NULL, NULL, NULL);
     if (m0 != m) {
@@ -532,11 +635,26 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
      * model (obs2y of a copy of obs, whose non-finite entries stay masked). */
     for (size_t j = 0; j < n; j++) {
       const size_t r0 = (j + 1) * nr;
+      if (fov) {
+        /* the disturbed results through the same convolution */
+        fobs->nr = nr;
+        for (int ir = 0; ir < nr; ir++) {
+          fobs->time[ir] = obs->time[ir];
+          fobs->tpz[ir] = tp[r0 + ir];
+          for (int id = 0; id < nd; id++) {
+            fobs->rad[id][ir] = rad[(r0 + ir) * nd + id];
+            fobs->tau[id][ir] = tau[(r0 + ir) * nd + id];
+          }
+        }
+        if ((st = fov_convolve(ctl, fobs))) goto done;
+      }
       size_t c = 0;
       for (int ir = 0; ir < nr; ir++)
         for (int id = 0; id < nd; id++) {
           if (!isfinite(obs->rad[id][ir])) continue;
-          const double v = out_rad(ctl, rad, r0 + ir, id);
+          const double v = fov ? (ctl->write_bbt ? brightness(fobs->rad[id][ir], ctl->nu[id])
+                                                 : fobs->rad[id][ir])
+                               : out_rad(ctl, rad, r0 + ir, id);
           if (!isfinite(v)) continue;
           if (c < m) y1[c] = v;
           c++;
@@ -563,5 +681,6 @@ done:
   free(rays);
   free(ray_atm);
   free(res);
+  free(fobs);
   return st;
 }

@@ -275,6 +275,18 @@ def write_aero_file(path, layers):
             f.write("%g %g %g %s %s %g %g %g\n" % (lay[:3] + (kind,) + lay[3:7]))
 
 
+def write_fov_shape(path, fwhm=2.0, half_width=2.0, step=0.1):
+    """Field-of-view shape file (read_shape's 'dz weight' lines): a
+    Gaussian in tangent-height offset dz [km]."""
+    dz = np.arange(-half_width, half_width + step / 2, step)
+    w = np.exp(-4.0 * np.log(2.0) * (dz / fwhm) ** 2)
+    with open(path, "w") as f:
+        f.write("# $1 = offset [km]\n# $2 = weight\n")
+        for a, b in zip(dz, w):
+            f.write("%.4f %.8e\n" % (a, b))
+    return path
+
+
 def write_optical_database(path, nus):
     """External optical-property database (opt_prop_external's format): per
     line nu, extinction and scattering [1/km] and the phase function at

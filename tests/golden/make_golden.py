@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero]
+    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -131,11 +131,23 @@ JACOBIAN_RET = dict(rett_zmin=5.0, rett_zmax=40.0, retq_zmin=[20.0, 5.0], retq_z
                     retk_zmin=[10.0], retk_zmax=[15.0], retp_zmin=30.0, retp_zmax=35.0)
 
 
-def jacobian_case(workdir, bt=False):
+def fov_case(workdir):
+    """The clear limb case with a 2-km Gaussian field of view."""
+    ctlkw, atm, geom = synth.clear_limb_case(workdir)
+    shape = synth.write_fov_shape(os.path.join(workdir, "fov_gauss2km.dat"))
+    return dict(ctlkw, fov=shape), atm, geom
+
+
+def jacobian_case(workdir, bt=False, fov=False):
     """The clear limb case with the retrieval settings above (radiances,
     two observations masked and one ray fully masked), or with brightness
-    temperatures, temperature only and every fourth ray (bt=True)."""
+    temperatures, temperature only and every fourth ray (bt=True), or with
+    the field of view of fov_case and temperature only (fov=True)."""
     ctlkw, atm, geom = synth.clear_limb_case(workdir)
+    if fov:
+        ctlkw = dict(fov_case(workdir)[0], rett_zmin=5.0, rett_zmax=40.0)
+        mask = np.zeros((len(geom["obsz"]), len(ctlkw["nus"])), bool)
+        return ctlkw, atm, geom, mask
     if bt:
         ctlkw = dict(ctlkw, write_bbt=1, rett_zmin=10.0, rett_zmax=30.0)
         geom = {k: v[::4] for k, v in geom.items()}
@@ -148,9 +160,9 @@ def jacobian_case(workdir, bt=False):
     return ctlkw, atm, geom, mask
 
 
-def jacobian_fixture(workdir, name, bt):
+def jacobian_fixture(workdir, name, bt, fov=False):
     """Jacobian of the reference's own kernel() (oracle/_ref/libjurassic_ref_ret.so)."""
-    ctlkw, atm, geom, mask = jacobian_case(workdir, bt)
+    ctlkw, atm, geom, mask = jacobian_case(workdir, bt, fov)
     ref = refrun.reference_kernel(reference_ctl(ctlkw), atm, geom, mask=mask)
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"), k=ref["k"], x0=ref["x0"], iqa=ref["iqa"],
@@ -159,11 +171,26 @@ def jacobian_fixture(workdir, name, bt):
         **{"geom_" + k: v for k, v in geom.items()})
 
 
+def fov_fixtures(workdir):
+    """formod and kernel() with the field of view of fov_case."""
+    ctlkw, atm, geom = fov_case(workdir)
+    ra = np.zeros(len(geom["obsz"]), int)
+    ref = refrun.run(reference_ctl(ctlkw), [atm], ra, geom, los=True)
+    save_fov = dict(rad=ref["rad"], tau=ref["tau"], tpz=ref["tpz"],
+                    table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
+                    **{"geom_" + k: v for k, v in geom.items()})
+    np.savez_compressed(os.path.join(HERE, "clear_limb_fov.npz"), **save_fov)
+    jacobian_fixture(workdir, "jacobian_limb_fov", False, fov=True)
+
+
 def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
     if sys.argv[1:] == ["jacobian"]:
         jacobian_fixture(workdir, "jacobian_limb", False)
         jacobian_fixture(workdir, "jacobian_limb_bt", True)
+        return
+    if sys.argv[1:] == ["fov"]:
+        fov_fixtures(workdir)
         return
     if sys.argv[1:] == ["aero"]:
         aero_fixture(workdir, "aero_layers8", synth.layered_aero_files, list(synth.CFG2_NU[::2]),
@@ -202,6 +229,7 @@ def main():
                      sca_n=3)
     jacobian_fixture(workdir, "jacobian_limb", False)
     jacobian_fixture(workdir, "jacobian_limb_bt", True)
+    fov_fixtures(workdir)
     print("fixtures written to", HERE)
 
 

@@ -28,11 +28,12 @@ K_TOL = 1e-6
 REL_TOL = 1e-9
 
 
-def _setup(workdir, bt):
+def _setup(workdir, bt, fov=False):
     from jscat import structs as S
     from make_golden_shim import jacobian_case, tables_digest
-    ctlkw, atm, geom, mask = jacobian_case(workdir, bt)
-    g = dict(np.load(os.path.join(GOLDEN, "jacobian_limb_bt.npz" if bt else "jacobian_limb.npz")))
+    ctlkw, atm, geom, mask = jacobian_case(workdir, bt, fov)
+    name = "jacobian_limb_fov" if fov else "jacobian_limb_bt" if bt else "jacobian_limb"
+    g = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
     assert tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]) == str(g["table_sha256"])
     ctl = S.make_ctl(**ctlkw)
     a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm.get("k"))
@@ -44,10 +45,11 @@ def _setup(workdir, bt):
     return ctl, a, obs, g
 
 
-@pytest.mark.parametrize("bt", [False, True], ids=["radiance", "brightness"])
-def test_kernel_matches_reference(workdir, bt):
+@pytest.mark.parametrize("bt,fov", [(False, False), (True, False), (False, True)],
+                         ids=["radiance", "brightness", "field-of-view"])
+def test_kernel_matches_reference(workdir, bt, fov):
     from jscat import api, structs as S
-    ctl, a, obs, g = _setup(workdir, bt)
+    ctl, a, obs, g = _setup(workdir, bt, fov)
     k = api.kernel(ctl, a, obs)
     kref = g["k"]
     assert k.shape == kref.shape

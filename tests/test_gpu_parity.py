@@ -54,6 +54,27 @@ def test_clear_limb_dropin_formod(workdir):
     np.testing.assert_allclose(S.arr(obs.tpz)[:nr], g["tpz"], rtol=1e-9, atol=1e-9)
 
 
+def test_clear_limb_fov_formod(workdir):
+    """Drop-in formod with a field-of-view shape (formod_fov,
+    src/forwardmodel.c:156-220) against the reference run with the same
+    shape file."""
+    from jscat import structs as S, api
+    from make_golden_shim import fov_case
+    g = _load("clear_limb_fov")
+    ctlkw, atm, geom = fov_case(workdir)
+    _check_tables(g, ctlkw)
+    ctl = S.make_ctl(**ctlkw)
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm["k"])
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"])
+    api.formod(ctl, a, obs)
+    nr, nd = obs.nr, ctl.nd
+    rad = S.arr(obs.rad)[:nd, :nr].T
+    tau = S.arr(obs.tau)[:nd, :nr].T
+    assert bt_error(rad, g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(rad, g["rad"]) <= REL_TOL
+    assert max_rel(tau, g["tau"]) <= REL_TOL
+
+
 # EGA kernel families: -1 the default (variant 6 for clear air, 10 with
 # aerosol/cloud layers), 6 a thread per (ray, channel), 9 a lane per (ray,
 # channel, emitter)
