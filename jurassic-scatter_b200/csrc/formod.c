@@ -458,6 +458,13 @@ static double out_rad(const ctl_t *ctl, const double *rad, size_t ray, int id) {
   return ctl->write_bbt ? brightness(v, ctl->nu[id]) : v;
 }
 
+/* Aerosol parameter of a state-vector element (the value x2atm sets). */
+static double *aero_element(const ctl_t *ctl, int iqa, aero_t *aero) {
+  if (iqa == JSC_IDXNN(ctl)) return &aero->nn[0];
+  if (iqa == JSC_IDXRR(ctl)) return &aero->rr[0];
+  return &aero->ss[0];
+}
+
 int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size_t m,
                size_t n, size_t tda) {
   const int nd = ctl->nd, nr = obs->nr, np = atm->np, ng = ctl->ng, nw = ctl->nw;
@@ -467,12 +474,8 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
                   nd, ng, nw, nr, np);
     return JSC_ERR_ARG;
   }
-  if (ctl->retnn || ctl->retrr || ctl->retss) {
-    jsc_set_error(JSC_ERR_UNSUPPORTED,
-                  "jsc_kernel: aerosol parameters in the state vector (RETNN/RETRR/RETSS)");
-    return JSC_ERR_UNSUPPORTED;
-  }
-  if (ctl->sca_n > 0 && !aero) {
+  const int aero_ret = ctl->retnn || ctl->retrr || ctl->retss;
+  if ((ctl->sca_n > 0 || aero_ret) && !aero) {
     jsc_set_error(JSC_ERR_ARG, "jsc_kernel: SCA_N=%d needs the aerosol/cloud data", ctl->sca_n);
     return JSC_ERR_ARG;
   }
@@ -482,7 +485,8 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
     return JSC_ERR_ARG;
   }
 
-  /* Hydrostatic balance on the caller's atmosphere, as formod does. */
+  /* Hydrostatic balance on the caller's atmosphere and, for aerosol
+   * retrievals, fresh optical properties, as formod does. */
   const int ig_h2o = jsc_find_emitter(ctl, "H2O");
   jsc_hydrostatic(ctl->hydz, np, atm->z, atm->lon, atm->lat, atm->t,
                   ig_h2o >= 0 ? atm->q[ig_h2o] : NULL, atm->p);
@@ -492,42 +496,71 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
                   n0, n);
     return JSC_ERR_ARG;
   }
-  const size_t natm = n + 1, nl = natm * (size_t)np, nrays = natm * (size_t)nr;
-  if (nl > 0x7fffffff || nrays > 0x7fffffff) {
-    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: %zu profiles x %d rays exceed the batch limits",
-                  natm, nr);
-    return JSC_ERR_ARG;
-  }
 
   int st = JSC_OK;
+  if (aero_ret && (st = jsc_get_opt_prop(ctl, aero))) return st;
   double *x0 = (double *)malloc((n + 1) * sizeof(double));
   double *h = (double *)malloc((n + 1) * sizeof(double));
   int *iqa = (int *)malloc((n + 1) * sizeof(int)), *ipa = (int *)malloc((n + 1) * sizeof(int));
+  /* source of column j: disturbed profile col[j] >= 1 of the main batch, or
+   * -1 - a for the a-th aerosol parameter (its own run) */
+  long *col = (long *)malloc((n + 1) * sizeof(long));
   unsigned char *mask = (unsigned char *)malloc((size_t)nd * (nr > 0 ? nr : 1));
+  double *prof = NULL, *rays = NULL, *res = NULL, *ares = NULL, *bq = NULL, *bk = NULL;
+  int *atm_off = NULL, *ray_atm = NULL;
+  aero_t *aero1 = NULL;
+  obs_t *fobs = NULL;
+  size_t natm = 1, naero = 0;
+  if (!x0 || !h || !iqa || !ipa || !col || !mask) {
+    st = JSC_ERR_NOMEM;
+    goto done;
+  }
+  jsc_atm2x(ctl, atm, aero, x0, iqa, ipa);
+  for (size_t j = 0; j < n; j++) {
+    h[j] = perturbation(ctl, iqa[j], x0[j]);
+    if (iqa[j] == JSC_IDXNN(ctl)) h[j] = gmax(fabs(0.5 * x0[j]), 0.1);
+    if (iqa[j] == JSC_IDXRR(ctl)) h[j] = gmax(fabs(0.25 * x0[j]), 0.1);
+    if (iqa[j] == JSC_IDXSS(ctl)) h[j] = gmax(fabs(0.1 * x0[j]), 0.01);
+    if (h[j] <= 0) {
+      jsc_set_error(JSC_ERR_ARG, "jsc_kernel: cannot set perturbation size");
+      st = JSC_ERR_ARG;
+      goto done;
+    }
+    col[j] = iqa[j] >= JSC_IDXNN(ctl) ? -1 - (long)naero++ : (long)natm++;
+  }
+  const size_t nl = natm * (size_t)np, nrays = natm * (size_t)nr;
+  if (nl > 0x7fffffff || nrays > 0x7fffffff) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: %zu profiles x %d rays exceed the batch limits",
+                  natm, nr);
+    st = JSC_ERR_ARG;
+    goto done;
+  }
   /* packed profiles: z lon lat p t [nl], q [ng][nl], k [nw][nl] */
-  double *prof = (double *)malloc(nl * (5 + (size_t)ng + nw) * sizeof(double));
-  int *atm_off = (int *)malloc((natm + 1) * sizeof(int));
+  prof = (double *)malloc(nl * (5 + (size_t)ng + nw) * sizeof(double));
+  atm_off = (int *)malloc((natm + 1) * sizeof(int));
   /* rays: time obsz obslon obslat vpz vplon vplat [nrays]; outputs */
-  double *rays = (double *)malloc(nrays * 7 * sizeof(double) + 1);
-  int *ray_atm = (int *)malloc(nrays * sizeof(int) + 1);
-  double *res = (double *)malloc((nrays * (2 * (size_t)nd + 3) + 2 * m + 1) * sizeof(double));
-  obs_t *fobs = ctl->fov[0] != '-' ? (obs_t *)malloc(sizeof(obs_t)) : NULL;
-  if (!x0 || !h || !iqa || !ipa || !mask || !prof || !atm_off || !rays || !ray_atm || !res ||
+  rays = (double *)malloc(nrays * 7 * sizeof(double) + 1);
+  ray_atm = (int *)malloc(nrays * sizeof(int) + 1);
+  res = (double *)malloc((nrays * (2 * (size_t)nd + 3) + 2 * m + 1) * sizeof(double));
+  /* aerosol columns: rad, tau [nr][nd] and tpz, tplon, tplat [nr] each */
+  ares = (double *)malloc((naero * (size_t)nr * (2 * (size_t)nd + 3) + 1) * sizeof(double));
+  if (naero) {
+    aero1 = (aero_t *)malloc(sizeof(aero_t));
+    bq = (double *)malloc(((size_t)(ng + nw) * np + 1) * sizeof(double));
+    if (bq) {
+      bk = bq + (size_t)ng * np;
+      for (int ig = 0; ig < ng; ig++) memcpy(bq + (size_t)ig * np, atm->q[ig], np * sizeof(double));
+      for (int iw = 0; iw < nw; iw++) memcpy(bk + (size_t)iw * np, atm->k[iw], np * sizeof(double));
+    }
+  }
+  if (ctl->fov[0] != '-') fobs = (obs_t *)malloc(sizeof(obs_t));
+  if (!prof || !atm_off || !rays || !ray_atm || !res || !ares || (naero && (!aero1 || !bq)) ||
       (ctl->fov[0] != '-' && !fobs)) {
     st = JSC_ERR_NOMEM;
     goto done;
   }
   for (int id = 0; id < nd; id++)
     for (int ir = 0; ir < nr; ir++) mask[(size_t)id * nr + ir] = !isfinite(obs->rad[id][ir]);
-  jsc_atm2x(ctl, atm, aero, x0, iqa, ipa);
-  for (size_t j = 0; j < n; j++) {
-    h[j] = perturbation(ctl, iqa[j], x0[j]);
-    if (h[j] <= 0) {
-      jsc_set_error(JSC_ERR_ARG, "jsc_kernel: cannot set perturbation size");
-      st = JSC_ERR_ARG;
-      goto done;
-    }
-  }
 
   {
     double *z = prof, *lon = z + nl, *lat = lon + nl, *p = lat + nl, *t = p + nl;
@@ -542,10 +575,12 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
       memcpy(t + o, atm->t, np * sizeof(double));
       for (int ig = 0; ig < ng; ig++) memcpy(q + (size_t)ig * nl + o, atm->q[ig], np * sizeof(double));
       for (int iw = 0; iw < nw; iw++) memcpy(kx + (size_t)iw * nl + o, atm->k[iw], np * sizeof(double));
-      if (a == 0) continue;
-      /* disturbed profile a: element a-1 of the state vector + h, then the
-       * hydrostatic balance formod applies to it */
-      const size_t j = a - 1;
+    }
+    /* disturbed profiles: state element + h, then the hydrostatic balance
+     * formod applies to them */
+    for (size_t j = 0; j < n; j++) {
+      if (col[j] < 1) continue;
+      const size_t o = (size_t)col[j] * np;
       *element(ctl, iqa[j], ipa[j], p + o, t + o, q + o, kx + o, nl) = x0[j] + h[j];
       jsc_hydrostatic(ctl->hydz, np, z + o, lon + o, lat + o, t + o,
                       ig_h2o >= 0 ? q + (size_t)ig_h2o * nl + o : NULL, p + o);
@@ -600,6 +635,34 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
       if (!st) st = jsc_batch_upload(g_jbatch, &in, NULL);
       if (!st) st = jsc_batch_run(g_jbatch, NULL);
       if (!st) st = jsc_batch_download(g_jbatch, &out, NULL);
+      /* aerosol parameters: the undisturbed profile with the optical
+       * properties of the disturbed parameter, one run each */
+      for (size_t j = 0; j < n && !st; j++) {
+        if (col[j] >= 0) continue;
+        memcpy(aero1, aero, sizeof(aero_t));
+        *aero_element(ctl, iqa[j], aero1) = x0[j] + h[j];
+        st = jsc_get_opt_prop(ctl, aero1);
+        double *ar = ares + (size_t)(-1 - col[j]) * nr * (2 * (size_t)nd + 3);
+        jsc_batch_input in1 = in;
+        int off1[2] = {0, np};
+        in1.n_atm = 1;
+        in1.n_levels = np;
+        in1.atm_off = off1;
+        in1.q = bq;       /* the undisturbed profile's blocks, [ng][np], [nw][np] */
+        in1.k = bk;
+        in1.n_rays = nr;  /* the first profile's rays, all on profile 0 */
+        jsc_batch_output out1;
+        memset(&out1, 0, sizeof(out1));
+        out1.rad = ar;
+        out1.tau = ar + (size_t)nr * nd;
+        out1.tpz = ar + 2 * (size_t)nr * nd;
+        out1.tplon = out1.tpz + nr;
+        out1.tplat = out1.tplon + nr;
+        if (!st) st = jsc_batch_set_aero(g_jbatch, aero1);
+        if (!st) st = jsc_batch_upload(g_jbatch, &in1, NULL);
+        if (!st) st = jsc_batch_run(g_jbatch, NULL);
+        if (!st) st = jsc_batch_download(g_jbatch, &out1, NULL);
+      }
       pthread_mutex_unlock(&g_lock);
     }
     if (st) goto done;
@@ -634,16 +697,25 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
     /* Disturbed columns: the measurement vector of each disturbed forward
      * model (obs2y of a copy of obs, whose non-finite entries stay masked). */
     for (size_t j = 0; j < n; j++) {
-      const size_t r0 = (j + 1) * nr;
+      const double *cr, *ct, *cz;  /* column's rad, tau [nr][nd], tpz [nr] */
+      if (col[j] >= 1) {
+        cr = rad + (size_t)col[j] * nr * nd;
+        ct = tau + (size_t)col[j] * nr * nd;
+        cz = tp + (size_t)col[j] * nr;
+      } else {
+        cr = ares + (size_t)(-1 - col[j]) * nr * (2 * (size_t)nd + 3);
+        ct = cr + (size_t)nr * nd;
+        cz = ct + (size_t)nr * nd;
+      }
       if (fov) {
         /* the disturbed results through the same convolution */
         fobs->nr = nr;
         for (int ir = 0; ir < nr; ir++) {
           fobs->time[ir] = obs->time[ir];
-          fobs->tpz[ir] = tp[r0 + ir];
+          fobs->tpz[ir] = cz[ir];
           for (int id = 0; id < nd; id++) {
-            fobs->rad[id][ir] = rad[(r0 + ir) * nd + id];
-            fobs->tau[id][ir] = tau[(r0 + ir) * nd + id];
+            fobs->rad[id][ir] = cr[(size_t)ir * nd + id];
+            fobs->tau[id][ir] = ct[(size_t)ir * nd + id];
           }
         }
         if ((st = fov_convolve(ctl, fobs))) goto done;
@@ -654,7 +726,7 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
           if (!isfinite(obs->rad[id][ir])) continue;
           const double v = fov ? (ctl->write_bbt ? brightness(fobs->rad[id][ir], ctl->nu[id])
                                                  : fobs->rad[id][ir])
-                               : out_rad(ctl, rad, r0 + ir, id);
+                               : out_rad(ctl, cr, (size_t)ir, id);
           if (!isfinite(v)) continue;
           if (c < m) y1[c] = v;
           c++;
@@ -675,12 +747,16 @@ done:
   free(h);
   free(iqa);
   free(ipa);
+  free(col);
   free(mask);
   free(prof);
   free(atm_off);
   free(rays);
   free(ray_atm);
   free(res);
+  free(ares);
+  free(bq);
+  free(aero1);
   free(fobs);
   return st;
 }

@@ -203,6 +203,15 @@ def _kernel_child(job):
                 if mask[ir][id_]:
                     rad[id_, ir] = np.nan
     aero = S.AeroT()
+    if job.get("aerofile"):
+        # the modes only: formod derives the optical properties itself for
+        # aerosol retrievals (src/forwardmodel.c:34-36)
+        lib.read_aero.argtypes = [C.c_char_p, C.c_char_p, P(S.CtlT), P(S.AeroT)]
+        lib.get_opt_prop.argtypes = [P(S.CtlT), P(S.AeroT)]
+        os.chdir(job["cwd"])
+        lib.read_aero(None, job["aerofile"].encode(), C.byref(ctl), C.byref(aero))
+        if not (ctl.retnn or ctl.retrr or ctl.retss):
+            lib.get_opt_prop(C.byref(ctl), C.byref(aero))
     m = lib.obs2y(C.byref(ctl), C.byref(obs), None, None, None)
     n = lib.atm2x(C.byref(ctl), C.byref(atm), C.byref(aero), None, None, None)
     k = lib.gsl_matrix_alloc(m, n)
@@ -276,11 +285,13 @@ def reference_state_vector(ctl_kw, atm, rad, scale=1.0, shift=0.0, timeout=600):
                    "scale": scale, "shift": shift}, timeout)
 
 
-def reference_kernel(ctl_kw, atm, geom, mask=None, timeout=3600):
+def reference_kernel(ctl_kw, atm, geom, mask=None, timeout=3600, aerofile=None, cwd=None):
     """Jacobian of the reference's kernel() for one profile (dict) and the
-    rays of geom; mask [n_rays][nd] marks observations set to NaN."""
+    rays of geom; mask [n_rays][nd] marks observations set to NaN; aerofile
+    (read in cwd) supplies the aerosol/cloud modes."""
     return _spawn({"kernel_job": True, "ctl": ctl_kw, "atm": atm, "geom": geom,
-                   "mask": None if mask is None else np.asarray(mask, bool)}, timeout)
+                   "mask": None if mask is None else np.asarray(mask, bool),
+                   "aerofile": aerofile, "cwd": cwd}, timeout)
 
 
 PORT_LIB = os.path.join(HERE, "build", "libjscat_oracle.so")

@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov]
+    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov|aerojac]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -171,6 +171,26 @@ def jacobian_fixture(workdir, name, bt, fov=False):
         **{"geom_" + k: v for k, v in geom.items()})
 
 
+def aerosol_jacobian_case(workdir):
+    """Aerosol extinction (beta_e) through the sulfate-like layer, state
+    vector temperature 10-30 km plus the layer's number concentration,
+    median radius and width (RETNN/RETRR/RETSS)."""
+    ctlkw, atm, geom, aerofile = aerosol_case(workdir, 0, sca_ext="beta_e")
+    ctlkw = dict(ctlkw, rett_zmin=10.0, rett_zmax=30.0, retnn=1, retrr=1, retss=1)
+    return ctlkw, atm, geom, aerofile
+
+
+def aerosol_jacobian_fixture(workdir):
+    ctlkw, atm, geom, aerofile = aerosol_jacobian_case(workdir)
+    ref = refrun.reference_kernel(ctlkw, atm, geom, aerofile=aerofile,
+                                  cwd=os.path.dirname(aerofile))
+    np.savez_compressed(
+        os.path.join(HERE, "jacobian_aerosol.npz"), k=ref["k"], x0=ref["x0"], iqa=ref["iqa"],
+        ipa=ref["ipa"], rad=ref["rad"], p=ref["p"],
+        table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
+        **{"geom_" + k: v for k, v in geom.items()})
+
+
 def fov_fixtures(workdir):
     """formod and kernel() with the field of view of fov_case."""
     ctlkw, atm, geom = fov_case(workdir)
@@ -191,6 +211,9 @@ def main():
         return
     if sys.argv[1:] == ["fov"]:
         fov_fixtures(workdir)
+        return
+    if sys.argv[1:] == ["aerojac"]:
+        aerosol_jacobian_fixture(workdir)
         return
     if sys.argv[1:] == ["aero"]:
         aero_fixture(workdir, "aero_layers8", synth.layered_aero_files, list(synth.CFG2_NU[::2]),
@@ -230,6 +253,7 @@ def main():
     jacobian_fixture(workdir, "jacobian_limb", False)
     jacobian_fixture(workdir, "jacobian_limb_bt", True)
     fov_fixtures(workdir)
+    aerosol_jacobian_fixture(workdir)
     print("fixtures written to", HERE)
 
 

@@ -90,3 +90,32 @@ def test_kernel_column_is_two_formods(workdir):
         api.formod(ctl2, a2, obs3)
         y1 = api.obs2y(ctl2, obs3)[0]
         np.testing.assert_array_equal(k[:, j], (y1 - y0) / h)
+
+
+def test_kernel_aerosol_parameters(workdir):
+    """Temperature plus the aerosol layer's number concentration, median
+    radius and width (RETNN/RETRR/RETSS) through aerosol extinction: the
+    optical properties of every aerosol column are recomputed (Mie on the
+    GPU) and the column runs as its own batch; against the reference's
+    kernel(), which calls its get_opt_prop inside every formod."""
+    from jscat import api, structs as S
+    from make_golden_shim import aerosol_jacobian_case, tables_digest
+    ctlkw, atm, geom, aerofile = aerosol_jacobian_case(workdir)
+    g = dict(np.load(os.path.join(GOLDEN, "jacobian_aerosol.npz")))
+    assert tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]) == str(g["table_sha256"])
+    ctl = S.make_ctl(**ctlkw)
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm.get("k"))
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"],
+                     geom["obslon"], geom["vplon"], geom["time"])
+    aero = api.read_aero(ctl, aerofile)
+    k = api.kernel(ctl, a, obs, aero)
+    kref = g["k"]
+    assert k.shape == kref.shape
+    x, iqa, ipa = api.atm2x(ctl, a, aero)
+    np.testing.assert_array_equal(iqa, g["iqa"])
+    assert max_rel(x, g["x0"]) <= 1e-12
+    rad = S.arr(obs.rad)[:ctl.nd, :obs.nr].T
+    assert max_rel(rad, g["rad"]) <= REL_TOL
+    scale = np.max(np.abs(kref), axis=0)
+    err = np.abs(k - kref) / np.where(scale > 0, scale, 1.0)
+    assert float(err.max()) <= K_TOL

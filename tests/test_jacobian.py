@@ -73,8 +73,8 @@ def test_empty_state_vector():
 
 
 def test_kernel_refusals_before_device_work():
-    """Aerosol parameters in the state vector and a matrix of the wrong
-    width are refused on the host, with the reference's message."""
+    """A matrix of the wrong width, and aerosol parameters in the state
+    vector without aerosol data, are refused on the host."""
     from jscat import api, lib as L, structs as S
     lib = L.load()
     ctlkw, atm = _case()
@@ -87,6 +87,5 @@ def test_kernel_refusals_before_device_work():
                         ctl.nd, n + 1, n + 1)
     assert st == 1 and b"state vector" in lib.jsc_last_error_message()
     ctl.retnn = 1
-    st = lib.jsc_kernel(C.byref(ctl), C.byref(a), C.byref(obs), C.byref(S.AeroT()), kp,
-                        ctl.nd, n, n)
-    assert st == 9 and b"RETNN" in lib.jsc_last_error_message()
+    st = lib.jsc_kernel(C.byref(ctl), C.byref(a), C.byref(obs), None, kp, ctl.nd, n + 1, n + 1)
+    assert st == 1 and b"aerosol" in lib.jsc_last_error_message()
