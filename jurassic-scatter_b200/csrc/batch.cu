@@ -38,6 +38,7 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   cudaFree(b->d_z);
   cudaFree(b->d_lon);
   cudaFree(b->d_lat);
+  cudaFree(b->d_psurf);
   cudaFree(b->d_p_in);
   cudaFree(b->d_t);
   cudaFree(b->d_q);
@@ -101,9 +102,19 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
     jsc_set_error(JSC_ERR_ARG, "jsc_batch_create: ctl does not match the model");
     return JSC_ERR_ARG;
   }
-  if (ctl->ip != 1) {
-    jsc_set_error(JSC_ERR_UNSUPPORTED, "only IP=1 (profile interpolation) runs on the GPU");
+  if (ctl->ip < 1 || ctl->ip > 3) {
+    jsc_set_error(JSC_ERR_ARG, "unknown interpolation method IP=%d", ctl->ip);
+    return JSC_ERR_ARG;
+  }
+  if (ctl->ip != 1 && ctl->sca_n > 0) {
+    jsc_set_error(JSC_ERR_UNSUPPORTED,
+                  "IP=%d with aerosol/cloud layers (the 3-D scattering source and the "
+                  "horizontally interpolated layer refinement are not on the GPU)", ctl->ip);
     return JSC_ERR_UNSUPPORTED;
+  }
+  if (ctl->ip == 3 && !(ctl->cz > 0 && ctl->cx > 0)) {
+    jsc_set_error(JSC_ERR_ARG, "IP=3 needs positive influence lengths CZ, CX");
+    return JSC_ERR_ARG;
   }
   JSC_CUDA_TRY(cudaSetDevice(m->device));
   jsc_batch *b = (jsc_batch *)calloc(1, sizeof(jsc_batch));
@@ -135,6 +146,11 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   st = st ? st : jsc_dmalloc(&b->d_z, (size_t)max_levels);
   st = st ? st : jsc_dmalloc(&b->d_lon, (size_t)max_levels);
   st = st ? st : jsc_dmalloc(&b->d_lat, (size_t)max_levels);
+  b->ip = ctl->ip;
+  b->cz = ctl->cz;
+  b->cx = ctl->cx;
+  if (ctl->ip != 1)
+    st = st ? st : jsc_dmalloc(&b->d_psurf, 3 * (size_t)(max_levels > max_atm ? max_levels : max_atm));
   st = st ? st : jsc_dmalloc(&b->d_p_in, (size_t)max_levels);
   st = st ? st : jsc_dmalloc(&b->d_t, (size_t)max_levels);
   st = st ? st : jsc_dmalloc(&b->d_q, (size_t)max_levels * ng);
@@ -493,6 +509,21 @@ static void fill_ray_args(const jsc_batch *b, RayArgs &ra) {
   ra.tsurf = b->d_tsurf;
   ra.tp = b->d_tp;
   ra.status = b->d_status;
+  ra.ip = b->ip;
+  ra.n_prof = b->n_atm;
+  ra.psurf = b->d_psurf;
+  ra.lat = b->d_lat;
+  ra.cz = b->cz;
+  ra.cx = b->cx;
+}
+
+// Counting or storing ray-tracing pass with the batch's interpolation.
+template <bool STORE>
+static void launch_raytrace(const jsc_batch *b, const RayArgs &ra, cudaStream_t s) {
+  const unsigned g = (unsigned)((ra.n_rays + 127) / 128);
+  if (b->ip == 2) raytrace_kernel<STORE, 2><<<g, 128, 0, s>>>(ra);
+  else if (b->ip == 3) raytrace_kernel<STORE, 3><<<g, 128, 0, s>>>(ra);
+  else raytrace_kernel<STORE><<<g, 128, 0, s>>>(ra);
 }
 
 static int batch_run(jsc_batch *b, cudaStream_t s);
@@ -928,7 +959,13 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   ra.nlos = refine ? b->d_nlos_b : b->d_nlos;
   ra.los_off = refine ? b->d_los_off_b : b->d_los_off;
   ev_record(b, JSC_T_RAYTRACE, 0, s);
-  raytrace_kernel<false><<<(nr + 127) / 128, 128, 0, s>>>(ra);
+  if (b->ip != 1) {  // surface positions of the profiles (IP 2) or levels (IP 3)
+    const int n = b->ip == 2 ? b->n_atm : b->n_levels;
+    psurf_kernel<<<(n + 127) / 128, 128, 0, s>>>(n, b->ip == 3, b->d_atm_off, b->d_lon, b->d_lat,
+                                                 b->d_psurf);
+    JSC_LAUNCH_CHECK();
+  }
+  launch_raytrace<false>(b, ra, s);
   JSC_LAUNCH_CHECK();
   scan_kernel<<<1, 1024, 0, s>>>(ra.nlos, nr, (int64_t *)ra.los_off);
   JSC_LAUNCH_CHECK();
@@ -966,7 +1003,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     ra.pts = b->d_pts;
     ra.max_seg = b->max_seg;
   }
-  raytrace_kernel<true><<<(nr + 127) / 128, 128, 0, s>>>(ra);
+  launch_raytrace<true>(b, ra, s);
   JSC_LAUNCH_CHECK();
   if (refine) {
     if (b->fixed) {  // keep the refinement's reads inside the base buffer

@@ -46,7 +46,7 @@ static int same_switches(const ctl_t *a, const ctl_t *b) {
          a->ctm_n2 == b->ctm_n2 && a->ctm_o2 == b->ctm_o2 &&
          a->refrac == b->refrac && a->rayds == b->rayds &&
          a->raydz == b->raydz && a->sca_n == b->sca_n &&
-         a->sca_mult == b->sca_mult && a->ip == b->ip &&
+         a->sca_mult == b->sca_mult && a->ip == b->ip && a->cz == b->cz && a->cx == b->cx &&
          a->transs == b->transs && !strcmp(a->sca_ext, b->sca_ext);
 }
 
@@ -84,7 +84,8 @@ static int ensure_cache(const ctl_t *ctl) {
     ctl_t c2;
     memcpy(&c2, ctl, sizeof(ctl_t));
     c2.hydz = -999;
-    if ((st = jsc_batch_create(g_model, &c2, 1, NPMAX, NRMAX, 0, &g_batch))) return st;
+    /* up to NPMAX / 2 profiles: an IP=2 atmosphere of two-level profiles */
+    if ((st = jsc_batch_create(g_model, &c2, NPMAX / 2, NPMAX, NRMAX, 0, &g_batch))) return st;
   }
   return JSC_OK;
 }
@@ -236,10 +237,23 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
       double *tau = rad + (size_t)nr * nd, *tp = tau + (size_t)nr * nd;
       for (int ig = 0; ig < ng; ig++) memcpy(q + (size_t)ig * np, atm->q[ig], np * sizeof(double));
       for (int iw = 0; iw < nw; iw++) memcpy(k + (size_t)iw * np, atm->k[iw], np * sizeof(double));
-      int off[2] = {0, np};
+      /* Profiles: one (IP 1, and IP 3, whose points are weighted one by
+       * one), or for IP 2 a new one wherever lon/lat change, as
+       * intpol_atm_2d groups them (src/atmosphere.c:343-356). */
+      int *off = (int *)malloc(((size_t)np + 1) * sizeof(int)), n_atm = 1;
+      if (!off) {
+        st = JSC_ERR_NOMEM;
+      } else {
+        off[0] = 0;
+        if (ctl->ip == 2)
+          for (int ip = 1; ip < np; ip++)
+            if (atm->lon[ip] != atm->lon[ip - 1] || atm->lat[ip] != atm->lat[ip - 1])
+              off[n_atm++] = ip;
+        off[n_atm] = np;
+      }
       jsc_batch_input in;
       memset(&in, 0, sizeof(in));
-      in.n_atm = 1;
+      in.n_atm = n_atm;
       in.n_levels = np;
       in.atm_off = off;
       in.z = atm->z;
@@ -267,7 +281,7 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
       out.tplat = tp + 2 * nr;
       /* Aerosol/cloud layers and optical properties (read_aero +
        * get_opt_prop of the caller, or of this call for retrievals). */
-      if (ctl->sca_n > 0) st = jsc_batch_set_aero(g_batch, aero);
+      if (!st && ctl->sca_n > 0) st = jsc_batch_set_aero(g_batch, aero);
       if (!st) st = jsc_batch_upload(g_batch, &in, NULL);
       if (!st) st = jsc_batch_run(g_batch, NULL);
       if (!st) st = jsc_batch_download(g_batch, &out, NULL);
@@ -282,6 +296,7 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
           }
         }
       }
+      free(off);
     }
     free(ray_atm);
   }
@@ -473,6 +488,12 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
     jsc_set_error(JSC_ERR_ARG, "jsc_kernel: invalid sizes (nd=%d ng=%d nw=%d nr=%d np=%d)",
                   nd, ng, nw, nr, np);
     return JSC_ERR_ARG;
+  }
+  if (ctl->ip != 1) {
+    jsc_set_error(JSC_ERR_UNSUPPORTED,
+                  "jsc_kernel: IP=%d (each column would need its own horizontally varying "
+                  "atmosphere)", ctl->ip);
+    return JSC_ERR_UNSUPPORTED;
   }
   const int aero_ret = ctl->retnn || ctl->retrr || ctl->retss;
   if ((ctl->sca_n > 0 || aero_ret) && !aero) {

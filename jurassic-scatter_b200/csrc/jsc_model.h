@@ -81,6 +81,9 @@ struct jsc_batch {
   double *d_z, *d_lon, *d_lat, *d_p_in, *d_t, *d_q, *d_k;
   double *d_p;              // pressure after hydrostatic balance
   double *d_zmin, *d_zmax;  // per profile
+  int ip;                   // atmosphere interpolation (1 profile, 2, 3)
+  double cz, cx;            // IP 3 influence lengths [km]
+  double *d_psurf;          // IP 2/3 surface positions [profiles or levels][3]
   int *d_ray_atm;
   double *d_ray;            // [9][max_rays]: time obsz obslon obslat vpz vplon vplat + 2 spare
 

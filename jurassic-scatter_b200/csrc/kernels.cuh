@@ -80,6 +80,12 @@ struct RayArgs {
   const double *grid_p, *grid_t;
   const int *grid_nt;
   int raw_q;  // store volume mixing ratios instead of column densities
+  // IP 2/3 (horizontally varying atmosphere, src/atmosphere.c:324-482):
+  // every profile of the batch belongs to the one atmosphere; psurf holds
+  // the surface Cartesian position of each profile (IP 2) or level (IP 3)
+  int ip, n_prof;
+  const double *psurf, *lat;
+  double cz, cx;
 };
 
 struct Profile {
@@ -108,6 +114,97 @@ __device__ __forceinline__ int atm_full(const Profile &a, double z0, double *p,
 __device__ __forceinline__ double atm_lin(const double *v, const Profile &a,
                                           int ip, double z0) {
   return jsc_lin(a.z[ip], v[ip], a.z[ip + 1], v[ip + 1], z0);
+}
+
+__device__ __forceinline__ double dist2(const double *a, const double *b) {
+  return (a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) +
+         (a[2] - b[2]) * (a[2] - b[2]);
+}
+
+// Atmospheric state at (z0, lon0, lat0) for IP 2 and 3: p, T and, when qk
+// is given, the VMRs [ng] then the extinctions [nw].
+// IP 2 (intpol_atm_2d, src/atmosphere.c:324-418): the two profiles nearest
+// in horizontal distance, each interpolated vertically (intpol_atm_1d),
+// blended linearly by the position between them.
+// IP 3 (intpol_atm_3d, :422-482): every level within cz vertically and cx
+// horizontally (and in latitude), weighted (1 - dz/cz)(1 - dx/cx).
+template <int IP>
+__device__ void atm_geo(const RayArgs &A, double z0, double lon0, double lat0, double *p,
+                        double *t, double *qk) {
+  double x0[3];
+  jsc_geo2cart(0, lon0, lat0, x0);
+  const int nq = A.ng + A.nw;
+  const size_t nl = (size_t)A.n_levels;
+  if (IP == 2) {
+    double dmin0 = 1e99, dmin1 = 1e99;
+    int ix0 = 0, ix1 = 0;
+    for (int ix = 0; ix < A.n_prof; ix++) {
+      const double dh = dist2(x0, A.psurf + 3 * ix);
+      if (dh <= dmin0) {
+        dmin1 = dmin0;
+        ix1 = ix0;
+        dmin0 = dh;
+        ix0 = ix;
+      } else if (dh <= dmin1) {
+        dmin1 = dh;
+        ix1 = ix;
+      }
+    }
+    const int lo0 = A.atm_off[ix0], lo1 = A.atm_off[ix1];
+    const int i0 = lo0 + jsc_locate(A.z + lo0, A.atm_off[ix0 + 1] - lo0, z0);
+    const int i1 = lo1 + jsc_locate(A.z + lo1, A.atm_off[ix1 + 1] - lo1, z0);
+    const double p0 = jsc_exp_interp(A.z[i0], A.p[i0], A.z[i0 + 1], A.p[i0 + 1], z0);
+    const double t0 = jsc_lin(A.z[i0], A.t[i0], A.z[i0 + 1], A.t[i0 + 1], z0);
+    const double p1 = jsc_exp_interp(A.z[i1], A.p[i1], A.z[i1 + 1], A.p[i1 + 1], z0);
+    const double t1 = jsc_lin(A.z[i1], A.t[i1], A.z[i1 + 1], A.t[i1 + 1], z0);
+    const double x2 = dist2(A.psurf + 3 * ix0, A.psurf + 3 * ix1);
+    const double x = sqrt(x2);
+    const double r0 = (dmin0 - dmin1 + x2) / (2 * x), r1 = x - r0;
+    const double r = r0 <= 0 ? 0 : (r1 <= 0 ? 1 : r0 / (r0 + r1));
+    *p = (1 - r) * p0 + r * p1;
+    *t = (1 - r) * t0 + r * t1;
+    if (qk)
+      for (int c = 0; c < nq; c++) {
+        const double *v = c < A.ng ? A.q + (size_t)c * nl : A.k + (size_t)(c - A.ng) * nl;
+        const double a0 = jsc_lin(A.z[i0], v[i0], A.z[i0 + 1], v[i0 + 1], z0);
+        const double a1 = jsc_lin(A.z[i1], v[i1], A.z[i1 + 1], v[i1 + 1], z0);
+        qk[c] = (1 - r) * a0 + r * a1;
+      }
+  } else {
+    double wsum = 0, sp = 0, st = 0;
+    if (qk)
+      for (int c = 0; c < nq; c++) qk[c] = 0;
+    for (int ip = 0; ip < A.n_levels; ip++) {
+      const double dz = fabs(A.z[ip] - z0);
+      if (dz > A.cz) continue;
+      if (fabs(A.lat[ip] - lat0) * 111.13 > A.cx) continue;
+      const double dx2 = dist2(x0, A.psurf + 3 * (size_t)ip);
+      if (dx2 > A.cx * A.cx) continue;
+      const double w = (1 - dz / A.cz) * (1 - sqrt(dx2) / A.cx);
+      wsum += w;
+      sp += w * A.p[ip];
+      st += w * A.t[ip];
+      if (qk)
+        for (int c = 0; c < nq; c++) {
+          const double *v = c < A.ng ? A.q + (size_t)c * nl : A.k + (size_t)(c - A.ng) * nl;
+          qk[c] += w * v[ip];
+        }
+    }
+    *p = sp / wsum;
+    *t = st / wsum;
+    if (qk)
+      for (int c = 0; c < nq; c++) qk[c] /= wsum;
+  }
+}
+
+// Surface Cartesian positions for IP 2 (first level of each profile) and
+// IP 3 (every level).
+static __global__ void psurf_kernel(int n, int per_level, const int *atm_off, const double *lon,
+                                    const double *lat, double *psurf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int l = per_level ? i : atm_off[i];
+  jsc_geo2cart(0, lon[l], lat[l], psurf + 3 * (size_t)i);
 }
 
 // One LOS point: geometry, state, raw step.  Written by the storing pass.
@@ -140,6 +237,32 @@ __device__ __forceinline__ void emit_point(const RayArgs &A, const Profile &a,
   }
 }
 
+// emit_point for IP 2/3 with the state interpolated horizontally: qk
+// holds the VMRs [ng] then the extinctions [nw] at the point.
+__device__ __forceinline__ void emit_point_geo(const RayArgs &A, int64_t idx, double z,
+                                               double lon, double lat, double p, double t,
+                                               const double *qk, double raw_ds, double ds) {
+  double *g = A.geo + idx * 4;
+  g[0] = z;
+  g[1] = lon;
+  g[2] = lat;
+  g[3] = raw_ds;
+  double *r = A.pts + idx * A.W;
+  r[REC_P] = p;
+  r[REC_T] = t;
+  r[REC_DS] = ds;
+  r[REC_QH2O] = A.ig_h2o >= 0 ? qk[A.ig_h2o] : 0.0;
+  r[REC_GRID] = A.grid_p ? (double)grid_code(A.grid_np, A.grid_p, A.grid_nt, A.grid_t, p, t) : -1.0;
+  r[REC_PLK] = (double)planck_index(t);
+  r[REC_AF] = 0.0;
+  r[REC_AI] = -999.0;
+  for (int w = 0; w < A.nw; w++) r[REC_K + w] = qk[A.ng + w];
+  for (int g2 = 0; g2 < A.ng; g2++) {
+    const double q = qk[g2];
+    r[REC_K + A.nw + g2] = A.raw_q ? q : 10 * q * p / (JSC_KBOLTZ * t) * ds;
+  }
+}
+
 // Observer and view point of one ray.
 struct RayIn {
   double obsz, obslon, obslat, vpz, vplon, vplat;
@@ -159,7 +282,7 @@ struct RayEnd {
 // point and surface temperature of ray r.  MODE 2 (ends): counts like
 // MODE 0 and reports the last two points and the surface temperature in
 // *end.
-template <int MODE>
+template <int MODE, int IP = 1>
 __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayEnd *end) {
   constexpr bool STORE = MODE == 1;
   const int lo = A.atm_off[ai];
@@ -171,7 +294,16 @@ __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayE
   a.t = A.t + lo;
   a.q = A.q + lo;
   a.k = A.k + lo;
-  const double zmin = A.zmin[ai], zmax = A.zmax[ai];
+  double zmin = A.zmin[ai], zmax = A.zmax[ai];
+  if (IP != 1) {  // the range of the whole atmosphere (src/lineofsight.c:26-27)
+    zmin = A.zmin[0];
+    zmax = A.zmax[0];
+    for (int ix = 1; ix < A.n_prof; ix++) {
+      zmin = A.zmin[ix] < zmin ? A.zmin[ix] : zmin;
+      zmax = A.zmax[ix] > zmax ? A.zmax[ix] : zmax;
+    }
+  }
+  double qk[IP == 1 ? 1 : NGMAX + NWMAX];
   const double obsz = in.obsz, vpz = in.vpz;
   int64_t base = 0;
   if (STORE) {
@@ -248,7 +380,11 @@ __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayE
     }
     int ipz = 0;
     pp = pt = 0;
-    if (STORE || !stop) ipz = atm_full(a, pz, &pp, &pt);
+    if (IP == 1) {
+      if (STORE || !stop) ipz = atm_full(a, pz, &pp, &pt);
+    } else {
+      if (STORE || !stop) atm_geo<IP>(A, pz, plon, plat, &pp, &pt, STORE ? qk : nullptr);
+    }
     if (!stop) {
       p = pp;
       t = pt;
@@ -265,7 +401,10 @@ __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayE
         atomicOr(A.status, JSC_DEV_ERR_NLOS);
         return np;
       }
-      emit_point<true>(A, a, base + np, pz, plon, plat, pp, pt, ipz, pz, raw, dsm);
+      if (IP == 1)
+        emit_point<true>(A, a, base + np, pz, plon, plat, pp, pt, ipz, pz, raw, dsm);
+      else
+        emit_point_geo(A, base + np, pz, plon, plat, pp, pt, qk, raw, dsm);
     }
     np++;
     if (MODE == 2) {
@@ -293,12 +432,14 @@ __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayE
     if (A.refrac && z <= JSC_ZREFRAC) {
       for (int i = 0; i < 3; i++) xh[i] = x[i] + 0.5 * ds * ex0[i];
       jsc_cart2geo(xh, &z, &lon, &lat);
-      atm_pt(a, z, &p, &t);
+      if (IP == 1) atm_pt(a, z, &p, &t);
+      else atm_geo<IP>(A, z, lon, lat, &p, &t, nullptr);
       n = jsc_refractivity(p, t);
       for (int i = 0; i < 3; i++) {
         xh[i] += JSC_FD_STEP;
         jsc_cart2geo(xh, &z, &lon, &lat);
-        atm_pt(a, z, &p, &t);
+        if (IP == 1) atm_pt(a, z, &p, &t);
+        else atm_geo<IP>(A, z, lon, lat, &p, &t, nullptr);
         const double naux = jsc_refractivity(p, t);
         ng[i] = (naux - n) / JSC_FD_STEP;
         xh[i] -= JSC_FD_STEP;
@@ -368,17 +509,17 @@ __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayE
   return np;
 }
 
-template <bool STORE>
+template <bool STORE, int IP>
 __device__ __forceinline__ int trace_ray(const RayArgs &A, int r) {
   const RayIn in = {A.obsz[r], A.obslon[r], A.obslat[r], A.vpz[r], A.vplon[r], A.vplat[r]};
-  return trace_core<STORE ? 1 : 0>(A, A.ray_atm[r], r, in, nullptr);
+  return trace_core<STORE ? 1 : 0, IP>(A, A.ray_atm[r], r, in, nullptr);
 }
 
-template <bool STORE>
+template <bool STORE, int IP = 1>
 __global__ void __launch_bounds__(128) raytrace_kernel(RayArgs A) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= A.n_rays) return;
-  const int np = trace_ray<STORE>(A, r);
+  const int np = trace_ray<STORE, IP>(A, r);
   if (!STORE) A.nlos[r] = np;
   else if (np != A.nlos[r]) atomicOr(A.status, JSC_DEV_ERR_NLOS);
 }

@@ -197,6 +197,38 @@ CFG1_EMITTERS = ["CO2", "H2O", "O3", "N2O", "CH4", "HNO3", "CO", "CCl4"]
 CFG1_NU = list(np.linspace(700.0, 1400.0, 64))
 
 
+def curtain_case(directory, seed=20261203, n_prof=5, dlat=5.0):
+    """Clear-air limb case through a horizontally varying atmosphere for
+    IP=2/3: n_prof profiles along the meridian (latitudes dlat apart,
+    centred on the tangent points), temperature offsets of -4..+4 K and
+    H2O scaled by 0.7..1.3 across the track, one atm_t of n_prof x 121
+    points ordered profile by profile; 31 limb rays 5-35 km.  Returns
+    (ctl kwargs, atmosphere dict with lon/lat per point, geometry)."""
+    rng = np.random.default_rng(seed)
+    base = atmosphere(CFG0_EMITTERS, rng, t_sigma=0.0, vmr_sigma=0.05)
+    lats = dlat * (np.arange(n_prof) - (n_prof - 1) / 2.0)
+    nz = len(base["z"])
+    z, lon, lat, p, t, q, k = [], [], [], [], [], [], []
+    for i, la in enumerate(lats):
+        f = i / (n_prof - 1)
+        z.append(base["z"])
+        lon.append(np.zeros(nz))
+        lat.append(np.full(nz, la))
+        p.append(base["p"])
+        t.append(base["t"] + (8.0 * f - 4.0))
+        qq = np.array(base["q"], dtype=float)
+        qq[1] = qq[1] * (0.7 + 0.6 * f)
+        q.append(qq)
+        k.append(np.asarray(base.get("k", np.zeros((1, nz))), dtype=float))
+    atm = {"z": np.concatenate(z), "lon": np.concatenate(lon), "lat": np.concatenate(lat),
+           "p": np.concatenate(p), "t": np.concatenate(t), "q": np.concatenate(q, axis=1),
+           "k": np.concatenate(k, axis=1)}
+    geom = limb_geometry(5.0 + 1.0 * np.arange(31))
+    tb = write_tables(directory, CFG0_EMITTERS, CFG0_NU, seed)
+    ctlkw = dict(emitters=CFG0_EMITTERS, nus=CFG0_NU, tblbase=tb, hydz=0.0)
+    return ctlkw, atm, geom
+
+
 def clear_limb_case(directory, seed=20261203):
     """Clear-air limb case: 2 emitters, 4 channels, 61 rays with tangent
     heights 5-35 km every 0.5 km from 800 km, one profile.  Returns

@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov|aerojac]
+    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov|aerojac|ip]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -191,6 +191,28 @@ def aerosol_jacobian_fixture(workdir):
         **{"geom_" + k: v for k, v in geom.items()})
 
 
+# IP=3 influence lengths of the curtain fixtures [km]
+IP3_CZ, IP3_CX = 3.0, 700.0
+
+
+def curtain_ctl(ctlkw, ip):
+    return dict(ctlkw, ip=ip, cz=IP3_CZ, cx=IP3_CX) if ip == 3 else dict(ctlkw, ip=ip)
+
+
+def curtain_fixtures(workdir):
+    """formod through the horizontally varying curtain atmosphere with
+    IP=2 (two nearest profiles) and IP=3 (distance-weighted points)."""
+    ctlkw, atm, geom = synth.curtain_case(workdir)
+    ra = np.zeros(len(geom["obsz"]), int)
+    for ip in (2, 3):
+        ref = refrun.run(reference_ctl(curtain_ctl(ctlkw, ip)), [atm], ra, geom, los=True)
+        np.savez_compressed(
+            os.path.join(HERE, "curtain_ip%d.npz" % ip), rad=ref["rad"], tau=ref["tau"],
+            tpz=ref["tpz"], tplat=ref["tplat"], nlos=ref["nlos"],
+            table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
+            **{"geom_" + k: v for k, v in geom.items()})
+
+
 def fov_fixtures(workdir):
     """formod and kernel() with the field of view of fov_case."""
     ctlkw, atm, geom = fov_case(workdir)
@@ -214,6 +236,9 @@ def main():
         return
     if sys.argv[1:] == ["aerojac"]:
         aerosol_jacobian_fixture(workdir)
+        return
+    if sys.argv[1:] == ["ip"]:
+        curtain_fixtures(workdir)
         return
     if sys.argv[1:] == ["aero"]:
         aero_fixture(workdir, "aero_layers8", synth.layered_aero_files, list(synth.CFG2_NU[::2]),
@@ -254,6 +279,7 @@ def main():
     jacobian_fixture(workdir, "jacobian_limb_bt", True)
     fov_fixtures(workdir)
     aerosol_jacobian_fixture(workdir)
+    curtain_fixtures(workdir)
     print("fixtures written to", HERE)
 
 

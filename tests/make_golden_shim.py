@@ -3,5 +3,5 @@ import os
 import sys
 
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
-from make_golden import (aerosol_case, aerosol_jacobian_case, fov_case,  # noqa: E402,F401
-                         jacobian_case, mixed_case, tables_digest)
+from make_golden import (aerosol_case, aerosol_jacobian_case, curtain_ctl,  # noqa: E402,F401
+                         fov_case, jacobian_case, mixed_case, tables_digest)

@@ -75,6 +75,31 @@ def test_clear_limb_fov_formod(workdir):
     assert max_rel(tau, g["tau"]) <= REL_TOL
 
 
+@pytest.mark.parametrize("ip", [2, 3])
+def test_curtain_formod(workdir, ip):
+    """Drop-in formod through a horizontally varying atmosphere (five
+    profiles along the track): IP=2 blends the two nearest profiles, IP=3
+    weights every point within CZ/CX (src/atmosphere.c:324-482), in the ray
+    tracer's state and refraction lookups; against the reference."""
+    from jscat import structs as S, synth, api
+    from make_golden_shim import curtain_ctl
+    g = _load("curtain_ip%d" % ip)
+    ctlkw, atm, geom = synth.curtain_case(workdir)
+    _check_tables(g, ctlkw)
+    ctl = S.make_ctl(**curtain_ctl(ctlkw, ip))
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm["k"], atm["lon"], atm["lat"])
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"])
+    api.formod(ctl, a, obs)
+    nr, nd = obs.nr, ctl.nd
+    rad = S.arr(obs.rad)[:nd, :nr].T
+    tau = S.arr(obs.tau)[:nd, :nr].T
+    assert bt_error(rad, g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(rad, g["rad"]) <= REL_TOL
+    assert max_rel(tau, g["tau"]) <= REL_TOL
+    np.testing.assert_allclose(S.arr(obs.tpz)[:nr], g["tpz"], rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(S.arr(obs.tplat)[:nr], g["tplat"], rtol=1e-9, atol=1e-9)
+
+
 # EGA kernel families: -1 the default (variant 6 for clear air, 10 with
 # aerosol/cloud layers), 6 a thread per (ray, channel), 9 a lane per (ray,
 # channel, emitter)
