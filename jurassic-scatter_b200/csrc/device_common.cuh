@@ -254,10 +254,11 @@ __device__ __forceinline__ bool near_interval(const jsc_node *row, int last, flo
 // hint still brackets x1 and the extended column falls in the interval
 // k + dj guessed from the previous point's distance -- then one or two
 // node pairs (8 bytes a node) answer both lookups.  A guess off by one or
-// two intervals is corrected by near_interval; otherwise the exact
+// two intervals is corrected by near_interval (NEAR; kernels that inline
+// many ega_node copies leave it out for code size); otherwise the exact
 // searches above find the intervals, starting from the guesses.  *kout and
 // *jout receive the intervals (they do not depend on the guesses).
-template <bool DIG>
+template <bool DIG, bool NEAR = true>
 __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, jsc_row rd,
                                            double x1, double useg, int hint, int dj, int *kout,
                                            int *jout, unsigned long long *dig) {
@@ -271,7 +272,7 @@ __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, j
   const float x1f = __double2float_rd(x1);
   // bracket for x1 on eps: (e[k] <= x1 or k == 0) and (x1 < e[k+1] or k == last)
   if (!(strict && (!(a.y > x1f) || k == 0) && (b.y > x1f || k == last) && x1 == x1) &&
-      !(strict && x1 == x1 && near_interval<false>(row, last, x1f, &k, &a, &b))) {
+      !(NEAR && strict && x1 == x1 && near_interval<false>(row, last, x1f, &k, &a, &b))) {
     k = find_interval<false>(row, n, strict, x1, k);
     a = __ldg(reinterpret_cast<const float2 *>(row + k));
     b = __ldg(reinterpret_cast<const float2 *>(row + k + 1));
@@ -285,7 +286,7 @@ __device__ __forceinline__ double ega_node(const jsc_node *__restrict__ nodes, j
     b = __ldg(reinterpret_cast<const float2 *>(row + j + 1));
   }
   if (!(strict && (!(a.x > x2f) || j == 0) && (b.x > x2f || j == last) && x2 == x2) &&
-      !(strict && x2 == x2 && near_interval<true>(row, last, x2f, &j, &a, &b))) {
+      !(NEAR && strict && x2 == x2 && near_interval<true>(row, last, x2f, &j, &a, &b))) {
     const int j0 = j;
     j = find_interval<true>(row, n, strict, x2, j0);
     if (j != j0) {

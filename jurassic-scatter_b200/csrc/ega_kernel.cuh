@@ -104,13 +104,13 @@ __global__ void __launch_bounds__(BLK, MINB) ega_rt_kernel(EgaArgs A) {
             if (hc >= 0 && hc != code) hp = remap_hints(hp, hc, code);
             const unsigned dj = dj_l[g];
             int k00, k01, k10, k11, j00, j01, j10, j11;
-            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(hp & 0xffff),
+            const double e00 = ega_node<DIG, ROLL>(m.nodes, r00, x1, useg, (int)(hp & 0xffff),
                                              (int)(dj & 0xff), &k00, &j00, dg);
-            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((hp >> 16) & 0xffff),
+            const double e01 = ega_node<DIG, ROLL>(m.nodes, r01, x1, useg, (int)((hp >> 16) & 0xffff),
                                              (int)((dj >> 8) & 0xff), &k01, &j01, dg);
-            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((hp >> 32) & 0xffff),
+            const double e10 = ega_node<DIG, ROLL>(m.nodes, r10, x1, useg, (int)((hp >> 32) & 0xffff),
                                              (int)((dj >> 16) & 0xff), &k10, &j10, dg);
-            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(hp >> 48),
+            const double e11 = ega_node<DIG, ROLL>(m.nodes, r11, x1, useg, (int)(hp >> 48),
                                              (int)(dj >> 24), &k11, &j11, dg);
             JSC_HINT(g) = (unsigned long long)(j00 & 0xffff) | ((unsigned long long)(j01 & 0xffff) << 16) |
                           ((unsigned long long)(j10 & 0xffff) << 32) |
