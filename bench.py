@@ -524,6 +524,38 @@ def jacobian_bench(args, torch, cpu=True):
     return res
 
 
+def ingest_bench(ctlkw, atms, ray_atm, geom, cpu=True):
+    """Table ingest of the headline workload (512 emissivity tables, 1.4 GB):
+    jsc_model_create (parallel mapped reads, packed device layout), median
+    of three after a warm-up, beside the reference's first-call overhead
+    (its formod reads every table on the first call): the first call on one
+    ray minus a warm call."""
+    from jscat import api, structs as S
+    ctl = S.make_ctl(**ctlkw)
+    api.Model(ctl).close()
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        m = api.Model(ctl)
+        times.append(time.perf_counter() - t0)
+        tb = m.table_bytes
+        m.close()
+    res = {"workload": "emissivity tables of the headline workload", "tables": len(ctlkw["nus"]) *
+           len(ctlkw["emitters"]), "device_table_bytes": tb,
+           "seconds": float(np.median(times)),
+           "timing": "host wall clock around jsc_model_create (files in the page cache)"}
+    if cpu:
+        from oracle import refrun
+        if refrun.available():
+            sel = np.array([0])
+            sub = {k: v[sel] for k, v in geom.items()}
+            kw = dict(ctlkw, sca_mult=0)
+            first = refrun.run(kw, atms[:1], ray_atm[sel], sub, warmup=False)["seconds"]
+            warm = refrun.run(kw, atms[:1], ray_atm[sel], sub, warmup=True)["seconds"]
+            res["reference_first_call_overhead_s"] = first - warm
+    return res
+
+
 def optprop_bench(args, torch, cpu=True):
     """Aerosol/cloud optical properties (get_opt_prop, src/scatter.c:330-512)
     of the benchmark's layers: jsc_get_opt_prop (Mie series on the GPU, 170
@@ -765,6 +797,12 @@ def main():
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
     batch.close()
     model.close()
+    if rank == 0 and world == 1 and args.jacobians > 0:
+        try:
+            line["table_ingest"] = ingest_bench(ctlkw, atms, ray_atm, geom,
+                                                cpu=not args.no_cpu_baseline)
+        except Exception as exc:
+            line["table_ingest"] = {"error": str(exc)[:300]}
     sur = None
     if rank == 0 and world == 1 and args.sca_rays > 0:
         try:

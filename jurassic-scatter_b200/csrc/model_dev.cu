@@ -21,8 +21,9 @@ static std::atomic<uint64_t> g_launches{0};
 extern "C" void jsc_count_launch(void) { g_launches.fetch_add(1); }
 extern "C" uint64_t jsc_launch_count(void) { return g_launches.load(); }
 
-// One warp per row slot builds the row's nodes.
-__global__ void build_nodes_kernel(const jsc_row *rows, const int64_t *row_pt,
+// One warp per row slot builds the row's nodes and sets the row's
+// JSC_ROW_STRICT flag when u and eps both increase strictly along it.
+__global__ void build_nodes_kernel(jsc_row *rows, const int64_t *row_pt,
                                    int nrows, const float *u, const float *e,
                                    jsc_node *nodes) {
   const int lane = threadIdx.x & 31;
@@ -30,15 +31,17 @@ __global__ void build_nodes_kernel(const jsc_row *rows, const int64_t *row_pt,
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int r = warp; r < nrows; r += nwarps) {
     const int n = rows[r].nf & 0xffff;
-    if (n < 2) continue;
     const int64_t pt = row_pt[r];
     const int off = rows[r].off;
+    bool inc = true;
     for (int k = lane; k < n; k += 32) {
       jsc_node v;
       v.u = u[pt + k];
       v.e = e[pt + k];
-      nodes[off + k] = v;
+      if (n >= 2) nodes[off + k] = v;
+      if (k + 1 < n && (!(v.u < u[pt + k + 1]) || !(v.e < e[pt + k + 1]))) inc = false;
     }
+    if (__all_sync(0xffffffffu, inc) && lane == 0) rows[r].nf |= JSC_ROW_STRICT << 16;
   }
 }
 
@@ -142,15 +145,8 @@ static int model_upload(jsc_model *m, const jsc_host_model *hm) {
           int n = t->nu[ip][it];
           if (n < 0) n = 0;
           int64_t pt = t->off[ip][it];
-          int strict = 1;
-          for (int k = 0; k + 1 < n; k++)
-            if (!(ht->u[pt + k] < ht->u[pt + k + 1]) ||
-                !(ht->eps[pt + k] < ht->eps[pt + k + 1])) {
-              strict = 0;
-              break;
-            }
           rows[s].off = (int)niv;
-          rows[s].nf = n | (strict ? (JSC_ROW_STRICT << 16) : 0);
+          rows[s].nf = n;  /* build_nodes_kernel adds the strictness flag */
           row_pt[s] = pt;
           if (n >= 2) niv += n;
           if (niv > 0x7fffffff) {

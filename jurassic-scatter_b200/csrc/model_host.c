@@ -10,6 +10,10 @@
 #include <stdlib.h>
 #include <string.h>
 #include <strings.h>
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "jsc_internal.h"
 #include "ckd_tables.h"
@@ -201,6 +205,149 @@ static int read_table_tab(FILE *in, const char *fn, jsc_host_tables *ht,
   return JSC_OK;
 }
 
+/* ---------------------------------------------- parallel binary loading */
+
+/* A binary table file mapped into memory and walked with bounds checks. */
+typedef struct {
+  const unsigned char *data;
+  size_t size, pos;
+} bin_cursor;
+
+static int cur_read(bin_cursor *c, void *dst, size_t bytes) {
+  if (bytes > c->size - c->pos) return 0;
+  if (dst) memcpy(dst, c->data + c->pos, bytes);
+  c->pos += bytes;
+  return 1;
+}
+
+/* Table header and row sizes of a mapped .bin file (the layout of
+ * read_table_bin); returns its point count in *npts, or a JSC status with
+ * the message in msg (set by the calling thread afterwards: the error
+ * state is per thread). */
+static int scan_table_bin(bin_cursor *c, jsc_host_table *tb, int64_t *npts, const char **msg) {
+  int64_t n_all = 0;
+  if (!cur_read(c, &tb->np, sizeof(int))) goto bad;
+  if (tb->np > TBLNPMAX) {
+    *msg = "Too many pressure levels";
+    return JSC_ERR_TABLE;
+  }
+  if (tb->np < 0) tb->np = 0;
+  if (!cur_read(c, tb->p, sizeof(double) * (size_t)tb->np)) goto bad;
+  if (!cur_read(c, tb->nt, sizeof(int) * (size_t)tb->np)) goto bad;
+  for (int ip = 0; ip < tb->np; ip++) {
+    if (tb->nt[ip] > TBLNTMAX) {
+      *msg = "Too many temperatures";
+      return JSC_ERR_TABLE;
+    }
+    if (tb->nt[ip] < 0) tb->nt[ip] = 0;
+    if (!cur_read(c, tb->t[ip], sizeof(double) * (size_t)tb->nt[ip])) goto bad;
+    if (!cur_read(c, tb->nu[ip], sizeof(int) * (size_t)tb->nt[ip])) goto bad;
+    for (int it = 0; it < tb->nt[ip]; it++) {
+      int n = tb->nu[ip][it];
+      if (n > TBLNUMAX) {
+        *msg = "Too many column densities";
+        return JSC_ERR_TABLE;
+      }
+      if (n < 0) n = tb->nu[ip][it] = 0;
+      tb->off[ip][it] = (int64_t)c->pos;  /* file position of the row for now */
+      if (!cur_read(c, NULL, 2 * sizeof(float) * (size_t)n)) goto bad;
+      n_all += n;
+    }
+  }
+  *npts = n_all;
+  return JSC_OK;
+bad:
+  *msg = "Error while reading";
+  return JSC_ERR_FILE;
+}
+
+/* All tables in binary form: the files are mapped and scanned in parallel,
+ * placed back to back in table order (the layout of the serial reader),
+ * and their rows copied in parallel.  Returns 1 in *fallback, without
+ * touching ht, when a table is missing in binary form. */
+static int read_tables_bin_parallel(const ctl_t *ctl, jsc_host_tables *ht, int *fallback) {
+  const int nt = ctl->ng * ctl->nd;
+  *fallback = 0;
+  char (*names)[2 * LEN] = (char (*)[2 * LEN])malloc((size_t)(nt > 0 ? nt : 1) * 2 * LEN);
+  bin_cursor *cur = (bin_cursor *)calloc((size_t)(nt > 0 ? nt : 1), sizeof(bin_cursor));
+  int64_t *npts = (int64_t *)calloc((size_t)nt + 1, sizeof(int64_t));
+  int *tst = (int *)calloc((size_t)(nt > 0 ? nt : 1), sizeof(int));
+  const char **tmsg = (const char **)calloc((size_t)(nt > 0 ? nt : 1), sizeof(char *));
+  int st = JSC_OK;
+  if (!names || !cur || !npts || !tst || !tmsg) {
+    st = JSC_ERR_NOMEM;
+    goto out;
+  }
+  for (int i = 0; i < nt && !*fallback; i++) {
+    const int id = i / ctl->ng, ig = i % ctl->ng;
+    snprintf(names[i], 2 * LEN, "%s_%.4f_%s.bin", ctl->tblbase, ctl->nu[id], ctl->emitter[ig]);
+    if (access(names[i], R_OK)) *fallback = 1;
+  }
+  if (*fallback) goto out;
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < nt; i++) {
+    const int fd = open(names[i], O_RDONLY);
+    struct stat sb;
+    if (fd < 0 || fstat(fd, &sb)) {
+      tst[i] = JSC_ERR_FILE;
+      tmsg[i] = "Error while reading";
+      if (fd >= 0) close(fd);
+      continue;
+    }
+    void *map = sb.st_size > 0 ? mmap(NULL, (size_t)sb.st_size, PROT_READ, MAP_PRIVATE, fd, 0)
+                               : NULL;
+    close(fd);
+    if (sb.st_size > 0 && map == MAP_FAILED) {
+      tst[i] = JSC_ERR_FILE;
+      tmsg[i] = "Error while reading";
+      continue;
+    }
+    cur[i].data = (const unsigned char *)map;
+    cur[i].size = (size_t)sb.st_size;
+    tst[i] = scan_table_bin(&cur[i], &ht->tab[i], &npts[i], &tmsg[i]);
+  }
+  for (int i = 0; i < nt; i++)
+    if (tst[i]) {
+      jsc_set_error(tst[i], "%s in %s", tmsg[i], names[i]);
+      st = tst[i];
+      goto out;
+    }
+  {
+    int64_t total = 0;
+    for (int i = 0; i < nt; i++) {
+      const int64_t n = npts[i];
+      npts[i] = total;  /* first point of table i */
+      total += n;
+    }
+    if ((st = tables_reserve(ht, total + 1))) goto out;
+    ht->n_points = total;
+  }
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < nt; i++) {
+    jsc_host_table *tb = &ht->tab[i];
+    int64_t o = npts[i];
+    for (int ip = 0; ip < tb->np; ip++)
+      for (int it = 0; it < tb->nt[ip]; it++) {
+        const int n = tb->nu[ip][it];
+        const unsigned char *row = cur[i].data + tb->off[ip][it];
+        memcpy(ht->u + o, row, (size_t)n * sizeof(float));
+        memcpy(ht->eps + o, row + (size_t)n * sizeof(float), (size_t)n * sizeof(float));
+        tb->off[ip][it] = o;
+        o += n;
+      }
+  }
+out:
+  if (cur)
+    for (int i = 0; i < nt; i++)
+      if (cur[i].data) munmap((void *)cur[i].data, cur[i].size);
+  free(names);
+  free(cur);
+  free(npts);
+  free(tst);
+  free(tmsg);
+  return st;
+}
+
 static int read_tables(const ctl_t *ctl, jsc_host_tables *ht) {
   char fn[2 * LEN];
   float *ubuf = NULL, *ebuf = NULL;
@@ -210,6 +357,11 @@ static int read_tables(const ctl_t *ctl, jsc_host_tables *ht) {
   ht->tab = (jsc_host_table *)calloc((size_t)(ctl->ng * ctl->nd + 1),
                                      sizeof(jsc_host_table));
   if (!ht->tab) return JSC_ERR_NOMEM;
+  /* Every table in binary form: parallel mapped reads.  Otherwise (a .tab
+   * or missing table) the serial reader below, file by file. */
+  int fallback = 0;
+  st = read_tables_bin_parallel(ctl, ht, &fallback);
+  if (st || !fallback) return st;
   for (int id = 0; id < ctl->nd && !st; id++)
     for (int ig = 0; ig < ctl->ng && !st; ig++) {
       jsc_host_table *tb = &ht->tab[id * ctl->ng + ig];
