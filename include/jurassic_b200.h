@@ -155,8 +155,9 @@ typedef struct {
  * ------------------------------------------------------------------------ */
 
 /* Replaces formod (src/forwardmodel.c:15-116), for ctl->ip 1 (one
- * profile) and, in clear air, 2 (profiles split where lon/lat change,
- * the two nearest blended) and 3 (points weighted within ctl->cz, cx):
+ * profile) and, without scattering (sca_mult 0 or no aerosol), 2 (profiles
+ * split where lon/lat change, the two nearest blended) and 3 (points
+ * weighted within ctl->cz, cx):
  * saves the NaN mask of
  * obs->rad, applies hydrostatic balance to atm->p (ctl->hydz >= 0), traces
  * every ray, evaluates EGA transmittances, continua, Planck source and

@@ -106,10 +106,10 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
     jsc_set_error(JSC_ERR_ARG, "unknown interpolation method IP=%d", ctl->ip);
     return JSC_ERR_ARG;
   }
-  if (ctl->ip != 1 && ctl->sca_n > 0) {
+  if (ctl->ip != 1 && ctl->sca_n > 0 && ctl->sca_mult > 0) {
     jsc_set_error(JSC_ERR_UNSUPPORTED,
-                  "IP=%d with aerosol/cloud layers (the 3-D scattering source and the "
-                  "horizontally interpolated layer refinement are not on the GPU)", ctl->ip);
+                  "IP=%d with scattering (SCA_MULT > 0 needs the 3-D scattering source)",
+                  ctl->ip);
     return JSC_ERR_UNSUPPORTED;
   }
   if (ctl->ip == 3 && !(ctl->cz > 0 && ctl->cx > 0)) {
@@ -1014,6 +1014,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     // Layer-edge points, chord steps and aerosol factors
     // (add_aerosol_layers, src/lineofsight.c:193-372).
     RefineArgs fa;
+    memset(&fa, 0, sizeof(fa));
     fa.n_rays = nr;
     fa.ng = b->cfg.ng;
     fa.nw = b->cfg.nw;
@@ -1069,7 +1070,18 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     fa.geo = b->d_geo;
     fa.pts = b->d_pts;
     fa.max_seg = b->max_seg;
-    refine_store_kernel<<<(unsigned)(((int64_t)nr * 32 + 127) / 128), 128, 0, s>>>(fa);
+    fa.ip = b->ip;
+    fa.n_prof = b->n_atm;
+    fa.psurf = b->d_psurf;
+    fa.lat = b->d_lat;
+    fa.cz = b->cz;
+    fa.cx = b->cx;
+    {
+      const unsigned g = (unsigned)(((int64_t)nr * 32 + 127) / 128);
+      if (b->ip == 2) refine_store_kernel<2><<<g, 128, 0, s>>>(fa);
+      else if (b->ip == 3) refine_store_kernel<3><<<g, 128, 0, s>>>(fa);
+      else refine_store_kernel<<<g, 128, 0, s>>>(fa);
+    }
     JSC_LAUNCH_CHECK();
   }
   if (b->fixed) {

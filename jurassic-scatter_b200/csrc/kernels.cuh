@@ -128,8 +128,36 @@ __device__ __forceinline__ double dist2(const double *a, const double *b) {
 // blended linearly by the position between them.
 // IP 3 (intpol_atm_3d, :422-482): every level within cz vertically and cx
 // horizontally (and in latitude), weighted (1 - dz/cz)(1 - dx/cx).
+// The atmosphere as the IP 2/3 lookups see it (all profiles of the batch).
+struct GeoAtm {
+  int ng, nw, n_levels, n_prof;
+  const int *atm_off;
+  const double *z, *p, *t, *q, *k, *lat, *psurf;
+  double cz, cx;
+};
+
+template <typename Args>
+__device__ __forceinline__ GeoAtm geo_atm(const Args &A) {
+  GeoAtm g;
+  g.ng = A.ng;
+  g.nw = A.nw;
+  g.n_levels = A.n_levels;
+  g.n_prof = A.n_prof;
+  g.atm_off = A.atm_off;
+  g.z = A.z;
+  g.p = A.p;
+  g.t = A.t;
+  g.q = A.q;
+  g.k = A.k;
+  g.lat = A.lat;
+  g.psurf = A.psurf;
+  g.cz = A.cz;
+  g.cx = A.cx;
+  return g;
+}
+
 template <int IP>
-__device__ void atm_geo(const RayArgs &A, double z0, double lon0, double lat0, double *p,
+__device__ void atm_geo(const GeoAtm &A, double z0, double lon0, double lat0, double *p,
                         double *t, double *qk) {
   double x0[3];
   jsc_geo2cart(0, lon0, lat0, x0);
@@ -304,6 +332,7 @@ __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayE
     }
   }
   double qk[IP == 1 ? 1 : NGMAX + NWMAX];
+  const GeoAtm G = geo_atm(A);
   const double obsz = in.obsz, vpz = in.vpz;
   int64_t base = 0;
   if (STORE) {
@@ -383,7 +412,7 @@ __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayE
     if (IP == 1) {
       if (STORE || !stop) ipz = atm_full(a, pz, &pp, &pt);
     } else {
-      if (STORE || !stop) atm_geo<IP>(A, pz, plon, plat, &pp, &pt, STORE ? qk : nullptr);
+      if (STORE || !stop) atm_geo<IP>(G, pz, plon, plat, &pp, &pt, STORE ? qk : nullptr);
     }
     if (!stop) {
       p = pp;
@@ -433,13 +462,13 @@ __device__ int trace_core(const RayArgs &A, int ai, int r, const RayIn &in, RayE
       for (int i = 0; i < 3; i++) xh[i] = x[i] + 0.5 * ds * ex0[i];
       jsc_cart2geo(xh, &z, &lon, &lat);
       if (IP == 1) atm_pt(a, z, &p, &t);
-      else atm_geo<IP>(A, z, lon, lat, &p, &t, nullptr);
+      else atm_geo<IP>(G, z, lon, lat, &p, &t, nullptr);
       n = jsc_refractivity(p, t);
       for (int i = 0; i < 3; i++) {
         xh[i] += JSC_FD_STEP;
         jsc_cart2geo(xh, &z, &lon, &lat);
         if (IP == 1) atm_pt(a, z, &p, &t);
-        else atm_geo<IP>(A, z, lon, lat, &p, &t, nullptr);
+        else atm_geo<IP>(G, z, lon, lat, &p, &t, nullptr);
         const double naux = jsc_refractivity(p, t);
         ng[i] = (naux - n) / JSC_FD_STEP;
         xh[i] -= JSC_FD_STEP;
@@ -544,10 +573,15 @@ struct RefineArgs {
   const double *grid_p, *grid_t;
   const int *grid_nt;
   unsigned *status;
+  // IP 2/3: as in RayArgs
+  int ip, n_prof;
+  const double *psurf, *lat;
+  double cz, cx;
 };
 
 // Point where the segment between raw points ip-1 and ip crosses znew, with
 // the atmospheric state there (intersection_point, src/lineofsight.c:385-407).
+template <int IP = 1>
 __device__ __forceinline__ void refine_cross(const RefineArgs &A, const Profile &a,
                                              const double *gb, int ip, double znew,
                                              double *go, double *po) {
@@ -558,10 +592,20 @@ __device__ __forceinline__ void refine_cross(const RefineArgs &A, const Profile 
   jsc_geo2cart(g1[0], g1[1], g1[2], x2);
   for (int i = 0; i < 3; i++) x2[i] = x1[i] + frac * (x2[i] - x1[i]);
   jsc_cart2geo(x2, &zz, &lon, &lat);
-  const int ipz = atm_full(a, zz, &p, &t);
   go[0] = zz;
   go[1] = lon;
   go[2] = lat;
+  if (IP != 1) {
+    double qk[NGMAX + NWMAX];
+    atm_geo<IP>(geo_atm(A), zz, lon, lat, &p, &t, qk);
+    po[REC_P] = p;
+    po[REC_T] = t;
+    po[REC_QH2O] = A.ig_h2o >= 0 ? qk[A.ig_h2o] : 0.0;
+    for (int w = 0; w < A.nw; w++) po[REC_K + w] = qk[A.ng + w];
+    for (int g = 0; g < A.ng; g++) po[REC_K + A.nw + g] = qk[g];
+    return;
+  }
+  const int ipz = atm_full(a, zz, &p, &t);
   po[REC_P] = p;
   po[REC_T] = t;
   po[REC_QH2O] = A.ig_h2o >= 0 ? atm_lin(a.q + (size_t)A.ig_h2o * a.stride, a, ipz, zz) : 0.0;
@@ -650,7 +694,8 @@ __device__ __forceinline__ Profile refine_profile(const RefineArgs &A, int r) {
 // take 32 refined points at a time for refine_point, with the neighbours'
 // Cartesian positions passed by shuffles.  Same outputs as the serial pass,
 // including its overflow status.
-static __global__ void __launch_bounds__(128) refine_store_kernel(RefineArgs A) {
+template <int IP = 1>
+__global__ void __launch_bounds__(128) refine_store_kernel(RefineArgs A) {
   const int r = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
@@ -697,11 +742,11 @@ static __global__ void __launch_bounds__(128) refine_store_kernel(RefineArgs A) 
         for (int il = 0; il < A.n_alti; il++) {
           const double z1 = A.alti[il], z2 = A.alti[A.n_alti - il - 1];
           if (zp > z1 && zc < z1) {
-            refine_cross(A, a, gb, ip, z1, A.geo + (base + slot) * 4, A.pts + (base + slot) * W);
+            refine_cross<IP>(A, a, gb, ip, z1, A.geo + (base + slot) * 4, A.pts + (base + slot) * W);
             slot++;
           }
           if (zp < z2 && zc > z2) {
-            refine_cross(A, a, gb, ip, z2, A.geo + (base + slot) * 4, A.pts + (base + slot) * W);
+            refine_cross<IP>(A, a, gb, ip, z2, A.geo + (base + slot) * 4, A.pts + (base + slot) * W);
             slot++;
           }
         }

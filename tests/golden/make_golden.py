@@ -211,6 +211,17 @@ def curtain_fixtures(workdir):
             tpz=ref["tpz"], tplat=ref["tplat"], nlos=ref["nlos"],
             table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
             **{"geom_" + k: v for k, v in geom.items()})
+    # with aerosol extinction through the sulfate-like layer
+    ctlx = dict(ctlkw, sca_n=1, sca_mult=0, sca_ext="beta_e")
+    aerofile = synth.sulfate_layer_files(os.path.join(workdir, "aero"))
+    aero = refrun.reference_aero(ctlx, aerofile, os.path.dirname(aerofile))
+    for ip in (2, 3):
+        ref = refrun.run(curtain_ctl(ctlx, ip), [atm], ra, geom, aero=aero, los=True)
+        np.savez_compressed(
+            os.path.join(HERE, "curtain_ip%d_ext.npz" % ip), rad=ref["rad"], tau=ref["tau"],
+            tpz=ref["tpz"], nlos=ref["nlos"], aero=np.frombuffer(aero, dtype=np.uint8),
+            table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
+            **{"geom_" + k: v for k, v in geom.items()})
 
 
 def fov_fixtures(workdir):

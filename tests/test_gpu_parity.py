@@ -100,6 +100,28 @@ def test_curtain_formod(workdir, ip):
     np.testing.assert_allclose(S.arr(obs.tplat)[:nr], g["tplat"], rtol=1e-9, atol=1e-9)
 
 
+@pytest.mark.parametrize("ip", [2, 3])
+def test_curtain_aerosol_extinction(workdir, ip):
+    """IP=2/3 with aerosol extinction (SCA_MULT=0, beta_e): the layer-edge
+    points of the refined line of sight take their state from the same
+    horizontal interpolation; against the reference."""
+    from jscat import structs as S, synth, api
+    from make_golden_shim import curtain_ctl
+    g = _load("curtain_ip%d_ext" % ip)
+    ctlkw, atm, geom = synth.curtain_case(workdir)
+    _check_tables(g, ctlkw)
+    ctl = S.make_ctl(**curtain_ctl(dict(ctlkw, sca_n=1, sca_mult=0, sca_ext="beta_e"), ip))
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm["k"], atm["lon"], atm["lat"])
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"])
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    api.formod(ctl, a, obs, aero)
+    nr, nd = obs.nr, ctl.nd
+    rad = S.arr(obs.rad)[:nd, :nr].T
+    assert bt_error(rad, g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(rad, g["rad"]) <= REL_TOL
+    assert max_rel(S.arr(obs.tau)[:nd, :nr].T, g["tau"]) <= REL_TOL
+
+
 # EGA kernel families: -1 the default (variant 6 for clear air, 10 with
 # aerosol/cloud layers), 6 a thread per (ray, channel), 9 a lane per (ray,
 # channel, emitter)
