@@ -106,12 +106,6 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
     jsc_set_error(JSC_ERR_ARG, "unknown interpolation method IP=%d", ctl->ip);
     return JSC_ERR_ARG;
   }
-  if (ctl->ip != 1 && ctl->sca_n > 0 && ctl->sca_mult > 0) {
-    jsc_set_error(JSC_ERR_UNSUPPORTED,
-                  "IP=%d with scattering (SCA_MULT > 0 needs the 3-D scattering source)",
-                  ctl->ip);
-    return JSC_ERR_UNSUPPORTED;
-  }
   if (ctl->ip == 3 && !(ctl->cz > 0 && ctl->cx > 0)) {
     jsc_set_error(JSC_ERR_ARG, "IP=3 needs positive influence lengths CZ, CX");
     return JSC_ERR_ARG;
@@ -642,13 +636,66 @@ static const int64_t kScatterChunk = 8192;
 // then the solar term.
 // The plain scattering source (srcfunc_sca) of n point records sp
 // (profiles sp_atm) into src [n][nd].
+// Solar term of n scattering points (srcfunc_sca_sun, src/scatter.c:899-995):
+// the refracted sun direction by repeated ray tracing, the solar pencils as
+// a child batch, and the phase-function weighted solar source added to src.
+static int sun_sources(jsc_batch *b, const double *sp, const int *sp_atm, int n, double *src,
+                       cudaStream_t s) {
+  jsc_batch *sc = b->sun_child;
+  SunArgs sn;
+  fill_ray_args(b, sn.ra);
+  sn.n_pts = n;
+  sn.sp = sp;
+  sn.sp_atm = sp_atm;
+  sn.n_alti = b->n_alti;
+  sn.altimax = b->altimax;
+  sn.altimin = b->altimin;
+  sn.alti = b->d_aero + 3 * NLMAX;
+  sn.ray_atm = sc->d_ray_atm;
+  sn.ray = sc->d_ray;
+  sn.theta2 = b->d_theta2;
+  sc->n_rays = n;
+  if (b->ip != 1) {  // surface positions for the direction search
+    const int np = b->ip == 2 ? b->n_atm : b->n_levels;
+    psurf_kernel<<<(np + 127) / 128, 128, 0, s>>>(np, b->ip == 3, b->d_atm_off, b->d_lon,
+                                                  b->d_lat, b->d_psurf);
+    JSC_LAUNCH_CHECK();
+  }
+  if (b->ip == 2) sun_kernel<2><<<(n + 127) / 128, 128, 0, s>>>(sn);
+  else if (b->ip == 3) sun_kernel<3><<<(n + 127) / 128, 128, 0, s>>>(sn);
+  else sun_kernel<<<(n + 127) / 128, 128, 0, s>>>(sn);
+  JSC_LAUNCH_CHECK();
+  int st = batch_run(sc, s);
+  if (st) return st;
+  status_or_kernel<<<1, 1, 0, s>>>(b->d_status, sc->d_status);
+  JSC_LAUNCH_CHECK();
+  SunAddArgs aa;
+  aa.n_pts = n;
+  aa.nd = b->cfg.nd;
+  aa.sp = sp;
+  aa.theta2 = b->d_theta2;
+  aa.tau = sc->d_tau;
+  aa.phase = b->d_phase;
+  aa.planck_sun = b->d_planck_sun;
+  aa.src = src;
+  sun_add_kernel<<<(n * b->cfg.nd + 127) / 128, 128, 0, s>>>(aa);
+  JSC_LAUNCH_CHECK();
+  return JSC_OK;
+}
+
+// Scattering points per chunk of the 3-D source (32,400 pencils each).
+static const int64_t kScatterChunk3 = 16;
+
 static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int64_t n_pts,
                          double *src, cudaStream_t s) {
   int st = JSC_OK;
   if (n_pts <= 0) return JSC_OK;
   const int nd = b->cfg.nd, na = b->nalpha;
-  const int64_t chunk = n_pts < kScatterChunk ? n_pts : kScatterChunk;
-  if ((st = ensure_child(b, &b->child, (int)(chunk * na), b->depth - 1))) return st;
+  const bool three_d = b->ip != 1;  // srcfunc_sca_3d (src/scatter.c:654-657)
+  const int64_t cap = three_d ? kScatterChunk3 : kScatterChunk;
+  const int64_t chunk = n_pts < cap ? n_pts : cap;
+  const int64_t per_pt = three_d ? JSC_NDIR3 : na;
+  if ((st = ensure_child(b, &b->child, (int)(chunk * per_pt), b->depth - 1))) return st;
   if ((st = ensure_child(b, &b->sun_child, (int)chunk, 0))) return st;
   if (!b->d_planck_sun) {
     double h[NDMAX];
@@ -674,7 +721,33 @@ static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int6
   if (shmem > 48 * 1024)
     JSC_CUDA_TRY(cudaFuncSetAttribute(sp_integral_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
-  for (int64_t c0 = 0; c0 < n_pts; c0 += chunk) {
+  for (int64_t c0 = 0; c0 < n_pts && three_d; c0 += chunk) {
+    const int n = (int)((n_pts - c0) < chunk ? (n_pts - c0) : chunk);
+    // Pencils in every direction around the line of sight (src/scatter.c:835-856).
+    Spawn3Args pa;
+    pa.n_pts = n;
+    pa.sp = sp + c0 * JSC_SP_REC;
+    pa.sp_atm = sp_atm + c0;
+    pa.ray_atm = c->d_ray_atm;
+    pa.ray = c->d_ray;
+    c->n_rays = (int)(n * JSC_NDIR3);
+    sp_spawn3_kernel<<<(unsigned)(((int64_t)n * JSC_NDIR3 + 127) / 128), 128, 0, s>>>(pa);
+    JSC_LAUNCH_CHECK();
+    if ((st = batch_run(c, s))) return st;
+    status_or_kernel<<<1, 1, 0, s>>>(b->d_status, c->d_status);
+    JSC_LAUNCH_CHECK();
+    Integral3Args ia;
+    ia.n_pts = n;
+    ia.nd = nd;
+    ia.sp = pa.sp;
+    ia.rad = c->d_rad;
+    ia.phase = b->d_phase;
+    ia.src = src + c0 * nd;
+    sp_integral3_kernel<<<n, JSC_INT_THREADS, 0, s>>>(ia);
+    JSC_LAUNCH_CHECK();
+    if ((st = sun_sources(b, pa.sp, pa.sp_atm, n, src + c0 * nd, s))) return st;
+  }
+  for (int64_t c0 = 0; c0 < n_pts && !three_d; c0 += chunk) {
     const int n = (int)((n_pts - c0) < chunk ? (n_pts - c0) : chunk);
     // Secondary pencils (src/scatter.c:717-736).
     SpawnArgs pa;
@@ -704,36 +777,7 @@ static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int6
     ia.src = src + c0 * nd;
     sp_integral_kernel<<<n, JSC_INT_THREADS, shmem, s>>>(ia);
     JSC_LAUNCH_CHECK();
-    // Solar term (src/scatter.c:899-995).
-    SunArgs sn;
-    fill_ray_args(b, sn.ra);
-    sn.n_pts = n;
-    sn.sp = pa.sp;
-    sn.sp_atm = pa.sp_atm;
-    sn.n_alti = b->n_alti;
-    sn.altimax = b->altimax;
-    sn.altimin = b->altimin;
-    sn.alti = b->d_aero + 3 * NLMAX;
-    sn.ray_atm = sc->d_ray_atm;
-    sn.ray = sc->d_ray;
-    sn.theta2 = b->d_theta2;
-    sc->n_rays = n;
-    sun_kernel<<<(n + 127) / 128, 128, 0, s>>>(sn);
-    JSC_LAUNCH_CHECK();
-    if ((st = batch_run(sc, s))) return st;
-    status_or_kernel<<<1, 1, 0, s>>>(b->d_status, sc->d_status);
-    JSC_LAUNCH_CHECK();
-    SunAddArgs aa;
-    aa.n_pts = n;
-    aa.nd = nd;
-    aa.sp = pa.sp;
-    aa.theta2 = b->d_theta2;
-    aa.tau = sc->d_tau;
-    aa.phase = b->d_phase;
-    aa.planck_sun = b->d_planck_sun;
-    aa.src = src + c0 * nd;
-    sun_add_kernel<<<(n * nd + 127) / 128, 128, 0, s>>>(aa);
-    JSC_LAUNCH_CHECK();
+    if ((st = sun_sources(b, pa.sp, pa.sp_atm, n, src + c0 * nd, s))) return st;
   }
   return JSC_OK;
 }

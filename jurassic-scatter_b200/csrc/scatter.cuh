@@ -357,7 +357,8 @@ __device__ inline void refined_prev(const SunArgs &A, const double *g0, const do
 // refracted ray arrives from the sun's direction (up to 10 corrections),
 // then, when that ray does not end on the ground, hand it to the solar
 // child batch with the scattering angle to the LOS direction.
-static __global__ void __launch_bounds__(128) sun_kernel(SunArgs A) {
+template <int IP = 1>
+__global__ void __launch_bounds__(128) sun_kernel(SunArgs A) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= A.n_pts) return;
   const double *o = A.sp + (size_t)k * JSC_SP_REC;
@@ -380,7 +381,7 @@ static __global__ void __launch_bounds__(128) sun_kernel(SunArgs A) {
       x1[i] = x[i] + 10 * ek[i];
     }
     jsc_cart2geo(x1, &in.vpz, &in.vplon, &in.vplat);
-    const int np = trace_core<2>(A.ra, ai, 0, in, &end);
+    const int np = trace_core<2, IP>(A.ra, ai, 0, in, &end);
     if (np < 2) break;
     double g0[3], xa[3], xb[3], dout[3];
     refined_prev(A, end.g[0], end.g[1], g0);
@@ -433,4 +434,127 @@ static __global__ void sun_add_kernel(SunAddArgs A) {
   const double phase2 = jsc_lin(M_PI * (double)lo / (NTHETA - 1), ph[lo],
                                 M_PI * (double)(lo + 1) / (NTHETA - 1), ph[lo + 1], th2);
   A.src[t] += 6.764e-5 * phase2 * A.planck_sun[id] * A.tau[t];
+}
+
+// ------------------------------------------------- 3-D scattering source --
+// srcfunc_sca_3d (src/scatter.c:811-895), used with horizontally varying
+// atmospheres (IP 2/3): a secondary pencil in every direction of the
+// 180 x 180 (polar, azimuth) grid around the line of sight, cast 10 km
+// towards its view point, and the phase-function weighted sum of their
+// radiances.
+
+#define JSC_NDIR3 (JSC_NTH_SCA * JSC_NPHI_SCA)
+
+struct Spawn3Args {
+  int n_pts;
+  const double *sp;          // first record of the chunk
+  const int *sp_atm;
+  int *ray_atm;              // child batch inputs, n_pts * JSC_NDIR3 rays
+  double *ray;               // [7][n_pts * JSC_NDIR3]
+};
+
+static __global__ void sp_spawn3_kernel(Spawn3Args A) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n = (int64_t)A.n_pts * JSC_NDIR3;
+  if (t >= n) return;
+  const int k = (int)(t / JSC_NDIR3), dir = (int)(t - (int64_t)k * JSC_NDIR3);
+  const int it = dir / JSC_NPHI_SCA, iq = dir - it * JSC_NPHI_SCA;
+  const double *o = A.sp + (size_t)k * JSC_SP_REC;
+  const double x[3] = {o[SP_X], o[SP_X + 1], o[SP_X + 2]};
+  const double dx[3] = {o[SP_DX], o[SP_DX + 1], o[SP_DX + 2]};
+  double sx[3], sy[3], sz[3], xv[3];
+  jsc_bascoord(dx, x, sx, sy, sz);
+  const double theta2 = (0.5 + it) / JSC_NTH_SCA * M_PI;
+  const double phi = (0.5 + iq) / JSC_NPHI_SCA * 2 * M_PI;
+  for (int i = 0; i < 3; i++)
+    xv[i] = x[i] + 10 * sin(theta2) * sin(phi) * sx[i] + 10 * sin(theta2) * cos(phi) * sy[i] +
+            10 * cos(theta2) * sz[i];
+  double oz, olon, olat, vz, vlon, vlat;
+  jsc_cart2geo(x, &oz, &olon, &olat);
+  jsc_cart2geo(xv, &vz, &vlon, &vlat);
+  A.ray_atm[t] = A.sp_atm[k];
+  A.ray[t] = 0;  // the secondary observation time stays 0, as in the reference
+  A.ray[(size_t)n + t] = oz;
+  A.ray[2 * (size_t)n + t] = olon;
+  A.ray[3 * (size_t)n + t] = olat;
+  A.ray[4 * (size_t)n + t] = vz;
+  A.ray[5 * (size_t)n + t] = vlon;
+  A.ray[6 * (size_t)n + t] = vlat;
+}
+
+struct Integral3Args {
+  int n_pts, nd;
+  const double *sp;          // first record of the chunk
+  const double *rad;         // [n_pts * JSC_NDIR3][nd] secondary radiances
+  const double *phase;       // [nl][nd][NTHETA]
+  double *src;               // [n_pts][nd] of the chunk
+};
+
+// One block per scattering point, channels in passes of JSC_INT_CH: the
+// weight pi/180 * 2 pi sin(theta2)/180 * phase(theta2) of each (polar
+// angle, channel) in shared memory, directions spread over the threads.
+// The reference divides every channel by one sum of the weights over all
+// directions *and* channels (src/scatter.c:872-891); so does this.
+static __global__ void __launch_bounds__(JSC_INT_THREADS) sp_integral3_kernel(Integral3Args A) {
+  __shared__ double wt[JSC_NTH_SCA][JSC_INT_CH];
+  __shared__ double red[JSC_INT_THREADS / 32][JSC_INT_CH + 1];
+  __shared__ double total;
+  const int k = blockIdx.x;
+  if (k >= A.n_pts) return;
+  const int nd = A.nd;
+  const double *o = A.sp + (size_t)k * JSC_SP_REC;
+  const int il = (int)o[SP_IL];
+  const double *ph = A.phase + (size_t)il * nd * NTHETA;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) total = 0;
+  for (int c0 = 0; c0 < nd; c0 += JSC_INT_CH) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < JSC_NTH_SCA * JSC_INT_CH; i += blockDim.x) {
+      const int it = i / JSC_INT_CH, c = i - it * JSC_INT_CH, id = c0 + c;
+      double w = 0;
+      if (id < nd) {
+        const double theta2 = (0.5 + it) / JSC_NTH_SCA * M_PI;
+        // locate(theta, NTHETA, theta2) on theta[i] = pi i / (NTHETA - 1)
+        int j = 0, hi = NTHETA - 1;
+        while (hi > j + 1) {
+          const int mid = (hi + j) >> 1;
+          if (M_PI * (double)mid / (NTHETA - 1) > theta2) hi = mid; else j = mid;
+        }
+        const double a0 = M_PI * (double)j / (NTHETA - 1), a1 = M_PI * (double)(j + 1) / (NTHETA - 1);
+        const double phase2 = jsc_lin(a0, ph[(size_t)id * NTHETA + j], a1,
+                                      ph[(size_t)id * NTHETA + j + 1], theta2);
+        w = M_PI / JSC_NTH_SCA * 2 * M_PI * sin(theta2) / JSC_NPHI_SCA * phase2;
+      }
+      wt[it][c] = w;
+    }
+    __syncthreads();
+    double acc[JSC_INT_CH], ws = 0;
+#pragma unroll
+    for (int c = 0; c < JSC_INT_CH; c++) acc[c] = 0;
+    for (int dir = threadIdx.x; dir < JSC_NDIR3; dir += blockDim.x) {
+      const int it = dir / JSC_NPHI_SCA;
+      const double *r = A.rad + ((size_t)k * JSC_NDIR3 + dir) * nd + c0;
+#pragma unroll
+      for (int c = 0; c < JSC_INT_CH; c++)
+        if (c0 + c < nd) {
+          acc[c] += wt[it][c] * r[c];
+          ws += wt[it][c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c <= JSC_INT_CH; c++) {
+      double v = c < JSC_INT_CH ? acc[c] : ws;
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0) red[warp][c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x <= JSC_INT_CH) {
+      double v = 0;
+      for (int w = 0; w < JSC_INT_THREADS / 32; w++) v += red[w][threadIdx.x];
+      if (threadIdx.x == JSC_INT_CH) total += v;
+      else if (c0 + (int)threadIdx.x < nd) A.src[(size_t)k * nd + c0 + threadIdx.x] = v;
+    }
+  }
+  __syncthreads();
+  for (int id = threadIdx.x; id < nd; id += blockDim.x) A.src[(size_t)k * nd + id] /= total;
 }

@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov|aerojac|ip]
+    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov|aerojac|ip|ip3d]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -224,6 +224,34 @@ def curtain_fixtures(workdir):
             **{"geom_" + k: v for k, v in geom.items()})
 
 
+def curtain_scattering_case(workdir):
+    """Single scattering (SCA_MULT=1, 3-D source) through the curtain with
+    the sulfate-like layer: one limb ray at 16 km at noon (solar term on),
+    two of the four channels."""
+    ctlkw, atm, geom = synth.curtain_case(workdir)
+    ctlkw = dict(ctlkw, nus=list(ctlkw["nus"][:2]), sca_n=1, sca_mult=1, ip=2)
+    sel = [11]  # tangent height 16 km
+    geom = {k: v[sel] for k, v in geom.items()}
+    geom["time"] = np.full(1, 43200.0)
+    aerofile = synth.sulfate_layer_files(os.path.join(workdir, "aero"))
+    return ctlkw, atm, geom, aerofile
+
+
+def curtain_scattering_fixture(workdir):
+    """The reference's formod on curtain_scattering_case: 32,400 secondary
+    pencils per scattering point (srcfunc_sca_3d).  Slow: several minutes
+    of reference CPU time."""
+    ctlkw, atm, geom, aerofile = curtain_scattering_case(workdir)
+    aero = refrun.reference_aero(ctlkw, aerofile, os.path.dirname(aerofile))
+    ra = np.zeros(1, int)
+    ref = refrun.run(ctlkw, [atm], ra, geom, aero=aero, los=True, timeout=7200)
+    np.savez_compressed(
+        os.path.join(HERE, "curtain_ip2_sca1.npz"), rad=ref["rad"], tau=ref["tau"],
+        nlos=ref["nlos"], aero=np.frombuffer(aero, dtype=np.uint8), seconds=ref["seconds"],
+        table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
+        **{"geom_" + k: v for k, v in geom.items()})
+
+
 def fov_fixtures(workdir):
     """formod and kernel() with the field of view of fov_case."""
     ctlkw, atm, geom = fov_case(workdir)
@@ -250,6 +278,9 @@ def main():
         return
     if sys.argv[1:] == ["ip"]:
         curtain_fixtures(workdir)
+        return
+    if sys.argv[1:] == ["ip3d"]:
+        curtain_scattering_fixture(workdir)
         return
     if sys.argv[1:] == ["aero"]:
         aero_fixture(workdir, "aero_layers8", synth.layered_aero_files, list(synth.CFG2_NU[::2]),
@@ -291,6 +322,8 @@ def main():
     fov_fixtures(workdir)
     aerosol_jacobian_fixture(workdir)
     curtain_fixtures(workdir)
+    if os.environ.get("JSC_SLOW_FIXTURES"):
+        curtain_scattering_fixture(workdir)
     print("fixtures written to", HERE)
 
 
