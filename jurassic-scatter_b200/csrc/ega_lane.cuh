@@ -128,9 +128,21 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
     tp = tp * (1 - eps);
     // Segment transmittance: the product over emitters in emitter order,
     // as the reference accumulates it (lanes past ng hold eps = 0).
+    // All GP factors are fetched first (independent shuffles), then
+    // multiplied in emitter order; lanes past ng hold exactly 1.
     const double f = 1 - eps;
-    double tau_gas = __shfl_sync(gmask, f, gbase);
-    for (int j = 1; j < ng; j++) tau_gas *= __shfl_sync(gmask, f, gbase + j);
+    double tau_gas;
+    if constexpr (GP <= 8) {
+      double fs[GP];
+#pragma unroll
+      for (int j = 0; j < GP; j++) fs[j] = __shfl_sync(gmask, f, gbase + j);
+      tau_gas = fs[0];
+#pragma unroll
+      for (int j = 1; j < GP; j++) tau_gas *= fs[j];
+    } else {  // wider groups: one factor at a time (registers)
+      tau_gas = __shfl_sync(gmask, f, gbase);
+      for (int j = 1; j < ng; j++) tau_gas *= __shfl_sync(gmask, f, gbase + j);
+    }
 
     const double beta = *bc, src = *sp;
     const double af = rec[REC_AF];
