@@ -155,9 +155,9 @@ typedef struct {
  * ------------------------------------------------------------------------ */
 
 /* Replaces formod (src/forwardmodel.c:15-116), for ctl->ip 1 (one
- * profile) and, without scattering (sca_mult 0 or no aerosol), 2 (profiles
- * split where lon/lat change, the two nearest blended) and 3 (points
- * weighted within ctl->cz, cx):
+ * profile), 2 (profiles split where lon/lat change, the two nearest
+ * blended) and 3 (points weighted within ctl->cz, cx; with scattering the
+ * 3-D source of 32,400 secondary pencils per scattering point):
  * saves the NaN mask of
  * obs->rad, applies hydrostatic balance to atm->p (ctl->hydz >= 0), traces
  * every ray, evaluates EGA transmittances, continua, Planck source and
@@ -281,7 +281,9 @@ size_t jsc_obs2y(const ctl_t *ctl, const obs_t *obs, double *y, int *ida, int *i
  * recomputed with jsc_get_opt_prop, as formod does, and each aerosol
  * column runs the undisturbed profile as its own batch with the optical
  * properties of its disturbed parameter.  The field-of-view convolution
- * (ctl->fov) applies to every column as in formod. */
+ * (ctl->fov) applies to every column as in formod.  For ctl->ip 2/3 (one
+ * horizontally varying atmosphere per batch) each column is its own GPU
+ * forward model, as in the reference. */
 int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size_t m,
                size_t n, size_t tda);
 

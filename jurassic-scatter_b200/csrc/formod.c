@@ -473,6 +473,89 @@ static double out_rad(const ctl_t *ctl, const double *rad, size_t ray, int id) {
   return ctl->write_bbt ? brightness(v, ctl->nu[id]) : v;
 }
 
+/* Jacobian with one forward model per column, the reference's own scheme
+ * (kernel, src/retrievalmodel.c:201-298), for atmospheres a batch cannot
+ * hold several disturbed copies of (IP 2/3: all profiles form one
+ * horizontally varying atmosphere).  Each column runs formod_impl on a
+ * copy of the undisturbed atm/obs/aero with one state element moved. */
+static int kernel_columns(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k,
+                          size_t m, size_t n, size_t tda) {
+  aero_t empty;
+  if (!aero) {
+    memset(&empty, 0, sizeof(empty));
+    aero = &empty;
+  }
+  int st = formod_impl(ctl, atm, obs, aero);
+  if (st) return st;
+  const size_t n0 = jsc_atm2x(ctl, atm, aero, NULL, NULL, NULL);
+  const size_t m0 = jsc_obs2y(ctl, obs, NULL, NULL, NULL);
+  if (n0 != n || m0 != m) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: %zu x %zu matrix for %zu measurements and %zu "
+                  "state elements", m, n, m0, n0);
+    return JSC_ERR_ARG;
+  }
+  if ((m > 0 && n > 0 && !k) || tda < n) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_kernel: no matrix, or row stride %zu below %zu columns",
+                  tda, n);
+    return JSC_ERR_ARG;
+  }
+  double *x0 = (double *)malloc((n + 1) * sizeof(double));
+  double *x1 = (double *)malloc((n + 1) * sizeof(double));
+  double *y = (double *)malloc((2 * m + 1) * sizeof(double));
+  int *iqa = (int *)malloc((n + 1) * sizeof(int));
+  atm_t *atm1 = (atm_t *)malloc(sizeof(atm_t));
+  obs_t *obs1 = (obs_t *)malloc(sizeof(obs_t));
+  aero_t *aero1 = (aero_t *)malloc(sizeof(aero_t));
+  if (!x0 || !x1 || !y || !iqa || !atm1 || !obs1 || !aero1) {
+    st = JSC_ERR_NOMEM;
+  } else {
+    jsc_atm2x(ctl, atm, aero, x0, iqa, NULL);
+    jsc_obs2y(ctl, obs, y, NULL, NULL);
+    for (size_t j = 0; j < n && !st; j++) {
+      double h = perturbation(ctl, iqa[j], x0[j]);
+      if (iqa[j] == JSC_IDXNN(ctl)) h = gmax(fabs(0.5 * x0[j]), 0.1);
+      if (iqa[j] == JSC_IDXRR(ctl)) h = gmax(fabs(0.25 * x0[j]), 0.1);
+      if (iqa[j] == JSC_IDXSS(ctl)) h = gmax(fabs(0.1 * x0[j]), 0.01);
+      if (h <= 0) {
+        jsc_set_error(JSC_ERR_ARG, "jsc_kernel: cannot set perturbation size");
+        st = JSC_ERR_ARG;
+        break;
+      }
+      memcpy(x1, x0, n * sizeof(double));
+      x1[j] += h;
+      memcpy(atm1, atm, sizeof(atm_t));
+      memcpy(obs1, obs, sizeof(obs_t));
+      memcpy(aero1, aero, sizeof(aero_t));
+      jsc_x2atm(ctl, x1, atm1, aero1);
+      if ((st = formod_impl(ctl, atm1, obs1, aero1))) break;
+      double *y1 = y + m;
+      size_t c = 0;
+      for (int ir = 0; ir < obs1->nr; ir++)
+        for (int id = 0; id < ctl->nd; id++)
+          if (isfinite(obs1->rad[id][ir])) {
+            if (c < m) y1[c] = obs1->rad[id][ir];
+            c++;
+          }
+      if (c != m) {
+        jsc_set_error(JSC_ERR_ARG,
+                      "jsc_kernel: disturbed forward model %zu has %zu finite radiances, "
+                      "the undisturbed one %zu", j, c, m);
+        st = JSC_ERR_ARG;
+        break;
+      }
+      for (size_t i = 0; i < m; i++) k[i * tda + j] = (y1[i] - y[i]) / h;
+    }
+  }
+  free(x0);
+  free(x1);
+  free(y);
+  free(iqa);
+  free(atm1);
+  free(obs1);
+  free(aero1);
+  return st;
+}
+
 /* Aerosol parameter of a state-vector element (the value x2atm sets). */
 static double *aero_element(const ctl_t *ctl, int iqa, aero_t *aero) {
   if (iqa == JSC_IDXNN(ctl)) return &aero->nn[0];
@@ -489,12 +572,7 @@ int jsc_kernel(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k, size
                   nd, ng, nw, nr, np);
     return JSC_ERR_ARG;
   }
-  if (ctl->ip != 1) {
-    jsc_set_error(JSC_ERR_UNSUPPORTED,
-                  "jsc_kernel: IP=%d (each column would need its own horizontally varying "
-                  "atmosphere)", ctl->ip);
-    return JSC_ERR_UNSUPPORTED;
-  }
+  if (ctl->ip != 1) return kernel_columns(ctl, atm, obs, aero, k, m, n, tda);
   const int aero_ret = ctl->retnn || ctl->retrr || ctl->retss;
   if ((ctl->sca_n > 0 || aero_ret) && !aero) {
     jsc_set_error(JSC_ERR_ARG, "jsc_kernel: SCA_N=%d needs the aerosol/cloud data", ctl->sca_n);

@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov|aerojac|ip|ip3d]
+    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -224,6 +224,25 @@ def curtain_fixtures(workdir):
             **{"geom_" + k: v for k, v in geom.items()})
 
 
+def curtain_jacobian_case(workdir):
+    """Jacobian through the IP=2 curtain: temperature at 10-30 km of every
+    profile, every third limb ray."""
+    ctlkw, atm, geom = synth.curtain_case(workdir)
+    ctlkw = dict(ctlkw, ip=2, rett_zmin=10.0, rett_zmax=30.0)
+    geom = {k: v[::3] for k, v in geom.items()}
+    return ctlkw, atm, geom
+
+
+def curtain_jacobian_fixture(workdir):
+    ctlkw, atm, geom = curtain_jacobian_case(workdir)
+    ref = refrun.reference_kernel(reference_ctl(ctlkw), atm, geom)
+    np.savez_compressed(
+        os.path.join(HERE, "jacobian_curtain_ip2.npz"), k=ref["k"], x0=ref["x0"],
+        iqa=ref["iqa"], ipa=ref["ipa"], rad=ref["rad"],
+        table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]),
+        **{"geom_" + k: v for k, v in geom.items()})
+
+
 def curtain_scattering_case(workdir):
     """Single scattering (SCA_MULT=1, 3-D source) through the curtain with
     the sulfate-like layer: one limb ray at 16 km at noon (solar term on),
@@ -279,6 +298,9 @@ def main():
     if sys.argv[1:] == ["ip"]:
         curtain_fixtures(workdir)
         return
+    if sys.argv[1:] == ["ipjac"]:
+        curtain_jacobian_fixture(workdir)
+        return
     if sys.argv[1:] == ["ip3d"]:
         curtain_scattering_fixture(workdir)
         return
@@ -322,6 +344,7 @@ def main():
     fov_fixtures(workdir)
     aerosol_jacobian_fixture(workdir)
     curtain_fixtures(workdir)
+    curtain_jacobian_fixture(workdir)
     if os.environ.get("JSC_SLOW_FIXTURES"):
         curtain_scattering_fixture(workdir)
     print("fixtures written to", HERE)

@@ -119,3 +119,28 @@ def test_kernel_aerosol_parameters(workdir):
     scale = np.max(np.abs(kref), axis=0)
     err = np.abs(k - kref) / np.where(scale > 0, scale, 1.0)
     assert float(err.max()) <= K_TOL
+
+
+def test_kernel_curtain_ip2(workdir):
+    """Temperature of every profile of the IP=2 curtain: each column is its
+    own GPU forward model through the whole horizontally varying
+    atmosphere; against the reference's kernel()."""
+    from jscat import api, structs as S
+    from make_golden_shim import curtain_jacobian_case, tables_digest
+    ctlkw, atm, geom = curtain_jacobian_case(workdir)
+    g = dict(np.load(os.path.join(GOLDEN, "jacobian_curtain_ip2.npz")))
+    assert tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]) == str(g["table_sha256"])
+    ctl = S.make_ctl(**ctlkw)
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm["k"], atm["lon"], atm["lat"])
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"],
+                     geom["obslon"], geom["vplon"], geom["time"])
+    k = api.kernel(ctl, a, obs)
+    kref = g["k"]
+    assert k.shape == kref.shape
+    x, iqa, ipa = api.atm2x(ctl, a)
+    np.testing.assert_array_equal(ipa, g["ipa"])
+    assert max_rel(x, g["x0"]) <= 1e-12
+    assert max_rel(S.arr(obs.rad)[:ctl.nd, :obs.nr].T, g["rad"]) <= REL_TOL
+    scale = np.max(np.abs(kref), axis=0)
+    err = np.abs(k - kref) / np.where(scale > 0, scale, 1.0)
+    assert float(err.max()) <= K_TOL
