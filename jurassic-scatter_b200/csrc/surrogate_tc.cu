@@ -1,5 +1,6 @@
 // Surrogate inference on the 5th-generation tensor cores (tcgen05, sm_100a):
-// 128 scattering points per tile, one thread per point, the four layers as
+// 128 scattering points per tile, two threads per point (each half of the
+// columns of the point's accumulator row), the four layers as
 // tcgen05.mma (kind::f16, BF16 operands from shared memory, FP32
 // accumulator in tensor memory), bias + tanh in registers between layers.
 //
@@ -16,6 +17,7 @@
 #include "surrogate_tc.h"
 
 #define TC_M 128
+#define TC_T 256          // threads per block: two warps per TMEM lane quadrant
 #define TC_K0 16          // first-layer K: the 8 features padded to one k-step
 #define TC_W 128          // hidden width
 #define TC_SPIN (1 << 21) // polls with 64 ns sleeps: a wait gives up after ~0.2 s
@@ -140,12 +142,12 @@ static __global__ void tc_pack_kernel(int nout, int noutp16, const float *w0, co
   }
 }
 
-// bias + tanh of this thread's row of the accumulator, written as the next
-// layer's K-major BF16 activation row.
+// bias + tanh of columns [c0, c0 + 64) of this thread's row of the
+// accumulator, written as the next layer's K-major BF16 activation row.
 __device__ __forceinline__ void tc_act(uint32_t tmem_row, const float *bias, unsigned char *act,
-                                       int row) {
+                                       int row, int c0) {
 #pragma unroll 1
-  for (int c = 0; c < TC_W; c += 16) {
+  for (int c = c0; c < c0 + TC_W / 2; c += 16) {
     float v[16];
     tmem_ld16(tmem_row + (uint32_t)c, v);
     __align__(16) __nv_bfloat16 h[16];
@@ -157,7 +159,7 @@ __device__ __forceinline__ void tc_act(uint32_t tmem_row, const float *bias, uns
 }
 
 template <int NOUT16>
-static __global__ void __launch_bounds__(TC_M, 1) sur_infer_tc_kernel(TcInferArgs A) {
+static __global__ void __launch_bounds__(TC_T, 2) sur_infer_tc_kernel(TcInferArgs A) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const size_t ib = tc_image_bytes(NOUT16 * 16);
   unsigned char *w0 = sm;
@@ -169,8 +171,11 @@ static __global__ void __launch_bounds__(TC_M, 1) sur_infer_tc_kernel(TcInferArg
   __shared__ __align__(8) unsigned long long mbar;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5;
+  // warp w reads TMEM lanes (rows) 32 (w % 4) .. +31, columns of half w / 4
+  const int quad = warp & 3, half = warp >> 2;
+  const int row = quad * 32 + (tid & 31);
 
-  for (size_t i = (size_t)tid * 16; i < ib; i += TC_M * 16)
+  for (size_t i = (size_t)tid * 16; i < ib; i += TC_T * 16)
     *reinterpret_cast<uint4 *>(sm + i) = *reinterpret_cast<const uint4 *>(A.image + i);
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar)) : "memory");
@@ -186,7 +191,7 @@ static __global__ void __launch_bounds__(TC_M, 1) sur_infer_tc_kernel(TcInferArg
   __syncthreads();
   tc_after_sync();
   const uint32_t tmem = tmem_slot;
-  const uint32_t tmem_row = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
+  const uint32_t tmem_row = tmem + ((uint32_t)(quad * 32) << 16);  // this warp's 32 lanes
   const uint32_t mb = smem_addr(&mbar);
   uint32_t phase = 0;
   const uint32_t a_base = smem_addr(act), w0a = smem_addr(w0), w1a = smem_addr(w1),
@@ -195,8 +200,8 @@ static __global__ void __launch_bounds__(TC_M, 1) sur_infer_tc_kernel(TcInferArg
   const int ntiles = (A.n + TC_M - 1) / TC_M;
   bool aborted = false;  // block-uniform
   for (int tile = blockIdx.x; tile < ntiles && !aborted; tile += gridDim.x) {
-    const int p = tile * TC_M + tid;
-    {
+    const int p = tile * TC_M + row;
+    if (half == 0) {
       // layer 0 input: standardised features as a 128 x 16 K-major tile
       __align__(16) __nv_bfloat16 h[16];
 #pragma unroll
@@ -205,8 +210,8 @@ static __global__ void __launch_bounds__(TC_M, 1) sur_infer_tc_kernel(TcInferArg
         if (c < 8 && p < A.n) v = (A.feat[(size_t)p * 8 + c] - A.xm[c]) / A.xs[c];
         h[c] = __float2bfloat16_rn(v);
       }
-      *reinterpret_cast<uint4 *>(act + tc_off(tid, 0, TC_K0)) = *reinterpret_cast<uint4 *>(&h[0]);
-      *reinterpret_cast<uint4 *>(act + tc_off(tid, 8, TC_K0)) = *reinterpret_cast<uint4 *>(&h[8]);
+      *reinterpret_cast<uint4 *>(act + tc_off(row, 0, TC_K0)) = *reinterpret_cast<uint4 *>(&h[0]);
+      *reinterpret_cast<uint4 *>(act + tc_off(row, 8, TC_K0)) = *reinterpret_cast<uint4 *>(&h[8]);
     }
 #pragma unroll 1
     for (int layer = 0; layer < 4; layer++) {
@@ -234,11 +239,11 @@ static __global__ void __launch_bounds__(TC_M, 1) sur_infer_tc_kernel(TcInferArg
       }
       tc_after_sync();
       if (layer < 3) {
-        tc_act(tmem_row, bias + layer * TC_W, act, tid);
+        tc_act(tmem_row, bias + layer * TC_W, act, row, half * (TC_W / 2));
       } else {
         const float *b3 = bias + 3 * TC_W;
 #pragma unroll 1
-        for (int c = 0; c < NOUT16 * 16; c += 16) {
+        for (int c = half * 16; c < NOUT16 * 16; c += 32) {
           float v[16];
           tmem_ld16(tmem_row + (uint32_t)c, v);
 #pragma unroll
@@ -276,8 +281,16 @@ int jsc_sur_tc_infer(const TcInferArgs &a, cudaStream_t st) {
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  // two resident blocks per SM where the shared memory allows it: one
+  // block's epilogue (tanh, BF16 stores) overlaps the other's MMAs
   const int tiles = (a.n + TC_M - 1) / TC_M;
-  const int blocks = tiles < nsm ? tiles : nsm;
+  int per_sm = 1;
+  {
+    int smem_sm = 0;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (2 * (smem + 2048) <= (size_t)smem_sm) per_sm = 2;
+  }
+  const int blocks = tiles < per_sm * nsm ? tiles : per_sm * nsm;
   if (blocks < 1) return 0;
   cudaError_t e = cudaSuccess;
 #define TC_LAUNCH(N)                                                                        \
@@ -285,7 +298,7 @@ int jsc_sur_tc_infer(const TcInferArgs &a, cudaStream_t st) {
     e = cudaFuncSetAttribute(sur_infer_tc_kernel<N>,                                        \
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);       \
     if (e != cudaSuccess) return (int)e;                                                    \
-    sur_infer_tc_kernel<N><<<blocks, TC_M, smem, st>>>(a);                                  \
+    sur_infer_tc_kernel<N><<<blocks, TC_T, smem, st>>>(a);                                  \
   } while (0)
   switch (n16) {
     case 1: TC_LAUNCH(1); break;
