@@ -480,23 +480,29 @@ static double out_rad(const ctl_t *ctl, const double *rad, size_t ray, int id) {
  * copy of the undisturbed atm/obs/aero with one state element moved. */
 static int kernel_columns(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, double *k,
                           size_t m, size_t n, size_t tda) {
-  aero_t empty;
+  aero_t *empty = NULL;  /* aero_t is ~2 MB: never on the stack */
   if (!aero) {
-    memset(&empty, 0, sizeof(empty));
-    aero = &empty;
+    empty = (aero_t *)calloc(1, sizeof(aero_t));
+    if (!empty) return JSC_ERR_NOMEM;
+    aero = empty;
   }
   int st = formod_impl(ctl, atm, obs, aero);
-  if (st) return st;
+  if (st) {
+    free(empty);
+    return st;
+  }
   const size_t n0 = jsc_atm2x(ctl, atm, aero, NULL, NULL, NULL);
   const size_t m0 = jsc_obs2y(ctl, obs, NULL, NULL, NULL);
   if (n0 != n || m0 != m) {
     jsc_set_error(JSC_ERR_ARG, "jsc_kernel: %zu x %zu matrix for %zu measurements and %zu "
                   "state elements", m, n, m0, n0);
+    free(empty);
     return JSC_ERR_ARG;
   }
   if ((m > 0 && n > 0 && !k) || tda < n) {
     jsc_set_error(JSC_ERR_ARG, "jsc_kernel: no matrix, or row stride %zu below %zu columns",
                   tda, n);
+    free(empty);
     return JSC_ERR_ARG;
   }
   double *x0 = (double *)malloc((n + 1) * sizeof(double));
@@ -553,6 +559,7 @@ static int kernel_columns(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, doub
   free(atm1);
   free(obs1);
   free(aero1);
+  free(empty);
   return st;
 }
 
