@@ -323,7 +323,7 @@ def _pad(inp, n_atm, n_rays, lev):
     return out
 
 
-def mixed_bench(args, local, torch, sur=None):
+def mixed_bench(args, local, torch, sur=None, variant=-1):
     """Mixed-size request batch: requests are admitted in arrival order into
     packed batches per model (up to RAY_CAP rays and ATM_CAP profiles);
     clear-air batches replay a CUDA graph captured once per model (fixed
@@ -375,7 +375,8 @@ def mixed_bench(args, local, torch, sur=None):
         models.append(m)
         first = [r for r in reqs if not r["aerosol"] and r["nd"] == nd][:1]
         shape = _pad(_pack(first), ATM_CAP, RAY_CAP, lev)
-        runners[nd] = api.GraphBatch(m, ctl, shape, sp, pin, max_seg=RAY_CAP * 420)
+        runners[nd] = api.GraphBatch(m, ctl, shape, sp, pin, max_seg=RAY_CAP * 420,
+                                     variant=variant)
     a_nus = [float(v) for v in g["nus"]]
     a_base = synth.write_tables(workdir, synth.CFG0_EMITTERS, a_nus, 20261203)
     a_ctl = S.make_ctl(emitters=synth.CFG0_EMITTERS, nus=a_nus, tblbase=a_base, hydz=0.0,
@@ -813,7 +814,10 @@ def main():
             line["scattering"] = {"error": str(exc)[:300]}
     if rank == 0 and world == 1 and args.requests > 0:
         try:
-            line["mixed_requests"] = mixed_bench(args, local, torch, sur)
+            # clear-air graph batches replay the launch variant the headline's
+            # autotuner chose on the same emitters and channel grid
+            line["mixed_requests"] = mixed_bench(args, local, torch, sur,
+                                                 variant=tuned.get("variant", -1))
         except Exception as exc:
             line["mixed_requests"] = {"error": str(exc)[:300]}
     if sur is not None:

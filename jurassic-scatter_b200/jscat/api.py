@@ -359,7 +359,7 @@ class GraphBatch:
     _KEYS = ("z", "lon", "lat", "p", "t", "q", "k", "time", "obsz", "obslon", "obslat",
              "vpz", "vplon", "vplat")
 
-    def __init__(self, model, ctl, inp, stream, pin, max_seg=0, aero=None):
+    def __init__(self, model, ctl, inp, stream, pin, max_seg=0, aero=None, variant=-1):
         lib = L.load()
         self.nd = ctl.nd
         self.stream = stream
@@ -367,6 +367,8 @@ class GraphBatch:
         self.batch = Batch(model, ctl, n_atm, len(inp["z"]), len(inp["ray_atm"]), max_seg)
         if aero is not None:
             self.batch.set_aero(aero)
+        if variant >= 0:
+            self.batch.set_variant(variant)
         L.check(lib.jsc_batch_set_fixed(self.batch.h, 1), "jsc_batch_set_fixed")
         self.host = {k: pin(np.ascontiguousarray(inp[k], dtype=np.float64)) for k in self._KEYS}
         self.host["atm_off"] = pin(np.ascontiguousarray(inp["atm_off"], dtype=np.int32))
