@@ -629,7 +629,14 @@ static int list_scattering_points(jsc_batch *b, cudaStream_t s) {
 
 // Scattering points per chunk: the secondary pencils of a chunk run as one
 // child batch of chunk * nalpha rays.
-static const int64_t kScatterChunk = 8192;
+// Scattering points per child-batch round of the 1-D source: large rounds
+// keep the GPU busy between the host's LOS-size reads, bounded so the
+// child's per-(LOS point, channel) buffers stay near 20 GB (32768 points at
+// 16 channels, 8192 at 64).
+static int64_t scatter_chunk(int nd) {
+  const int64_t c = 524288 / (nd > 0 ? nd : 1);
+  return c < 8192 ? 8192 : (c > 32768 ? 32768 : c);
+}
 
 // Scattering source of every scattering point (srcfunc_sca,
 // src/scatter.c:643-662): thermal radiation from the secondary pencils,
@@ -692,7 +699,7 @@ static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int6
   if (n_pts <= 0) return JSC_OK;
   const int nd = b->cfg.nd, na = b->nalpha;
   const bool three_d = b->ip != 1;  // srcfunc_sca_3d (src/scatter.c:654-657)
-  const int64_t cap = three_d ? kScatterChunk3 : kScatterChunk;
+  const int64_t cap = three_d ? kScatterChunk3 : scatter_chunk(nd);
   const int64_t chunk = n_pts < cap ? n_pts : cap;
   const int64_t per_pt = three_d ? JSC_NDIR3 : na;
   if ((st = ensure_child(b, &b->child, (int)(chunk * per_pt), b->depth - 1))) return st;
