@@ -722,8 +722,9 @@ static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int6
   if ((st = copy_profiles(b, b->sun_child, s))) return st;
 
   jsc_batch *c = b->child, *sc = b->sun_child;
-  const size_t shmem = ((size_t)JSC_NTH_SCA * nd + (size_t)na * nd + 4 * JSC_NTH_SCA +
-                        (JSC_INT_THREADS / 32) * JSC_INT_CH + (size_t)na * JSC_INT_CH) *
+  const size_t shmem = ((size_t)JSC_NTH_SCA * nd + (size_t)na * (nd | 1) + 4 * JSC_NTH_SCA +
+                        (JSC_INT_THREADS / 32) * JSC_INT_CH + (size_t)na * (JSC_INT_CH + 1) +
+                        (size_t)na) *
                        sizeof(double);
   if (shmem > 48 * 1024)
     JSC_CUDA_TRY(cudaFuncSetAttribute(sp_integral_kernel,

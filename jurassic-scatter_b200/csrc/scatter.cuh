@@ -185,19 +185,24 @@ struct IntegralArgs {
 
 // One block per scattering point.  Directions (itheta, iphi) are spread
 // over the threads; the polar factor sin(theta2) * phase(theta2) of each
-// (itheta, channel) and the secondary radiances sit in shared memory.
-// Weighted sums follow src/scatter.c:737-805 up to the order of the sum.
+// (itheta, channel), the secondary radiances, their slopes and the pencil
+// angles sit in shared memory.  The radiance and slope rows have odd
+// strides in doubles, so lanes whose directions fall in different alpha
+// intervals read different banks.  Weighted sums follow
+// src/scatter.c:737-805 up to the order of the sum.
 static __global__ void __launch_bounds__(JSC_INT_THREADS)
 sp_integral_kernel(IntegralArgs A) {
   extern __shared__ double sh[];
   const int k = blockIdx.x;
   if (k >= A.n_pts) return;
   const int nd = A.nd, na = A.nalpha;
+  const int ndp = nd | 1, SL = JSC_INT_CH + 1;      // odd row strides
   double *wt = sh;                                   // [JSC_NTH_SCA][nd]
-  double *rd = wt + (size_t)JSC_NTH_SCA * nd;        // [na][nd]
-  double *trig = rd + (size_t)na * nd;               // sin/cos of theta2 and phi
+  double *rd = wt + (size_t)JSC_NTH_SCA * nd;        // [na][ndp]
+  double *trig = rd + (size_t)na * ndp;              // sin/cos of theta2 and phi
   double *red = trig + 4 * JSC_NTH_SCA;              // [JSC_INT_THREADS / 32][JSC_INT_CH]
-  double *slp = red + (JSC_INT_THREADS / 32) * JSC_INT_CH;  // [na - 1][JSC_INT_CH]
+  double *slp = red + (JSC_INT_THREADS / 32) * JSC_INT_CH;  // [na - 1][SL]
+  double *alf = slp + (size_t)na * SL;               // [na] pencil angles
   const double *o = A.sp + (size_t)k * JSC_SP_REC;
   const int il = (int)o[SP_IL];
   for (int i = threadIdx.x; i < JSC_NTH_SCA; i += blockDim.x) {
@@ -210,8 +215,9 @@ sp_integral_kernel(IntegralArgs A) {
   }
   for (int i = threadIdx.x; i < na * nd; i += blockDim.x) {
     const int ir = i / nd, id = i - ir * nd;
-    rd[i] = A.rad[((size_t)k * na + ir) * nd + id];
+    rd[(size_t)ir * ndp + id] = A.rad[((size_t)k * na + ir) * nd + id];
   }
+  for (int i = threadIdx.x; i < na; i += blockDim.x) alf[i] = A.alpha[i];
   __syncthreads();
   // Polar weight sin(theta2) * phase(theta2); phase on the 1-degree grid.
   const double *ph = A.phase + (size_t)il * nd * NTHETA;
@@ -246,8 +252,8 @@ sp_integral_kernel(IntegralArgs A) {
     for (int i = threadIdx.x; i < (na - 1) * JSC_INT_CH; i += blockDim.x) {
       const int lo = i / JSC_INT_CH, c = i - lo * JSC_INT_CH;
       if (c0 + c < nd)
-        slp[i] = (rd[(size_t)(lo + 1) * nd + c0 + c] - rd[(size_t)lo * nd + c0 + c]) /
-                 (A.alpha[lo + 1] - A.alpha[lo]);
+        slp[lo * SL + c] = (rd[(size_t)(lo + 1) * ndp + c0 + c] - rd[(size_t)lo * ndp + c0 + c]) /
+                           (alf[lo + 1] - alf[lo]);
     }
     __syncthreads();
     double acc[JSC_INT_CH];
@@ -264,11 +270,11 @@ sp_integral_kernel(IntegralArgs A) {
       int lo = 0, hi = na - 1;
       while (hi > lo + 1) {
         const int mid = (hi + lo) >> 1;
-        if (A.alpha[mid] > alpha2) hi = mid; else lo = mid;
+        if (alf[mid] > alpha2) hi = mid; else lo = mid;
       }
-      const double da = alpha2 - A.alpha[lo];
+      const double da = alpha2 - alf[lo];
       const double *w = wt + (size_t)it * nd + c0;
-      const double *r0 = rd + (size_t)lo * nd + c0, *s0 = slp + lo * JSC_INT_CH;
+      const double *r0 = rd + (size_t)lo * ndp + c0, *s0 = slp + lo * SL;
 #pragma unroll
       for (int c = 0; c < JSC_INT_CH; c++)
         if (c0 + c < nd) acc[c] += w[c] * (r0[c] + s0[c] * da);  // jsc_lin, slope precomputed
