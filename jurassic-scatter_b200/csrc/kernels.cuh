@@ -545,7 +545,7 @@ __device__ __forceinline__ int trace_ray(const RayArgs &A, int r) {
 }
 
 template <bool STORE, int IP = 1>
-__global__ void __launch_bounds__(128) raytrace_kernel(RayArgs A) {
+__global__ void __launch_bounds__(128, 7) raytrace_kernel(RayArgs A) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= A.n_rays) return;
   const int np = trace_ray<STORE, IP>(A, r);
@@ -695,7 +695,7 @@ __device__ __forceinline__ Profile refine_profile(const RefineArgs &A, int r) {
 // Cartesian positions passed by shuffles.  Same outputs as the serial pass,
 // including its overflow status.
 template <int IP = 1>
-__global__ void __launch_bounds__(128) refine_store_kernel(RefineArgs A) {
+__global__ void __launch_bounds__(128, 8) refine_store_kernel(RefineArgs A) {
   const int r = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
