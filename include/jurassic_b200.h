@@ -150,6 +150,39 @@ typedef struct {
   int init;
 } atm_t;
 
+/* Line of sight of one ray (src/jurassic.h:352-393): what raytrace
+ * writes and formod_pencil integrates.  Only the host helpers
+ * formod_continua and intpol_tbl below take it; the GPU path keeps its own
+ * packed LOS records in device memory. */
+typedef struct {
+  int np;
+  double z[NLOS], lon[NLOS], lat[NLOS];
+  double p[NLOS], t[NLOS];
+  double q[NLOS][NGMAX];
+  double k[NLOS][NWMAX];
+  int aeroi[NLOS];              /* aerosol/cloud layer index */
+  double aerofac[NLOS];         /* aerosol/cloud layer factor */
+  double tsurf;                 /* surface temperature [K], <= 0: none */
+  double ds[NLOS];              /* segment length [km] */
+  double u[NLOS][NGMAX];        /* column density [molecules/cm^2] */
+} los_t;
+
+/* Emissivity look-up tables in the reference's fixed layout
+ * (src/jurassic.h:438-471, about 12.5 GB): what read_tbl fills and the
+ * host helpers intpol_tbl* read.  The GPU path never uses it; its device
+ * tables hold only the rows that exist (jsc_model_create). */
+typedef struct {
+  int np[NGMAX][NDMAX];
+  int nt[NGMAX][NDMAX][TBLNPMAX];
+  int nu[NGMAX][NDMAX][TBLNPMAX][TBLNTMAX];
+  double p[NGMAX][NDMAX][TBLNPMAX];
+  double t[NGMAX][NDMAX][TBLNPMAX][TBLNTMAX];
+  float u[NGMAX][NDMAX][TBLNPMAX][TBLNTMAX][TBLNUMAX];
+  float eps[NGMAX][NDMAX][TBLNPMAX][TBLNTMAX][TBLNUMAX];
+  double st[TBLNSMAX];
+  double sr[NDMAX][TBLNSMAX];
+} tbl_t;
+
 /* ------------------------------------------------------------------------
  * Drop-in entry points.
  * ------------------------------------------------------------------------ */
@@ -175,6 +208,57 @@ double brightness(double rad, double nu);
 
 /* Planck function (src/forwardmodel.c:569-573). */
 double planck(double t, double nu);
+
+/* The rest of the reference's forwardmodel.h (src/forwardmodel.h:21-85),
+ * so that programs and objects written against it (its scatter.o calls
+ * formod_pencil, misc.o read_shape) link this library in place of
+ * forwardmodel.o.  Errors follow formod()'s convention. */
+
+/* Replaces formod_pencil (src/forwardmodel.c:224-405): ray ir of obs
+ * through atm as given (no hydrostatic balance, mask or field of view),
+ * traced, refined at aerosol/cloud layer edges and integrated ON THE GPU
+ * with scattering sources of order `scattering` (0: none, aerosol/cloud
+ * extinction per ctl->sca_ext when ctl->sca_n > 0); writes obs->rad[*][ir],
+ * obs->tau[*][ir] and obs->tpz/tplon/tplat[ir]. */
+void formod_pencil(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, int scattering, int ir);
+
+/* Replaces formod_fov (src/forwardmodel.c:156-220): field-of-view
+ * convolution of obs over tangent height with the shape of ctl->fov
+ * (nothing when it is "-"); host post-processing, as in formod(). */
+void formod_fov(ctl_t *ctl, obs_t *obs);
+
+/* Replaces read_shape (src/forwardmodel.c:577-606): the two columns of a
+ * filter or field-of-view file into x, y (NSHAPE points at most), *n the
+ * count.  Host file input. */
+void read_shape(const char *filename, double *x, double *y, int *n);
+
+/* Host helpers on the reference's host-side structs (a caller's tbl_t and
+ * los_t live in host memory; the GPU forward model never calls these).
+ *
+ * read_tbl (src/forwardmodel.c:610-739): the emissivity tables
+ * <tblbase>_<nu>_<emitter>.bin, else .tab, of every (emitter, channel)
+ * into tbl (np = -1 for a missing table); binary rows longer than
+ * TBLNUMAX are refused rather than read misaligned.
+ * srcfunc_planck (src/forwardmodel.c:743-794): filter-weighted Planck
+ * source of every channel at temperature t into src[nd] (the table of a
+ * channel set is built on first use and kept).
+ * formod_continua (src/forwardmodel.c:120-152): continuum extinction of
+ * every channel at LOS point ip into beta[nd].
+ * intpol_tbl (src/forwardmodel.c:409-502): EGA transmittances of LOS point
+ * ip; tau_path carries the path state (initialised to 1 at ip <= 0),
+ * tau_seg[nd] receives the segment transmittance.
+ * intpol_tbl_eps / intpol_tbl_u (src/forwardmodel.c:506-542): emissivity
+ * at column density u, column density at emissivity eps, on row
+ * (ig, id, ip, it).  locate_tbl (src/forwardmodel.c:546-565): bisection
+ * on a float array, the largest i < n-1 with xx[i] <= x. */
+void read_tbl(ctl_t *ctl, tbl_t *tbl);
+void srcfunc_planck(ctl_t *ctl, double t, double *src);
+void formod_continua(ctl_t *ctl, los_t *los, int ip, double *beta);
+void intpol_tbl(ctl_t *ctl, tbl_t *tbl, los_t *los, int ip, double tau_path[NGMAX][NDMAX],
+                double tau_seg[NDMAX]);
+double intpol_tbl_eps(tbl_t *tbl, int ig, int id, int ip, int it, double u);
+double intpol_tbl_u(tbl_t *tbl, int ig, int id, int ip, int it, double eps);
+int locate_tbl(float *xx, int n, double x);
 
 /* ------------------------------------------------------------------------
  * Plain C-ABI.
@@ -383,8 +467,8 @@ int jsc_formod_batch(jsc_model *m, const ctl_t *ctl, const jsc_batch_input *in,
  * Concurrency: the scratch is one per device, so two calls whose GPU work
  * overlaps would race on it.  The library holds a per-device lock for the
  * whole call and every call waits for its stream before it returns, so
- * calls from several host threads run one after another.  After a call that
- * returned JSC_ERR_CUDA, synchronise the stream before the next call. */
+ * calls from several host threads run one after another; a call that fails
+ * after queueing GPU work waits for its stream before it releases the lock. */
 #define JSC_NOALLOC_SCRATCH_BYTES (64u << 20)
 int jsc_formod_batch_noalloc(jsc_model *m, const ctl_t *ctl,
                              const jsc_batch_input *in,
@@ -458,8 +542,8 @@ int jsc_batch_set_nalpha(jsc_batch *b, int nalpha);
  * (ipr,it0+1), (ipr+1,it1), (ipr+1,it1+1), the interval found for the
  * path emissivity (intpol_tbl_u) and the one found for the extended column
  * (intpol_tbl_eps); the checksum folds D_0, D_1, ... the same way.  Enable
- * before jsc_batch_run (the run then uses the default launch variant of
- * the selected kernel family); out is [n_rays][nd]. */
+ * before jsc_batch_run (the run keeps the selected launch variant, which
+ * computes its digests like every other); out is [n_rays][nd]. */
 int jsc_batch_set_digest(jsc_batch *b, int on);
 int jsc_batch_index_digest(jsc_batch *b, uint64_t *out);
 

@@ -22,7 +22,7 @@ OBJ = os.path.join(OUT, "obj")
 LIB = os.path.join(OUT, "libjurassic_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-C_SRCS = ["model_host.c", "formod.c", "optprop.c"]
+C_SRCS = ["model_host.c", "formod.c", "optprop.c", "compat.c"]
 CU_SRCS = ["model_dev.cu", "batch.cu", "ega_g2.cu", "ega_g4.cu", "ega_g8.cu",
            "ega_gmax.cu", "ega_lane_s.cu", "ega_lane_l.cu", "noalloc.cu", "surrogate.cu",
            "surrogate_tc.cu", "mie.cu"]

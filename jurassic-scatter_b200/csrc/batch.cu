@@ -421,7 +421,6 @@ static const int kNumEgaVariants = 14;
 static_assert(kNumEgaVariants <= 32, "ega_variant_ms holds 32 timings");
 static const int kLaneBase = 9;
 static const int kEgaDefault = JSC_EGA_DEFAULT_VARIANT;  // default of clear-air runs
-// Index digests run the default variant of the selected kernel family.
 
 // Default launch variant of runs with aerosol/cloud layers (the scattering
 // path and its child batches): the lane family, 10 % faster than the
@@ -448,9 +447,9 @@ static int launch_ega(const EgaArgs &ea, int nr, int ndp, int ng, int variant,
   const unsigned g128 = (unsigned)((threads + 127) / 128);
   const unsigned g256 = (unsigned)((threads + 255) / 256);
   const int v = (variant >= 0 && variant < kNumEgaVariants) ? variant : kEgaDefault;
-  const bool dig = ea.digest != nullptr;  // index digests: default variant only
+  const bool dig = ea.digest != nullptr;  // index digests (every variant has them)
   if (kEgaVariants[v].lane) {
-    const int lv = dig ? 0 : v - kLaneBase;
+    const int lv = v - kLaneBase;
     if (ng <= 4) jsc_ega_lane_launch_s(ea, lv, dig, s);
     else jsc_ega_lane_launch_l(ea, lv, dig, s);
     JSC_LAUNCH_CHECK();

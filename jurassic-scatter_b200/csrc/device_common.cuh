@@ -46,50 +46,16 @@ __device__ __forceinline__ int grid_code(int np, const double *gp, const int *gn
 
 
 // Continuum extinction of one channel at one LOS point
-// (src/forwardmodel.c:120-152 with src/continua.c:5-2049).
+// (src/forwardmodel.c:120-152 with src/continua.c:5-2049): jsc_continuum
+// with the model's emitter indices and the run's switches.
 __device__ __forceinline__ double continua(const jsc_dev_model &m,
                                            const jsc_run_cfg &cfg,
                                            const jsc_ctm_coef &c, double nu,
                                            double kwin, double P, double T,
                                            double DS, double qh2o,
                                            const double *u) {
-  double beta = kwin;
-  if (cfg.ctm_co2) {
-    double ctm = 0;
-    if (m.ig_co2 >= 0 && c.co2_on) {
-      const double dt230 = T - 230, dt260 = T - 260, dt296 = T - 296;
-      const double ctw = dt260 * 5.050505e-4 * dt296 * c.co2_c230 -
-                         dt230 * 9.259259e-4 * dt296 * c.co2_c260 +
-                         dt230 * 4.208754e-4 * dt260 * c.co2_c296;
-      ctm = u[m.ig_co2] / JSC_AVOGADRO / 1000 * P / JSC_P0 * ctw;
-    }
-    beta += ctm / DS;
-  }
-  if (cfg.ctm_h2o) {
-    double ctm = 0;
-    if (m.ig_h2o >= 0 && c.h2o_on) {
-      const double ctwslf = c.h2o_self296 * pow(c.h2o_ratio, (296 - T) / (296 - 260));
-      const double a1 = nu * u[m.ig_h2o] * tanh(.7193876 / T * nu);
-      const double a2 = 296 / T;
-      const double a3 = P / JSC_P0 * (qh2o * ctwslf + (1 - qh2o) * c.h2o_frn) * 1e-20;
-      ctm = a1 * a2 * a3;
-    }
-    beta += ctm / DS;
-  }
-  if (cfg.ctm_n2 && c.n2_on) {
-    const double t0 = 273, tr = 296, q_n2 = 0.79;
-    const double pp = P / JSC_P0, tt = t0 / T;
-    beta += 0.1 * (pp * pp) * (tt * tt) * q_n2 * c.n2_b *
-            exp(c.n2_beta * (1 / tr - 1 / T)) *
-            (q_n2 + (1 - q_n2) * (1.294 - 0.4545 * T / tr));
-  }
-  if (cfg.ctm_o2 && c.o2_on) {
-    const double t0 = 273, tr = 296, q_o2 = 0.21;
-    const double pp = P / JSC_P0, tt = t0 / T;
-    beta += 0.1 * (pp * pp) * (tt * tt) * q_o2 * c.o2_b *
-            exp(c.o2_beta * (1 / tr - 1 / T));
-  }
-  return beta;
+  return jsc_continuum(&c, m.ig_co2, m.ig_h2o, cfg.ctm_co2, cfg.ctm_h2o, cfg.ctm_n2,
+                       cfg.ctm_o2, nu, kwin, P, T, DS, qh2o, u);
 }
 
 // Key of node i (u or eps).

@@ -211,12 +211,13 @@ void jsc_ega_launch_g4(const EgaArgs &, unsigned, unsigned, int, bool, cudaStrea
 void jsc_ega_launch_g8(const EgaArgs &, unsigned, unsigned, int, bool, cudaStream_t);
 void jsc_ega_launch_gmax(const EgaArgs &, unsigned, unsigned, int, bool, cudaStream_t);
 
-// Index digests run variant 6 (128 threads, 12 blocks per SM, rolled
-// emitter loop), the default of this kernel family.
+// Default variant of this kernel family: 128 threads, 12 blocks per SM,
+// rolled emitter loop.  Index digests run the selected variant (every
+// variant has a digest instance).
 #define JSC_EGA_DEFAULT_VARIANT 6
 #define JSC_EGA_LAUNCHER(NAME, G)                                                      \
   void NAME(const EgaArgs &ea, unsigned g128, unsigned g256, int v, bool dig,          \
             cudaStream_t s) {                                                          \
-    if (dig) ega_launch_variant<G, true>(ea, g128, g256, JSC_EGA_DEFAULT_VARIANT, s);  \
+    if (dig) ega_launch_variant<G, true>(ea, g128, g256, v, s);                        \
     else ega_launch_variant<G, false>(ea, g128, g256, v, s);                           \
   }

@@ -194,15 +194,10 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
 }
 
 // Launch variants of ega_lane_kernel: (threads per block, minimum resident
-// blocks per SM).  Index digests run variant 0 only.
-template <int GP>
-static void ega_lane_variant(const EgaArgs &ea, int v, bool dig, cudaStream_t s) {
+// blocks per SM), each with and without index digests.
+template <int GP, bool DIG>
+static void ega_lane_launch(const EgaArgs &ea, int v, cudaStream_t s) {
   const int64_t threads = (int64_t)ea.n_rays * ea.m.nd * GP;
-  if (dig) {
-    ega_lane_kernel<GP, true, 128, 12><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(ea);
-    return;
-  }
-  constexpr bool DIG = false;
   switch (v) {
     case 1: ega_lane_kernel<GP, DIG, 128, 8><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(ea); break;
     case 2: ega_lane_kernel<GP, DIG, 256, 4><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(ea); break;
@@ -210,6 +205,12 @@ static void ega_lane_variant(const EgaArgs &ea, int v, bool dig, cudaStream_t s)
     case 4: ega_lane_kernel<GP, DIG, 512, 2><<<(unsigned)((threads + 511) / 512), 512, 0, s>>>(ea); break;
     default: ega_lane_kernel<GP, DIG, 128, 12><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(ea); break;
   }
+}
+
+template <int GP>
+static void ega_lane_variant(const EgaArgs &ea, int v, bool dig, cudaStream_t s) {
+  if (dig) ega_lane_launch<GP, true>(ea, v, s);
+  else ega_lane_launch<GP, false>(ea, v, s);
 }
 
 // Launchers (ega_lane_s.cu: up to 4 emitters, ega_lane_l.cu: more and the

@@ -20,6 +20,9 @@ static pthread_mutex_t g_lock = PTHREAD_MUTEX_INITIALIZER;
 static jsc_model *g_model;
 static jsc_batch *g_batch;
 static ctl_t *g_key;          /* ctl the cache was built for */
+/* Batch of formod_pencil (one ray; its scattering order in sca_mult). */
+static jsc_batch *g_pbatch;
+static ctl_t *g_pkey;
 /* Batch of jsc_kernel (undisturbed + disturbed profiles) and its capacity. */
 static jsc_batch *g_jbatch;
 static int g_jcap_atm, g_jcap_lev, g_jcap_rays;
@@ -63,9 +66,11 @@ static int ensure_cache(const ctl_t *ctl) {
   if (g_key && !same_tables(g_key, ctl)) {
     jsc_batch_destroy(g_batch);
     jsc_batch_destroy(g_jbatch);
+    jsc_batch_destroy(g_pbatch);
     jsc_model_destroy(g_model);
     g_batch = NULL;
     g_jbatch = NULL;
+    g_pbatch = NULL;
     g_model = NULL;
   }
   if (g_key && !same_switches(g_key, ctl)) {
@@ -188,6 +193,85 @@ static int fov_convolve(const ctl_t *ctl, obs_t *obs) {
   return st;
 }
 
+/* Run rays [r0, r0 + nr) of obs through atm on batch b (held under g_lock)
+ * and write their radiances, transmittances and tangent points into obs:
+ * the atmosphere is packed as one profile (IP 1 and IP 3, whose points are
+ * weighted one by one) or, for IP 2, as a new profile wherever lon/lat
+ * change, as intpol_atm_2d groups them (src/atmosphere.c:343-356). */
+static int run_rays(jsc_batch *b, const ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero,
+                    int r0, int nr) {
+  const int nd = ctl->nd, np = atm->np, ng = ctl->ng, nw = ctl->nw;
+  int st = JSC_OK;
+  size_t nbuf = (size_t)np * (size_t)(ng + nw) + 2 * (size_t)nr * nd + 3 * (size_t)nr;
+  double *buf = (double *)malloc(nbuf * sizeof(double));
+  int *ray_atm = (int *)calloc((size_t)nr, sizeof(int));
+  int *off = (int *)malloc(((size_t)np + 1) * sizeof(int)), n_atm = 1;
+  if (!buf || !ray_atm || !off) {
+    st = JSC_ERR_NOMEM;
+  } else {
+    double *q = buf, *k = q + (size_t)np * ng, *rad = k + (size_t)np * nw;
+    double *tau = rad + (size_t)nr * nd, *tp = tau + (size_t)nr * nd;
+    for (int ig = 0; ig < ng; ig++) memcpy(q + (size_t)ig * np, atm->q[ig], np * sizeof(double));
+    for (int iw = 0; iw < nw; iw++) memcpy(k + (size_t)iw * np, atm->k[iw], np * sizeof(double));
+    off[0] = 0;
+    if (ctl->ip == 2)
+      for (int ip = 1; ip < np; ip++)
+        if (atm->lon[ip] != atm->lon[ip - 1] || atm->lat[ip] != atm->lat[ip - 1])
+          off[n_atm++] = ip;
+    off[n_atm] = np;
+    jsc_batch_input in;
+    memset(&in, 0, sizeof(in));
+    in.n_atm = n_atm;
+    in.n_levels = np;
+    in.atm_off = off;
+    in.z = atm->z;
+    in.lon = atm->lon;
+    in.lat = atm->lat;
+    in.p = atm->p;
+    in.t = atm->t;
+    in.q = q;
+    in.k = k;
+    in.n_rays = nr;
+    in.ray_atm = ray_atm;
+    in.time = obs->time + r0;
+    in.obsz = obs->obsz + r0;
+    in.obslon = obs->obslon + r0;
+    in.obslat = obs->obslat + r0;
+    in.vpz = obs->vpz + r0;
+    in.vplon = obs->vplon + r0;
+    in.vplat = obs->vplat + r0;
+    jsc_batch_output out;
+    memset(&out, 0, sizeof(out));
+    out.rad = rad;
+    out.tau = tau;
+    out.tpz = tp;
+    out.tplon = tp + nr;
+    out.tplat = tp + 2 * nr;
+    /* Aerosol/cloud layers and optical properties (read_aero +
+     * get_opt_prop of the caller, or of this call for retrievals). */
+    if (ctl->sca_n > 0) st = jsc_batch_set_aero(b, aero);
+    if (!st) st = jsc_batch_upload(b, &in, NULL);
+    if (!st) st = jsc_batch_run(b, NULL);
+    if (!st) st = jsc_batch_download(b, &out, NULL);
+    if (!st) {
+      for (int i = 0; i < nr; i++) {
+        const int ir = r0 + i;
+        obs->tpz[ir] = tp[i];
+        obs->tplon[ir] = tp[nr + i];
+        obs->tplat[ir] = tp[2 * nr + i];
+        for (int id = 0; id < nd; id++) {
+          obs->rad[id][ir] = rad[(size_t)i * nd + id];
+          obs->tau[id][ir] = tau[(size_t)i * nd + id];
+        }
+      }
+    }
+  }
+  free(off);
+  free(ray_atm);
+  free(buf);
+  return st;
+}
+
 static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
   const int nd = ctl->nd, nr = obs->nr, np = atm->np, ng = ctl->ng, nw = ctl->nw;
   int st = JSC_OK;
@@ -204,7 +288,6 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
 
   /* Observation mask (src/forwardmodel.c:25-28). */
   unsigned char *mask = (unsigned char *)malloc((size_t)nd * (nr > 0 ? nr : 1));
-  double *buf = NULL;
   if (!mask) return JSC_ERR_NOMEM;
   for (int id = 0; id < nd; id++)
     for (int ir = 0; ir < nr; ir++) mask[(size_t)id * nr + ir] = !isfinite(obs->rad[id][ir]);
@@ -225,83 +308,8 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
 
   pthread_mutex_lock(&g_lock);
   st = ensure_cache(ctl);
-  if (!st && nr > 0) {
-    /* Pack the atmosphere as one profile and the rays. */
-    size_t nbuf = (size_t)np * (size_t)(ng + nw) + 2 * (size_t)nr * nd + 3 * (size_t)nr;
-    buf = (double *)malloc(nbuf * sizeof(double));
-    int *ray_atm = (int *)calloc((size_t)nr, sizeof(int));
-    if (!buf || !ray_atm) {
-      st = JSC_ERR_NOMEM;
-    } else {
-      double *q = buf, *k = q + (size_t)np * ng, *rad = k + (size_t)np * nw;
-      double *tau = rad + (size_t)nr * nd, *tp = tau + (size_t)nr * nd;
-      for (int ig = 0; ig < ng; ig++) memcpy(q + (size_t)ig * np, atm->q[ig], np * sizeof(double));
-      for (int iw = 0; iw < nw; iw++) memcpy(k + (size_t)iw * np, atm->k[iw], np * sizeof(double));
-      /* Profiles: one (IP 1, and IP 3, whose points are weighted one by
-       * one), or for IP 2 a new one wherever lon/lat change, as
-       * intpol_atm_2d groups them (src/atmosphere.c:343-356). */
-      int *off = (int *)malloc(((size_t)np + 1) * sizeof(int)), n_atm = 1;
-      if (!off) {
-        st = JSC_ERR_NOMEM;
-      } else {
-        off[0] = 0;
-        if (ctl->ip == 2)
-          for (int ip = 1; ip < np; ip++)
-            if (atm->lon[ip] != atm->lon[ip - 1] || atm->lat[ip] != atm->lat[ip - 1])
-              off[n_atm++] = ip;
-        off[n_atm] = np;
-      }
-      jsc_batch_input in;
-      memset(&in, 0, sizeof(in));
-      in.n_atm = n_atm;
-      in.n_levels = np;
-      in.atm_off = off;
-      in.z = atm->z;
-      in.lon = atm->lon;
-      in.lat = atm->lat;
-      in.p = atm->p;
-      in.t = atm->t;
-      in.q = q;
-      in.k = k;
-      in.n_rays = nr;
-      in.ray_atm = ray_atm;
-      in.time = obs->time;
-      in.obsz = obs->obsz;
-      in.obslon = obs->obslon;
-      in.obslat = obs->obslat;
-      in.vpz = obs->vpz;
-      in.vplon = obs->vplon;
-      in.vplat = obs->vplat;
-      jsc_batch_output out;
-      memset(&out, 0, sizeof(out));
-      out.rad = rad;
-      out.tau = tau;
-      out.tpz = tp;
-      out.tplon = tp + nr;
-      out.tplat = tp + 2 * nr;
-      /* Aerosol/cloud layers and optical properties (read_aero +
-       * get_opt_prop of the caller, or of this call for retrievals). */
-      if (!st && ctl->sca_n > 0) st = jsc_batch_set_aero(g_batch, aero);
-      if (!st) st = jsc_batch_upload(g_batch, &in, NULL);
-      if (!st) st = jsc_batch_run(g_batch, NULL);
-      if (!st) st = jsc_batch_download(g_batch, &out, NULL);
-      if (!st) {
-        for (int ir = 0; ir < nr; ir++) {
-          obs->tpz[ir] = tp[ir];
-          obs->tplon[ir] = tp[nr + ir];
-          obs->tplat[ir] = tp[2 * nr + ir];
-          for (int id = 0; id < nd; id++) {
-            obs->rad[id][ir] = rad[(size_t)ir * nd + id];
-            obs->tau[id][ir] = tau[(size_t)ir * nd + id];
-          }
-        }
-      }
-      free(off);
-    }
-    free(ray_atm);
-  }
+  if (!st && nr > 0) st = run_rays(g_batch, ctl, atm, obs, aero, 0, nr);
   pthread_mutex_unlock(&g_lock);
-  free(buf);
 
   /* Field-of-view convolution (src/forwardmodel.c:102). */
   if (!st && ctl->fov[0] != '-') st = fov_convolve(ctl, obs);
@@ -320,14 +328,83 @@ static int formod_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
   return st;
 }
 
-void formod(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
-  int st = formod_impl(ctl, atm, obs, aero);
+/* End of a drop-in call: record the status for jsc_last_status() and, with
+ * exit-on-error (the default), print the message and exit like the
+ * reference's ERRMSG (src/jurassic.h:48-52). */
+int jsc_finish_call(int st, const char *func) {
   g_last_status = st;
   if (st && g_exit_on_error) {
-    printf("\nError (%s, %s, l%d): %s: %s\n\n", __FILE__, __func__, __LINE__,
+    printf("\nError (%s, %s, l%d): %s: %s\n\n", __FILE__, func, __LINE__,
            jsc_status_string(st), jsc_last_error_message());
     exit(EXIT_FAILURE);
   }
+  return st;
+}
+
+void formod(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero) {
+  jsc_finish_call(formod_impl(ctl, atm, obs, aero), "formod");
+}
+
+/* Batch of formod_pencil for the switches of c (hydrostatic balance off,
+ * scattering order in c->sca_mult), one ray; held under g_lock after
+ * ensure_cache. */
+static int ensure_pencil(const ctl_t *c) {
+  if (g_pbatch && same_switches(g_pkey, c)) return JSC_OK;
+  jsc_batch_destroy(g_pbatch);
+  g_pbatch = NULL;
+  if (!g_pkey && !(g_pkey = (ctl_t *)malloc(sizeof(ctl_t)))) return JSC_ERR_NOMEM;
+  memcpy(g_pkey, c, sizeof(ctl_t));
+  return jsc_batch_create(g_model, c, NPMAX / 2, NPMAX, 1, 0, &g_pbatch);
+}
+
+static int pencil_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, int scattering,
+                       int ir) {
+  const int nd = ctl->nd, np = atm->np, ng = ctl->ng, nw = ctl->nw;
+  if (nd < 1 || nd > NDMAX || ng < 0 || ng > NGMAX || nw < 0 || nw > NWMAX || np < 2 ||
+      np > NPMAX || ir < 0 || ir >= obs->nr || obs->nr > NRMAX || scattering < 0) {
+    jsc_set_error(JSC_ERR_ARG, "formod_pencil: invalid sizes or ray (nd=%d ng=%d np=%d "
+                  "ir=%d nr=%d scattering=%d)", nd, ng, np, ir, obs->nr, scattering);
+    return JSC_ERR_ARG;
+  }
+  if (ctl->sca_n > 0 && !aero) {
+    jsc_set_error(JSC_ERR_ARG, "formod_pencil: SCA_N=%d needs the aerosol/cloud data",
+                  ctl->sca_n);
+    return JSC_ERR_ARG;
+  }
+  ctl_t *c = (ctl_t *)malloc(sizeof(ctl_t));
+  if (!c) return JSC_ERR_NOMEM;
+  memcpy(c, ctl, sizeof(ctl_t));
+  c->hydz = -999;          /* the pencil takes atm as it is */
+  c->sca_mult = scattering;
+  pthread_mutex_lock(&g_lock);
+  int st = ensure_cache(ctl);
+  if (!st) st = ensure_pencil(c);
+  if (!st) st = run_rays(g_pbatch, c, atm, obs, aero, ir, 1);
+  pthread_mutex_unlock(&g_lock);
+  free(c);
+  return st;
+}
+
+/* Replaces formod_pencil (src/forwardmodel.c:224-405): ray ir of obs through
+ * atm as it is (no hydrostatic balance, no mask, no field of view), traced,
+ * refined at aerosol/cloud layer edges and integrated on the GPU with
+ * scattering sources of order `scattering` (0: none); writes
+ * obs->rad[*][ir], obs->tau[*][ir] and obs->tp*[ir]. */
+void formod_pencil(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, int scattering, int ir) {
+  jsc_finish_call(pencil_impl(ctl, atm, obs, aero, scattering, ir), "formod_pencil");
+}
+
+/* Replaces formod_fov (src/forwardmodel.c:156-220): the field-of-view
+ * convolution of obs over tangent height, nothing when ctl->fov is "-". */
+void formod_fov(ctl_t *ctl, obs_t *obs) {
+  if (ctl->fov[0] == '-') return;
+  jsc_finish_call(fov_convolve(ctl, obs), "formod_fov");
+}
+
+/* Replaces read_shape (src/forwardmodel.c:577-606): two columns x, y of a
+ * filter or field-of-view file, *n points (at most NSHAPE). */
+void read_shape(const char *filename, double *x, double *y, int *n) {
+  jsc_finish_call(jsc_read_filter(filename, x, y, n), "read_shape");
 }
 
 /* Release the cached model and batches (tests and long-running hosts). */
@@ -335,12 +412,16 @@ void jsc_release_cache(void) {
   pthread_mutex_lock(&g_lock);
   jsc_batch_destroy(g_batch);
   jsc_batch_destroy(g_jbatch);
+  jsc_batch_destroy(g_pbatch);
   jsc_model_destroy(g_model);
   g_batch = NULL;
   g_jbatch = NULL;
+  g_pbatch = NULL;
   g_model = NULL;
   free(g_key);
   g_key = NULL;
+  free(g_pkey);
+  g_pkey = NULL;
   pthread_mutex_unlock(&g_lock);
 }
 

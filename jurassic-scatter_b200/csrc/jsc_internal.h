@@ -6,6 +6,8 @@
 #ifndef JSC_INTERNAL_H
 #define JSC_INTERNAL_H
 
+#include <math.h>
+
 #include "jurassic_b200.h"
 
 #ifdef __CUDACC__
@@ -98,6 +100,55 @@ typedef struct {
   double o2_b, o2_beta;
 } jsc_ctm_coef;
 
+/* Continuum extinction of one channel at one LOS point
+ * (src/forwardmodel.c:120-152 with src/continua.c:5-2049): the window
+ * extinction kwin, the CO2 and H2O continua over the segment's columns u
+ * (per emitter; emitter indices ig_co2/ig_h2o, -1 when absent) divided by
+ * the segment length DS, and the N2 and O2 collision-induced bands; c holds
+ * the channel's coefficients (jsc_ctm_coefficients), ctm_* the CTM_*
+ * switches.  Shared by the GPU kernels and the host helper formod_continua. */
+JSC_HD double jsc_continuum(const jsc_ctm_coef *c, int ig_co2, int ig_h2o, int ctm_co2,
+                            int ctm_h2o, int ctm_n2, int ctm_o2, double nu, double kwin,
+                            double P, double T, double DS, double qh2o, const double *u) {
+  double beta = kwin;
+  if (ctm_co2) {
+    double ctm = 0;
+    if (ig_co2 >= 0 && c->co2_on) {
+      const double dt230 = T - 230, dt260 = T - 260, dt296 = T - 296;
+      const double ctw = dt260 * 5.050505e-4 * dt296 * c->co2_c230 -
+                         dt230 * 9.259259e-4 * dt296 * c->co2_c260 +
+                         dt230 * 4.208754e-4 * dt260 * c->co2_c296;
+      ctm = u[ig_co2] / JSC_AVOGADRO / 1000 * P / JSC_P0 * ctw;
+    }
+    beta += ctm / DS;
+  }
+  if (ctm_h2o) {
+    double ctm = 0;
+    if (ig_h2o >= 0 && c->h2o_on) {
+      const double ctwslf = c->h2o_self296 * pow(c->h2o_ratio, (296 - T) / (296 - 260));
+      const double a1 = nu * u[ig_h2o] * tanh(.7193876 / T * nu);
+      const double a2 = 296 / T;
+      const double a3 = P / JSC_P0 * (qh2o * ctwslf + (1 - qh2o) * c->h2o_frn) * 1e-20;
+      ctm = a1 * a2 * a3;
+    }
+    beta += ctm / DS;
+  }
+  if (ctm_n2 && c->n2_on) {
+    const double t0 = 273, tr = 296, q_n2 = 0.79;
+    const double pp = P / JSC_P0, tt = t0 / T;
+    beta += 0.1 * (pp * pp) * (tt * tt) * q_n2 * c->n2_b *
+            exp(c->n2_beta * (1 / tr - 1 / T)) *
+            (q_n2 + (1 - q_n2) * (1.294 - 0.4545 * T / tr));
+  }
+  if (ctm_o2 && c->o2_on) {
+    const double t0 = 273, tr = 296, q_o2 = 0.21;
+    const double pp = P / JSC_P0, tt = t0 / T;
+    beta += 0.1 * (pp * pp) * (tt * tt) * q_o2 * c->o2_b *
+            exp(c->o2_beta * (1 / tr - 1 / T));
+  }
+  return beta;
+}
+
 /* Everything the host reads or derives before upload. */
 typedef struct {
   int ng, nd, nw;
@@ -115,6 +166,8 @@ typedef struct {
 int jsc_host_model_load(const ctl_t *ctl, jsc_host_model *hm);
 void jsc_host_model_free(jsc_host_model *hm);
 int jsc_read_filter(const char *filename, double *nu, double *f, int *n);
+int jsc_read_tables(const ctl_t *ctl, jsc_host_tables *ht);
+int jsc_planck_only(const ctl_t *ctl, jsc_host_model *hm);
 void jsc_ctm_coefficients(const ctl_t *ctl, jsc_ctm_coef *c, int id);
 double jsc_gsl_expm1(double x);
 double jsc_gsl_log1p(double x);
@@ -122,6 +175,9 @@ int jsc_find_emitter(const ctl_t *ctl, const char *name);
 
 /* Error reporting shared by C and CUDA parts. */
 void jsc_set_error(int status, const char *fmt, ...);
+/* End of a drop-in call (formod.c): records the status, and prints and
+ * exits like the reference's ERRMSG unless jsc_set_exit_on_error(0). */
+int jsc_finish_call(int st, const char *func);
 
 /* Mie efficiencies and phase functions of n (size parameter, refractive
  * index) tasks on GPU `device` (mie.cu): out[i][0] = Q_ext,

@@ -586,6 +586,27 @@ int jsc_host_model_load(const ctl_t *ctl, jsc_host_model *hm) {
   return JSC_OK;
 }
 
+/* The emissivity tables of ctl alone (read_tbl's part of the model). */
+int jsc_read_tables(const ctl_t *ctl, jsc_host_tables *ht) {
+  memset(ht, 0, sizeof(*ht));
+  if (ctl->ng < 0 || ctl->ng > NGMAX || ctl->nd < 1 || ctl->nd > NDMAX) {
+    jsc_set_error(JSC_ERR_ARG, "Invalid NG/ND (%d/%d)", ctl->ng, ctl->nd);
+    return JSC_ERR_ARG;
+  }
+  return read_tables(ctl, ht);
+}
+
+/* The filter-weighted Planck tables of ctl's channels alone. */
+int jsc_planck_only(const ctl_t *ctl, jsc_host_model *hm) {
+  memset(hm, 0, sizeof(*hm));
+  if (ctl->nd < 1 || ctl->nd > NDMAX) {
+    jsc_set_error(JSC_ERR_ARG, "Invalid ND (%d)", ctl->nd);
+    return JSC_ERR_ARG;
+  }
+  hm->nd = ctl->nd;
+  return planck_tables(ctl, hm);
+}
+
 void jsc_host_model_free(jsc_host_model *hm) {
   free(hm->tables.tab);
   free(hm->tables.u);

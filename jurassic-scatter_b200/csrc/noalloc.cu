@@ -340,6 +340,10 @@ extern "C" int jsc_formod_batch_noalloc(jsc_model *m, const ctl_t *ctl,
     st = JSC_ERR_CUDA;
   } else {
     st = noalloc_run(m, ctl, in, out, (cudaStream_t)stream, g_scratch[dev]);
+    // A failed call may leave copies or kernels queued on its stream that
+    // still write the scratch; wait for them before the next caller (on any
+    // stream) gets the lock.  The wait's own error is not this call's.
+    if (st != JSC_OK) (void)cudaStreamSynchronize((cudaStream_t)stream);
   }
   pthread_mutex_unlock(&g_lock[dev]);
   return st;

@@ -35,6 +35,19 @@ def formod(ctl, atm, obs, aero=None, exit_on_error=False):
     L.check(lib.jsc_last_status(), "formod")
 
 
+def formod_pencil(ctl, atm, obs, aero=None, scattering=0, ir=0):
+    """Drop-in formod_pencil: ray ir of obs through atm as given, on the
+    GPU, scattering sources of order `scattering`; raises JscError on
+    failure."""
+    lib = L.load()
+    if aero is None:
+        aero = S.AeroT()
+    lib.jsc_set_exit_on_error(0)
+    lib.formod_pencil(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero),
+                      int(scattering), int(ir))
+    L.check(lib.jsc_last_status(), "formod_pencil")
+
+
 def read_aero(ctl, filename, dirname=None):
     """aero_t with the modes of an aerosol file (jsc_read_aero)."""
     aero = S.AeroT()

@@ -27,6 +27,8 @@ EXPORTS = [
     "jsc_batch_set_fixed", "jsc_batch_download_async", "jsc_batch_async_status",
     "jsc_batch_graph_capture", "jsc_batch_graph_launch", "jsc_surrogate_set_tensor_path",
     "jsc_atm2x", "jsc_x2atm", "jsc_obs2y", "jsc_kernel", "jsc_read_aero", "jsc_get_opt_prop",
+    "formod_pencil", "formod_fov", "read_shape", "read_tbl", "srcfunc_planck",
+    "formod_continua", "intpol_tbl", "intpol_tbl_eps", "intpol_tbl_u", "locate_tbl",
 ]
 
 
@@ -130,6 +132,16 @@ def load():
         "jsc_batch_surrogate_stats": (i, [vp, P(C.c_int64), P(C.c_int64), P(C.c_int64), P(d),
                                           P(i)]),
         "jsc_formod_batch_noalloc": (i, [vp, P(S.CtlT), P(BatchInput), P(BatchOutput), vp]),
+        "formod_pencil": (None, [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT), i, i]),
+        "formod_fov": (None, [P(S.CtlT), P(S.ObsT)]),
+        "read_shape": (None, [C.c_char_p, P(d), P(d), P(i)]),
+        "read_tbl": (None, [P(S.CtlT), vp]),
+        "srcfunc_planck": (None, [P(S.CtlT), d, P(d)]),
+        "formod_continua": (None, [P(S.CtlT), P(S.LosT), i, P(d)]),
+        "intpol_tbl": (None, [P(S.CtlT), vp, P(S.LosT), i, P(d), P(d)]),
+        "intpol_tbl_eps": (d, [vp, i, i, i, i, d]),
+        "intpol_tbl_u": (d, [vp, i, i, i, i, d]),
+        "locate_tbl": (i, [P(C.c_float), i, d]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -80,16 +80,55 @@ def select_rays(inp, start, end):
     return out
 
 
+def gather_device(group=None):
+    """Device of the all-gather buffers: NCCL moves CUDA tensors only (the
+    rank's current GPU), gloo and MPI move CPU tensors."""
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
 def gather_rows(local, ranges, group=None):
     """All-gather per-rank row blocks (ranges from shard_ranges) into the
-    full array on every rank, over torch.distributed."""
+    full array on every rank, over torch.distributed.  local is this rank's
+    block as a numpy array; the exchange runs on gather_device(group), the
+    result comes back as a numpy array."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size(group)
+    dev = gather_device(group)
+    local = np.ascontiguousarray(local, dtype=np.float64)
     width = local.shape[1:] if local.ndim > 1 else ()
     n_max = max(e - s for s, e in ranges)
-    buf = torch.zeros((n_max,) + tuple(width), dtype=torch.float64)
-    buf[: local.shape[0]] = torch.from_numpy(np.ascontiguousarray(local))
+    buf = torch.zeros((n_max,) + tuple(width), dtype=torch.float64, device=dev)
+    if local.shape[0]:
+        buf[: local.shape[0]] = torch.from_numpy(local).to(dev)
     parts = [torch.zeros_like(buf) for _ in range(world)]
     dist.all_gather(parts, buf, group=group)
-    return np.concatenate([parts[i][: e - s].numpy() for i, (s, e) in enumerate(ranges)])
+    return np.concatenate([parts[i][: e - s].cpu().numpy() for i, (s, e) in enumerate(ranges)])
+
+
+def forward_sharded(ctl, inp, device, group=None, model=None, aero=None, variant=-1):
+    """The multi-GPU forward model of one batch input (every rank passes the
+    same inp): rays are cut into contiguous ranges balanced by the
+    geometric LOS estimate, each rank runs its range on its own GPU
+    through the batch C-ABI, and one all-gather returns the radiances and
+    transmittances of every ray, [n_rays][nd] each, to every rank."""
+    import torch.distributed as dist
+    from . import api
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    geom = {k: inp[k] for k in ("obsz", "obslon", "obslat", "vpz", "vplon", "vplat")}
+    ranges = shard_ranges(estimate_los_points(geom), world)
+    s, e = ranges[rank]
+    nd = ctl.nd
+    if e > s:
+        out = api.formod_batch(ctl, select_rays(inp, s, e), device=device, model=model,
+                               aero=aero, variant=variant)
+        rad, tau = out["rad"], out["tau"]
+    else:
+        rad = tau = np.zeros((0, nd))
+    both = gather_rows(np.concatenate([rad, tau], axis=1), ranges, group)
+    return {"rad": both[:, :nd], "tau": both[:, nd:], "ranges": ranges}

@@ -132,6 +132,43 @@ def set_str(obj, name, value, index=None):
         C.memmove(C.addressof(elem), b, len(b))
 
 
+class LosT(C.Structure):
+    """los_t (src/jurassic.h:352-393): one ray's line of sight."""
+    _fields_ = [
+        ("np", C.c_int),
+        ("z", C.c_double * NLOS), ("lon", C.c_double * NLOS),
+        ("lat", C.c_double * NLOS), ("p", C.c_double * NLOS),
+        ("t", C.c_double * NLOS),
+        ("q", (C.c_double * NGMAX) * NLOS),
+        ("k", (C.c_double * NWMAX) * NLOS),
+        ("aeroi", C.c_int * NLOS),
+        ("aerofac", C.c_double * NLOS),
+        ("tsurf", C.c_double),
+        ("ds", C.c_double * NLOS),
+        ("u", (C.c_double * NGMAX) * NLOS),
+    ]
+
+
+TBLNSMAX = 1201
+
+
+class TblT(C.Structure):
+    """tbl_t (src/jurassic.h:438-471), about 12.5 GB: for layout checks and
+    pointer arithmetic only (allocate it with calloc, never as a ctypes
+    instance)."""
+    _fields_ = [
+        ("np", (C.c_int * NDMAX) * NGMAX),
+        ("nt", ((C.c_int * TBLNPMAX) * NDMAX) * NGMAX),
+        ("nu", (((C.c_int * TBLNTMAX) * TBLNPMAX) * NDMAX) * NGMAX),
+        ("p", ((C.c_double * TBLNPMAX) * NDMAX) * NGMAX),
+        ("t", (((C.c_double * TBLNTMAX) * TBLNPMAX) * NDMAX) * NGMAX),
+        ("u", ((((C.c_float * TBLNUMAX) * TBLNTMAX) * TBLNPMAX) * NDMAX) * NGMAX),
+        ("eps", ((((C.c_float * TBLNUMAX) * TBLNTMAX) * TBLNPMAX) * NDMAX) * NGMAX),
+        ("st", C.c_double * TBLNSMAX),
+        ("sr", (C.c_double * TBLNSMAX) * NDMAX),
+    ]
+
+
 def make_ctl(emitters, nus, tblbase, **kw):
     """ctl_t with the defaults of the reference's read_ctl
     (src/control.c:7-100), then the keyword overrides (lower-case names)."""

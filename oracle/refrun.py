@@ -23,21 +23,7 @@ sys.path.insert(0, os.path.join(REPO, "jurassic-scatter_b200"))
 from jscat import structs as S  # noqa: E402
 
 
-class LosT(C.Structure):
-    """los_t of src/jurassic.h:352-393 (raytrace output)."""
-    _fields_ = [
-        ("np", C.c_int),
-        ("z", C.c_double * S.NLOS), ("lon", C.c_double * S.NLOS),
-        ("lat", C.c_double * S.NLOS), ("p", C.c_double * S.NLOS),
-        ("t", C.c_double * S.NLOS),
-        ("q", (C.c_double * S.NGMAX) * S.NLOS),
-        ("k", (C.c_double * S.NWMAX) * S.NLOS),
-        ("aeroi", C.c_int * S.NLOS),
-        ("aerofac", C.c_double * S.NLOS),
-        ("tsurf", C.c_double),
-        ("ds", C.c_double * S.NLOS),
-        ("u", (C.c_double * S.NGMAX) * S.NLOS),
-    ]
+LosT = S.LosT  # los_t of src/jurassic.h:352-393 (raytrace output)
 
 
 def available():
@@ -149,6 +135,115 @@ def _child(job):
                         "t": S.arr(los.t)[:n].copy(), "ds": S.arr(los.ds)[:n].copy(),
                         "u": S.arr(los.u)[:n, :ng].copy(), "tsurf": los.tsurf})
     return out
+
+
+def _helpers_child(job):
+    """The forwardmodel.h helpers of library job["lib"] (the reference
+    build, or the library under test) on one line of sight: read_tbl into a
+    calloc'd tbl_t, then per LOS point intpol_tbl (path state carried),
+    formod_continua and srcfunc_planck at the point's temperature; plus
+    intpol_tbl_eps/_u on a few rows and locate_tbl on a float array.  The
+    LOS (a los_t as bytes) comes from the reference's raytrace."""
+    _silence()
+    lib = C.CDLL(job["lib"])
+    libc = C.CDLL(None)
+    libc.calloc.restype = C.c_void_p
+    libc.calloc.argtypes = [C.c_size_t, C.c_size_t]
+    P = C.POINTER
+    vp = C.c_void_p
+    lib.read_tbl.argtypes = [P(S.CtlT), vp]
+    lib.intpol_tbl.argtypes = [P(S.CtlT), vp, P(S.LosT), C.c_int, vp, vp]
+    lib.formod_continua.argtypes = [P(S.CtlT), P(S.LosT), C.c_int, P(C.c_double)]
+    lib.srcfunc_planck.argtypes = [P(S.CtlT), C.c_double, P(C.c_double)]
+    for f in (lib.intpol_tbl_eps, lib.intpol_tbl_u):
+        f.restype = C.c_double
+        f.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
+    lib.locate_tbl.restype = C.c_int
+    lib.locate_tbl.argtypes = [P(C.c_float), C.c_int, C.c_double]
+    ctl = S.make_ctl(**job["ctl"])
+    los = S.LosT.from_buffer_copy(job["los"])
+    ng, nd = ctl.ng, ctl.nd
+    tbl = libc.calloc(1, C.sizeof(S.TblT))
+    if not tbl:
+        raise MemoryError("tbl_t")
+    lib.read_tbl(C.byref(ctl), C.c_void_p(tbl))
+    T = S.TblT
+
+    def view(field, ctype, shape):
+        off = getattr(T, field).offset
+        n = int(np.prod(shape))
+        return np.ctypeslib.as_array((ctype * n).from_address(tbl + off)).reshape(shape).copy()
+
+    out = {"np": view("np", C.c_int, (S.NGMAX, S.NDMAX))[:ng, :nd],
+           "nt": view("nt", C.c_int, (S.NGMAX, S.NDMAX, S.TBLNPMAX))[:ng, :nd],
+           "nu": view("nu", C.c_int, (S.NGMAX, S.NDMAX, S.TBLNPMAX, S.TBLNTMAX))[:ng, :nd],
+           "p": view("p", C.c_double, (S.NGMAX, S.NDMAX, S.TBLNPMAX))[:ng, :nd],
+           "t": view("t", C.c_double, (S.NGMAX, S.NDMAX, S.TBLNPMAX, S.TBLNTMAX))[:ng, :nd]}
+    # rows of emitter 0, channel 0 (the u and eps blocks of one table)
+    blk = (S.TBLNPMAX, S.TBLNTMAX, S.TBLNUMAX)
+    nblk = int(np.prod(blk))
+    for f in ("u", "eps"):
+        base = tbl + getattr(T, f).offset
+        out[f + "00"] = np.ctypeslib.as_array((C.c_float * nblk).from_address(base)).reshape(blk).copy()
+    tau_path = ((C.c_double * S.NDMAX) * S.NGMAX)()
+    tau_seg = (C.c_double * S.NDMAX)()
+    beta = (C.c_double * S.NDMAX)()
+    src = (C.c_double * S.NDMAX)()
+    seg, ctm, plk = [], [], []
+    for ip in range(los.np):
+        lib.intpol_tbl(C.byref(ctl), C.c_void_p(tbl), C.byref(los), ip, C.byref(tau_path),
+                       C.byref(tau_seg))
+        seg.append(np.array(tau_seg[:nd]))
+        lib.formod_continua(C.byref(ctl), C.byref(los), ip, beta)
+        ctm.append(np.array(beta[:nd]))
+        lib.srcfunc_planck(C.byref(ctl), los.t[ip], src)
+        plk.append(np.array(src[:nd]))
+    out["tau_seg"], out["beta"], out["src"] = np.array(seg), np.array(ctm), np.array(plk)
+    out["tau_path"] = np.array([tau_path[g][:nd] for g in range(ng)])
+    vals = []
+    for (ig, id_, ip, it) in ((0, 0, 10, 5), (1, nd - 1, 30, 20), (0, 1, 39, 29)):
+        for x in np.logspace(12, 25, 7):
+            vals.append(lib.intpol_tbl_eps(C.c_void_p(tbl), ig, id_, ip, it, float(x)))
+        for e in np.linspace(0.0, 0.999, 7):
+            vals.append(lib.intpol_tbl_u(C.c_void_p(tbl), ig, id_, ip, it, float(e)))
+    out["lookups"] = np.array(vals)
+    xs = (C.c_float * 9)(*[0.5, 1.0, 2.0, 2.0, 3.5, 7.0, 7.25, 9.0, 12.0])
+    out["locate"] = np.array([lib.locate_tbl(xs, 9, float(x))
+                              for x in (-1.0, 0.5, 1.999, 2.0, 2.0000001, 7.1, 11.99, 12.0, 99.0,
+                                        float("nan"))])
+    return out
+
+
+def forwardmodel_helpers(ctl_kw, los_bytes, lib=REF_LIB, timeout=600):
+    """Outputs of the forwardmodel.h helpers of lib on one line of sight
+    (see _helpers_child)."""
+    return _spawn({"helpers_job": True, "ctl": ctl_kw, "los": los_bytes, "lib": lib}, timeout)
+
+
+def reference_los(ctl_kw, atm, geom, ir=0, timeout=600):
+    """los_t (as bytes) of ray ir traced by the reference's raytrace through
+    atm after its hydrostatic balance."""
+    return _spawn({"los_job": True, "ctl": ctl_kw, "atm": atm, "geom": geom, "ir": ir},
+                  timeout)
+
+
+def _los_child(job):
+    _silence()
+    lib = C.CDLL(REF_LIB)
+    P = C.POINTER
+    lib.raytrace.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT), P(S.LosT), C.c_int]
+    lib.hydrostatic.argtypes = [P(S.CtlT), P(S.AtmT)]
+    ctl = S.make_ctl(**job["ctl"])
+    atm = _atm_struct(job["atm"])
+    g = job["geom"]
+    obs = S.make_obs(g["obsz"], g["obslat"], g["vpz"], g["vplat"], g["obslon"], g["vplon"],
+                     g["time"])
+    lib.hydrostatic(C.byref(ctl), C.byref(atm))
+    los = S.LosT()
+    aero = S.AeroT()
+    lib.raytrace(C.byref(ctl), C.byref(atm), C.byref(obs), C.byref(aero), C.byref(los),
+                 job["ir"])
+    return bytes(los)
 
 
 REF_RET_LIB = os.path.join(HERE, "_ref", "libjurassic_ref_ret.so")
@@ -380,6 +475,10 @@ if __name__ == "__main__":
         _out = _aero_child(_job)
     elif _job.get("kernel_job"):
         _out = _kernel_child(_job)
+    elif _job.get("helpers_job"):
+        _out = _helpers_child(_job)
+    elif _job.get("los_job"):
+        _out = _los_child(_job)
     elif _job.get("sv_job"):
         _out = _state_vector_child(_job)
     else:

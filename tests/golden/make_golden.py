@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
+    make -C oracle ref && python tests/golden/make_golden.py [headline|jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -44,6 +44,26 @@ def mixed_case(workdir):
     ctlkw, atms, ray_atm, geom = synth.batched_case(
         workdir, n_rays=320, rays_per_atm=40, seed=20261203, nus=nus)
     return ctlkw, atms, ray_atm, geom
+
+
+def headline_case(workdir):
+    """The benchmark's headline shape on a small ray count: 8 emitters, all
+    64 channels 700-1400 cm^-1 (the top four take the O2 continuum,
+    src/continua.c:1997-2049), the benchmark's own tables, 3 profiles x 50
+    rays (limb and nadir interleaved)."""
+    return synth.batched_case(workdir, n_rays=150, rays_per_atm=50, seed=20261203)
+
+
+# Channels in the O2 (1360-1805 cm^-1) and N2 (2120-2605 cm^-1) continuum
+# bands (src/continua.c:1935-2049), plus one below both.
+BAND_NU = [1250.0, 1370.0, 1500.0, 1700.0, 2150.0, 2300.0, 2450.0, 2590.0]
+
+
+def band_case(workdir):
+    """2 emitters, the BAND_NU channels, 2 profiles x 30 rays (limb and
+    nadir interleaved): exercises ctmn2 and ctmo2."""
+    return synth.batched_case(workdir, n_rays=60, rays_per_atm=30, seed=20261205,
+                              emitters=synth.CFG0_EMITTERS, nus=BAND_NU)
 
 
 def reference_ctl(ctlkw):
@@ -284,8 +304,21 @@ def fov_fixtures(workdir):
     jacobian_fixture(workdir, "jacobian_limb_fov", False, fov=True)
 
 
+def headline_fixtures(workdir):
+    """headline_batch (the benchmark's 64-channel, 8-emitter shape) and
+    continuum_bands (O2 and N2 continuum channels)."""
+    for name, case in (("headline_batch", headline_case), ("continuum_bands", band_case)):
+        ctlkw, atms, ray_atm, geom = case(workdir)
+        ref = refrun.run(reference_ctl(ctlkw), atms, ray_atm, geom, los=True)
+        port = refrun.run_port(ctlkw, atms, ray_atm, geom, los=True)
+        save(name, ctlkw, atms, ray_atm, geom, ref, port)
+
+
 def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
+    if sys.argv[1:] == ["headline"]:
+        headline_fixtures(workdir)
+        return
     if sys.argv[1:] == ["jacobian"]:
         jacobian_fixture(workdir, "jacobian_limb", False)
         jacobian_fixture(workdir, "jacobian_limb_bt", True)
@@ -318,6 +351,7 @@ def main():
     ref = refrun.run(reference_ctl(ctlkw), atms, ray_atm, geom, los=True)
     port = refrun.run_port(ctlkw, atms, ray_atm, geom, los=True)
     save("mixed_batch", ctlkw, atms, ray_atm, geom, ref, port)
+    headline_fixtures(workdir)
     for ext in ("beta_a", "beta_e"):
         ctlkw, atm, geom, aerofile = aerosol_case(workdir, 0, sca_ext=ext)
         aero = refrun.reference_aero(ctlkw, aerofile, os.path.dirname(aerofile))

@@ -18,7 +18,7 @@ sys.path.insert(0, os.path.join(REPO, "jurassic-scatter_b200"))
 from jscat import structs as S  # noqa: E402
 
 STRUCTS = {"ctl_t": S.CtlT, "obs_t": S.ObsT, "aero_t": S.AeroT, "atm_t": S.AtmT,
-           "queue_t": S.QueueT}
+           "queue_t": S.QueueT, "los_t": S.LosT, "tbl_t": S.TblT}
 
 
 def layout_program(header_include):
@@ -45,7 +45,9 @@ def measure(include_line, cflags):
 
 
 if __name__ == "__main__":
-    ref = measure('#include "jurassic.h"', ["-I/root/reference/src",
+    sys.path.insert(0, REPO)
+    from oracle import refpath
+    ref = measure('#include "jurassic.h"', ["-I" + refpath.reference_path("src"),
                                            "-I" + os.path.join(REPO, "oracle", "_ref", "include")])
     with open(os.path.join(HERE, "struct_layout.json"), "w") as f:
         json.dump(ref, f, indent=0, sort_keys=True)

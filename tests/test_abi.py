@@ -31,7 +31,7 @@ def test_ctypes_layout_matches_reference():
     from jscat import structs as S
     ref = _golden_layout()
     classes = {"ctl_t": S.CtlT, "obs_t": S.ObsT, "aero_t": S.AeroT,
-               "atm_t": S.AtmT, "queue_t": S.QueueT}
+               "atm_t": S.AtmT, "queue_t": S.QueueT, "los_t": S.LosT, "tbl_t": S.TblT}
     for cname, cls in classes.items():
         assert C.sizeof(cls) == ref[cname + ".sizeof"], cname
         for f in cls._fields_:
@@ -79,27 +79,36 @@ def test_known_answers_planck_brightness():
     assert abs(lib.brightness(REF_PLANCK_270_960, 960.0) - 270.0) < 1e-9
 
 
-def test_drop_in_links_in_place_of_forwardmodel():
-    """A C program written against the reference's API (formod, brightness,
-    planck with the reference structs) compiles and links against the
-    library."""
-    prog = r'''
-#include <stdio.h>
-#include "jurassic_b200.h"
-int main(void) {
-  static ctl_t ctl; static atm_t atm; static obs_t obs; static aero_t aero;
-  void (*f)(ctl_t *, atm_t *, obs_t *, aero_t *) = formod;
-  printf("%p %.6f %.6f\n", (void *)f, brightness(0.0231451, 960.0), planck(270.0, 960.0));
-  (void)ctl; (void)atm; (void)obs; (void)aero;
-  return 0;
-}
-'''
+def test_drop_in_links_in_place_of_forwardmodel(tmp_path):
+    """The reference's own programs formod and kernel (src/formod.c,
+    src/kernel.c), compiled from its sources and linked against its objects
+    WITHOUT forwardmodel.o plus this library: every symbol they and the
+    reference's scatter.o/misc.o need from forwardmodel.o (formod,
+    formod_pencil, read_shape, planck, brightness, ...) resolves here.
+    Needs the reference tree and the oracle build (make -C oracle ref ret)."""
+    sys.path.insert(0, REPO)
+    from oracle import refpath
     from jscat import lib as L
-    with tempfile.TemporaryDirectory() as d:
-        src, exe = os.path.join(d, "p.c"), os.path.join(d, "p")
-        open(src, "w").write(prog)
-        subprocess.run(["gcc", "-I" + os.path.join(REPO, "include"), src, "-o", exe,
-                        L.LIB_PATH, "-Wl,-rpath," + os.path.dirname(L.LIB_PATH)],
-                       check=True)
-        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
-        assert "225.575414 0.063630" in out
+    ref = os.path.join(REPO, "oracle", "_ref")
+    objs = [os.path.join(ref, "refobj", f + ".o") for f in
+            ("atmosphere", "continua", "control", "lineofsight", "misc", "scatter", "workqueue")]
+    ret = os.path.join(ref, "retobj")
+    if not refpath.available() or not all(os.path.exists(o) for o in objs) or \
+            not os.path.isdir(ret):
+        pytest.skip("reference tree or oracle objects absent")
+    extra = sorted(os.path.join(ret, f) for f in os.listdir(ret) if f.endswith(".o"))
+    for prog in ("formod", "kernel"):
+        exe = str(tmp_path / prog)
+        res = subprocess.run(
+            ["gcc", "-O2", "-fopenmp", "-DWORK_QUEUE", "-DHAVE_INLINE", "-w",
+             "-I" + os.path.join(ref, "include"), "-o", exe,
+             refpath.reference_path("src", prog + ".c")] + objs + extra +
+            [os.path.join(ref, "libgslsubset.a"), L.LIB_PATH,
+             "-Wl,-rpath," + os.path.dirname(L.LIB_PATH), "-lm"],
+            capture_output=True, text=True)
+        assert res.returncode == 0, res.stderr[-2000:]
+        # the program's formod is the library's
+        nm = subprocess.run(["nm", exe], capture_output=True, text=True, check=True).stdout
+        assert re.search(r"\bU formod\b", nm) and re.search(r"\bU formod_pencil\b", nm)
+        ldd = subprocess.run(["ldd", exe], capture_output=True, text=True, check=True).stdout
+        assert "libjurassic_b200.so" in ldd

@@ -264,3 +264,75 @@ def _aero_for(aero, g, nus):
             for a in range(181):
                 out.p[il][j][a] = aero.p[il][i][a]
     return out
+
+
+# Every launch variant the autotuner can pick: 0-8 a thread per (ray,
+# channel), 9-13 a lane per (ray, channel, emitter).
+ALL_VARIANTS = list(range(14))
+
+
+@pytest.fixture(scope="module", params=["headline_batch", "continuum_bands"])
+def shape_case(request, workdir):
+    """The benchmark's 64-channel, 8-emitter shape (O2 continuum in its top
+    channels) and the O2/N2 continuum-band case, with one device model per
+    case shared by all launch variants."""
+    from jscat import api, structs as S, synth
+    from make_golden_shim import band_case, headline_case
+    name = request.param
+    g = _load(name)
+    ctlkw, atms, ray_atm, geom = (headline_case if name == "headline_batch" else band_case)(workdir)
+    _check_tables(g, ctlkw)
+    ctl = S.make_ctl(**ctlkw)
+    m = api.Model(ctl)
+    yield name, g, ctlkw, ctl, synth.batch_from(atms, ray_atm, geom), m
+    m.close()
+
+
+@pytest.mark.parametrize("variant", ALL_VARIANTS)
+def test_every_launch_variant(shape_case, variant):
+    """Each launch variant on the headline shape and on the continuum-band
+    channels: LOS point counts and every EGA table index (digests) exactly
+    the reference's, radiances within 1e-9 relative and 0.01 K."""
+    from jscat import api
+    name, g, ctlkw, ctl, inp, m = shape_case
+    out = api.formod_batch(ctl, inp, model=m, digest=True, variant=variant)
+    np.testing.assert_array_equal(out["nlos"], g["nlos"], err_msg=name)
+    np.testing.assert_array_equal(out["digest"], g["digest"], err_msg=name)
+    assert bt_error(out["rad"], g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(out["rad"], g["rad"]) <= REL_TOL
+    assert max_rel(out["tau"], g["tau"]) <= REL_TOL
+    np.testing.assert_allclose(out["tpz"], g["tpz"], rtol=1e-9, atol=1e-9)
+
+
+def test_formod_pencil_clear_and_scattering(workdir):
+    """The drop-in formod_pencil (one ray on the GPU, atm as given) on rays
+    of the clear limb case and of the daytime single-scattering case, after
+    the hydrostatic balance formod applies: the reference's radiances."""
+    from jscat import structs as S, synth, api
+    from make_golden_shim import aerosol_case
+    g = _load("clear_limb")
+    ctlkw, atm, geom = synth.clear_limb_case(workdir)
+    ctl = S.make_ctl(**ctlkw)
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm["k"])
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"])
+    api.formod(ctl, a, obs)          # hydrostatic balance of a, as formod leaves it
+    nd = ctl.nd
+    for ir in (0, 17, 60):
+        for id_ in range(nd):
+            obs.rad[id_][ir] = obs.tau[id_][ir] = -1.0
+        api.formod_pencil(ctl, a, obs, scattering=ctl.sca_mult if ctl.sca_n else 0, ir=ir)
+        rad = S.arr(obs.rad)[:nd, ir]
+        assert max_rel(rad, g["rad"][ir]) <= REL_TOL
+        assert max_rel(S.arr(obs.tau)[:nd, ir], g["tau"][ir]) <= REL_TOL
+    ga = _load("aerosol_sca1_day")
+    ctlkw, atm, geom, _ = aerosol_case(workdir, 1)
+    n = len(geom["obsz"])
+    ctl = S.make_ctl(**ctlkw)
+    a = S.make_atm(atm["z"], atm["p"], atm["t"], atm["q"], atm["k"])
+    obs = S.make_obs(geom["obsz"], geom["obslat"], geom["vpz"], geom["vplat"],
+                     geom["obslon"], geom["vplon"], np.full(n, 43200.0))
+    aero = S.AeroT.from_buffer_copy(ga["aero"].tobytes())
+    api.formod(ctl, a, obs, aero)
+    for ir in (3, 11):
+        api.formod_pencil(ctl, a, obs, aero, scattering=1, ir=ir)
+        assert max_rel(S.arr(obs.rad)[:ctl.nd, ir], ga["rad"][ir]) <= REL_TOL

@@ -10,7 +10,9 @@ import pytest
 
 from conftest import GOLDEN, REPO
 
-REF_EXAMPLES = "/root/reference/examples"
+from oracle import refpath  # noqa: E402
+
+REF_EXAMPLES = refpath.reference_path("examples")
 PORT = os.path.join(REPO, "oracle", "build", "libjscat_oracle.so")
 
 
@@ -44,6 +46,19 @@ def test_port_bit_exact_mixed_batch(workdir, port):
     from oracle import refrun
     g = _golden("mixed_batch")
     ctlkw, atms, ray_atm, geom = mixed_case(workdir)
+    r = refrun.run_port(ctlkw, atms, ray_atm, geom, los=True)
+    for k in ("rad", "tau", "tpz", "tplon", "tplat", "nlos", "digest"):
+        assert np.array_equal(r[k], g[k]), k
+
+
+@pytest.mark.parametrize("name", ["headline_batch", "continuum_bands"])
+def test_port_bit_exact_shapes(workdir, port, name):
+    """The benchmark's 64-channel, 8-emitter shape (O2 continuum in the top
+    channels) and the O2/N2 continuum-band case."""
+    from make_golden_shim import band_case, headline_case
+    from oracle import refrun
+    g = _golden(name)
+    ctlkw, atms, ray_atm, geom = (headline_case if name == "headline_batch" else band_case)(workdir)
     r = refrun.run_port(ctlkw, atms, ray_atm, geom, los=True)
     for k in ("rad", "tau", "tpz", "tplon", "tplat", "nlos", "digest"):
         assert np.array_equal(r[k], g[k]), k
@@ -129,7 +144,7 @@ def _climatology_atm(ctlname, extra, tmpdir):
     clim = os.path.join(REPO, "oracle", "_ref", "climatology")
     src = os.path.join(REF_EXAMPLES, ctlname)
     ctl = os.path.join(tmpdir, ctlname)
-    txt = open(src, "rb").read().replace(b"../clim", b"/root/reference/clim")
+    txt = open(src, "rb").read().replace(b"../clim", refpath.reference_path("clim").encode())
     open(ctl, "wb").write(txt)
     out = os.path.join(tmpdir, ctlname + ".atm")
     subprocess.run([clim, ctl, "-", out] + extra, check=True, capture_output=True)

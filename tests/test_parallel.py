@@ -81,3 +81,42 @@ def test_two_rank_shard_and_gather(workdir, tmp_path):
     g = dict(np.load(os.path.join(REPO, "tests", "golden", "mixed_batch.npz")))
     rad = np.load(os.path.join(tmp_path, "rad.npy"))
     assert np.array_equal(rad, g["rad"])
+
+
+def test_gather_device_follows_the_backend(monkeypatch):
+    """NCCL all-gathers CUDA tensors only: the gather buffers live on the
+    rank's current GPU under nccl and in host memory under gloo."""
+    import torch
+    import torch.distributed as dist
+    from jscat import parallel
+    monkeypatch.setattr(dist, "get_backend", lambda group=None: "gloo")
+    assert parallel.gather_device() == torch.device("cpu")
+    monkeypatch.setattr(dist, "get_backend", lambda group=None: "nccl")
+    monkeypatch.setattr(torch.cuda, "current_device", lambda: 3)
+    assert parallel.gather_device() == torch.device("cuda", 3)
+
+
+def _rank_gather(rank, world, port, outdir):
+    sys.path.insert(0, PKG)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    from jscat import parallel
+    full = np.arange(7 * 3, dtype=np.float64).reshape(7, 3)
+    ranges = parallel.shard_ranges(np.r_[np.ones(2), np.full(5, 0.1)], world)
+    s, e = ranges[rank]
+    got = parallel.gather_rows(full[s:e], ranges)
+    np.save(os.path.join(outdir, "g%d.npy" % rank), got)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_gather_rows_uneven_ranges(tmp_path):
+    """Ranges of unequal length (one of them possibly empty) come back in
+    ray order on every rank."""
+    port = _free_port()
+    tmp.spawn(_rank_gather, args=(3, port, str(tmp_path)), nprocs=3, join=True)
+    full = np.arange(7 * 3, dtype=np.float64).reshape(7, 3)
+    for r in range(3):
+        assert np.array_equal(np.load(os.path.join(tmp_path, "g%d.npy" % r)), full)
