@@ -222,6 +222,20 @@ double planck(double t, double nu);
  * obs->tau[*][ir] and obs->tpz/tplon/tplat[ir]. */
 void formod_pencil(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, int scattering, int ir);
 
+/* The scattering source of srcfunc_sca (src/scatter.c:643-662) at n points
+ * at once, ON THE GPU: point k at Cartesian position x[3k..3k+2] [km] on a
+ * line of sight along dx[3k..3k+2], in aerosol/cloud layer layer[k], at time
+ * sec[k] [s since 2000-01-01T00:00Z]; the thermal source of the secondary
+ * pencils of order scattering - 1 (srcfunc_sca_1d for ctl->ip 1,
+ * srcfunc_sca_3d's 32,400 pencils for ip 2/3) plus the solar term
+ * (srcfunc_sca_sun), into src[n][nd].  atm is taken as given (formod
+ * applies the hydrostatic balance before its pencils call srcfunc_sca);
+ * aero holds the layers and optical properties; ctl->sca_n must be > 0 and
+ * scattering >= 1.  Returns a JSC_* status (no exit). */
+int jsc_srcfunc_sca(ctl_t *ctl, atm_t *atm, aero_t *aero, int n, const double *x,
+                    const double *dx, const int *layer, const double *sec, int scattering,
+                    double *src);
+
 /* Replaces formod_fov (src/forwardmodel.c:156-220): field-of-view
  * convolution of obs over tangent height with the shape of ctl->fov
  * (nothing when it is "-"); host post-processing, as in formod(). */
@@ -534,6 +548,17 @@ int jsc_batch_set_aero(jsc_batch *b, const aero_t *aero);
  * every scattering order of the batch's later runs. */
 int jsc_batch_set_nalpha(jsc_batch *b, int nalpha);
 
+/* Scattering sources at n given points through the batch's uploaded
+ * profiles (the jsc_srcfunc_sca computation on a batch created with
+ * ctl->sca_n > 0 and ctl->sca_mult >= 1, after jsc_batch_set_aero and
+ * jsc_batch_upload; hydrostatic balance when ctl->hydz >= 0): x, dx [n][3],
+ * layer [n], time [n], prof [n] (the profile of each point; NULL: 0) in
+ * host memory, src [n][nd] out.  The source's order is the batch's
+ * scattering depth; waits for the stream. */
+int jsc_batch_scatter_points(jsc_batch *b, int n, const double *x, const double *dx,
+                             const int *layer, const double *time, const int *prof,
+                             double *src, void *stream);
+
 /* Per-(ray, channel) checksum of every emissivity-table index the EGA
  * interpolation selected in the last run, for parity checks against the
  * reference's indices.  Per emitter g, D_g folds d = d*1000003 + v over the
@@ -575,6 +600,12 @@ void jsc_surrogate_destroy(jsc_surrogate *s);
 int jsc_surrogate_param_count(const jsc_surrogate *s);
 int jsc_surrogate_get_params(const jsc_surrogate *s, float *out);
 int jsc_surrogate_set_params(jsc_surrogate *s, const float *in);
+
+/* Standardisation set by jsc_surrogate_train: the network sees features
+ * (X - xm) / xs (8 each) and predicts (log S - ym) / ys (nd each).  Arrays
+ * may be NULL. */
+int jsc_surrogate_get_scaling(const jsc_surrogate *s, float *xm, float *xs, float *ym,
+                              float *ys);
 
 /* Loss (mean over the n rows of the squared error summed over outputs) and
  * its gradient with respect to every parameter (layout of get_params), for

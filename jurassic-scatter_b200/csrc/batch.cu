@@ -520,6 +520,8 @@ static void launch_raytrace(const jsc_batch *b, const RayArgs &ra, cudaStream_t 
 }
 
 static int batch_run(jsc_batch *b, cudaStream_t s);
+static int run_hydro(jsc_batch *b, cudaStream_t s);
+static int map_status(unsigned st);
 
 // Fixed-capacity runs: rays whose line of sight did not fit (the storing
 // pass flagged them) keep only the points inside the buffer, so that no
@@ -576,6 +578,24 @@ static int copy_profiles(const jsc_batch *b, jsc_batch *c, cudaStream_t s) {
   return JSC_OK;
 }
 
+// Room for n scattering point records, their profiles and sources.
+static int reserve_points(jsc_batch *b, int64_t n_sp) {
+  if (n_sp <= b->max_sp) return JSC_OK;
+  int st;
+  cudaFree(b->d_sp);
+  cudaFree(b->d_sp_atm);
+  cudaFree(b->d_src);
+  b->d_sp = b->d_src = nullptr;
+  b->d_sp_atm = nullptr;
+  b->max_sp = 0;
+  const int64_t n = n_sp + n_sp / 4 + 256;
+  if ((st = jsc_dmalloc(&b->d_sp, (size_t)n * JSC_SP_REC))) return st;
+  if ((st = jsc_dmalloc(&b->d_sp_atm, (size_t)n))) return st;
+  if ((st = jsc_dmalloc(&b->d_src, (size_t)n * b->cfg.nd))) return st;
+  b->max_sp = n;
+  return JSC_OK;
+}
+
 // Scattering points per ray and their list (src/forwardmodel.c:317-331).
 static int list_scattering_points(jsc_batch *b, cudaStream_t s) {
   const int nr = b->n_rays;
@@ -605,19 +625,7 @@ static int list_scattering_points(jsc_batch *b, cudaStream_t s) {
                                cudaMemcpyDeviceToHost, s));
   JSC_CUDA_TRY(cudaStreamSynchronize(s));
   b->n_sp = *b->h_total;
-  if (b->n_sp > b->max_sp) {
-    cudaFree(b->d_sp);
-    cudaFree(b->d_sp_atm);
-    cudaFree(b->d_src);
-    b->d_sp = b->d_src = nullptr;
-    b->d_sp_atm = nullptr;
-    b->max_sp = 0;
-    const int64_t n = b->n_sp + b->n_sp / 4 + 256;
-    if ((st = jsc_dmalloc(&b->d_sp, (size_t)n * JSC_SP_REC))) return st;
-    if ((st = jsc_dmalloc(&b->d_sp_atm, (size_t)n))) return st;
-    if ((st = jsc_dmalloc(&b->d_src, (size_t)n * b->cfg.nd))) return st;
-    b->max_sp = n;
-  }
+  if ((st = reserve_points(b, b->n_sp))) return st;
   if (b->n_sp == 0) return JSC_OK;
   sa.sp = b->d_sp;
   sa.sp_atm = b->d_sp_atm;
@@ -955,6 +963,73 @@ static int scatter_sources(jsc_batch *b, cudaStream_t s) {
   return JSC_OK;
 }
 
+extern "C" int jsc_batch_scatter_points(jsc_batch *b, int n, const double *x, const double *dx,
+                                        const int *layer, const double *time, const int *prof,
+                                        double *src, void *stream) {
+  if (!b || n < 0 || (n > 0 && (!x || !dx || !layer || !time || !src))) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_scatter_points: invalid arguments");
+    return JSC_ERR_ARG;
+  }
+  if (b->depth < 1 || !b->d_aero || b->n_atm < 1) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_scatter_points: needs a batch with SCA_N > 0, "
+                               "SCA_MULT >= 1, jsc_batch_set_aero and uploaded profiles");
+    return JSC_ERR_ARG;
+  }
+  for (int k = 0; k < n; k++)
+    if (layer[k] < 0 || layer[k] >= b->aero_nl || (prof && (prof[k] < 0 || prof[k] >= b->n_atm))) {
+      jsc_set_error(JSC_ERR_ARG, "jsc_batch_scatter_points: point %d names layer %d of %d or "
+                    "profile %d of %d", k, layer[k], b->aero_nl, prof ? prof[k] : 0, b->n_atm);
+      return JSC_ERR_ARG;
+    }
+  JSC_CUDA_TRY(cudaSetDevice(b->m->device));
+  (void)cudaGetLastError();
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n == 0) return JSC_OK;
+  int st = reserve_points(b, n);
+  if (st) return st;
+  double *rec = (double *)malloc((size_t)n * JSC_SP_REC * sizeof(double));
+  int *pa = (int *)malloc((size_t)n * sizeof(int));
+  if (!rec || !pa) {
+    free(rec);
+    free(pa);
+    return JSC_ERR_NOMEM;
+  }
+  for (int k = 0; k < n; k++) {
+    double *o = rec + (size_t)k * JSC_SP_REC;
+    for (int i = 0; i < 3; i++) {
+      o[SP_X + i] = x[3 * k + i];
+      o[SP_DX + i] = dx[3 * k + i];
+    }
+    o[SP_IL] = layer[k];
+    o[SP_TIME] = time[k];
+    o[SP_P] = o[SP_T] = 0;  // read by the surrogate's features only
+    pa[k] = prof ? prof[k] : 0;
+  }
+  for (int k = 0; k < JSC_T_N; k++) b->ran[k] = 0;
+  cudaError_t e = cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_sp, rec, (size_t)n * JSC_SP_REC * sizeof(double),
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_sp_atm, pa, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // rec and pa are freed next
+  free(rec);
+  free(pa);
+  if (e != cudaSuccess) {
+    jsc_set_error(JSC_ERR_CUDA, "jsc_batch_scatter_points: %s", cudaGetErrorString(e));
+    return JSC_ERR_CUDA;
+  }
+  b->n_sp = n;
+  if ((st = run_hydro(b, s))) return st;
+  if ((st = plain_sources(b, b->d_sp, b->d_sp_atm, n, b->d_src, s))) return st;
+  unsigned status = 0;
+  JSC_CUDA_TRY(cudaMemcpyAsync(src, b->d_src, (size_t)n * b->cfg.nd * sizeof(double),
+                               cudaMemcpyDeviceToHost, s));
+  JSC_CUDA_TRY(cudaMemcpyAsync(&status, b->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  JSC_CUDA_TRY(cudaStreamSynchronize(s));
+  return map_status(status);
+}
+
 extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   if (!b) return JSC_ERR_ARG;
   JSC_CUDA_TRY(cudaSetDevice(b->m->device));
@@ -962,13 +1037,10 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   return batch_run(b, (cudaStream_t)stream);
 }
 
-static int batch_run(jsc_batch *b, cudaStream_t s) {
+// Hydrostatic balance of the uploaded profiles (when hydz >= 0) into d_p,
+// and each profile's altitude range.
+static int run_hydro(jsc_batch *b, cudaStream_t s) {
   const jsc_model *m = b->m;
-  const int nr = b->n_rays;
-  for (int k = 0; k < JSC_T_N; k++) b->ran[k] = 0;
-  JSC_CUDA_TRY(cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s));
-  JSC_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(unsigned long long), s));
-
   AtmArgs aa;
   aa.n_atm = b->n_atm;
   aa.n_levels = b->n_levels;
@@ -991,6 +1063,19 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   hydro_kernel<<<(b->n_atm + 127) / 128, 128, 0, s>>>(aa);
   JSC_LAUNCH_CHECK();
   ev_record(b, JSC_T_HYDRO, 1, s);
+  return JSC_OK;
+}
+
+static int batch_run(jsc_batch *b, cudaStream_t s) {
+  const jsc_model *m = b->m;
+  const int nr = b->n_rays;
+  for (int k = 0; k < JSC_T_N; k++) b->ran[k] = 0;
+  JSC_CUDA_TRY(cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), s));
+  JSC_CUDA_TRY(cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(unsigned long long), s));
+  {
+    int st = run_hydro(b, s);
+    if (st) return st;
+  }
   if (nr == 0) return JSC_OK;
 
   RayArgs ra;

@@ -193,82 +193,109 @@ static int fov_convolve(const ctl_t *ctl, obs_t *obs) {
   return st;
 }
 
+/* Host arrays of one packed batch input; they must live until the stream
+ * has passed the upload. */
+typedef struct {
+  double *buf;   /* q [ng][np], k [nw][np], then room for rad, tau, tp of nr rays */
+  int *ray_atm;
+  int *off;
+} packed_t;
+
+static void packed_free(packed_t *pk) {
+  free(pk->buf);
+  free(pk->ray_atm);
+  free(pk->off);
+  memset(pk, 0, sizeof(*pk));
+}
+
+/* Pack atm and rays [r0, r0 + nr) of obs as the input of batch b and upload
+ * it (the aerosol layers first when ctl->sca_n > 0): one profile (IP 1 and
+ * IP 3, whose points are weighted one by one) or, for IP 2, a new profile
+ * wherever lon/lat change, as intpol_atm_2d groups them
+ * (src/atmosphere.c:343-356). */
+static int upload_atm(jsc_batch *b, const ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero,
+                      int r0, int nr, packed_t *pk) {
+  const int nd = ctl->nd, np = atm->np, ng = ctl->ng, nw = ctl->nw;
+  size_t nbuf = (size_t)np * (size_t)(ng + nw) + 2 * (size_t)nr * nd + 3 * (size_t)nr + 1;
+  memset(pk, 0, sizeof(*pk));
+  pk->buf = (double *)malloc(nbuf * sizeof(double));
+  pk->ray_atm = (int *)calloc((size_t)nr + 1, sizeof(int));
+  pk->off = (int *)malloc(((size_t)np + 1) * sizeof(int));
+  if (!pk->buf || !pk->ray_atm || !pk->off) {
+    packed_free(pk);
+    return JSC_ERR_NOMEM;
+  }
+  double *q = pk->buf, *k = q + (size_t)np * ng;
+  int *off = pk->off, n_atm = 1;
+  for (int ig = 0; ig < ng; ig++) memcpy(q + (size_t)ig * np, atm->q[ig], np * sizeof(double));
+  for (int iw = 0; iw < nw; iw++) memcpy(k + (size_t)iw * np, atm->k[iw], np * sizeof(double));
+  off[0] = 0;
+  if (ctl->ip == 2)
+    for (int ip = 1; ip < np; ip++)
+      if (atm->lon[ip] != atm->lon[ip - 1] || atm->lat[ip] != atm->lat[ip - 1])
+        off[n_atm++] = ip;
+  off[n_atm] = np;
+  jsc_batch_input in;
+  memset(&in, 0, sizeof(in));
+  in.n_atm = n_atm;
+  in.n_levels = np;
+  in.atm_off = off;
+  in.z = atm->z;
+  in.lon = atm->lon;
+  in.lat = atm->lat;
+  in.p = atm->p;
+  in.t = atm->t;
+  in.q = q;
+  in.k = k;
+  in.n_rays = nr;
+  in.ray_atm = pk->ray_atm;
+  in.time = obs->time + r0;
+  in.obsz = obs->obsz + r0;
+  in.obslon = obs->obslon + r0;
+  in.obslat = obs->obslat + r0;
+  in.vpz = obs->vpz + r0;
+  in.vplon = obs->vplon + r0;
+  in.vplat = obs->vplat + r0;
+  /* Aerosol/cloud layers and optical properties (read_aero +
+   * get_opt_prop of the caller, or of this call for retrievals). */
+  int st = JSC_OK;
+  if (ctl->sca_n > 0) st = jsc_batch_set_aero(b, aero);
+  if (!st) st = jsc_batch_upload(b, &in, NULL);
+  return st;
+}
+
 /* Run rays [r0, r0 + nr) of obs through atm on batch b (held under g_lock)
- * and write their radiances, transmittances and tangent points into obs:
- * the atmosphere is packed as one profile (IP 1 and IP 3, whose points are
- * weighted one by one) or, for IP 2, as a new profile wherever lon/lat
- * change, as intpol_atm_2d groups them (src/atmosphere.c:343-356). */
+ * and write their radiances, transmittances and tangent points into obs. */
 static int run_rays(jsc_batch *b, const ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero,
                     int r0, int nr) {
   const int nd = ctl->nd, np = atm->np, ng = ctl->ng, nw = ctl->nw;
-  int st = JSC_OK;
-  size_t nbuf = (size_t)np * (size_t)(ng + nw) + 2 * (size_t)nr * nd + 3 * (size_t)nr;
-  double *buf = (double *)malloc(nbuf * sizeof(double));
-  int *ray_atm = (int *)calloc((size_t)nr, sizeof(int));
-  int *off = (int *)malloc(((size_t)np + 1) * sizeof(int)), n_atm = 1;
-  if (!buf || !ray_atm || !off) {
-    st = JSC_ERR_NOMEM;
-  } else {
-    double *q = buf, *k = q + (size_t)np * ng, *rad = k + (size_t)np * nw;
-    double *tau = rad + (size_t)nr * nd, *tp = tau + (size_t)nr * nd;
-    for (int ig = 0; ig < ng; ig++) memcpy(q + (size_t)ig * np, atm->q[ig], np * sizeof(double));
-    for (int iw = 0; iw < nw; iw++) memcpy(k + (size_t)iw * np, atm->k[iw], np * sizeof(double));
-    off[0] = 0;
-    if (ctl->ip == 2)
-      for (int ip = 1; ip < np; ip++)
-        if (atm->lon[ip] != atm->lon[ip - 1] || atm->lat[ip] != atm->lat[ip - 1])
-          off[n_atm++] = ip;
-    off[n_atm] = np;
-    jsc_batch_input in;
-    memset(&in, 0, sizeof(in));
-    in.n_atm = n_atm;
-    in.n_levels = np;
-    in.atm_off = off;
-    in.z = atm->z;
-    in.lon = atm->lon;
-    in.lat = atm->lat;
-    in.p = atm->p;
-    in.t = atm->t;
-    in.q = q;
-    in.k = k;
-    in.n_rays = nr;
-    in.ray_atm = ray_atm;
-    in.time = obs->time + r0;
-    in.obsz = obs->obsz + r0;
-    in.obslon = obs->obslon + r0;
-    in.obslat = obs->obslat + r0;
-    in.vpz = obs->vpz + r0;
-    in.vplon = obs->vplon + r0;
-    in.vplat = obs->vplat + r0;
-    jsc_batch_output out;
-    memset(&out, 0, sizeof(out));
-    out.rad = rad;
-    out.tau = tau;
-    out.tpz = tp;
-    out.tplon = tp + nr;
-    out.tplat = tp + 2 * nr;
-    /* Aerosol/cloud layers and optical properties (read_aero +
-     * get_opt_prop of the caller, or of this call for retrievals). */
-    if (ctl->sca_n > 0) st = jsc_batch_set_aero(b, aero);
-    if (!st) st = jsc_batch_upload(b, &in, NULL);
-    if (!st) st = jsc_batch_run(b, NULL);
-    if (!st) st = jsc_batch_download(b, &out, NULL);
-    if (!st) {
-      for (int i = 0; i < nr; i++) {
-        const int ir = r0 + i;
-        obs->tpz[ir] = tp[i];
-        obs->tplon[ir] = tp[nr + i];
-        obs->tplat[ir] = tp[2 * nr + i];
-        for (int id = 0; id < nd; id++) {
-          obs->rad[id][ir] = rad[(size_t)i * nd + id];
-          obs->tau[id][ir] = tau[(size_t)i * nd + id];
-        }
+  packed_t pk;
+  int st = upload_atm(b, ctl, atm, obs, aero, r0, nr, &pk);
+  if (st) return st;
+  double *rad = pk.buf + (size_t)np * (size_t)(ng + nw);
+  double *tau = rad + (size_t)nr * nd, *tp = tau + (size_t)nr * nd;
+  jsc_batch_output out;
+  memset(&out, 0, sizeof(out));
+  out.rad = rad;
+  out.tau = tau;
+  out.tpz = tp;
+  out.tplon = tp + nr;
+  out.tplat = tp + 2 * nr;
+  st = jsc_batch_run(b, NULL);
+  if (!st) st = jsc_batch_download(b, &out, NULL);
+  if (!st) {
+    for (int i = 0; i < nr; i++) {
+      const int ir = r0 + i;
+      obs->tpz[ir] = tp[i];
+      obs->tplon[ir] = tp[nr + i];
+      obs->tplat[ir] = tp[2 * nr + i];
+      for (int id = 0; id < nd; id++) {
+        obs->rad[id][ir] = rad[(size_t)i * nd + id];
+        obs->tau[id][ir] = tau[(size_t)i * nd + id];
       }
     }
   }
-  free(off);
-  free(ray_atm);
-  free(buf);
+  packed_free(&pk);
   return st;
 }
 
@@ -392,6 +419,53 @@ static int pencil_impl(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, int sca
  * obs->rad[*][ir], obs->tau[*][ir] and obs->tp*[ir]. */
 void formod_pencil(ctl_t *ctl, atm_t *atm, obs_t *obs, aero_t *aero, int scattering, int ir) {
   jsc_finish_call(pencil_impl(ctl, atm, obs, aero, scattering, ir), "formod_pencil");
+}
+
+static int srcfunc_impl(ctl_t *ctl, atm_t *atm, aero_t *aero, int n, const double *x,
+                        const double *dx, const int *layer, const double *sec, int scattering,
+                        double *src) {
+  const int nd = ctl->nd, np = atm->np, ng = ctl->ng, nw = ctl->nw;
+  if (nd < 1 || nd > NDMAX || ng < 0 || ng > NGMAX || nw < 0 || nw > NWMAX || np < 2 ||
+      np > NPMAX || n < 0 || scattering < 1 || ctl->sca_n < 1 || !aero) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_srcfunc_sca: invalid sizes (nd=%d np=%d n=%d "
+                  "scattering=%d sca_n=%d) or no aerosol data", nd, np, n, scattering,
+                  ctl->sca_n);
+    return JSC_ERR_ARG;
+  }
+  ctl_t *c = (ctl_t *)malloc(sizeof(ctl_t));
+  if (!c) return JSC_ERR_NOMEM;
+  memcpy(c, ctl, sizeof(ctl_t));
+  c->hydz = -999;          /* atm as given, as srcfunc_sca takes it */
+  c->sca_mult = scattering;
+  int st;
+  pthread_mutex_lock(&g_lock);
+  st = ensure_cache(ctl);
+  jsc_batch *b = NULL;
+  if (!st) st = jsc_batch_create(g_model, c, NPMAX / 2, NPMAX, 1, 0, &b);
+  packed_t pk;
+  memset(&pk, 0, sizeof(pk));
+  if (!st) {
+    /* the atmosphere as formod packs it, no rays */
+    obs_t *none = (obs_t *)calloc(1, sizeof(obs_t));
+    if (!none) st = JSC_ERR_NOMEM;
+    if (!st) st = upload_atm(b, c, atm, none, aero, 0, 0, &pk);
+    free(none);
+  }
+  /* synchronises its stream before it returns: the upload has passed */
+  if (!st) st = jsc_batch_scatter_points(b, n, x, dx, layer, sec, NULL, src, NULL);
+  packed_free(&pk);
+  jsc_batch_destroy(b);
+  pthread_mutex_unlock(&g_lock);
+  free(c);
+  return st;
+}
+
+int jsc_srcfunc_sca(ctl_t *ctl, atm_t *atm, aero_t *aero, int n, const double *x,
+                    const double *dx, const int *layer, const double *sec, int scattering,
+                    double *src) {
+  const int st = srcfunc_impl(ctl, atm, aero, n, x, dx, layer, sec, scattering, src);
+  g_last_status = st;
+  return st;
 }
 
 /* Replaces formod_fov (src/forwardmodel.c:156-220): the field-of-view

@@ -532,6 +532,20 @@ extern "C" int jsc_surrogate_create(int nd, int device, uint64_t seed, jsc_surro
   return JSC_OK;
 }
 
+extern "C" int jsc_surrogate_get_scaling(const jsc_surrogate *s, float *xm, float *xs, float *ym,
+                                         float *ys) {
+  if (!s) return JSC_ERR_ARG;
+  for (int c = 0; c < SUR_NF; c++) {
+    if (xm) xm[c] = s->xm[c];
+    if (xs) xs[c] = s->xs[c];
+  }
+  for (int d = 0; d < s->nout; d++) {
+    if (ym) ym[d] = s->h_ym[d];
+    if (ys) ys[d] = s->h_ys[d];
+  }
+  return JSC_OK;
+}
+
 extern "C" int jsc_surrogate_get_params(const jsc_surrogate *s, float *out) {
   if (!s || !out) return JSC_ERR_ARG;
   JSC_CUDA_TRY(cudaSetDevice(s->device));

@@ -48,6 +48,23 @@ def formod_pencil(ctl, atm, obs, aero=None, scattering=0, ir=0):
     L.check(lib.jsc_last_status(), "formod_pencil")
 
 
+def srcfunc_sca(ctl, atm, aero, x, dx, layer, sec, scattering=1):
+    """Scattering sources [n][nd] at n points on the GPU (jsc_srcfunc_sca):
+    x, dx [n][3] Cartesian position and line-of-sight direction [km],
+    layer [n], sec [n]; atm as given (hydrostatically balanced by the
+    caller)."""
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+    dx = np.ascontiguousarray(dx, dtype=np.float64).reshape(-1, 3)
+    n = len(x)
+    layer = np.ascontiguousarray(layer, dtype=np.int32)
+    sec = np.ascontiguousarray(sec, dtype=np.float64)
+    src = np.zeros((n, ctl.nd))
+    L.check(L.load().jsc_srcfunc_sca(C.byref(ctl), C.byref(atm), C.byref(aero), n, _dptr(x),
+                                     _dptr(dx), _iptr(layer), _dptr(sec), int(scattering),
+                                     _dptr(src)), "jsc_srcfunc_sca")
+    return src
+
+
 def read_aero(ctl, filename, dirname=None):
     """aero_t with the modes of an aerosol file (jsc_read_aero)."""
     aero = S.AeroT()
@@ -428,6 +445,15 @@ def _fptr(a):
     return a.ctypes.data_as(_F)
 
 
+# The surrogate's sampled accuracy check, as the benchmark and the tests use
+# it: every SURROGATE_CHECK_STRIDE-th point inside the training envelope is
+# also computed by the plain path, and an albedo-weighted relative source
+# deviation above SURROGATE_CHECK_TOL sends the whole batch down the plain
+# path (jsc_batch_set_surrogate).
+SURROGATE_CHECK_TOL = 0.01
+SURROGATE_CHECK_STRIDE = 256
+
+
 class Surrogate:
     """Scattering-source surrogate (jsc_surrogate_*): a 4-layer MLP trained
     on the GPU on plain-path samples, BF16 tensor-core inference."""
@@ -464,6 +490,14 @@ class Surrogate:
             o += r
             out.append((w, b))
         return out
+
+    def scaling(self):
+        """Feature and target standardisation (xm, xs, ym, ys)."""
+        xm, xs = np.zeros(self.NF, np.float32), np.zeros(self.NF, np.float32)
+        ym, ys = np.zeros(self.nd, np.float32), np.zeros(self.nd, np.float32)
+        L.check(L.load().jsc_surrogate_get_scaling(self.h, _fptr(xm), _fptr(xs), _fptr(ym),
+                                                   _fptr(ys)), "jsc_surrogate_get_scaling")
+        return xm, xs, ym, ys
 
     def loss_grad(self, x, t):
         x = np.ascontiguousarray(x, dtype=np.float32)

@@ -29,6 +29,7 @@ EXPORTS = [
     "jsc_atm2x", "jsc_x2atm", "jsc_obs2y", "jsc_kernel", "jsc_read_aero", "jsc_get_opt_prop",
     "formod_pencil", "formod_fov", "read_shape", "read_tbl", "srcfunc_planck",
     "formod_continua", "intpol_tbl", "intpol_tbl_eps", "intpol_tbl_u", "locate_tbl",
+    "jsc_srcfunc_sca", "jsc_batch_scatter_points", "jsc_surrogate_get_scaling",
 ]
 
 
@@ -142,6 +143,11 @@ def load():
         "intpol_tbl_eps": (d, [vp, i, i, i, i, d]),
         "intpol_tbl_u": (d, [vp, i, i, i, i, d]),
         "locate_tbl": (i, [P(C.c_float), i, d]),
+        "jsc_srcfunc_sca": (i, [P(S.CtlT), P(S.AtmT), P(S.AeroT), i, P(d), P(d), P(i), P(d), i,
+                                P(d)]),
+        "jsc_batch_scatter_points": (i, [vp, i, P(d), P(d), P(i), P(d), P(i), P(d), vp]),
+        "jsc_surrogate_get_scaling": (i, [vp, P(C.c_float), P(C.c_float), P(C.c_float),
+                                          P(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -39,3 +39,28 @@ def loss_and_grads(params, x, t):
         grads[li] = (dh.T @ acts[li], dh.sum(axis=0))
         dh = dh @ w
     return loss, grads
+
+
+def bf16(a):
+    """Round float32 values to bfloat16 (round to nearest, ties to even),
+    returned as float32."""
+    u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16 << 16
+    return u.astype(np.uint32).view(np.float32)
+
+
+def infer_bf16(params, feat, xm, xs, ym, ys):
+    """The inference the GPU runs, restated in numpy: standardised features
+    and every hidden activation rounded to BF16, BF16-rounded weights, FP32
+    biases, products summed in FP64 (the GPU sums in FP32), exact tanh (the
+    GPU's tcgen05 path uses the hardware approximation), sources
+    exp(y * ys + ym)."""
+    h = bf16((np.asarray(feat, np.float32) - xm) / xs).astype(np.float64)
+    for li, (w, b) in enumerate(params):
+        z = h @ bf16(w).astype(np.float64).T + np.asarray(b, np.float32).astype(np.float64)
+        if li < len(params) - 1:
+            h = bf16(np.tanh(z).astype(np.float32)).astype(np.float64)
+        else:
+            h = z.astype(np.float32)
+    y = h * np.asarray(ys, np.float32) + np.asarray(ym, np.float32)   # float32, as the GPU
+    return np.exp(y.astype(np.float64))

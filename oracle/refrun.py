@@ -246,6 +246,45 @@ def _los_child(job):
     return bytes(los)
 
 
+def _srcfunc_child(job):
+    """The reference's srcfunc_sca (src/scatter.c:643-662: the thermal
+    source of srcfunc_sca_1d or, for IP 2/3, srcfunc_sca_3d, plus
+    srcfunc_sca_sun) at single points, with the queue inactive as formod
+    leaves it (src/forwardmodel.c:54-55), after the reference's
+    hydrostatic balance of the atmosphere.  Returns the sources [n][nd], the
+    balanced pressures and the seconds per point."""
+    _silence()
+    lib = C.CDLL(REF_LIB)
+    P = C.POINTER
+    V3 = C.c_double * 3
+    lib.hydrostatic.argtypes = [P(S.CtlT), P(S.AtmT)]
+    lib.srcfunc_sca.argtypes = [P(S.CtlT), P(S.AtmT), P(S.AeroT), C.c_double, P(V3), P(V3),
+                                C.c_int, P(C.c_double), C.c_int]
+    lib.srcfunc_sca.restype = None
+    ctl = S.make_ctl(**job["ctl"])
+    ctl.queue.state = -1            # Queue_Inactive (src/workqueue.h:8)
+    atm = _atm_struct(job["atm"])
+    aero = S.AeroT.from_buffer_copy(job["aero"])
+    lib.hydrostatic(C.byref(ctl), C.byref(atm))
+    nd = ctl.nd
+    src = (C.c_double * S.NDMAX)()
+    out, secs = [], []
+    for x, dx, il, sec in job["points"]:
+        t0 = time.perf_counter()
+        lib.srcfunc_sca(C.byref(ctl), C.byref(atm), C.byref(aero), float(sec), V3(*x), V3(*dx),
+                        int(il), src, int(job["scattering"]))
+        secs.append(time.perf_counter() - t0)
+        out.append(np.array(src[:nd]))
+    return {"src": np.array(out), "p": S.arr(atm.p)[:atm.np].copy(), "seconds": np.array(secs)}
+
+
+def reference_srcfunc(ctl_kw, atm, aero, points, scattering, timeout=14400):
+    """srcfunc_sca of the reference build at points [(x[3], dx[3], layer,
+    time)], scattering order `scattering`; see _srcfunc_child."""
+    return _spawn({"srcfunc_job": True, "ctl": ctl_kw, "atm": atm, "aero": bytes(aero),
+                   "points": points, "scattering": scattering}, timeout)
+
+
 REF_RET_LIB = os.path.join(HERE, "_ref", "libjurassic_ref_ret.so")
 
 
@@ -475,6 +514,8 @@ if __name__ == "__main__":
         _out = _aero_child(_job)
     elif _job.get("kernel_job"):
         _out = _kernel_child(_job)
+    elif _job.get("srcfunc_job"):
+        _out = _srcfunc_child(_job)
     elif _job.get("helpers_job"):
         _out = _helpers_child(_job)
     elif _job.get("los_job"):

@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [headline|jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
+    make -C oracle ref && python tests/golden/make_golden.py [headline|points [kind...]|jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -215,6 +215,10 @@ def aerosol_jacobian_fixture(workdir):
 IP3_CZ, IP3_CX = 3.0, 700.0
 
 
+# horizontal influence length of the IP=3 scattering-point fixture [km]
+IP3_SCA_CX = 20000.0
+
+
 def curtain_ctl(ctlkw, ip):
     return dict(ctlkw, ip=ip, cz=IP3_CZ, cx=IP3_CX) if ip == 3 else dict(ctlkw, ip=ip)
 
@@ -304,6 +308,82 @@ def fov_fixtures(workdir):
     jacobian_fixture(workdir, "jacobian_limb_fov", False, fov=True)
 
 
+def _geo2cart(z, lon, lat):
+    r = 6367.421 + z
+    la, lo = np.radians(lat), np.radians(lon)
+    return [r * np.cos(la) * np.cos(lo), r * np.cos(la) * np.sin(lo), r * np.sin(la)]
+
+
+def _chord(z, lon, lat, azimuth_deg, dip_deg, length=20.0):
+    """Direction of a line of sight through (z, lon, lat): azimuth from
+    north towards east, dip below the local horizontal (a chord dx of the
+    given length)."""
+    la, lo = np.radians(lat), np.radians(lon)
+    up = np.array([np.cos(la) * np.cos(lo), np.cos(la) * np.sin(lo), np.sin(la)])
+    east = np.array([-np.sin(lo), np.cos(lo), 0.0])
+    north = np.cross(up, east)
+    a, d = np.radians(azimuth_deg), np.radians(dip_deg)
+    v = np.cos(d) * (np.cos(a) * north + np.sin(a) * east) - np.sin(d) * up
+    return list(length * v)
+
+
+# Scattering points inside the sulfate layer (15-20 km): (z, lon, lat,
+# azimuth, dip, time [s since 2000-01-01T00:00Z]).
+SCA_POINTS_1D = [(17.3, 0.0, 0.0, 0.0, 1.0, 43200.0), (15.8, 10.0, 5.0, 90.0, -2.0, 43200.0),
+                 (19.2, -20.0, -10.0, 200.0, 0.5, 0.0)]
+SCA_POINTS_3D = [(17.3, 0.0, 1.5, 10.0, 0.8, 43200.0)]
+
+
+def scattering_point_case(workdir, kind):
+    """Per-point scattering sources through the sulfate-like layer, 2 of the
+    aerosol channels: 'order1' single scattering at three points (IP=1, two
+    by day), 'order2' the depth-2 source (SCA_MULT=2) at one point by night
+    and one by day with the CO2/H2O continua off (with them on, leaf pencils
+    that start on a layer-edge point get a zero-length segment and the
+    reference's continuum 0/0 turns the source into NaN), 'ip2'/'ip3' the
+    3-D source (32,400 pencils) at one point of the curtain atmosphere."""
+    nus = [synth.CFG2_NU[i] for i in (0, 10)]
+    aerofile = synth.sulfate_layer_files(os.path.join(workdir, "aero"))
+    if kind in ("ip2", "ip3"):
+        ctlkw, atm, _ = synth.curtain_case(workdir)
+        base = synth.write_tables(workdir, synth.CFG0_EMITTERS, nus, 20261203)
+        ctlkw = curtain_ctl(dict(ctlkw, nus=nus, tblbase=base, sca_n=1, sca_mult=1),
+                            int(kind[2]))
+        if kind == "ip3":
+            # pencils in every direction leave the curtain; with the curtain's
+            # 700 km influence length some then see no profile point and the
+            # reference stops ("Too many LOS points!")
+            ctlkw = dict(ctlkw, cx=IP3_SCA_CX)
+        pts, order = SCA_POINTS_3D, 1
+    else:
+        ctlkw, atm, _, _ = aerosol_case(workdir, 1, nus=nus)
+        pts, order = SCA_POINTS_1D, 1
+        if kind == "order2":
+            ctlkw = dict(ctlkw, sca_mult=2, ctm_co2=0, ctm_h2o=0)
+            pts, order = [SCA_POINTS_1D[2], SCA_POINTS_1D[0]], 2
+    points = [(_geo2cart(z, lo, la), _chord(z, lo, la, az, dip), 0, t)
+              for z, lo, la, az, dip, t in pts]
+    return ctlkw, atm, aerofile, points, order
+
+
+def scattering_point_fixture(workdir, kind):
+    ctlkw, atm, aerofile, points, order = scattering_point_case(workdir, kind)
+    aero = refrun.reference_aero(ctlkw, aerofile, os.path.dirname(aerofile))
+    ref = refrun.reference_srcfunc(ctlkw, atm, S_aero(aero), points, order)
+    np.savez_compressed(
+        os.path.join(HERE, "sca_points_%s.npz" % kind), src=ref["src"], p=ref["p"],
+        seconds=ref["seconds"], x=np.array([p[0] for p in points]),
+        dx=np.array([p[1] for p in points]), il=np.array([p[2] for p in points]),
+        time=np.array([p[3] for p in points]), order=order,
+        aero=np.frombuffer(aero, dtype=np.uint8),
+        table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"], ctlkw["nus"]))
+
+
+def S_aero(aero_bytes):
+    from jscat import structs as S
+    return S.AeroT.from_buffer_copy(aero_bytes)
+
+
 def headline_fixtures(workdir):
     """headline_batch (the benchmark's 64-channel, 8-emitter shape) and
     continuum_bands (O2 and N2 continuum channels)."""
@@ -318,6 +398,12 @@ def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
     if sys.argv[1:] == ["headline"]:
         headline_fixtures(workdir)
+        return
+    if sys.argv[1:2] == ["points"]:
+        # per-point scattering sources; slow kinds (order2, ip2, ip3) take
+        # CPU minutes each
+        for kind in sys.argv[2:] or ["order1", "order2", "ip2", "ip3"]:
+            scattering_point_fixture(workdir, kind)
         return
     if sys.argv[1:] == ["jacobian"]:
         jacobian_fixture(workdir, "jacobian_limb", False)

@@ -135,3 +135,79 @@ def test_tcgen05_inference_matches_mma_sync(nd):
         assert np.max(np.abs(np.log(b) - np.log(a))) < 2e-3
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("nd", [4, 16, 40])
+def test_tcgen05_inference_matches_fp32_restatement(nd):
+    """The tcgen05 inference (BF16 operands, FP32 accumulators in tensor
+    memory) against the numpy restatement of the same inference
+    (oracle/mlp_ref.infer_bf16: the same BF16-rounded weights, features and
+    hidden activations, FP64 sums, exact tanh).  The remaining differences
+    are the FP32 accumulation order and the hardware tanh (relative error
+    about 2^-11) before each BF16 rounding."""
+    from jscat import api
+    from oracle import mlp_ref
+    rng = np.random.default_rng(13)
+    s = api.Surrogate(nd=nd, seed=4)
+    try:
+        n = 600
+        feat = rng.normal(0, 1, (n, 8)).astype(np.float32) * 3 + 10
+        src = np.exp(rng.normal(-3, 0.5, (n, nd)))
+        s.train(feat, src, epochs=3, batch=128, lr=2e-3)
+        s.set_tensor_path(True)
+        got = s.predict(feat)
+        want = mlp_ref.infer_bf16(s.layers(s.get_params()), feat, *s.scaling())
+        assert np.all(np.isfinite(got)) and np.all(got > 0)
+        assert np.max(np.abs(np.log(got) - np.log(want))) < 3e-3
+    finally:
+        s.close()
+
+
+def test_surrogate_accuracy_held_out(workdir):
+    """Out-of-sample accuracy: the network is trained on the plain sources of
+    limb rays A and then replaces the plain source on disjoint rays B
+    (other tangent heights and times of day), with the benchmark's sampled
+    check (api.SURROGATE_CHECK_TOL, every 16th point here): the surrogate
+    path is kept and its brightness temperatures stay within 0.05 K of the
+    plain path's."""
+    from jscat import api, synth, structs as S
+    from make_golden_shim import aerosol_case
+    g = dict(np.load(GOLDEN + "/aerosol_sca1_day.npz"))
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    ctlkw, atm, _, _ = aerosol_case(workdir, 1, n_rays=4)
+    ctl = S.make_ctl(**ctlkw)
+    rng = np.random.default_rng(21)
+
+    def rays(th, times):
+        geom = synth.limb_geometry(th)
+        geom["time"] = times
+        return synth.batch_from([atm], np.zeros(len(th), np.int32), geom)
+
+    na, nb = 480, 96
+    train = rays(rng.uniform(8.0, 30.0, na), rng.uniform(0.0, 86400.0, na))
+    test = rays(rng.uniform(8.0, 30.0, nb), rng.uniform(0.0, 86400.0, nb))
+    m = api.Model(ctl)
+    b = api.Batch(m, ctl, 1, len(train["z"]), na)
+    sur = api.Surrogate(ctl.nd, seed=3)
+    try:
+        b.set_aero(aero)
+        b.set_nalpha(10)
+        b.upload(train)
+        b.run()
+        feat, src = b.scatter_samples()
+        sur.train(feat, src, epochs=200, batch=512, lr=3e-3)
+        b.upload(test)
+        b.run()
+        plain = b.download()
+        b.set_surrogate(sur, tol_rel=api.SURROGATE_CHECK_TOL, check_stride=16)
+        b.run()
+        out = b.download()
+        st = b.surrogate_stats()
+        assert st["points"] > 1000 and st["checked"] > 50
+        assert st["fallback"] <= 0.05 * st["points"]
+        assert st["used"], st
+        assert bt_error(out["rad"], plain["rad"], ctlkw["nus"]) <= 0.05
+    finally:
+        sur.close()
+        b.close()
+        m.close()
