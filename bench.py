@@ -54,11 +54,29 @@ def parse():
     ap.add_argument("--sca-rays", type=int, default=20_000,
                     help="rays of the scattering (plain vs surrogate) workload; 0 skips it")
     ap.add_argument("--sca-epochs", type=int, default=40)
+    ap.add_argument("--ms-rays", type=int, default=5_000,
+                    help="rays of the depth-2 scattering workload; 0 skips it")
+    ap.add_argument("--ms-train-rays", type=int, default=1_000,
+                    help="rays of the depth-2 surrogate's training batch")
+    ap.add_argument("--ms-epochs", type=int, default=400,
+                    help="training epochs of the depth-2 surrogate")
+    ap.add_argument("--ms-plain-rays", type=int, default=1_000,
+                    help="rays of the depth-2 workload timed on the plain path (its first ones)")
     ap.add_argument("--requests", type=int, default=512,
                     help="requests of the mixed-size request batch; 0 skips it")
     ap.add_argument("--jacobians", type=int, default=5,
                     help="timed Jacobians / optical-property calls; 0 skips both sections")
     return ap.parse_args()
+
+
+def note(msg):
+    """Progress of the benchmark sections on stderr (the JSON line goes to
+    stdout at the end)."""
+    sys.stderr.write("[bench %.0f s] %s\n" % (time.perf_counter() - T0, msg))
+    sys.stderr.flush()
+
+
+T0 = time.perf_counter()
 
 
 def dist_env():
@@ -291,10 +309,148 @@ def scattering_bench(args, local, torch, oracle_sample=True):
     return res
 
 
+MS_WORKLOAD = ("multiple scattering (depth 2) through an ice-cloud-like layer at 9-11 km: limb "
+               "rays TH U[6, 14] km, times of day U[0, 86400] s, 8 channels 780-1219 cm-1, 2 "
+               "emitters, 20 secondary pencils per scattering point at depth 1 and 10 at depth 2, "
+               "CO2/H2O continua off")
+
+
+def ice_case(n, seed):
+    """Config-3 rays through the ice layer (optical properties of the
+    reference's get_opt_prop for the ice layer, tests/golden/aero_ice8.npz).
+    CO2/H2O continua off: with them on, leaf pencils that start on a
+    layer-edge point get a zero-length segment whose continuum term is 0/0
+    in the reference (src/forwardmodel.c:133-141), so its depth-2 radiances
+    are NaN."""
+    from jscat import synth, structs as S
+    workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
+    g = np.load(os.path.join(REPO, "tests", "golden", "aero_ice8.npz"))
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    nus = [float(v) for v in g["nus"]]
+    rng = np.random.default_rng(seed)
+    atm = synth.atmosphere(synth.CFG0_EMITTERS, rng)
+    geom = synth.limb_geometry(rng.uniform(6.0, 14.0, n))
+    geom["time"] = rng.uniform(0.0, 86400.0, n)
+    base = synth.write_tables(workdir, synth.CFG0_EMITTERS, nus, 20261203)
+    ctlkw = dict(emitters=synth.CFG0_EMITTERS, nus=nus, tblbase=base, hydz=0.0, sca_n=1,
+                 sca_mult=2, ctm_co2=0, ctm_h2o=0)
+    return ctlkw, atm, geom, aero
+
+
+MS_NALPHA = {2: 20, 1: 10}   # pencils per scattering point by scattering order
+
+
+def multiple_scattering_bench(args, local, torch):
+    """Depth-2 scattering (config 3): the plain path (secondary pencils of
+    order 1 and their own scattering points with pencils of order 0) and the
+    surrogate path (trained on the order-2 sources of a disjoint training
+    batch) on a held-out batch, device-timed; BT errors against the plain
+    GPU path and, on two rays of the stored oracle fixture, against the C
+    oracle with the same pencil counts."""
+    from jscat import api, structs as S, synth
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    from helpers import bt_error
+    n = args.ms_rays
+    ctlkw, atm, geom, aero = ice_case(n, 31)
+    ctl = S.make_ctl(**ctlkw)
+    nd = ctl.nd
+    inp = synth.batch_from([atm], np.zeros(n, np.int32), geom)
+    model = api.Model(ctl, device=local)
+    b = api.Batch(model, ctl, 1, len(inp["z"]), max(n, args.ms_train_rays))
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b.set_aero(aero)
+    for depth, na in MS_NALPHA.items():
+        b.set_nalpha_depth(depth, na)
+    # training samples: order-2 sources of a disjoint batch (also the warm-up)
+    c2, a2, g2, _ = ice_case(args.ms_train_rays, 32)
+    b.upload(synth.batch_from([a2], np.zeros(args.ms_train_rays, np.int32), g2), stream=sp)
+    b.run(stream=sp)
+    stream.synchronize()
+    X, Y = b.scatter_samples()
+    # the plain path on the first ms_plain_rays rays (about 20 ms per ray)
+    npl = min(n, args.ms_plain_rays)
+    sub = synth.batch_from([atm], np.zeros(npl, np.int32), {k: v[:npl] for k, v in geom.items()})
+    b.upload(sub, stream=sp)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.run(stream=sp)
+    e1.record(stream)
+    stream.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain = b.download(stream=sp)
+    b.upload(inp, stream=sp)
+    sur = api.Surrogate(nd, device=local, seed=6)
+    t0 = time.perf_counter()
+    sur.train(X, Y, epochs=args.ms_epochs, batch=512, lr=3e-3)
+    train_s = time.perf_counter() - t0
+    b.set_surrogate(sur, tol_rel=api.SURROGATE_CHECK_TOL, check_stride=api.SURROGATE_CHECK_STRIDE)
+    for _ in range(2):
+        b.run(stream=sp)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(3):
+        b.run(stream=sp)
+    e1.record(stream)
+    stream.synchronize()
+    sur_ms = e0.elapsed_time(e1) / 3
+    out = b.download(stream=sp)
+    st = b.surrogate_stats()
+    res = {"workload": MS_WORKLOAD, "rays": n, "channels": nd, "scattering_points": st["points"],
+           "plain": {"value": npl * nd / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
+                     "rays": npl, "steps": 1, "warmup": 1,
+                     "sample": "the first %d of the %d rays (about 20 ms per ray)" % (npl, n)},
+           "surrogate": {"value": n * nd / (sur_ms / 1e3), "unit": UNIT, "ms_per_step": sur_ms,
+                         "rays": n, "steps": 3, "warmup": 2,
+                         "speedup_vs_plain": (n * nd / (sur_ms / 1e3)) / (npl * nd / (plain_ms / 1e3)),
+                         "bt_err_k_vs_plain": bt_error(out["rad"][:npl], plain["rad"], ctlkw["nus"]),
+                         "used": st["used"], "fallback_points": st["fallback"],
+                         "checked_points": st["checked"],
+                         "max_albedo_weighted_src_err_checked": st["max_rel_err"],
+                         "check_tolerance": api.SURROGATE_CHECK_TOL,
+                         "held_out": "timed batch (seed 31) disjoint from the training batch "
+                                     "(seed 32)"},
+           "training": {"samples": int(len(X)), "rays": args.ms_train_rays,
+                        "epochs": args.ms_epochs, "seconds": train_s},
+           "pencils_per_point": {"depth %d" % d: na for d, na in MS_NALPHA.items()}}
+    # against the C oracle: two depth-2 rays with the same pencil counts
+    # through the same layer (tests/golden/ice_sca2_port.npz, channels 1 and
+    # 5 of these 8, computed by oracle/jurassic_oracle.c in CPU minutes),
+    # run here on the plain and the surrogate path
+    try:
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        from make_golden_shim import ice_depth2_case
+        gf = np.load(os.path.join(REPO, "tests", "golden", "ice_sca2_port.npz"))
+        _, fatm, fgeom, _ = ice_depth2_case(os.environ.get("JSC_WORKDIR", "/tmp/jsc"))
+        finp = synth.batch_from([fatm], np.zeros(len(fgeom["obsz"]), np.int32), fgeom)
+        cols = [0, 4]
+        fnus = [ctlkw["nus"][c] for c in cols]
+        b.upload(finp, stream=sp)
+        b.run(stream=sp)
+        f_sur = b.download(stream=sp)["rad"][:, cols]
+        b.set_surrogate(None)
+        b.upload(finp, stream=sp)
+        b.run(stream=sp)
+        f_plain = b.download(stream=sp)["rad"][:, cols]
+        res["oracle_fixture"] = {
+            "rays": int(len(fgeom["obsz"])), "channels": cols, "kind": "port (stored)",
+            "bt_err_k_plain": bt_error(f_plain, gf["rad"], fnus),
+            "bt_err_k_surrogate": bt_error(f_sur, gf["rad"], fnus)}
+    except Exception as exc:  # reported, never required
+        res["oracle_fixture"] = {"error": str(exc)[:200]}
+    b.close()
+    model.close()
+    res["_surrogate"] = sur
+    return res
+
+
 MIX_WORKLOAD = ("independent forward-model requests, rays log-uniform in [50, 5000], 50 % clear "
                 "air (8 emitters, 4/8/16/32/64 of the 64 channels 700-1400 cm-1, limb and nadir) "
-                "and 50 % aerosol (sulfate layer, 2 emitters, the 16 channels 780-1250 cm-1, "
-                "limb, single scattering)")
+                "and 50 % aerosol/cloud with recursion depth 0, 1 or 2 (depth 0: extinction by the "
+                "sulfate layer, depth 1: single scattering on it, 16 channels 780-1250 cm-1; depth "
+                "2: double scattering through the ice-cloud layer, 8 channels, 20/10 pencils, "
+                "CO2/H2O continua off; 2 emitters, limb)")
 
 RAY_CAP, ATM_CAP = 16384, 64   # rays and profiles per packed batch
 
@@ -316,7 +472,6 @@ def _pad(inp, n_atm, n_rays, lev):
     out = {}
     na = len(inp["atm_off"]) - 1
     nr = len(inp["ray_atm"])
-    add_l = (n_atm - na) * lev
     for k in ("z", "lon", "lat", "p", "t"):
         out[k] = np.concatenate([inp[k], np.tile(inp[k][:lev], n_atm - na)])
     for k in ("q", "k"):
@@ -325,150 +480,234 @@ def _pad(inp, n_atm, n_rays, lev):
     out["ray_atm"] = np.concatenate([inp["ray_atm"], np.zeros(n_rays - nr, np.int32)])
     for k in ("time", "obsz", "obslon", "obslat", "vpz", "vplon", "vplat"):
         out[k] = np.concatenate([inp[k], np.full(n_rays - nr, inp[k][0])])
-    assert len(out["z"]) == n_atm * lev and add_l >= 0
+    assert len(out["z"]) == n_atm * lev
     return out
 
 
-def mixed_bench(args, local, torch, sur=None, variant=-1):
-    """Mixed-size request batch: requests are admitted in arrival order into
-    packed batches per model (up to RAY_CAP rays and ATM_CAP profiles);
-    clear-air batches replay a CUDA graph captured once per model (fixed
-    capacity, padded), aerosol batches run the scattering path with the
-    surrogate (per-point fallback to the plain path).  All requests arrive
-    at t = 0; a request's latency is the end of its batch on the device
-    (CUDA events).  Depth-2 requests are not generated: the reference's
-    multiple scattering returns NaN whenever a scattering point sits on a
-    layer edge, which its own refinement makes the common case."""
-    from jscat import api, structs as S, synth
-    workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
+def _mixed_requests(nreq):
+    from jscat import synth
     rng = np.random.default_rng(20261203)
-    nreq = args.requests
     reqs = []
     for i in range(nreq):
         n = int(round(np.exp(rng.uniform(np.log(50), np.log(5000)))))
         aerosol = rng.uniform() < 0.5
-        # aerosol requests: the scattering workload's profile family (the
-        # surrogate's training distribution); clear air: the batched one
-        atm = (synth.atmosphere(synth.CFG0_EMITTERS, rng) if aerosol else
-               synth.atmosphere(synth.CFG1_EMITTERS, rng, t_sigma=5.0, vmr_sigma=0.2))
-        if aerosol:
-            geom = synth.limb_geometry(rng.uniform(8.0, 30.0, n))
-            nd = 16
-        else:
+        depth = int(rng.integers(0, 3)) if aerosol else 0
+        if not aerosol:
+            atm = synth.atmosphere(synth.CFG1_EMITTERS, rng, t_sigma=5.0, vmr_sigma=0.2)
             nl = n // 2
             g1 = synth.limb_geometry(rng.uniform(5.0, 60.0, nl))
             g2 = synth.nadir_geometry(rng.uniform(0.0, 60.0, n - nl))
             geom = {k: np.concatenate([g1[k], g2[k]]) for k in g1}
             nd = int(rng.choice([4, 8, 16, 32, 64]))
+            key = ("clear", nd)
+        else:
+            # the scattering workloads' profile families (the surrogates'
+            # training distributions)
+            atm = synth.atmosphere(synth.CFG0_EMITTERS, rng)
+            if depth == 2:
+                geom = synth.limb_geometry(rng.uniform(6.0, 14.0, n))
+                nd, key = 8, ("sca2",)
+            else:
+                geom = synth.limb_geometry(rng.uniform(8.0, 30.0, n))
+                nd, key = 16, ("sca1",) if depth == 1 else ("ext",)
         geom["time"] = rng.uniform(0.0, 86400.0, n)
-        reqs.append({"i": i, "n": n, "aerosol": aerosol, "nd": nd, "atm": atm, "geom": geom})
+        reqs.append({"i": i, "n": n, "depth": depth, "nd": nd, "key": key, "atm": atm,
+                     "geom": geom})
+    return reqs
+
+
+def mixed_bench(args, local, torch, sur=None, sur2=None, variant=-1, depth2=True):
+    """Mixed-size request batch (config 4): requests are admitted in arrival
+    order into packed batches per model (up to RAY_CAP rays and ATM_CAP
+    profiles).  Depth-0 batches (clear air, aerosol extinction) replay a
+    CUDA graph captured once per model (fixed capacity, padded), two
+    graph instances per model alternating, on one stream; depth-1 and
+    depth-2 batches run the scattering path with the surrogates (per-point
+    fallback to the plain path) on a second stream.  All requests arrive at
+    t = 0; a request's latency is the end of its batch on the device (CUDA
+    events).  Run twice: overlapped (no host synchronisation between
+    batches except before reusing a graph's staging arrays) and serial (the
+    host waits for every batch, one stream), for comparison."""
+    from jscat import api, structs as S, synth
+    workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
+    reqs = _mixed_requests(args.requests)
+    skipped = 0
+    if not depth2:
+        # without an accepted depth-2 surrogate every depth-2 request runs the
+        # plain path (about 20 ms per ray): left out, and counted
+        skipped = sum(1 for r in reqs if r["depth"] == 2)
+        reqs = [r for r in reqs if r["depth"] != 2]
     lev = len(reqs[0]["atm"]["z"])
-    stream = torch.cuda.Stream()
-    sp = stream.cuda_stream
+    stream_g, stream_s = torch.cuda.Stream(), torch.cuda.Stream()
+    sg, ss = stream_g.cuda_stream, stream_s.cuda_stream
 
     def pin(a):
         return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
 
-    # models, graphs (clear air) and the scattering batch (aerosol)
     g = np.load(os.path.join(REPO, "tests", "golden", "aero_sulfate16.npz"))
     aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
-    runners, models = {}, []
-    for nd in sorted({r["nd"] for r in reqs if not r["aerosol"]}):
-        nus = list(synth.CFG1_NU[::64 // nd])
-        base = synth.write_tables(workdir, synth.CFG1_EMITTERS, nus, 20261203)
-        ctl = S.make_ctl(emitters=synth.CFG1_EMITTERS, nus=nus, tblbase=base, hydz=0.0)
-        m = api.Model(ctl, device=local)
-        models.append(m)
-        first = [r for r in reqs if not r["aerosol"] and r["nd"] == nd][:1]
-        shape = _pad(_pack(first), ATM_CAP, RAY_CAP, lev)
-        runners[nd] = api.GraphBatch(m, ctl, shape, sp, pin, max_seg=RAY_CAP * 420,
-                                     variant=variant)
     a_nus = [float(v) for v in g["nus"]]
     a_base = synth.write_tables(workdir, synth.CFG0_EMITTERS, a_nus, 20261203)
-    a_ctl = S.make_ctl(emitters=synth.CFG0_EMITTERS, nus=a_nus, tblbase=a_base, hydz=0.0,
-                       sca_n=1, sca_mult=1, sca_ext="beta_a")
-    a_model = api.Model(a_ctl, device=local)
-    models.append(a_model)
-    a_batch = api.Batch(a_model, a_ctl, ATM_CAP, ATM_CAP * lev, RAY_CAP)
-    a_batch.set_aero(aero)
-    a_batch.set_nalpha(20)
-    if sur is not None:
-        a_batch.set_surrogate(sur, tol_rel=api.SURROGATE_CHECK_TOL,
-                              check_stride=api.SURROGATE_CHECK_STRIDE)
+    models, runners, sbatch, ctls = [], {}, {}, {}
+    first = {}
+    for r in reqs:
+        first.setdefault(r["key"], r)
+    for key, r0 in first.items():
+        if key[0] == "clear":
+            nus = list(synth.CFG1_NU[::64 // key[1]])
+            base = synth.write_tables(workdir, synth.CFG1_EMITTERS, nus, 20261203)
+            ctl = S.make_ctl(emitters=synth.CFG1_EMITTERS, nus=nus, tblbase=base, hydz=0.0)
+            kw = dict(variant=variant)
+        elif key[0] == "ext":
+            ctl = S.make_ctl(emitters=synth.CFG0_EMITTERS, nus=a_nus, tblbase=a_base, hydz=0.0,
+                             sca_n=1, sca_mult=0, sca_ext="beta_a")
+            kw = dict(aero=aero)
+        elif key[0] == "sca1":
+            ctl = S.make_ctl(emitters=synth.CFG0_EMITTERS, nus=a_nus, tblbase=a_base, hydz=0.0,
+                             sca_n=1, sca_mult=1, sca_ext="beta_a")
+        else:
+            c3, _, _, ice_aero = ice_case(1, 31)
+            ctl = S.make_ctl(**c3)
+        ctls[key] = ctl
+        m = api.Model(ctl, device=local)
+        models.append(m)
+        if key[0] in ("clear", "ext"):
+            shape = _pad(_pack([r0]), ATM_CAP, RAY_CAP, lev)
+            runners[key] = [api.GraphBatch(m, ctl, shape, sg, pin, max_seg=RAY_CAP * 420, **kw)
+                            for _ in range(2)]
+        else:
+            b = api.Batch(m, ctl, ATM_CAP, ATM_CAP * lev, RAY_CAP)
+            if key[0] == "sca1":
+                b.set_aero(aero)
+                b.set_nalpha(20)
+                if sur is not None:
+                    b.set_surrogate(sur, tol_rel=api.SURROGATE_CHECK_TOL,
+                                    check_stride=api.SURROGATE_CHECK_STRIDE)
+            else:
+                b.set_aero(ice_aero)
+                for depth, na in MS_NALPHA.items():
+                    b.set_nalpha_depth(depth, na)
+                if sur2 is not None:
+                    b.set_surrogate(sur2, tol_rel=api.SURROGATE_CHECK_TOL,
+                                    check_stride=api.SURROGATE_CHECK_STRIDE)
+            sbatch[key] = b
 
     # admission: arrival order, per model key, up to the caps
     batches, open_b = [], {}
     for r in reqs:
-        key = ("aero",) if r["aerosol"] else ("clear", r["nd"])
-        cur = open_b.get(key)
+        cur = open_b.get(r["key"])
         if cur is None or cur["rays"] + r["n"] > RAY_CAP or len(cur["reqs"]) >= ATM_CAP:
-            cur = {"key": key, "reqs": [], "rays": 0}
-            open_b[key] = cur
+            cur = {"key": r["key"], "reqs": [], "rays": 0}
+            open_b[r["key"]] = cur
             batches.append(cur)
         cur["reqs"].append(r)
         cur["rays"] += r["n"]
     packed = [(b_, _pack(b_["reqs"])) for b_ in batches]
-    ev0 = torch.cuda.Event(enable_timing=True)
-    evs = [torch.cuda.Event(enable_timing=True) for _ in packed]
-    outs = {}
-    l0 = api.launch_count()
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    for (b_, inp), ev in zip(packed, evs):
-        if b_["key"][0] == "clear":
-            gr = runners[b_["key"][1]]
-            gr.launch(_pad(inp, ATM_CAP, RAY_CAP, lev))
-            ev.record(stream)
-            stream.synchronize()        # the staging arrays are reused by the next batch
+
+    def execute(overlap):
+        outs = {}
+        ev0 = torch.cuda.Event(enable_timing=True)
+        evs = [torch.cuda.Event(enable_timing=True) for _ in packed]
+        pending = {}          # graph runner -> (batch, event) whose outputs are not read yet
+        turn = {k: 0 for k in runners}
+        l0 = api.launch_count()
+
+        def collect(gr):
+            b_, ev = pending.pop(id(gr))
+            ev.synchronize()
             gr.status()
             outs[id(b_)] = gr.out["rad"][:b_["rays"]].copy()
-        else:
-            a_batch.upload(inp, stream=sp)
-            a_batch.run(stream=sp)
-            res = a_batch.download(stream=sp)
-            ev.record(stream)
-            outs[id(b_)] = res["rad"]
-    stream.synchronize()
-    launches = api.launch_count() - l0
-    lat, units = [], 0
-    for (b_, _), ev in zip(packed, evs):
-        t = ev0.elapsed_time(ev)
-        for r in b_["reqs"]:
-            lat.append(t)
-            units += r["n"] * r["nd"]
-    make = max(lat)
-    # accuracy: aerosol batches against the plain path, clear against the
-    # ordinary (non-graph) batch path
+
+        torch.cuda.synchronize()
+        ev0.record(stream_g)
+        stream_s.wait_event(ev0)
+        for (b_, inp), ev in zip(packed, evs):
+            key = b_["key"]
+            if key in runners:
+                gr = runners[key][turn[key]]
+                turn[key] ^= 1
+                if id(gr) in pending:   # its staging arrays are about to be reused
+                    collect(gr)
+                gr.launch(_pad(inp, ATM_CAP, RAY_CAP, lev))
+                ev.record(stream_g)
+                pending[id(gr)] = (b_, ev)
+                if not overlap:
+                    collect(gr)
+            else:
+                st = sg if not overlap else ss
+                bb = sbatch[key]
+                bb.upload(inp, stream=st)
+                bb.run(stream=st)
+                res = bb.download(stream=st)
+                ev.record(stream_g if not overlap else stream_s)
+                outs[id(b_)] = res["rad"]
+        for gr in [g for rr in runners.values() for g in rr]:
+            if id(gr) in pending:
+                collect(gr)
+        torch.cuda.synchronize()
+        launches = api.launch_count() - l0
+        lat, units = [], 0
+        for (b_, _), ev in zip(packed, evs):
+            t = ev0.elapsed_time(ev)
+            for r in b_["reqs"]:
+                lat.append(t)
+                units += r["n"] * r["nd"]
+        make = max(lat)
+        return outs, {"value": units / (make / 1e3), "unit": UNIT, "makespan_ms": make,
+                      "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                                     "p99": float(np.percentile(lat, 99))},
+                      "gpu_launches": int(launches)}
+
+    execute(True)                      # warm-up (allocations of the scattering path)
+    outs, over = execute(True)
+    _, serial = execute(False)
+    # accuracy: scattering batches against their plain path, graph batches
+    # against the ordinary (non-graph) batch path
     errs = {}
     sys.path.insert(0, os.path.join(REPO, "tests"))
     from helpers import bt_error
-    a_b = next((bb for bb, _ in packed if bb["key"][0] == "aero"), None)
-    if a_b is not None:
-        a_batch.set_surrogate(None)
-        a_batch.upload(_pack(a_b["reqs"]), stream=sp)
-        a_batch.run(stream=sp)
-        plain = a_batch.download(stream=sp)
-        errs["aerosol_surrogate_vs_plain_k"] = bt_error(outs[id(a_b)], plain["rad"], a_nus)
-    c_b = next((bb for bb, _ in packed if bb["key"][0] == "clear"), None)
-    if c_b is not None:
-        nd = c_b["key"][1]
-        nus = list(synth.CFG1_NU[::64 // nd])
-        base = synth.write_tables(workdir, synth.CFG1_EMITTERS, nus, 20261203)
-        ctl = S.make_ctl(emitters=synth.CFG1_EMITTERS, nus=nus, tblbase=base, hydz=0.0)
-        ref = api.formod_batch(ctl, _pack(c_b["reqs"]), device=local)
-        errs["clear_graph_vs_batch_k"] = bt_error(outs[id(c_b)], ref["rad"], nus)
-    for gr in runners.values():
-        gr.close()
-    a_batch.close()
+    for key in sbatch:
+        bb = next((x for x, _ in packed if x["key"] == key), None)
+        if bb is None:
+            continue
+        # the first request of the first batch, its first 200 rays
+        r0 = bb["reqs"][0]
+        k = min(200, r0["n"])
+        one = dict(r0, geom={kk: v[:k] for kk, v in r0["geom"].items()})
+        plain_b = sbatch[key]
+        plain_b.set_surrogate(None)
+        plain_b.upload(_pack([one]), stream=ss)
+        plain_b.run(stream=ss)
+        plain = plain_b.download(stream=ss)
+        errs["%s_surrogate_vs_plain_k" % key[0]] = bt_error(outs[id(bb)][:k], plain["rad"],
+                                                             list(ctls[key].nu[:ctls[key].nd]))
+    for key in runners:
+        bb = next((x for x, _ in packed if x["key"] == key), None)
+        if bb is None:
+            continue
+        ref = api.formod_batch(ctls[key], _pack(bb["reqs"]), device=local,
+                               aero=aero if key[0] == "ext" else None)
+        errs["%s_graph_vs_batch_k" % "_".join(str(k) for k in key)] = bt_error(
+            outs[id(bb)], ref["rad"], list(ctls[key].nu[:ctls[key].nd]))
+    for rr in runners.values():
+        for gr in rr:
+            gr.close()
+    for bb in sbatch.values():
+        bb.close()
     for m in models:
         m.close()
-    return {"workload": MIX_WORKLOAD, "requests": nreq, "batches": len(packed),
-            "graph_batches": sum(1 for bb, _ in packed if bb["key"][0] == "clear"),
-            "value": units / (make / 1e3), "unit": UNIT, "makespan_ms": make,
-            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-            "gpu_launches": int(launches), "bt_err": errs,
+    kinds = {}
+    for r in reqs:
+        kinds["depth%d" % r["depth"] + ("_clear" if r["key"][0] == "clear" else "")] = \
+            kinds.get("depth%d" % r["depth"] + ("_clear" if r["key"][0] == "clear" else ""), 0) + 1
+    return {"workload": MIX_WORKLOAD, "requests": args.requests, "request_kinds": kinds,
+            "depth2_requests_left_out": skipped,
+            "batches": len(packed),
+            "graph_batches": sum(1 for bb, _ in packed if bb["key"] in runners),
+            **over, "serial": serial, "bt_err": errs,
             "admission": "arrival order, per model, <= %d rays and %d profiles per batch; "
-                         "clear-air batches replay a CUDA graph (padded to capacity)"
+                         "depth-0 batches replay CUDA graphs (padded to capacity, two per model) "
+                         "on one stream, scattering batches run on a second stream"
                          % (RAY_CAP, ATM_CAP)}
 
 
@@ -609,6 +848,60 @@ def optprop_bench(args, torch, cpu=True):
             "cpu_baseline_kind": "reference (1 core)"}
 
 
+def sharded_bench(args, rank, world, local, torch, dist):
+    """The multi-GPU product path on one common ray set (every rank builds
+    the same seeded workload): contiguous ray ranges balanced by the
+    geometric LOS estimate (jscat.parallel), each rank runs its range
+    through the batch C-ABI on its GPU, and one all-gather collects the
+    radiances and transmittances of every ray on every rank (NCCL, device
+    buffers).  Timed per step from the upload to the end of the gather,
+    CUDA events, max over ranks."""
+    from jscat import parallel, synth, api, structs as S
+    ctlkw, atms, ray_atm, geom = make_workload(args.rays, seed_offset=0)
+    ctl = S.make_ctl(**ctlkw)
+    model = api.Model(ctl, device=local)
+    inp = synth.batch_from(atms, ray_atm, geom)
+    ranges = parallel.shard_ranges(parallel.estimate_los_points(geom), world)
+    s, e = ranges[rank]
+    sub = parallel.select_rays(inp, s, e)
+    nd = ctl.nd
+    b = api.Batch(model, ctl, len(sub["atm_off"]) - 1, len(sub["z"]), max(1, e - s))
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+
+    def step():
+        if e > s:
+            b.upload(sub, stream=sp)
+            b.run(stream=sp)
+            out = b.download(stream=sp)
+            loc = np.concatenate([out["rad"], out["tau"]], axis=1)
+        else:
+            loc = np.zeros((0, 2 * nd))
+        return parallel.gather_rows(loc, ranges)
+
+    for _ in range(args.warmup):
+        full = step()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        full = step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([ev0.elapsed_time(ev1)], device=parallel.gather_device())
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = t.item() / args.steps
+    b.close()
+    model.close()
+    return {"workload": WORKLOAD + " (one common ray set, sharded)", "rays": args.rays,
+            "ranges": ranges, "value": args.rays * nd / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms, "scaling": "strong",
+            "gathered_rows": int(full.shape[0]),
+            "path": "jscat.parallel: shard_ranges + select_rays + batch C-ABI + all-gather "
+                    "(NCCL, device buffers)"}
+
+
 def cpu_baseline(ctlkw, atms, ray_atm, geom, n_sample):
     """The reference's OpenMP formod on a bounded sample of the workload
     (whole profiles, first n_sample rays), all host cores, after a warm-up
@@ -684,12 +977,15 @@ def main():
         run_reference_arm(args, rank, world)
         return
     import torch
+    # more ranks than GPUs only where a test asks for it (the gloo backend)
+    local = local % max(1, torch.cuda.device_count())
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        dist.init_process_group(os.environ.get("JSC_DIST_BACKEND", "nccl"),
+                                timeout=timedelta(seconds=300))
     from jscat import api, structs as S, synth, lib as L
 
     ctlkw, atms, ray_atm, geom = make_workload(args.rays, seed_offset=rank)
@@ -753,7 +1049,8 @@ def main():
     e_ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     if dist:
-        tt = torch.tensor([t_ms, e_ms], device="cuda")
+        from jscat import parallel
+        tt = torch.tensor([t_ms, e_ms], device=parallel.gather_device())
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_ms, e_ms = tt.tolist()
     ms_step = t_ms / args.steps
@@ -761,6 +1058,9 @@ def main():
     value = units / (ms_step / 1e3)
     e2e = units / (e_ms / args.steps / 1e3)
 
+    sharded = None
+    if dist:
+        sharded = sharded_bench(args, rank, world, local, torch, dist)
     ega = float(np.mean(ega_ms))
     B = algorithmic_bytes(n_ega, n_points, args.rays, nd, ng)
     peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
@@ -793,6 +1093,9 @@ def main():
                          "kernel": "ega_rt", "kernel_ms": ega,
                          "algorithmic_bytes_per_launch": B},
             "clocks": clk}
+    if sharded is not None:
+        line["sharded"] = sharded
+    note("headline done: %.1f ms per step" % ms_step)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cb, ref, sel = cpu_baseline(ctlkw, atms, ray_atm, geom, args.cpu_rays)
@@ -812,6 +1115,7 @@ def main():
                                                 cpu=not args.no_cpu_baseline)
         except Exception as exc:
             line["table_ingest"] = {"error": str(exc)[:300]}
+    note("cpu baseline / ingest done")
     sur = None
     if rank == 0 and world == 1 and args.sca_rays > 0:
         try:
@@ -820,16 +1124,29 @@ def main():
             sur = line["scattering"].pop("_surrogate")
         except Exception as exc:  # reported beside the headline, never required
             line["scattering"] = {"error": str(exc)[:300]}
+    note("scattering done")
+    sur2 = None
+    if rank == 0 and world == 1 and args.ms_rays > 0:
+        try:
+            line["multiple_scattering"] = multiple_scattering_bench(args, local, torch)
+            sur2 = line["multiple_scattering"].pop("_surrogate")
+        except Exception as exc:
+            line["multiple_scattering"] = {"error": str(exc)[:300]}
+    note("multiple scattering done")
     if rank == 0 and world == 1 and args.requests > 0:
         try:
             # clear-air graph batches replay the launch variant the headline's
             # autotuner chose on the same emitters and channel grid
-            line["mixed_requests"] = mixed_bench(args, local, torch, sur,
-                                                 variant=tuned.get("variant", -1))
+            ms = line.get("multiple_scattering", {})
+            ok2 = bool(ms.get("surrogate", {}).get("used"))
+            line["mixed_requests"] = mixed_bench(args, local, torch, sur, sur2 if ok2 else None,
+                                                 variant=tuned.get("variant", -1), depth2=ok2)
         except Exception as exc:
             line["mixed_requests"] = {"error": str(exc)[:300]}
-    if sur is not None:
-        sur.close()
+    note("mixed requests done")
+    for sx in (sur, sur2):
+        if sx is not None:
+            sx.close()
     if rank == 0 and world == 1 and args.jacobians > 0:
         try:
             line["jacobian"] = jacobian_bench(args, torch, cpu=not args.no_cpu_baseline)

@@ -559,6 +559,14 @@ int jsc_batch_scatter_points(jsc_batch *b, int n, const double *x, const double 
                              const int *layer, const double *time, const int *prof,
                              double *src, void *stream);
 
+/* Secondary pencils per scattering point for one scattering order only:
+ * the points whose source srcfunc_sca computes with scattering = depth
+ * (depth = ctl->sca_mult for this batch's own points, one less for the
+ * points of its secondary pencils, and so on) cast nalpha pencils (even,
+ * 10..28, angles as in jsc_batch_set_nalpha); other orders keep the
+ * batch's count.  jsc_batch_set_nalpha resets every order to its count. */
+int jsc_batch_set_nalpha_depth(jsc_batch *b, int depth, int nalpha);
+
 /* Per-(ray, channel) checksum of every emissivity-table index the EGA
  * interpolation selected in the last run, for parity checks against the
  * reference's indices.  Per emitter g, D_g folds d = d*1000003 + v over the

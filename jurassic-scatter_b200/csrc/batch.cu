@@ -223,6 +223,25 @@ extern "C" int jsc_batch_set_nalpha(jsc_batch *b, int nalpha) {
     return JSC_ERR_ARG;
   }
   b->nalpha = nalpha;
+  for (int d = 0; d <= JSC_MAX_DEPTH; d++) b->nalpha_at[d] = 0;
+  // child batches are sized per pencil count: rebuild on the next run
+  jsc_batch_destroy(b->child);
+  b->child = nullptr;
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_set_nalpha_depth(jsc_batch *b, int depth, int nalpha) {
+  double alpha[32];
+  if (!b || depth < 1 || depth > JSC_MAX_DEPTH || depth > b->depth || sca_alpha(alpha, nalpha)) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_set_nalpha_depth: depth %d (1..%d) with %d pencils "
+                  "(even, 10..%d)", depth, b ? b->depth : 0, nalpha, JSC_NALPHA_REF);
+    return JSC_ERR_ARG;
+  }
+  b->nalpha_at[depth] = nalpha;
+  if (depth == b->depth) {
+    b->nalpha = nalpha;
+    memcpy(b->alpha, alpha, sizeof(alpha));
+  }
   // child batches are sized per pencil count: rebuild on the next run
   jsc_batch_destroy(b->child);
   b->child = nullptr;
@@ -548,8 +567,9 @@ static int ensure_child(jsc_batch *b, jsc_batch **pc, int max_rays, int depth) {
   if (st) return st;
   c->cfg.hydz = -1;  // profiles arrive hydrostatically balanced
   c->depth = depth;
-  c->nalpha = b->nalpha;
-  memcpy(c->alpha, b->alpha, sizeof(b->alpha));
+  memcpy(c->nalpha_at, b->nalpha_at, sizeof(b->nalpha_at));
+  c->nalpha = (depth <= JSC_MAX_DEPTH && b->nalpha_at[depth]) ? b->nalpha_at[depth] : b->nalpha;
+  sca_alpha(c->alpha, c->nalpha);
   c->ega_variant = b->ega_variant;
   if ((st = jsc_batch_set_aero(c, b->h_aero))) {
     jsc_batch_destroy(c);

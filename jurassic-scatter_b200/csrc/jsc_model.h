@@ -67,6 +67,7 @@ struct EgaArgs {
 enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_SCATTER, JSC_T_CTM, JSC_T_SUR, JSC_T_N };
 
 #define JSC_NALPHA_REF 28  // secondary pencils per scattering point (src/scatter.c:673)
+#define JSC_MAX_DEPTH 7    // deepest scattering order with its own pencil count
 
 struct jsc_batch {
   jsc_model *m;
@@ -107,6 +108,7 @@ struct jsc_batch {
   // that run the secondary and the solar pencils.
   int depth, nalpha;
   double alpha[32];
+  int nalpha_at[JSC_MAX_DEPTH + 1];  // per-depth pencil counts (0: inherit nalpha)
   int *d_nsp;               // [max_rays]
   int64_t *d_sp_off;        // [max_rays+1]
   double *d_sp;             // [max_sp][JSC_SP_REC]

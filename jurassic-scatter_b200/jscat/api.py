@@ -287,6 +287,11 @@ class Batch:
         """Secondary pencils per scattering point (even, 10..28; 28 default)."""
         L.check(L.load().jsc_batch_set_nalpha(self.h, int(nalpha)), "jsc_batch_set_nalpha")
 
+    def set_nalpha_depth(self, depth, nalpha):
+        """Pencils per scattering point of one scattering order."""
+        L.check(L.load().jsc_batch_set_nalpha_depth(self.h, int(depth), int(nalpha)),
+                "jsc_batch_set_nalpha_depth")
+
     def set_timing(self, on=True):
         L.load().jsc_batch_set_timing(self.h, 1 if on else 0)
 

@@ -30,6 +30,7 @@ EXPORTS = [
     "formod_pencil", "formod_fov", "read_shape", "read_tbl", "srcfunc_planck",
     "formod_continua", "intpol_tbl", "intpol_tbl_eps", "intpol_tbl_u", "locate_tbl",
     "jsc_srcfunc_sca", "jsc_batch_scatter_points", "jsc_surrogate_get_scaling",
+    "jsc_batch_set_nalpha_depth",
 ]
 
 
@@ -148,6 +149,7 @@ def load():
         "jsc_batch_scatter_points": (i, [vp, i, P(d), P(d), P(i), P(d), P(i), P(d), vp]),
         "jsc_surrogate_get_scaling": (i, [vp, P(C.c_float), P(C.c_float), P(C.c_float),
                                           P(C.c_float)]),
+        "jsc_batch_set_nalpha_depth": (i, [vp, i, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -916,10 +916,19 @@ static void o_sca_alpha(double *alpha, int nalpha) {
  * count from 10 to 28 with the same angle construction (for checking the
  * GPU path's pencil-count option). */
 static int g_nalpha = 28;
+static int g_nalpha_at[8];  /* per scattering order (0: g_nalpha) */
 
 int oracle_set_nalpha(int nalpha) {
   if (nalpha < 10 || nalpha > 28 || (nalpha & 1)) return JSC_ERR_ARG;
   g_nalpha = nalpha;
+  for (int i = 0; i < 8; i++) g_nalpha_at[i] = 0;
+  return 0;
+}
+
+/* Pencil count of the sources of one scattering order only. */
+int oracle_set_nalpha_order(int order, int nalpha) {
+  if (order < 1 || order > 7 || nalpha < 10 || nalpha > 28 || (nalpha & 1)) return JSC_ERR_ARG;
+  g_nalpha_at[order] = nalpha;
   return 0;
 }
 
@@ -930,7 +939,8 @@ static int o_srcfunc_sca_1d(const ctl_t *ctl, const atm_t *atm, const aero_t *ae
                             const double *x, const double *dx, int il, double *src_sca,
                             int scattering) {
   enum { NPHI = 180, NTHETA2 = 180 };
-  const int NALPHA = g_nalpha;
+  const int NALPHA = (scattering >= 1 && scattering < 8 && g_nalpha_at[scattering])
+                        ? g_nalpha_at[scattering] : g_nalpha;
   double alpha[28], dnorth[3], ek[3], lx[3], ly[3], lz[3], sx[3], sy[3], sz[3],
          theta[NTHETA], wsum[NDMAX], xv[3], mlz[3];
   obs_t *obs2 = (obs_t *)calloc(1, sizeof(obs_t));

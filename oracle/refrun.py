@@ -50,8 +50,13 @@ def _child(job):
     port = job.get("port", False)
     fm = lib.oracle_formod if port else lib.formod
     if port and job.get("nalpha"):
-        if lib.oracle_set_nalpha(int(job["nalpha"])):
-            raise RuntimeError("oracle_set_nalpha(%r) refused" % job["nalpha"])
+        na = job["nalpha"]
+        if isinstance(na, dict):    # {scattering order: pencils}
+            for order, n in na.items():
+                if lib.oracle_set_nalpha_order(int(order), int(n)):
+                    raise RuntimeError("oracle_set_nalpha_order(%r, %r) refused" % (order, n))
+        elif lib.oracle_set_nalpha(int(na)):
+            raise RuntimeError("oracle_set_nalpha(%r) refused" % na)
     fm.argtypes = [P(S.CtlT), P(S.AtmT), P(S.ObsT), P(S.AeroT)]
     fm.restype = C.c_int if port else None
     if not port:

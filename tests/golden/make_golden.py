@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [headline|points [kind...]|jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
+    make -C oracle ref && python tests/golden/make_golden.py [headline|points [kind...]|ice2|jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -384,6 +384,55 @@ def S_aero(aero_bytes):
     return S.AeroT.from_buffer_copy(aero_bytes)
 
 
+def ice_depth2_case(workdir):
+    """Depth-2 scattering through the ice-cloud layer (9-11 km) with the
+    per-order pencil counts of the benchmark (20 pencils per point of order
+    2, 10 per point of order 1), two of its channels, CO2/H2O continua off,
+    two limb rays by day.  The C restatement computes it (its per-order
+    pencil count is an option the reference does not have; with 28 pencils
+    at every order it reproduces the reference bit for bit)."""
+    g = np.load(os.path.join(HERE, "aero_ice8.npz"))
+    nus = [float(v) for v in g["nus"][[0, 4]]]
+    rng = np.random.default_rng(20261207)
+    atm = synth.atmosphere(synth.CFG0_EMITTERS, rng)
+    geom = synth.limb_geometry(np.array([10.4, 12.2]))
+    geom["time"] = np.array([43200.0, 50000.0])
+    base = synth.write_tables(workdir, synth.CFG0_EMITTERS, nus, 20261203)
+    ctlkw = dict(emitters=synth.CFG0_EMITTERS, nus=nus, tblbase=base, hydz=0.0, sca_n=1,
+                 sca_mult=2, ctm_co2=0, ctm_h2o=0)
+    return ctlkw, atm, geom, {2: 20, 1: 10}
+
+
+def ice_depth2_fixture(workdir):
+    from jscat import structs as S
+    ctlkw, atm, geom, nalpha = ice_depth2_case(workdir)
+    g = np.load(os.path.join(HERE, "aero_ice8.npz"))
+    full = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    aero = aero_channels(full, [0, 4])
+    ref = refrun.run_port(ctlkw, [atm], np.zeros(2, int), geom, aero=bytes(aero), los=True,
+                          nalpha=nalpha, threads=os.cpu_count(), timeout=7200)
+    np.savez_compressed(os.path.join(HERE, "ice_sca2_port.npz"), rad=ref["rad"], tau=ref["tau"],
+                        nlos=ref["nlos"], aero=np.frombuffer(bytes(aero), dtype=np.uint8),
+                        seconds=ref["seconds"],
+                        table_sha256=tables_digest(ctlkw["tblbase"], ctlkw["emitters"],
+                                                   ctlkw["nus"]),
+                        **{"geom_" + k: v for k, v in geom.items()})
+
+
+def aero_channels(aero, idx):
+    """aero_t restricted to the channels idx (in that order)."""
+    from jscat import structs as S
+    out = S.AeroT.from_buffer_copy(bytes(aero))
+    for il in range(aero.nl):
+        for j, i in enumerate(idx):
+            out.beta_e[il][j] = aero.beta_e[il][i]
+            out.beta_s[il][j] = aero.beta_s[il][i]
+            out.beta_a[il][j] = aero.beta_a[il][i]
+            for a in range(181):
+                out.p[il][j][a] = aero.p[il][i][a]
+    return out
+
+
 def headline_fixtures(workdir):
     """headline_batch (the benchmark's 64-channel, 8-emitter shape) and
     continuum_bands (O2 and N2 continuum channels)."""
@@ -398,6 +447,9 @@ def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
     if sys.argv[1:] == ["headline"]:
         headline_fixtures(workdir)
+        return
+    if sys.argv[1:] == ["ice2"]:
+        ice_depth2_fixture(workdir)
         return
     if sys.argv[1:2] == ["points"]:
         # per-point scattering sources; slow kinds (order2, ip2, ip3) take

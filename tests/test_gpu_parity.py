@@ -336,3 +336,34 @@ def test_formod_pencil_clear_and_scattering(workdir):
     for ir in (3, 11):
         api.formod_pencil(ctl, a, obs, aero, scattering=1, ir=ir)
         assert max_rel(S.arr(obs.rad)[:ctl.nd, ir], ga["rad"][ir]) <= REL_TOL
+
+
+def test_double_scattering_per_depth_pencils(workdir):
+    """Depth 2 with per-order pencil counts (20 pencils per point of order 2,
+    10 of order 1) through the ice-cloud layer, CO2/H2O continua off: the
+    radiances of the C restatement with the same counts
+    (tests/golden/ice_sca2_port.npz)."""
+    from jscat import api, structs as S, synth
+    from make_golden_shim import ice_depth2_case
+    g = _load("ice_sca2_port")
+    ctlkw, atm, geom, nalpha = ice_depth2_case(workdir)
+    _check_tables(g, ctlkw)
+    ctl = S.make_ctl(**ctlkw)
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    m = api.Model(ctl)
+    inp = synth.batch_from([atm], np.zeros(len(geom["obsz"]), np.int32), geom)
+    b = api.Batch(m, ctl, 1, len(inp["z"]), len(geom["obsz"]))
+    try:
+        b.set_aero(aero)
+        for depth, na in nalpha.items():
+            b.set_nalpha_depth(depth, na)
+        b.upload(inp)
+        b.run()
+        out = b.download()
+    finally:
+        b.close()
+        m.close()
+    np.testing.assert_array_equal(out["nlos"], g["nlos"])
+    assert np.all(np.isfinite(g["rad"]))
+    assert bt_error(out["rad"], g["rad"], ctlkw["nus"]) <= BT_TOL_K
+    assert max_rel(out["rad"], g["rad"]) <= REL_TOL
