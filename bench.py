@@ -235,6 +235,34 @@ def scattering_bench(args, local, torch, oracle_sample=True):
     stream.synchronize()
     plain_ms = timed(1)
     plain = b.download(stream=sp)
+    # the same plain step without host read-backs: fixed capacity, point
+    # list and rounds of pencils on the device, replayed from a CUDA graph
+    fixed = None
+    try:
+        def pin(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        gb = api.GraphBatch(model, ctl, inp, sp, pin, aero=aero, nalpha=20)
+        gb.launch()
+        stream.synchronize()
+        gb.status()
+        l0 = api.launch_count()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        gb.launch()
+        e1.record(stream)
+        stream.synchronize()
+        gb.status()
+        fixed_ms = e0.elapsed_time(e1)
+        fixed = {"value": n * nd / (fixed_ms / 1e3), "unit": UNIT, "ms_per_step": fixed_ms,
+                 "steps": 1, "warmup": 1, "graph_kernels": api.launch_count() - l0,
+                 "host_launches": 1,
+                 "radiances_equal_plain": bool(np.array_equal(gb.out["rad"], plain["rad"])),
+                 "path": "fixed capacity: scattering points counted and listed on the device, "
+                         "rounds of secondary/solar pencils (null pencils past the device count), "
+                         "no host read-back, one CUDA graph"}
+        gb.close()
+    except Exception as exc:
+        fixed = {"error": str(exc)[:200]}
     sur = api.Surrogate(nd, device=local, seed=5)
     t0 = time.perf_counter()
     losses = sur.train(X, Y, epochs=args.sca_epochs, batch=4096, lr=3e-3)
@@ -265,6 +293,7 @@ def scattering_bench(args, local, torch, oracle_sample=True):
     res = {"workload": SCA_WORKLOAD, "rays": n, "channels": nd, "scattering_points": st["points"],
            "plain": {"value": n * nd / (plain_ms / 1e3), "unit": UNIT, "ms_per_step": plain_ms,
                      "steps": 1, "warmup": 1},
+           "plain_graph": fixed,
            "surrogate": {"value": n * nd / (sur_ms / 1e3), "unit": UNIT, "ms_per_step": sur_ms,
                          "steps": 5, "warmup": 3, "speedup_vs_plain": plain_ms / sur_ms,
                          "bt_err_k_vs_plain": bt_error(out["rad"], plain["rad"], ctlkw["nus"]),

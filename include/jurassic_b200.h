@@ -507,9 +507,21 @@ int jsc_batch_variant(const jsc_batch *b, int *variant, int *block, int *min_blo
 /* Fixed-capacity runs (on != 0): jsc_batch_run then never reads back from
  * the device (LOS buffers hold the capacity given at jsc_batch_create, a
  * longer line of sight sets JSC_ERR_NLOS in the status), so upload + run +
- * download can be captured into a CUDA graph.  Depth 0 only (clear air or
- * aerosol extinction, ctl->sca_mult = 0). */
+ * download can be captured into a CUDA graph.  Covers clear air, aerosol
+ * extinction (ctl->sca_mult = 0) and single scattering (ctl->sca_mult = 1,
+ * ctl->ip = 1, no surrogate): there the scattering points are counted and
+ * listed on the device, and a fixed number of rounds of secondary and solar
+ * pencils (null pencils past the device count) run from a point list of
+ * the capacity jsc_batch_set_fixed_points sets (default 40 per ray); more
+ * points than that set JSC_ERR_QUEUE.  With scattering, call
+ * jsc_batch_set_aero and jsc_batch_set_nalpha first: switching on
+ * allocates everything the runs use (room for 144 LOS points per
+ * secondary pencil and 256 per solar pencil of a round, on average). */
 int jsc_batch_set_fixed(jsc_batch *b, int on);
+
+/* Scattering-point capacity of a fixed-capacity single-scattering batch
+ * (0: 40 per ray); takes effect at the next jsc_batch_set_fixed(b, 1). */
+int jsc_batch_set_fixed_points(jsc_batch *b, int64_t max_points);
 
 /* Enqueue the result copies (and the device status word) without waiting;
  * jsc_batch_async_status maps the status once the stream has passed them.
@@ -566,6 +578,20 @@ int jsc_batch_scatter_points(jsc_batch *b, int n, const double *x, const double 
  * 10..28, angles as in jsc_batch_set_nalpha); other orders keep the
  * batch's count.  jsc_batch_set_nalpha resets every order to its count. */
 int jsc_batch_set_nalpha_depth(jsc_batch *b, int depth, int nalpha);
+
+/* Device waits.  The multi-block prefix scans that place LOS points and
+ * scattering points (one pass, tiles waiting on their predecessors) poll an
+ * unpublished predecessor at most `polls` times (0: the default, about
+ * 4 M polls of at least 64 ns); a wait that runs out sets the run's status
+ * to JSC_ERR_WATCHDOG and the device stays usable. */
+int jsc_batch_set_wait_budget(jsc_batch *b, unsigned polls);
+
+/* Self-test of the device-wait watchdog on `device`: the prefix scan of n
+ * (1..2^26) counts with a wait budget of `budget` polls (0: default),
+ * checked on the host.  stall >= 0 makes that tile never publish its sum
+ * (a flag nothing sets), so its successor's wait must run out.  Returns
+ * JSC_OK (scan correct), JSC_ERR_WATCHDOG (a wait gave up) or an error. */
+int jsc_scan_selftest(int device, int n, unsigned budget, int stall);
 
 /* Per-(ray, channel) checksum of every emissivity-table index the EGA
  * interpolation selected in the last run, for parity checks against the

@@ -12,6 +12,7 @@
 #include "surrogate.h"
 
 static int sca_alpha(double *alpha, int nalpha);
+static int map_status(unsigned st);
 
 static void batch_free_los(jsc_batch *b) {
   cudaFree(b->d_geo);
@@ -58,6 +59,8 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   cudaFree(b->d_status);
   cudaFree(b->d_counters);
   cudaFree(b->d_digest);
+  cudaFree(b->d_scan);
+  cudaFree(b->d_sp_listed);
   cudaFree(b->d_aero);
   cudaFree(b->d_beta);
   cudaFree(b->d_phase);
@@ -163,6 +166,9 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   st = st ? st : jsc_dmalloc(&b->d_status, 1);
   st = st ? st : jsc_dmalloc(&b->d_counters, 2);
   if (!st) st = batch_alloc_los(b, max_seg > 0 ? max_seg : (int64_t)max_rays * 512);
+  b->scan_tiles = (max_rays + JSC_SCAN_TILE - 1) / JSC_SCAN_TILE + 1;
+  st = st ? st : jsc_dmalloc(&b->d_scan, (size_t)b->scan_tiles + 1);
+  b->wait_budget = JSC_WAIT_BUDGET;
   b->ega_variant = -1;
   for (int v = 0; v < 32; v++) b->ega_variant_ms[v] = -1;
   b->depth = ctl->sca_n > 0 ? ctl->sca_mult : 0;
@@ -423,6 +429,114 @@ extern "C" int jsc_batch_upload(jsc_batch *b, const jsc_batch_input *in,
   return JSC_OK;
 }
 
+// Exclusive prefix sum of n counts into out[0..n] (scan_lookback_kernel),
+// on the batch's scan scratch (n <= max_rays); waits give up after the
+// batch's wait budget with JSC_DEV_ERR_WATCHDOG in its status word.
+static int launch_scan(jsc_batch *b, const int *in, int n, int64_t *out, cudaStream_t s) {
+  if (n <= 0) {
+    JSC_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
+    return JSC_OK;
+  }
+  const int tiles = (n + JSC_SCAN_TILE - 1) / JSC_SCAN_TILE;
+  if (tiles > b->scan_tiles) {
+    jsc_set_error(JSC_ERR_ARG, "scan of %d counts exceeds the batch's %d tiles", n, b->scan_tiles);
+    return JSC_ERR_ARG;
+  }
+  JSC_CUDA_TRY(cudaMemsetAsync(b->d_scan, 0, ((size_t)tiles + 1) * sizeof(unsigned long long), s));
+  ScanArgs a;
+  a.in = in;
+  a.n = n;
+  a.out = out;
+  a.flags = b->d_scan + 1;
+  a.ticket = reinterpret_cast<unsigned *>(b->d_scan);
+  a.status = b->d_status;
+  a.budget = b->wait_budget;
+  a.stall_tile = -1;
+  scan_lookback_kernel<<<tiles, JSC_SCAN_THREADS, 0, s>>>(a);
+  JSC_LAUNCH_CHECK();
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_set_wait_budget(jsc_batch *b, unsigned polls) {
+  if (!b) return JSC_ERR_ARG;
+  b->wait_budget = polls ? polls : JSC_WAIT_BUDGET;
+  return JSC_OK;
+}
+
+extern "C" int jsc_scan_selftest(int device, int n, unsigned budget, int stall) {
+  if (n < 1 || n > (1 << 26)) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_scan_selftest: n = %d outside 1..2^26", n);
+    return JSC_ERR_ARG;
+  }
+  JSC_CUDA_TRY(cudaSetDevice(device));
+  const int tiles = (n + JSC_SCAN_TILE - 1) / JSC_SCAN_TILE;
+  int *d_in = nullptr;
+  int64_t *d_out = nullptr;
+  unsigned long long *d_scan = nullptr;
+  unsigned *d_status = nullptr;
+  int st = jsc_dmalloc(&d_in, (size_t)n);
+  if (!st) st = jsc_dmalloc(&d_out, (size_t)n + 1);
+  if (!st) st = jsc_dmalloc(&d_scan, (size_t)tiles + 1);
+  if (!st) st = jsc_dmalloc(&d_status, 1);
+  int *h_in = (int *)malloc((size_t)n * sizeof(int));
+  int64_t *h_out = (int64_t *)malloc(((size_t)n + 1) * sizeof(int64_t));
+  if (!st && (!h_in || !h_out)) st = JSC_ERR_NOMEM;
+  cudaStream_t s = nullptr;
+  if (!st && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) st = JSC_ERR_CUDA;
+  unsigned status = 0;
+  if (!st) {
+    for (int i = 0; i < n; i++) h_in[i] = (int)((i * 2654435761u) >> 27);  // 0..31
+    cudaError_t e = cudaMemcpyAsync(d_in, h_in, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_scan, 0, ((size_t)tiles + 1) * 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_status, 0, sizeof(unsigned), s);
+    if (e == cudaSuccess) {
+      ScanArgs a;
+      a.in = d_in;
+      a.n = n;
+      a.out = d_out;
+      a.flags = d_scan + 1;
+      a.ticket = reinterpret_cast<unsigned *>(d_scan);
+      a.status = d_status;
+      a.budget = budget ? budget : JSC_WAIT_BUDGET;
+      a.stall_tile = stall;
+      scan_lookback_kernel<<<tiles, JSC_SCAN_THREADS, 0, s>>>(a);
+      jsc_count_launch();
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h_out, d_out, ((size_t)n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&status, d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      jsc_set_error(JSC_ERR_CUDA, "jsc_scan_selftest: %s", cudaGetErrorString(e));
+      st = JSC_ERR_CUDA;
+    }
+  }
+  if (!st) {
+    st = map_status(status);
+    if (!st) {
+      int64_t run = 0;
+      for (int i = 0; i <= n && !st; i++) {
+        if (h_out[i] != run) {
+          jsc_set_error(JSC_ERR_CUDA, "jsc_scan_selftest: prefix %d is %lld, expected %lld", i,
+                        (long long)h_out[i], (long long)run);
+          st = JSC_ERR_CUDA;
+        }
+        if (i < n) run += h_in[i];
+      }
+    }
+  }
+  if (s) cudaStreamDestroy(s);
+  cudaFree(d_in);
+  cudaFree(d_out);
+  cudaFree(d_scan);
+  cudaFree(d_status);
+  free(h_in);
+  free(h_out);
+  return st;
+}
+
 // Launch variants of the EGA + radiative-transfer step.  0-8: ega_rt_kernel,
 // a thread per (ray, channel) with all emitters' path state: (threads per
 // block, minimum resident blocks per SM, emitter loop rolled); the second
@@ -540,7 +654,6 @@ static void launch_raytrace(const jsc_batch *b, const RayArgs &ra, cudaStream_t 
 
 static int batch_run(jsc_batch *b, cudaStream_t s);
 static int run_hydro(jsc_batch *b, cudaStream_t s);
-static int map_status(unsigned st);
 
 // Fixed-capacity runs: rays whose line of sight did not fit (the storing
 // pass flagged them) keep only the points inside the buffer, so that no
@@ -557,13 +670,13 @@ static __global__ void status_or_kernel(unsigned *dst, const unsigned *src) { *d
 
 // A child batch for the secondary (depth - 1) or solar (depth 0) pencils
 // of this batch's scattering points, with room for max_rays rays.
-static int ensure_child(jsc_batch *b, jsc_batch **pc, int max_rays, int depth) {
+static int ensure_child(jsc_batch *b, jsc_batch **pc, int max_rays, int depth, int los_per_ray = 128) {
   jsc_batch *c = *pc;
-  if (c && c->max_rays >= max_rays) return JSC_OK;
+  if (c && c->max_rays >= max_rays && c->max_seg >= (int64_t)max_rays * los_per_ray) return JSC_OK;
   jsc_batch_destroy(c);
   *pc = nullptr;
   int st = jsc_batch_create(b->m, b->ctl, b->max_atm, b->max_levels, max_rays,
-                            (int64_t)max_rays * 128, &c);
+                            (int64_t)max_rays * los_per_ray, &c);
   if (st) return st;
   c->cfg.hydz = -1;  // profiles arrive hydrostatically balanced
   c->depth = depth;
@@ -637,10 +750,13 @@ static int list_scattering_points(jsc_batch *b, cudaStream_t s) {
   sa.sp_off = b->d_sp_off;
   sa.sp = nullptr;
   sa.sp_atm = nullptr;
+  sa.max_sp = 0;
+  sa.nlos_mut = nullptr;
+  sa.status = b->d_status;
+  sa.n_listed = nullptr;
   sp_count_kernel<<<(nr + 127) / 128, 128, 0, s>>>(sa);
   JSC_LAUNCH_CHECK();
-  scan_kernel<<<1, 1024, 0, s>>>(b->d_nsp, nr, b->d_sp_off);
-  JSC_LAUNCH_CHECK();
+  if ((st = launch_scan(b, b->d_nsp, nr, b->d_sp_off, s))) return st;
   JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, b->d_sp_off + nr, sizeof(int64_t),
                                cudaMemcpyDeviceToHost, s));
   JSC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -674,11 +790,13 @@ static int64_t scatter_chunk(int nd) {
 // the refracted sun direction by repeated ray tracing, the solar pencils as
 // a child batch, and the phase-function weighted solar source added to src.
 static int sun_sources(jsc_batch *b, const double *sp, const int *sp_atm, int n, double *src,
-                       cudaStream_t s) {
+                       cudaStream_t s, const int64_t *n_total = nullptr, int64_t first = 0) {
   jsc_batch *sc = b->sun_child;
   SunArgs sn;
   fill_ray_args(b, sn.ra);
   sn.n_pts = n;
+  sn.n_total = n_total;
+  sn.first = first;
   sn.sp = sp;
   sn.sp_atm = sp_atm;
   sn.n_alti = b->n_alti;
@@ -788,6 +906,8 @@ static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int6
     SpawnArgs pa;
     pa.n_pts = n;
     pa.nalpha = na;
+    pa.n_total = nullptr;
+    pa.first = c0;
     pa.sp = sp + c0 * JSC_SP_REC;
     pa.sp_atm = sp_atm + c0;
     memcpy(pa.alpha, b->alpha, sizeof(pa.alpha));
@@ -803,6 +923,8 @@ static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int6
     IntegralArgs ia;
     ia.n_pts = n;
     ia.nalpha = na;
+    ia.n_total = nullptr;
+    ia.first = c0;
     ia.nd = nd;
     ia.nl = b->aero_nl;
     ia.sp = pa.sp;
@@ -814,6 +936,151 @@ static int plain_sources(jsc_batch *b, const double *sp, const int *sp_atm, int6
     JSC_LAUNCH_CHECK();
     if ((st = sun_sources(b, pa.sp, pa.sp_atm, n, src + c0 * nd, s))) return st;
   }
+  return JSC_OK;
+}
+
+// Scattering sources of a fixed-capacity run (single scattering, IP 1),
+// without a host read-back: the point list is counted and placed on the
+// device (with its total in d_sp_off[n_rays]), then fx_rounds rounds of
+// fx_chunk points each spawn their secondary pencils into the child batch
+// (null pencils past the device count), run it, integrate the sources and
+// add the solar term.  The launch sequence is the same for every input, so
+// the run can be captured into a CUDA graph.  Points beyond the capacity
+// fx_max_sp empty their ray's LOS and set JSC_DEV_ERR_QUEUE.
+static int fixed_sources(jsc_batch *b, cudaStream_t s) {
+  const int nr = b->n_rays, nd = b->cfg.nd, na = b->nalpha;
+  int st;
+  SpArgs sa;
+  sa.n_rays = nr;
+  sa.W = b->W;
+  sa.nlos = b->d_nlos;
+  sa.los_off = b->d_los_off;
+  sa.geo = b->d_geo;
+  sa.pts = b->d_pts;
+  sa.time = b->d_ray;
+  sa.ray_atm = b->d_ray_atm;
+  sa.nsp = b->d_nsp;
+  sa.sp_off = b->d_sp_off;
+  sa.sp = b->d_sp;
+  sa.sp_atm = b->d_sp_atm;
+  sa.max_sp = b->fx_max_sp;
+  sa.nlos_mut = b->d_nlos;
+  sa.status = b->d_status;
+  sa.n_listed = b->d_sp_listed;
+  sp_count_kernel<<<(nr + 127) / 128, 128, 0, s>>>(sa);
+  JSC_LAUNCH_CHECK();
+  if ((st = launch_scan(b, b->d_nsp, nr, b->d_sp_off, s))) return st;
+  sp_listed_init_kernel<<<1, 1, 0, s>>>(b->d_sp_off + nr, b->fx_max_sp, b->d_sp_listed);
+  JSC_LAUNCH_CHECK();
+  sp_list_kernel<<<(nr + 127) / 128, 128, 0, s>>>(sa);
+  JSC_LAUNCH_CHECK();
+  if ((st = copy_profiles(b, b->child, s))) return st;
+  if ((st = copy_profiles(b, b->sun_child, s))) return st;
+  const int64_t *n_total = reinterpret_cast<const int64_t *>(b->d_sp_listed);
+  const int chunk = (int)b->fx_chunk;
+  jsc_batch *c = b->child;
+  const size_t shmem = ((size_t)JSC_NTH_SCA * nd + (size_t)na * (nd | 1) + 4 * JSC_NTH_SCA +
+                        (JSC_INT_THREADS / 32) * JSC_INT_CH + (size_t)na * (JSC_INT_CH + 1) +
+                        (size_t)na) *
+                       sizeof(double);
+  for (int r = 0; r < b->fx_rounds; r++) {
+    const int64_t c0 = (int64_t)r * chunk;
+    SpawnArgs pa;
+    pa.n_pts = chunk;
+    pa.nalpha = na;
+    pa.n_total = n_total;
+    pa.first = c0;
+    pa.sp = b->d_sp + c0 * JSC_SP_REC;
+    pa.sp_atm = b->d_sp_atm + c0;
+    memcpy(pa.alpha, b->alpha, sizeof(pa.alpha));
+    pa.ray_atm = c->d_ray_atm;
+    pa.ray = c->d_ray;
+    c->n_rays = chunk * na;
+    sp_spawn_kernel<<<(chunk * na + 127) / 128, 128, 0, s>>>(pa);
+    JSC_LAUNCH_CHECK();
+    if ((st = batch_run(c, s))) return st;
+    status_or_kernel<<<1, 1, 0, s>>>(b->d_status, c->d_status);
+    JSC_LAUNCH_CHECK();
+    IntegralArgs ia;
+    ia.n_pts = chunk;
+    ia.nalpha = na;
+    ia.n_total = n_total;
+    ia.first = c0;
+    ia.nd = nd;
+    ia.nl = b->aero_nl;
+    ia.sp = pa.sp;
+    memcpy(ia.alpha, b->alpha, sizeof(ia.alpha));
+    ia.rad = c->d_rad;
+    ia.phase = b->d_phase;
+    ia.src = b->d_src + c0 * nd;
+    sp_integral_kernel<<<chunk, JSC_INT_THREADS, shmem, s>>>(ia);
+    JSC_LAUNCH_CHECK();
+    if ((st = sun_sources(b, pa.sp, pa.sp_atm, chunk, b->d_src + c0 * nd, s, n_total, c0)))
+      return st;
+  }
+  return JSC_OK;
+}
+
+// Everything a fixed-capacity single-scattering run uses, allocated before
+// the first run (a captured run cannot allocate): the point list of
+// fx_max_sp points, the child batches of one round (fx_chunk points: their
+// secondary and solar pencils, themselves fixed-capacity), the solar data.
+static int prepare_fixed_scattering(jsc_batch *b) {
+  if (b->depth != 1 || b->ip != 1 || b->sur_on) {
+    jsc_set_error(JSC_ERR_UNSUPPORTED, "fixed-capacity scattering runs cover single scattering "
+                                       "(SCA_MULT=1) in 1-D atmospheres without a surrogate");
+    return JSC_ERR_UNSUPPORTED;
+  }
+  if (!b->h_aero || !b->d_aero) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_set_fixed with scattering: call jsc_batch_set_aero first");
+    return JSC_ERR_ARG;
+  }
+  const int nd = b->cfg.nd, na = b->nalpha;
+  int st;
+  int64_t chunk = scatter_chunk(nd);
+  const int64_t want = b->fx_points_req > 0 ? b->fx_points_req
+                                            : (int64_t)b->max_rays * JSC_FIXED_POINTS_PER_RAY;
+  if (chunk > want) chunk = want;
+  b->fx_chunk = chunk;
+  b->fx_rounds = (int)((want + chunk - 1) / chunk);
+  b->fx_max_sp = (int64_t)b->fx_rounds * chunk;
+  if (!b->d_nsp) {
+    if ((st = jsc_dmalloc(&b->d_nsp, (size_t)b->max_rays))) return st;
+    if ((st = jsc_dmalloc(&b->d_sp_off, (size_t)b->max_rays + 1))) return st;
+  }
+  if ((st = reserve_points(b, b->fx_max_sp))) return st;
+  if (!b->d_sp_listed && (st = jsc_dmalloc(&b->d_sp_listed, 1))) return st;
+  if ((st = ensure_child(b, &b->child, (int)(chunk * na), 0, JSC_FIXED_PENCIL_LOS))) return st;
+  if ((st = ensure_child(b, &b->sun_child, (int)chunk, 0, JSC_FIXED_SUN_LOS))) return st;
+  if ((st = jsc_batch_set_fixed(b->child, 1))) return st;
+  if ((st = jsc_batch_set_fixed(b->sun_child, 1))) return st;
+  if (!b->d_planck_sun) {
+    double h[NDMAX];
+    for (int id = 0; id < nd; id++) h[id] = planck(JSC_TSUN, b->m->nu[id]);
+    if ((st = jsc_dmalloc(&b->d_planck_sun, (size_t)nd))) return st;
+    JSC_CUDA_TRY(cudaMemcpy(b->d_planck_sun, h, (size_t)nd * sizeof(double),
+                            cudaMemcpyHostToDevice));
+  }
+  if (b->n_theta2 < b->sun_child->max_rays) {
+    cudaFree(b->d_theta2);
+    b->d_theta2 = nullptr;
+    b->n_theta2 = 0;
+    if ((st = jsc_dmalloc(&b->d_theta2, (size_t)b->sun_child->max_rays))) return st;
+    b->n_theta2 = b->sun_child->max_rays;
+  }
+  const size_t shmem = ((size_t)JSC_NTH_SCA * nd + (size_t)na * (nd | 1) + 4 * JSC_NTH_SCA +
+                        (JSC_INT_THREADS / 32) * JSC_INT_CH + (size_t)na * (JSC_INT_CH + 1) +
+                        (size_t)na) *
+                       sizeof(double);
+  if (shmem > 48 * 1024)
+    JSC_CUDA_TRY(cudaFuncSetAttribute(sp_integral_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem));
+  return JSC_OK;
+}
+
+extern "C" int jsc_batch_set_fixed_points(jsc_batch *b, int64_t max_points) {
+  if (!b || max_points < 0) return JSC_ERR_ARG;
+  b->fx_points_req = max_points;
   return JSC_OK;
 }
 
@@ -898,7 +1165,10 @@ static __global__ void sur_merge_kernel(int m, int nd, const int *idx, const int
 // envelope and the plain path for the rest and for a sample of the inside
 // points, which checks the surrogate; if a checked point deviates by more
 // than the tolerance the whole batch takes the plain path.
+static int fixed_sources(jsc_batch *b, cudaStream_t s);
+
 static int scatter_sources(jsc_batch *b, cudaStream_t s) {
+  if (b->fixed) return fixed_sources(b, s);
   int st = list_scattering_points(b, s);
   if (st || b->n_sp == 0) return st;
   const int nd = b->cfg.nd;
@@ -1123,8 +1393,10 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   }
   launch_raytrace<false>(b, ra, s);
   JSC_LAUNCH_CHECK();
-  scan_kernel<<<1, 1024, 0, s>>>(ra.nlos, nr, (int64_t *)ra.los_off);
-  JSC_LAUNCH_CHECK();
+  {
+    const int st = launch_scan(b, ra.nlos, nr, (int64_t *)ra.los_off, s);
+    if (st) return st;
+  }
   // The LOS buffer is sized from the counting pass (one small copy).
   if (b->fixed) {
     // Fixed capacity (graph capture): no read-back, the buffers hold
@@ -1135,10 +1407,11 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
                                  cudaMemcpyDeviceToHost, s));
     JSC_CUDA_TRY(cudaStreamSynchronize(s));
   }
-  if (b->fixed && (b->depth > 0 || (refine && b->max_seg_b < b->max_seg))) {
+  if (b->fixed && (b->depth > 1 || (b->depth == 1 && b->fx_rounds < 1) ||
+                   (refine && b->max_seg_b < b->max_seg))) {
     jsc_set_error(JSC_ERR_UNSUPPORTED,
-                  "fixed-capacity runs cover clear air and aerosol extinction; the base LOS "
-                  "buffer is sized by jsc_batch_set_fixed");
+                  "fixed-capacity runs cover clear air, aerosol extinction and single "
+                  "scattering prepared by jsc_batch_set_fixed");
     return JSC_ERR_UNSUPPORTED;
   }
   if (refine) {
@@ -1209,8 +1482,10 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     fa.max_seg = b->max_seg;
     refine_count_kernel<<<(nr + 127) / 128, 128, 0, s>>>(fa);
     JSC_LAUNCH_CHECK();
-    scan_kernel<<<1, 1024, 0, s>>>(b->d_nlos, nr, b->d_los_off);
-    JSC_LAUNCH_CHECK();
+    {
+      const int st = launch_scan(b, b->d_nlos, nr, b->d_los_off, s);
+      if (st) return st;
+    }
     if (b->fixed) {
       *b->h_total = 0;
     } else {
@@ -1279,8 +1554,8 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   ea.digest = b->digest ? b->d_digest : nullptr;
   ea.beta = b->d_beta;
   ea.aero_nl = b->aero_nl;
-  ea.src_sca = (scattering && b->n_sp > 0) ? b->d_src : nullptr;
-  ea.sp_off = (scattering && b->n_sp > 0) ? b->d_sp_off : nullptr;
+  ea.src_sca = (scattering && (b->n_sp > 0 || b->fixed)) ? b->d_src : nullptr;
+  ea.sp_off = (scattering && (b->n_sp > 0 || b->fixed)) ? b->d_sp_off : nullptr;
   ea.beta_ctm = b->d_ctm;
   ea.src_pl = b->d_srcp;
   const int variant = run_variant(b);
@@ -1294,6 +1569,7 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     ca.pts = b->d_pts;
     ca.beta = b->d_ctm;
     ca.src = b->d_srcp;
+    ca.n_live = b->fixed ? b->d_los_off + nr : nullptr;
     ev_record(b, JSC_T_CTM, 0, s);
     jsc_ctm_src_launch(ca, s);
     JSC_LAUNCH_CHECK();
@@ -1534,11 +1810,8 @@ extern "C" int jsc_batch_set_fixed(jsc_batch *b, int on) {
   if (!b) return JSC_ERR_ARG;
   JSC_CUDA_TRY(cudaSetDevice(b->m->device));
   if (on) {
-    if (b->depth > 0) {
-      jsc_set_error(JSC_ERR_UNSUPPORTED, "fixed-capacity runs cover depth 0 (no scattering source)");
-      return JSC_ERR_UNSUPPORTED;
-    }
     int st;
+    if (b->depth > 0 && (st = prepare_fixed_scattering(b))) return st;
     if (b->cfg.sca_n > 0 && b->max_seg_b < b->max_seg &&
         (st = batch_alloc_los_b(b, b->max_seg)))
       return st;

@@ -27,21 +27,24 @@ struct CtmArgs {
   int W;
   const double *pts;
   double *beta, *src;  // [n_points][nd]
+  const int64_t *n_live;  // LOS points on the device (fixed-capacity runs), or null
 };
 
 static __global__ void __launch_bounds__(256) ctm_src_kernel(CtmArgs A) {
   const int nd = A.m.nd;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= A.n_points * nd) return;
-  const int64_t pt = t / nd;
-  const int d = (int)(t - pt * nd);
-  const double *rec = A.pts + pt * A.W;
-  const double P = rec[REC_P], T = rec[REC_T], DS = rec[REC_DS];
-  const int w = A.m.window[d];
-  A.beta[t] = continua(A.m, A.cfg, A.m.ctm[d], A.m.nu[d], w < A.m.nw ? rec[REC_K + w] : 0.0, P,
-                       T, DS, rec[REC_QH2O], rec + REC_K + A.m.nw);
-  const int itp = (int)rec[REC_PLK];
-  A.src[t] = planck_src(A.m, d, itp, T);
+  const int64_t total = (A.n_live ? *A.n_live : A.n_points) * nd;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pt = t / nd;
+    const int d = (int)(t - pt * nd);
+    const double *rec = A.pts + pt * A.W;
+    const double P = rec[REC_P], T = rec[REC_T], DS = rec[REC_DS];
+    const int w = A.m.window[d];
+    A.beta[t] = continua(A.m, A.cfg, A.m.ctm[d], A.m.nu[d], w < A.m.nw ? rec[REC_K + w] : 0.0, P,
+                         T, DS, rec[REC_QH2O], rec + REC_K + A.m.nw);
+    const int itp = (int)rec[REC_PLK];
+    A.src[t] = planck_src(A.m, d, itp, T);
+  }
 }
 
 template <int GP, bool DIG, int BLK, int MINB>

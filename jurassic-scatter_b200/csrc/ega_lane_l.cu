@@ -10,5 +10,9 @@ void jsc_ega_lane_launch_l(const EgaArgs &ea, int v, bool dig, cudaStream_t s) {
 
 void jsc_ctm_src_launch(const CtmArgs &ca, cudaStream_t s) {
   const int64_t n = ca.n_points * ca.m.nd;
-  if (n > 0) ctm_src_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ca);
+  if (n <= 0) return;
+  int64_t blocks = (n + 255) / 256;
+  // a count known only on the device: a grid of a few blocks per SM walks it
+  if (ca.n_live && blocks > 148 * 16) blocks = 148 * 16;
+  ctm_src_kernel<<<(unsigned)blocks, 256, 0, s>>>(ca);
 }

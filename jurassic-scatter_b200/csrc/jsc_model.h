@@ -68,6 +68,10 @@ enum { JSC_T_HYDRO = 0, JSC_T_RAYTRACE, JSC_T_EGA, JSC_T_SCATTER, JSC_T_CTM, JSC
 
 #define JSC_NALPHA_REF 28  // secondary pencils per scattering point (src/scatter.c:673)
 #define JSC_MAX_DEPTH 7    // deepest scattering order with its own pencil count
+#define JSC_WAIT_BUDGET (1u << 22)  // default polls of a device wait (each >= 64 ns)
+#define JSC_FIXED_POINTS_PER_RAY 40  // default scattering-point capacity per primary ray
+#define JSC_FIXED_PENCIL_LOS 144     // LOS capacity per secondary pencil (fixed runs)
+#define JSC_FIXED_SUN_LOS 256        // LOS capacity per solar pencil (fixed runs)
 
 struct jsc_batch {
   jsc_model *m;
@@ -136,8 +140,14 @@ struct jsc_batch {
   int sur_used;
 
   // Fixed-capacity mode (no host read-backs; graph capture) and the
-  // captured upload + run + download graph.
+  // captured upload + run + download graph.  With scattering (depth 1):
+  // the scattering-point capacity and the points per round of secondary
+  // pencils (fx_max_sp = fx_rounds * fx_chunk).
   int fixed;
+  int64_t fx_points_req;    // requested point capacity (0: max_rays * JSC_FIXED_POINTS_PER_RAY)
+  int64_t fx_max_sp, fx_chunk;
+  int fx_rounds;
+  unsigned long long *d_sp_listed;  // points listed by the last fixed-capacity run
   unsigned *h_status;       // pinned: status word of the last asynchronous download
   cudaGraphExec_t gexec;
   jsc_batch_input gin;      // host inputs the graph copies from
@@ -158,6 +168,12 @@ struct jsc_batch {
   unsigned *d_status;
   unsigned long long *d_counters;  // [0] LOS points, [1] EGA evaluations
   int64_t *h_total;         // pinned: LOS points of the current batch
+
+  // Multi-block prefix scans: ticket (word 0) and one flag word per tile,
+  // and the polls a device wait may spend before it gives up.
+  unsigned long long *d_scan;
+  int scan_tiles;
+  unsigned wait_budget;
 
   unsigned long long *d_digest;  // [max_rays][nd] when index digests are on
   int digest;

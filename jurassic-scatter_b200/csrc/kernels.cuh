@@ -823,6 +823,119 @@ static __global__ void __launch_bounds__(128) refine_count_kernel(RefineArgs A) 
   A.nlos[r] = o;
 }
 
+// Exclusive prefix sum of n counts into off[0..n] in one pass over many
+// blocks (decoupled look-back, Merrill and Garland 2016).  Tiles of
+// JSC_SCAN_TILE counts are claimed in order through a ticket counter; a
+// tile publishes its own sum, walks back over the tiles before it adding
+// published values until it meets a published inclusive prefix, then
+// publishes its inclusive prefix.  Tiles are claimed only by running
+// blocks, so a tile waits only on tiles that resident blocks are working
+// on.  Every wait is bounded: after `budget` polls of an unpublished tile
+// the waiting tile flags JSC_DEV_ERR_WATCHDOG in the status word, publishes
+// a prefix anyway (no later tile waits on it for ever) and returns its
+// outputs invalid.  flags[] (one word per tile: value << 2 | state, state 1
+// sum, 2 inclusive prefix) and the ticket must be zero at launch.
+// stall_tile >= 0 names a tile that never publishes: the diagnostic of the
+// watchdog path (its successor's wait runs out).
+#define JSC_SCAN_THREADS 256
+#define JSC_SCAN_PER 8
+#define JSC_SCAN_TILE (JSC_SCAN_THREADS * JSC_SCAN_PER)
+
+struct ScanArgs {
+  const int *in;               // [n] counts
+  int n;
+  int64_t *out;                // [n + 1]
+  unsigned long long *flags;   // [tiles]
+  unsigned *ticket;
+  unsigned *status;
+  unsigned budget;             // polls of an unpublished tile before giving up
+  int stall_tile;
+};
+
+__device__ __forceinline__ void scan_publish(unsigned long long *f, int64_t v, unsigned st) {
+  atomicExch(f, ((unsigned long long)v << 2) | st);
+}
+
+static __global__ void __launch_bounds__(JSC_SCAN_THREADS) scan_lookback_kernel(ScanArgs A) {
+  __shared__ int tile_s;
+  __shared__ int64_t wsum[JSC_SCAN_THREADS / 32];
+  __shared__ int64_t prefix_s;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  constexpr int NW = JSC_SCAN_THREADS / 32;
+  if (tid == 0) tile_s = (int)atomicAdd(A.ticket, 1u);
+  __syncthreads();
+  const int tile = tile_s;
+  const int64_t base = (int64_t)tile * JSC_SCAN_TILE + (int64_t)tid * JSC_SCAN_PER;
+  int v[JSC_SCAN_PER];
+  int64_t s = 0;
+#pragma unroll
+  for (int q = 0; q < JSC_SCAN_PER; q++) {
+    const int64_t i = base + q;
+    v[q] = i < A.n ? A.in[i] : 0;
+    s += v[q];
+  }
+  int64_t x = s;  // inclusive scan within the warp
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int64_t t = lane < NW ? wsum[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < NW; d <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, t, d);
+      if (lane >= d) t += y;
+    }
+    if (lane < NW) wsum[lane] = t;
+  }
+  __syncthreads();
+  const int64_t excl = x - s + (w > 0 ? wsum[w - 1] : 0);
+  const int64_t agg = wsum[NW - 1];
+  if (tid == 0) {
+    int64_t prefix = 0;
+    if (tile == A.stall_tile) {
+      // never publishes (diagnostic)
+    } else if (tile == 0) {
+      scan_publish(&A.flags[0], agg, 2);
+    } else {
+      scan_publish(&A.flags[tile], agg, 1);
+      unsigned polls = 0;
+      bool gave_up = false;
+      for (int j = tile - 1; j >= 0;) {
+        const unsigned long long f = atomicAdd(&A.flags[j], 0ull);
+        const unsigned st = (unsigned)(f & 3ull);
+        if (st == 0) {
+          if (++polls > A.budget) {
+            gave_up = true;
+            break;
+          }
+          __nanosleep(64);
+          continue;
+        }
+        prefix += (int64_t)(f >> 2);
+        if (st == 2) break;
+        j--;
+      }
+      if (gave_up) atomicOr(A.status, JSC_DEV_ERR_WATCHDOG);
+      scan_publish(&A.flags[tile], prefix + agg, 2);
+    }
+    prefix_s = prefix;
+  }
+  __syncthreads();
+  int64_t run = prefix_s + excl;
+#pragma unroll
+  for (int q = 0; q < JSC_SCAN_PER; q++) {
+    const int64_t i = base + q;
+    if (i < A.n) A.out[i] = run;
+    run += v[q];
+  }
+  const int tiles = (A.n + JSC_SCAN_TILE - 1) / JSC_SCAN_TILE;
+  if (tile == tiles - 1 && tid == JSC_SCAN_THREADS - 1) A.out[A.n] = prefix_s + agg;
+}
+
 // Exclusive scan of nlos into off[0..n] by one block.
 static __global__ void scan_kernel(const int *nlos, int n, int64_t *off) {
   __shared__ int64_t part[1024];

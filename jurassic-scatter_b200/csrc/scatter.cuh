@@ -76,6 +76,20 @@ __device__ __forceinline__ void local_frame(const double *x, double *lx, double 
 
 // --------------------------------------------------------- point list --
 
+// Points of a chunk [first, first + n_pts) of a point list whose total
+// count is on the device (n_total; null: all n_pts are real).  Fixed-
+// capacity scattering runs launch every chunk up to the list's capacity;
+// slots past the real count become null pencils (observer and view point
+// far above the atmosphere: no LOS point, no work) and their sources are
+// never read.
+__device__ __forceinline__ int live_points(const int64_t *n_total, int64_t first, int n_pts) {
+  if (!n_total) return n_pts;
+  const int64_t left = *n_total - first;
+  return left <= 0 ? 0 : (left < n_pts ? (int)left : n_pts);
+}
+
+#define JSC_NULL_Z 1.0e4  // altitude of a null pencil's observer and view point [km]
+
 struct SpArgs {
   int n_rays, W;
   const int *nlos;
@@ -87,7 +101,19 @@ struct SpArgs {
   const int64_t *sp_off;    // [n_rays+1]
   double *sp;               // [n_sp][JSC_SP_REC]
   int *sp_atm;              // [n_sp] profile of the point
+  int64_t max_sp;           // capacity of sp (fixed-capacity runs; 0: unbounded)
+  int *nlos_mut;            // rays whose points do not fit: their LOS is emptied
+  unsigned *status;
+  unsigned long long *n_listed;  // points actually listed (fixed-capacity runs)
 };
+
+// Points a fixed-capacity run lists: all of them, or up to the first ray
+// whose points do not fit (sp_list_kernel lowers it with atomicMin).
+static __global__ void sp_listed_init_kernel(const int64_t *sp_total, int64_t max_sp,
+                                             unsigned long long *n_listed) {
+  const int64_t t = *sp_total;
+  *n_listed = (unsigned long long)(t < max_sp ? t : max_sp);
+}
 
 static __global__ void sp_count_kernel(SpArgs A) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -107,6 +133,14 @@ static __global__ void sp_list_kernel(SpArgs A) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= A.n_rays) return;
   const int np = A.nlos[r];
+  if (A.max_sp > 0 && A.sp_off[r + 1] > A.max_sp) {
+    // more scattering points than the fixed capacity: the run reports the
+    // overflow and this ray keeps no LOS point, so nothing reads past sp
+    atomicOr(A.status, JSC_DEV_ERR_QUEUE);
+    atomicMin(A.n_listed, (unsigned long long)A.sp_off[r]);
+    A.nlos_mut[r] = 0;
+    return;
+  }
   const double *rec = A.pts + A.los_off[r] * A.W;
   const double *geo = A.geo + A.los_off[r] * 4;
   int64_t k = A.sp_off[r];
@@ -136,6 +170,8 @@ static __global__ void sp_list_kernel(SpArgs A) {
 
 struct SpawnArgs {
   int n_pts, nalpha;        // points of this chunk, pencils per point
+  const int64_t *n_total;   // device count of the whole list (null: all real)
+  int64_t first;            // index of the chunk's first point in the list
   const double *sp;         // first record of the chunk
   const int *sp_atm;
   double alpha[JSC_NALPHA_MAX];
@@ -150,6 +186,11 @@ static __global__ void sp_spawn_kernel(SpawnArgs A) {
   const int n = A.n_pts * A.nalpha;
   if (t >= n) return;
   const int k = t / A.nalpha, ir = t - k * A.nalpha;
+  if (k >= live_points(A.n_total, A.first, A.n_pts)) {  // null pencil
+    A.ray_atm[t] = 0;
+    for (int i = 0; i < 7; i++) A.ray[(size_t)i * n + t] = (i == 1 || i == 4) ? JSC_NULL_Z : 0.0;
+    return;
+  }
   const double *o = A.sp + (size_t)k * JSC_SP_REC;
   const double x[3] = {o[SP_X], o[SP_X + 1], o[SP_X + 2]};
   double lx[3], ly[3], lz[3], xv[3];
@@ -173,6 +214,8 @@ static __global__ void sp_spawn_kernel(SpawnArgs A) {
 
 struct IntegralArgs {
   int n_pts, nalpha, nd, nl;
+  const int64_t *n_total;   // device count of the whole list (null: all real)
+  int64_t first;
   const double *sp;          // first record of the chunk
   double alpha[JSC_NALPHA_MAX];
   const double *rad;         // [n_pts * nalpha][nd] secondary radiances
@@ -194,7 +237,7 @@ static __global__ void __launch_bounds__(JSC_INT_THREADS)
 sp_integral_kernel(IntegralArgs A) {
   extern __shared__ double sh[];
   const int k = blockIdx.x;
-  if (k >= A.n_pts) return;
+  if (k >= live_points(A.n_total, A.first, A.n_pts)) return;
   const int nd = A.nd, na = A.nalpha;
   const int ndp = nd | 1, SL = JSC_INT_CH + 1;      // odd row strides
   double *wt = sh;                                   // [JSC_NTH_SCA][nd]
@@ -304,6 +347,8 @@ sp_integral_kernel(IntegralArgs A) {
 struct SunArgs {
   RayArgs ra;                // profiles, tracing switches, status word
   int n_pts;
+  const int64_t *n_total;    // device count of the whole list (null: all real)
+  int64_t first;
   const double *sp;          // first record of the chunk
   const int *sp_atm;
   // aerosol refinement edges (the last segment of each solar ray)
@@ -367,6 +412,13 @@ template <int IP = 1>
 __global__ void __launch_bounds__(128) sun_kernel(SunArgs A) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= A.n_pts) return;
+  if (k >= live_points(A.n_total, A.first, A.n_pts)) {  // null solar pencil, no term
+    const int n = A.n_pts;
+    A.ray_atm[k] = 0;
+    for (int i = 0; i < 7; i++) A.ray[(size_t)i * n + k] = (i == 1 || i == 4) ? JSC_NULL_Z : 0.0;
+    A.theta2[k] = -1.0;
+    return;
+  }
   const double *o = A.sp + (size_t)k * JSC_SP_REC;
   const double x[3] = {o[SP_X], o[SP_X + 1], o[SP_X + 2]};
   const double dx[3] = {o[SP_DX], o[SP_DX + 1], o[SP_DX + 2]};

@@ -394,7 +394,8 @@ class GraphBatch:
     _KEYS = ("z", "lon", "lat", "p", "t", "q", "k", "time", "obsz", "obslon", "obslat",
              "vpz", "vplon", "vplat")
 
-    def __init__(self, model, ctl, inp, stream, pin, max_seg=0, aero=None, variant=-1):
+    def __init__(self, model, ctl, inp, stream, pin, max_seg=0, aero=None, variant=-1,
+                 nalpha=None, fixed_points=None):
         lib = L.load()
         self.nd = ctl.nd
         self.stream = stream
@@ -404,6 +405,11 @@ class GraphBatch:
             self.batch.set_aero(aero)
         if variant >= 0:
             self.batch.set_variant(variant)
+        if nalpha is not None:
+            self.batch.set_nalpha(nalpha)
+        if fixed_points is not None:
+            L.check(lib.jsc_batch_set_fixed_points(self.batch.h, int(fixed_points)),
+                    "jsc_batch_set_fixed_points")
         L.check(lib.jsc_batch_set_fixed(self.batch.h, 1), "jsc_batch_set_fixed")
         self.host = {k: pin(np.ascontiguousarray(inp[k], dtype=np.float64)) for k in self._KEYS}
         self.host["atm_off"] = pin(np.ascontiguousarray(inp["atm_off"], dtype=np.int32))
@@ -545,6 +551,11 @@ class Surrogate:
             self.close()
         except Exception:
             pass
+
+
+def scan_selftest(device=0, n=100_000, budget=0, stall=-1):
+    """Status of the device-wait watchdog self-test (jsc_scan_selftest)."""
+    return L.load().jsc_scan_selftest(int(device), int(n), int(budget), int(stall))
 
 
 def launch_count():

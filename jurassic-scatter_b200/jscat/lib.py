@@ -30,7 +30,8 @@ EXPORTS = [
     "formod_pencil", "formod_fov", "read_shape", "read_tbl", "srcfunc_planck",
     "formod_continua", "intpol_tbl", "intpol_tbl_eps", "intpol_tbl_u", "locate_tbl",
     "jsc_srcfunc_sca", "jsc_batch_scatter_points", "jsc_surrogate_get_scaling",
-    "jsc_batch_set_nalpha_depth",
+    "jsc_batch_set_nalpha_depth", "jsc_batch_set_wait_budget", "jsc_scan_selftest",
+    "jsc_batch_set_fixed_points",
 ]
 
 
@@ -150,6 +151,9 @@ def load():
         "jsc_surrogate_get_scaling": (i, [vp, P(C.c_float), P(C.c_float), P(C.c_float),
                                           P(C.c_float)]),
         "jsc_batch_set_nalpha_depth": (i, [vp, i, i]),
+        "jsc_batch_set_wait_budget": (i, [vp, C.c_uint]),
+        "jsc_scan_selftest": (i, [i, i, C.c_uint, i]),
+        "jsc_batch_set_fixed_points": (i, [vp, C.c_int64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
