@@ -687,7 +687,20 @@ def mixed_bench(args, local, torch, sur=None, sur2=None, variant=-1, depth2=True
                                      "p99": float(np.percentile(lat, 99))},
                       "gpu_launches": int(launches)}
 
+    t0 = time.perf_counter()
     execute(True)                      # warm-up (allocations of the scattering path)
+    warm_s = time.perf_counter() - t0
+    if warm_s > 120:
+        for rr in runners.values():
+            for gr in rr:
+                gr.close()
+        for bb in sbatch.values():
+            bb.close()
+        for m in models:
+            m.close()
+        return {"workload": MIX_WORKLOAD, "requests": args.requests,
+                "error": "warm-up pass took %.0f s (a surrogate check sent batches to the plain "
+                         "path); timed passes skipped" % warm_s}
     outs, over = execute(True)
     _, serial = execute(False)
     # accuracy: scattering batches against their plain path, graph batches
@@ -1166,8 +1179,13 @@ def main():
         try:
             # clear-air graph batches replay the launch variant the headline's
             # autotuner chose on the same emitters and channel grid
-            ms = line.get("multiple_scattering", {})
-            ok2 = bool(ms.get("surrogate", {}).get("used"))
+            # depth-2 requests only with a depth-2 surrogate that passed its
+            # held-out check with margin: a rejected batch runs the plain
+            # path (about 20 ms per ray)
+            msur = line.get("multiple_scattering", {}).get("surrogate", {})
+            ok2 = bool(msur.get("used")) and \
+                msur.get("max_albedo_weighted_src_err_checked", 1.0) < 0.5 * msur.get(
+                    "check_tolerance", 0.0)
             line["mixed_requests"] = mixed_bench(args, local, torch, sur, sur2 if ok2 else None,
                                                  variant=tuned.get("variant", -1), depth2=ok2)
         except Exception as exc:

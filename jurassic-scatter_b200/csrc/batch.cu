@@ -61,6 +61,8 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   cudaFree(b->d_digest);
   cudaFree(b->d_scan);
   cudaFree(b->d_sp_listed);
+  cudaFree(b->d_live);
+  cudaFree(b->d_qhead);
   cudaFree(b->d_aero);
   cudaFree(b->d_beta);
   cudaFree(b->d_phase);
@@ -643,13 +645,36 @@ static void fill_ray_args(const jsc_batch *b, RayArgs &ra) {
   ra.cx = b->cx;
 }
 
-// Counting or storing ray-tracing pass with the batch's interpolation.
+// Counting or storing ray-tracing pass with the batch's interpolation; the
+// pencil batches of a fixed-capacity round pull their rays from the device
+// queue with a persistent grid (7 blocks of 128 per SM, the kernel's cap).
 template <bool STORE>
-static void launch_raytrace(const jsc_batch *b, const RayArgs &ra, cudaStream_t s) {
+static int launch_raytrace(const jsc_batch *b, const RayArgs &ra, cudaStream_t s) {
+  if (b->d_live) {
+    JSC_CUDA_TRY(cudaMemsetAsync(b->d_qhead, 0, sizeof(unsigned), s));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->m->device);
+    const unsigned g = (unsigned)(sms * 7);
+    if (b->ip == 2) raytrace_queue_kernel<STORE, 2><<<g, 128, 0, s>>>(ra, b->d_qhead, b->d_live);
+    else if (b->ip == 3) raytrace_queue_kernel<STORE, 3><<<g, 128, 0, s>>>(ra, b->d_qhead, b->d_live);
+    else raytrace_queue_kernel<STORE><<<g, 128, 0, s>>>(ra, b->d_qhead, b->d_live);
+    return JSC_OK;
+  }
   const unsigned g = (unsigned)((ra.n_rays + 127) / 128);
   if (b->ip == 2) raytrace_kernel<STORE, 2><<<g, 128, 0, s>>>(ra);
   else if (b->ip == 3) raytrace_kernel<STORE, 3><<<g, 128, 0, s>>>(ra);
   else raytrace_kernel<STORE><<<g, 128, 0, s>>>(ra);
+  return JSC_OK;
+}
+
+// Live rays of the pencil batches of round `first` (chunk points): the
+// secondary pencils (nalpha per listed point) and the solar pencils.
+static __global__ void round_live_kernel(const unsigned long long *n_listed, int64_t first,
+                                         int chunk, int nalpha, int *live_sec, int *live_sun) {
+  const int64_t left = (int64_t)*n_listed - first;
+  const int pts = left <= 0 ? 0 : (left < chunk ? (int)left : chunk);
+  *live_sec = pts * nalpha;
+  *live_sun = pts;
 }
 
 static int batch_run(jsc_batch *b, cudaStream_t s);
@@ -998,6 +1023,9 @@ static int fixed_sources(jsc_batch *b, cudaStream_t s) {
     c->n_rays = chunk * na;
     sp_spawn_kernel<<<(chunk * na + 127) / 128, 128, 0, s>>>(pa);
     JSC_LAUNCH_CHECK();
+    round_live_kernel<<<1, 1, 0, s>>>(b->d_sp_listed, c0, chunk, na, c->d_live,
+                                      b->sun_child->d_live);
+    JSC_LAUNCH_CHECK();
     if ((st = batch_run(c, s))) return st;
     status_or_kernel<<<1, 1, 0, s>>>(b->d_status, c->d_status);
     JSC_LAUNCH_CHECK();
@@ -1054,6 +1082,10 @@ static int prepare_fixed_scattering(jsc_batch *b) {
   if ((st = ensure_child(b, &b->sun_child, (int)chunk, 0, JSC_FIXED_SUN_LOS))) return st;
   if ((st = jsc_batch_set_fixed(b->child, 1))) return st;
   if ((st = jsc_batch_set_fixed(b->sun_child, 1))) return st;
+  for (jsc_batch *c : {b->child, b->sun_child}) {
+    if (!c->d_live && (st = jsc_dmalloc(&c->d_live, 1))) return st;
+    if (!c->d_qhead && (st = jsc_dmalloc(&c->d_qhead, 1))) return st;
+  }
   if (!b->d_planck_sun) {
     double h[NDMAX];
     for (int id = 0; id < nd; id++) h[id] = planck(JSC_TSUN, b->m->nu[id]);
@@ -1391,7 +1423,14 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
                                                  b->d_psurf);
     JSC_LAUNCH_CHECK();
   }
-  launch_raytrace<false>(b, ra, s);
+  if (b->d_live) {  // rays the queue leaves alone keep no LOS and no surface
+    JSC_CUDA_TRY(cudaMemsetAsync(ra.nlos, 0, (size_t)nr * sizeof(int), s));
+    JSC_CUDA_TRY(cudaMemsetAsync(b->d_tsurf, 0, (size_t)nr * sizeof(double), s));
+  }
+  {
+    const int st = launch_raytrace<false>(b, ra, s);
+    if (st) return st;
+  }
   JSC_LAUNCH_CHECK();
   {
     const int st = launch_scan(b, ra.nlos, nr, (int64_t *)ra.los_off, s);
@@ -1432,7 +1471,10 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
     ra.pts = b->d_pts;
     ra.max_seg = b->max_seg;
   }
-  launch_raytrace<true>(b, ra, s);
+  {
+    const int st = launch_raytrace<true>(b, ra, s);
+    if (st) return st;
+  }
   JSC_LAUNCH_CHECK();
   if (refine) {
     if (b->fixed) {  // keep the refinement's reads inside the base buffer

@@ -148,6 +148,10 @@ struct jsc_batch {
   int64_t fx_max_sp, fx_chunk;
   int fx_rounds;
   unsigned long long *d_sp_listed;  // points listed by the last fixed-capacity run
+  // Pencil batches of a fixed-capacity round: their rays form a device work
+  // queue (live count and head on the device) pulled by persistent tracing.
+  int *d_live;
+  unsigned *d_qhead;
   unsigned *h_status;       // pinned: status word of the last asynchronous download
   cudaGraphExec_t gexec;
   jsc_batch_input gin;      // host inputs the graph copies from

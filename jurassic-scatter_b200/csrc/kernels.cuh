@@ -553,6 +553,31 @@ __global__ void __launch_bounds__(128, 7) raytrace_kernel(RayArgs A) {
   else if (np != A.nlos[r]) atomicOr(A.status, JSC_DEV_ERR_NLOS);
 }
 
+// The pencils of one round of a fixed-capacity scattering run as a device
+// work queue: a persistent grid pulls them a warp (32 pencils) at a time
+// from the queue head until the round's live count, which only the device
+// knows; slots past it are never traced (their nlos stays 0, cleared
+// before the counting pass).  Pulling balances the uneven pencil lengths
+// across the SMs.
+template <bool STORE, int IP = 1>
+__global__ void __launch_bounds__(128, 7) raytrace_queue_kernel(RayArgs A, unsigned *head,
+                                                               const int *live) {
+  const int lane = threadIdx.x & 31;
+  const int n = *live < A.n_rays ? *live : A.n_rays;
+  for (;;) {
+    int r0 = 0;
+    if (lane == 0) r0 = (int)atomicAdd(head, 32u);
+    r0 = __shfl_sync(0xffffffffu, r0, 0);
+    if (r0 >= n) break;
+    const int r = r0 + lane;
+    if (r < n) {
+      const int np = trace_ray<STORE, IP>(A, r);
+      if (!STORE) A.nlos[r] = np;
+      else if (np != A.nlos[r]) atomicOr(A.status, JSC_DEV_ERR_NLOS);
+    }
+  }
+}
+
 // ------------------------------------------------------ aerosol layers --
 
 struct RefineArgs {
