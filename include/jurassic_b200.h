@@ -674,16 +674,40 @@ int jsc_batch_scatter_samples(jsc_batch *b, float *feat, double *src, int64_t ma
  * Points whose features leave the training envelope take the plain path;
  * every check_stride-th point inside it (0: none) is computed both ways,
  * and if for one of them omega * |S_surrogate - S_plain| / S_plain exceeds
- * tol_rel the whole batch is recomputed with the plain path.  omega = the
+ * tol_rel the chunk of points is recomputed with the plain path.  omega = the
  * layer's single-scattering albedo beta_s / beta_e bounds the weight of the
  * scattering source in the segment source (src/forwardmodel.c:344-349), so
  * the measure bounds the relative error of the segment source. */
 int jsc_batch_set_surrogate(jsc_batch *b, jsc_surrogate *s, double tol_rel, int check_stride);
 
-/* Surrogate counts of the last run: scattering points, fallbacks, checked
- * points, largest relative deviation found by the check, and whether the
- * surrogate's sources were used (0 after a rejection); the deviation is
- * the albedo-weighted one of jsc_batch_set_surrogate. */
+/* A surrogate for the points of one scattering order (1 .. ctl->sca_mult):
+ * depth = ctl->sca_mult is jsc_batch_set_surrogate; a lower depth
+ * replaces the sources at the scattering points of the batch's secondary
+ * pencils of that order (for SCA_MULT = 2 and depth 1: the order-1 sources
+ * along the order-1 pencils, the bulk of the cost, while the order-2
+ * sources keep the plain integral over their pencils), with the same
+ * envelope, sampled check and fallback, except that the check of a lower
+ * order bounds the MEAN of omega |dS| / S over its checked (point,
+ * channel) pairs: those sources reach the radiance only through the
+ * pencil integrals of the order above, never point by point. */
+int jsc_batch_set_surrogate_depth(jsc_batch *b, int depth, jsc_surrogate *s, double tol_rel,
+                                  int check_stride);
+
+/* jsc_batch_scatter_samples and jsc_batch_surrogate_stats of the batch
+ * generation at scattering depth `depth` in the last run (for a lower
+ * depth: the secondary-pencil batch; its samples are those of the last
+ * chunk of points it ran, its statistics add up over all its chunks). */
+int jsc_batch_scatter_samples_depth(jsc_batch *b, int depth, float *feat, double *src,
+                                    int64_t max, int64_t *n);
+int jsc_batch_surrogate_stats_depth(const jsc_batch *b, int depth, int64_t *points,
+                                    int64_t *fallback, int64_t *checked, double *max_rel_err,
+                                    double *mean_rel_err, int *used);
+
+/* Surrogate counts of the last jsc_batch_run, summed over its chunks of
+ * scattering points: points, fallbacks, checked points, largest relative
+ * deviation found by the check, and whether every chunk used the
+ * surrogate's sources (0 after any rejection); the deviation is the
+ * albedo-weighted one of jsc_batch_set_surrogate. */
 int jsc_batch_surrogate_stats(const jsc_batch *b, int64_t *points, int64_t *fallback,
                               int64_t *checked, double *max_rel_err, int *used);
 

@@ -705,9 +705,19 @@ static int ensure_child(jsc_batch *b, jsc_batch **pc, int max_rays, int depth, i
   if (st) return st;
   c->cfg.hydz = -1;  // profiles arrive hydrostatically balanced
   c->depth = depth;
+  c->inner = 1;
   memcpy(c->nalpha_at, b->nalpha_at, sizeof(b->nalpha_at));
   c->nalpha = (depth <= JSC_MAX_DEPTH && b->nalpha_at[depth]) ? b->nalpha_at[depth] : b->nalpha;
   sca_alpha(c->alpha, c->nalpha);
+  memcpy(c->sur_at, b->sur_at, sizeof(b->sur_at));
+  memcpy(c->sur_tol_at, b->sur_tol_at, sizeof(b->sur_tol_at));
+  memcpy(c->sur_stride_at, b->sur_stride_at, sizeof(b->sur_stride_at));
+  if (depth >= 1 && depth <= JSC_MAX_DEPTH && c->sur_at[depth]) {
+    c->sur = c->sur_at[depth];
+    c->sur_on = 1;
+    c->sur_tol = c->sur_tol_at[depth];
+    c->sur_stride = c->sur_stride_at[depth];
+  }
   c->ega_variant = b->ega_variant;
   if ((st = jsc_batch_set_aero(c, b->h_aero))) {
     jsc_batch_destroy(c);
@@ -1171,24 +1181,32 @@ static __global__ void sur_gather_kernel(int m, const int *idx, const double *sp
 // segment source ((bext - af bs) B + af bs S) / bext
 // (src/forwardmodel.c:344-349), where af bs / bext <= bs / be, the layer's
 // single-scattering albedo; the check measures omega |dS| / S, which bounds
-// the relative error of the segment source (largest value, as float bits).
+// the relative error of the segment source: its largest value (as float
+// bits) and its sum over the checked (point, channel) pairs.
 static __global__ void sur_merge_kernel(int m, int nd, const int *idx, const int *mark,
                                         const double *sp, const double *beta, int nl,
-                                        const double *src_sub, double *src, unsigned *maxerr) {
+                                        const double *src_sub, double *src, unsigned *maxerr,
+                                        float *errsum) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= m * nd) return;
-  const int i = t / nd, d = t - i * nd, k = idx[i];
-  const double plain = src_sub[(size_t)i * nd + d];
-  double *dst = src + (size_t)k * nd + d;
-  if (mark[k] == 1) {
-    *dst = plain;
-  } else {
-    const int il = (int)sp[(size_t)k * JSC_SP_REC + SP_IL];
-    const double be = beta[(size_t)il * nd + d], bs = beta[(size_t)(nl + il) * nd + d];
-    const double omega = be > 0 ? fmin(fmax(bs / be, 0.0), 1.0) : 1.0;
-    const float e = (float)(omega * fabs(*dst - plain) / fmax(fabs(plain), 1e-300));
-    atomicMax(maxerr, __float_as_uint(e == e ? e : 3.0e38f));
+  float e = 0.0f;
+  if (t < m * nd) {
+    const int i = t / nd, d = t - i * nd, k = idx[i];
+    const double plain = src_sub[(size_t)i * nd + d];
+    double *dst = src + (size_t)k * nd + d;
+    if (mark[k] == 1) {
+      *dst = plain;
+    } else {
+      const int il = (int)sp[(size_t)k * JSC_SP_REC + SP_IL];
+      const double be = beta[(size_t)il * nd + d], bs = beta[(size_t)(nl + il) * nd + d];
+      const double omega = be > 0 ? fmin(fmax(bs / be, 0.0), 1.0) : 1.0;
+      e = (float)(omega * fabs(*dst - plain) / fmax(fabs(plain), 1e-300));
+      e = e == e ? e : 3.0e38f;
+      atomicMax(maxerr, __float_as_uint(e));
+    }
   }
+  // every thread of the block takes part (blockDim.x is a multiple of 32)
+  for (int off = 16; off > 0; off >>= 1) e += __shfl_down_sync(0xffffffffu, e, off);
+  if ((threadIdx.x & 31) == 0 && e > 0.0f) atomicAdd(errsum, e);
 }
 
 // Scattering source of every scattering point (srcfunc_sca,
@@ -1199,16 +1217,44 @@ static __global__ void sur_merge_kernel(int m, int nd, const int *idx, const int
 // than the tolerance the whole batch takes the plain path.
 static int fixed_sources(jsc_batch *b, cudaStream_t s);
 
+// Fallback (outside the envelope) and checked points of the last marking.
+static int count_marks(jsc_batch *b, int n) {
+  int *hm = (int *)malloc((size_t)n * sizeof(int));
+  if (!hm) return JSC_ERR_NOMEM;
+  if (cudaMemcpy(hm, b->d_mark, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    free(hm);
+    jsc_set_error(JSC_ERR_CUDA, "surrogate marks read-back");
+    return JSC_ERR_CUDA;
+  }
+  for (int k = 0; k < n; k++) {
+    if (hm[k] == 1) b->sur_fallback++;
+    else if (hm[k] == 2) b->sur_checked++;
+  }
+  free(hm);
+  return JSC_OK;
+}
+
+// Zero the surrogate statistics of b and its children.
+static void sur_stats_reset(jsc_batch *b) {
+  for (jsc_batch *c = b; c; c = c->child) {
+    c->sur_points = c->sur_fallback = c->sur_checked = 0;
+    c->sur_maxerr = 0;
+    c->sur_errsum = 0;
+    c->sur_errn = 0;
+    c->sur_runs = c->sur_used_runs = 0;
+  }
+}
+
 static int scatter_sources(jsc_batch *b, cudaStream_t s) {
   if (b->fixed) return fixed_sources(b, s);
   int st = list_scattering_points(b, s);
   if (st || b->n_sp == 0) return st;
   const int nd = b->cfg.nd;
   const int n = (int)b->n_sp;
-  b->sur_points = b->n_sp;
-  b->sur_fallback = b->sur_checked = 0;
-  b->sur_maxerr = 0;
-  b->sur_used = 0;
+  // statistics add up over the chunks of one jsc_batch_run (a child batch
+  // runs once per chunk of its parent)
+  b->sur_points += b->n_sp;
+  b->sur_runs++;
   if (!(b->sur && b->sur_on && jsc_sur_trained(b->sur) && jsc_sur_nout(b->sur) == nd))
     return plain_sources(b, b->d_sp, b->d_sp_atm, b->n_sp, b->d_src, s);
   if (b->sur_cap < b->n_sp) {
@@ -1225,7 +1271,7 @@ static int scatter_sources(jsc_batch *b, cudaStream_t s) {
     const int64_t cap = b->max_sp;
     if ((st = jsc_dmalloc(&b->d_feat, (size_t)cap * SUR_NF))) return st;
     if ((st = jsc_dmalloc(&b->d_mark, (size_t)cap))) return st;
-    if ((st = jsc_dmalloc(&b->d_idx, (size_t)cap + 1))) return st;
+    if ((st = jsc_dmalloc(&b->d_idx, (size_t)cap + 2))) return st;  // + count, error sum
     if ((st = jsc_dmalloc(&b->d_sp_sub, (size_t)cap * JSC_SP_REC))) return st;
     if ((st = jsc_dmalloc(&b->d_atm_sub, (size_t)cap))) return st;
     if ((st = jsc_dmalloc(&b->d_src_sub, (size_t)cap * nd))) return st;
@@ -1251,37 +1297,40 @@ static int scatter_sources(jsc_batch *b, cudaStream_t s) {
                                                       b->d_sp_sub, b->d_atm_sub);
     JSC_LAUNCH_CHECK();
     if ((st = plain_sources(b, b->d_sp_sub, b->d_atm_sub, m, b->d_src_sub, s))) return st;
-    unsigned *d_err = (unsigned *)b->d_idx + b->sur_cap;  // reuse the count word
-    JSC_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
+    // the count word becomes the largest error, the word after it the sum
+    unsigned *d_err = (unsigned *)b->d_idx + b->sur_cap;
+    JSC_CUDA_TRY(cudaMemsetAsync(d_err, 0, 2 * sizeof(unsigned), s));
     sur_merge_kernel<<<(m * nd + 127) / 128, 128, 0, s>>>(m, nd, b->d_idx, b->d_mark, b->d_sp,
                                                           b->d_beta, b->aero_nl, b->d_src_sub,
-                                                          b->d_src, d_err);
+                                                          b->d_src, d_err, (float *)(d_err + 1));
     JSC_LAUNCH_CHECK();
-    unsigned eb = 0;
-    JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    JSC_CUDA_TRY(cudaMemcpyAsync(b->h_total, d_err, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                 s));
     JSC_CUDA_TRY(cudaStreamSynchronize(s));
-    eb = *(unsigned *)b->h_total;
-    float e;
-    memcpy(&e, &eb, sizeof(e));
-    b->sur_maxerr = e;
-  }
-  // marks: count fallback and checked points on the host side of the copy
-  {
-    int *hm = (int *)malloc((size_t)n * sizeof(int));
-    if (!hm) return JSC_ERR_NOMEM;
-    JSC_CUDA_TRY(cudaMemcpy(hm, b->d_mark, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
-    for (int k = 0; k < n; k++) {
-      if (hm[k] == 1) b->sur_fallback++;
-      else if (hm[k] == 2) b->sur_checked++;
+    float e, sum;
+    memcpy(&e, (const unsigned char *)b->h_total, sizeof(e));
+    memcpy(&sum, (const unsigned char *)b->h_total + sizeof(float), sizeof(sum));
+    const int64_t before = b->sur_checked;
+    if ((st = count_marks(b, n))) return st;
+    const int64_t pairs = (b->sur_checked - before) * nd;
+    b->sur_maxerr = fmaxf(b->sur_maxerr, e);
+    b->sur_errsum += sum;
+    b->sur_errn += pairs;
+    // The points of a scattering order below the top reach the radiance
+    // only through the source integrals of the order above (each a sum
+    // over pencils of line-of-sight integrals over many such points), so
+    // their check bounds the mean deviation; the top order's sources enter
+    // the radiance point by point, so its check bounds the largest one.
+    const double crit = b->inner ? (pairs > 0 ? sum / (double)pairs : 0.0) : e;
+    if (!(crit <= b->sur_tol)) {
+      // the check missed the tolerance: this chunk takes the plain path
+      b->sur_rejected++;
+      return plain_sources(b, b->d_sp, b->d_sp_atm, b->n_sp, b->d_src, s);
     }
-    free(hm);
+  } else if ((st = count_marks(b, n))) {
+    return st;
   }
-  if (b->sur_maxerr > b->sur_tol) {
-    // a checked point missed the tolerance: the whole batch takes the plain path
-    b->sur_rejected++;
-    return plain_sources(b, b->d_sp, b->d_sp_atm, b->n_sp, b->d_src, s);
-  }
-  b->sur_used = 1;
+  b->sur_used_runs++;
   return JSC_OK;
 }
 
@@ -1356,6 +1405,7 @@ extern "C" int jsc_batch_run(jsc_batch *b, void *stream) {
   if (!b) return JSC_ERR_ARG;
   JSC_CUDA_TRY(cudaSetDevice(b->m->device));
   (void)cudaGetLastError();  // launch checks below report this run's errors only
+  sur_stats_reset(b);
   return batch_run(b, (cudaStream_t)stream);
 }
 
@@ -1811,6 +1861,65 @@ extern "C" int jsc_batch_set_surrogate(jsc_batch *b, jsc_surrogate *s, double to
   return JSC_OK;
 }
 
+extern "C" int jsc_batch_set_surrogate_depth(jsc_batch *b, int depth, jsc_surrogate *s,
+                                             double tol_rel, int check_stride) {
+  if (!b || depth < 1 || depth > b->depth || depth > JSC_MAX_DEPTH) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_set_surrogate_depth: depth %d outside 1..%d", depth,
+                  b ? b->depth : 0);
+    return JSC_ERR_ARG;
+  }
+  if (depth == b->depth) return jsc_batch_set_surrogate(b, s, tol_rel, check_stride);
+  if (s && (jsc_sur_nout(s) != b->cfg.nd || tol_rel <= 0 || check_stride < 0)) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_set_surrogate_depth: channel count, tolerance or stride");
+    return JSC_ERR_ARG;
+  }
+  b->sur_at[depth] = s;
+  b->sur_tol_at[depth] = (float)tol_rel;
+  b->sur_stride_at[depth] = check_stride;
+  for (jsc_batch *c = b->child; c; c = c->child) {
+    c->sur_at[depth] = s;
+    c->sur_tol_at[depth] = (float)tol_rel;
+    c->sur_stride_at[depth] = check_stride;
+    if (c->depth == depth) {
+      c->sur = s;
+      c->sur_on = s != nullptr;
+      c->sur_tol = (float)tol_rel;
+      c->sur_stride = check_stride;
+    }
+  }
+  return JSC_OK;
+}
+
+// The batch of the last run at scattering depth `depth` (b or a child).
+static jsc_batch *batch_at_depth(jsc_batch *b, int depth) {
+  for (jsc_batch *c = b; c; c = c->child)
+    if (c->depth == depth) return c;
+  return nullptr;
+}
+
+extern "C" int jsc_batch_scatter_samples_depth(jsc_batch *b, int depth, float *feat, double *src,
+                                               int64_t max, int64_t *n) {
+  jsc_batch *c = b ? batch_at_depth(b, depth) : nullptr;
+  if (!c || !n) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_scatter_samples_depth: no batch of depth %d", depth);
+    return JSC_ERR_ARG;
+  }
+  return jsc_batch_scatter_samples(c, feat, src, max, n);
+}
+
+extern "C" int jsc_batch_surrogate_stats_depth(const jsc_batch *b, int depth, int64_t *points,
+                                               int64_t *fallback, int64_t *checked,
+                                               double *max_rel_err, double *mean_rel_err,
+                                               int *used) {
+  jsc_batch *c = b ? batch_at_depth(const_cast<jsc_batch *>(b), depth) : nullptr;
+  if (!c) {
+    jsc_set_error(JSC_ERR_ARG, "jsc_batch_surrogate_stats_depth: no batch of depth %d", depth);
+    return JSC_ERR_ARG;
+  }
+  if (mean_rel_err) *mean_rel_err = c->sur_errn > 0 ? c->sur_errsum / (double)c->sur_errn : 0.0;
+  return jsc_batch_surrogate_stats(c, points, fallback, checked, max_rel_err, used);
+}
+
 extern "C" int jsc_batch_surrogate_stats(const jsc_batch *b, int64_t *points, int64_t *fallback,
                                          int64_t *checked, double *max_rel_err, int *used) {
   if (!b) return JSC_ERR_ARG;
@@ -1818,7 +1927,8 @@ extern "C" int jsc_batch_surrogate_stats(const jsc_batch *b, int64_t *points, in
   if (fallback) *fallback = b->sur_fallback;
   if (checked) *checked = b->sur_checked;
   if (max_rel_err) *max_rel_err = b->sur_maxerr;
-  if (used) *used = b->sur_used;
+  // used: every chunk of the last run took its sources from the surrogate
+  if (used) *used = b->sur_runs > 0 && b->sur_used_runs == b->sur_runs;
   return JSC_OK;
 }
 

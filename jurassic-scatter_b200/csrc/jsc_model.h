@@ -131,13 +131,20 @@ struct jsc_batch {
   struct jsc_surrogate *sur;
   int sur_on, sur_stride;
   float sur_tol;
+  // surrogates for the points of other scattering orders (descendants)
+  struct jsc_surrogate *sur_at[JSC_MAX_DEPTH + 1];
+  float sur_tol_at[JSC_MAX_DEPTH + 1];
+  int sur_stride_at[JSC_MAX_DEPTH + 1];
   int64_t sur_cap;
   float *d_feat;
   int *d_mark, *d_idx, *d_atm_sub;
   double *d_sp_sub, *d_src_sub;
   int64_t sur_points, sur_fallback, sur_checked, sur_rejected;
   float sur_maxerr;
-  int sur_used;
+  double sur_errsum;            // checked deviations summed over (point, channel) pairs
+  int64_t sur_errn;             // ... and their number
+  int inner;                    // secondary-pencil batch of a deeper recursion
+  int sur_runs, sur_used_runs;  // chunks of the last run with points / from the surrogate
 
   // Fixed-capacity mode (no host read-backs; graph capture) and the
   // captured upload + run + download graph.  With scattering (depth 1):

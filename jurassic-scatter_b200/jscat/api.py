@@ -251,33 +251,57 @@ class Batch:
         """Aerosol/cloud layers (an AeroT) for runs with ctl.sca_n > 0."""
         L.check(L.load().jsc_batch_set_aero(self.h, C.byref(aero)), "jsc_batch_set_aero")
 
-    def scatter_samples(self):
+    def scatter_samples(self, depth=None):
         """Features [n][8] and plain scattering sources [n][nd] of the last
-        run's scattering points."""
+        run's scattering points (depth: those of the batch generation at
+        that scattering depth, default this batch's own)."""
         lib = L.load()
         n = C.c_int64()
-        L.check(lib.jsc_batch_scatter_samples(self.h, None, None, 0, C.byref(n)),
-                "jsc_batch_scatter_samples")
+        if depth is None:
+            def call(f, s_, m):
+                return lib.jsc_batch_scatter_samples(self.h, f, s_, m, C.byref(n))
+        else:
+            def call(f, s_, m):
+                return lib.jsc_batch_scatter_samples_depth(self.h, int(depth), f, s_, m,
+                                                           C.byref(n))
+        L.check(call(None, None, 0), "jsc_batch_scatter_samples")
         feat = np.empty((n.value, Surrogate.NF), np.float32)
         src = np.empty((n.value, self.nd))
         if n.value:
-            L.check(lib.jsc_batch_scatter_samples(self.h, _fptr(feat), _dptr(src), n.value,
-                                                  C.byref(n)), "jsc_batch_scatter_samples")
+            L.check(call(_fptr(feat), _dptr(src), n.value), "jsc_batch_scatter_samples")
         return feat, src
 
-    def set_surrogate(self, sur, tol_rel=0.05, check_stride=64):
-        L.check(L.load().jsc_batch_set_surrogate(self.h, sur.h if sur is not None else None,
-                                                 float(tol_rel), int(check_stride)),
-                "jsc_batch_set_surrogate")
+    def set_surrogate(self, sur, tol_rel=0.05, check_stride=64, depth=None):
+        """Attach a surrogate (None: none) for this batch's scattering
+        points, or for those of another scattering order (depth)."""
+        h = sur.h if sur is not None else None
+        if depth is None:
+            L.check(L.load().jsc_batch_set_surrogate(self.h, h, float(tol_rel), int(check_stride)),
+                    "jsc_batch_set_surrogate")
+        else:
+            L.check(L.load().jsc_batch_set_surrogate_depth(self.h, int(depth), h, float(tol_rel),
+                                                           int(check_stride)),
+                    "jsc_batch_set_surrogate_depth")
 
-    def surrogate_stats(self):
+    def surrogate_stats(self, depth=None):
+        """Surrogate counts of the last run (depth: those of the batch
+        generation at that scattering depth, which adds the mean checked
+        deviation)."""
         p, f, c, u = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int()
-        e = C.c_double()
-        L.check(L.load().jsc_batch_surrogate_stats(self.h, C.byref(p), C.byref(f), C.byref(c),
-                                                   C.byref(e), C.byref(u)),
-                "jsc_batch_surrogate_stats")
-        return {"points": p.value, "fallback": f.value, "checked": c.value,
-                "max_rel_err": e.value, "used": bool(u.value)}
+        e, mean = C.c_double(), C.c_double()
+        if depth is None:
+            st = L.load().jsc_batch_surrogate_stats(self.h, C.byref(p), C.byref(f), C.byref(c),
+                                                    C.byref(e), C.byref(u))
+        else:
+            st = L.load().jsc_batch_surrogate_stats_depth(self.h, int(depth), C.byref(p),
+                                                          C.byref(f), C.byref(c), C.byref(e),
+                                                          C.byref(mean), C.byref(u))
+        L.check(st, "jsc_batch_surrogate_stats")
+        out = {"points": p.value, "fallback": f.value, "checked": c.value,
+               "max_rel_err": e.value, "used": bool(u.value)}
+        if depth is not None:
+            out["mean_rel_err"] = mean.value
+        return out
 
     def set_variant(self, variant):
         """EGA launch variant (-1: default); see jsc_batch_set_variant."""

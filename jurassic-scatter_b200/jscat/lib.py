@@ -31,7 +31,8 @@ EXPORTS = [
     "formod_continua", "intpol_tbl", "intpol_tbl_eps", "intpol_tbl_u", "locate_tbl",
     "jsc_srcfunc_sca", "jsc_batch_scatter_points", "jsc_surrogate_get_scaling",
     "jsc_batch_set_nalpha_depth", "jsc_batch_set_wait_budget", "jsc_scan_selftest",
-    "jsc_batch_set_fixed_points",
+    "jsc_batch_set_fixed_points", "jsc_batch_set_surrogate_depth",
+    "jsc_batch_scatter_samples_depth", "jsc_batch_surrogate_stats_depth",
 ]
 
 
@@ -154,6 +155,11 @@ def load():
         "jsc_batch_set_wait_budget": (i, [vp, C.c_uint]),
         "jsc_scan_selftest": (i, [i, i, C.c_uint, i]),
         "jsc_batch_set_fixed_points": (i, [vp, C.c_int64]),
+        "jsc_batch_set_surrogate_depth": (i, [vp, i, vp, d, i]),
+        "jsc_batch_scatter_samples_depth": (i, [vp, i, P(C.c_float), P(d), C.c_int64,
+                                                P(C.c_int64)]),
+        "jsc_batch_surrogate_stats_depth": (i, [vp, i, P(C.c_int64), P(C.c_int64),
+                                                P(C.c_int64), P(d), P(d), P(i)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

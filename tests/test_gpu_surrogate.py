@@ -211,3 +211,59 @@ def test_surrogate_accuracy_held_out(workdir):
         sur.close()
         b.close()
         m.close()
+
+
+def test_order1_surrogate_inside_double_scattering(workdir):
+    """Depth-2 scattering through the ice-cloud layer with a surrogate for
+    the order-1 sources only (jsc_batch_set_surrogate_depth, depth 1): the
+    order-2 sources stay the plain integral over the order-1 pencils, whose
+    own scattering points take the network.  Trained on the order-1 points
+    of rays A, used on disjoint rays B: every chunk keeps the surrogate,
+    and the brightness temperatures stay within 0.05 K of the plain path."""
+    from jscat import api, synth, structs as S
+    from make_golden_shim import ice_depth2_case
+    ctlkw, atm, _, nalpha = ice_depth2_case(workdir)
+    g = np.load(GOLDEN + "/ice_sca2_port.npz")
+    aero = S.AeroT.from_buffer_copy(g["aero"].tobytes())
+    ctl = S.make_ctl(**ctlkw)
+    rng = np.random.default_rng(23)
+
+    def rays(n):
+        geom = synth.limb_geometry(rng.uniform(6.0, 14.0, n))
+        geom["time"] = rng.uniform(0.0, 86400.0, n)
+        return synth.batch_from([atm], np.zeros(n, np.int32), geom)
+
+    na, nb = 192, 64
+    train, test = rays(na), rays(nb)
+    m = api.Model(ctl)
+    b = api.Batch(m, ctl, 1, len(train["z"]), na)
+    sur = api.Surrogate(ctl.nd, seed=4)
+    try:
+        b.set_aero(aero)
+        for depth, na_ in nalpha.items():
+            b.set_nalpha_depth(depth, na_)
+        b.upload(train)
+        b.run()
+        feat, src = b.scatter_samples(depth=1)
+        assert len(feat) > 10000 and np.all(np.isfinite(src))
+        sur.train(feat, src, epochs=40, batch=4096, lr=3e-3)
+        b.upload(test)
+        b.run()
+        plain = b.download()
+        assert np.all(np.isfinite(plain["rad"]))
+        b.set_surrogate(sur, tol_rel=api.SURROGATE_CHECK_TOL, check_stride=16, depth=1)
+        b.run()
+        out = b.download()
+        st = b.surrogate_stats(depth=1)
+        assert st["points"] > 1000 and st["checked"] > 50, st
+        assert st["used"], st
+        assert b.surrogate_stats()["points"] > 0 and not b.surrogate_stats()["used"]
+        assert bt_error(out["rad"], plain["rad"], ctlkw["nus"]) <= 0.05
+        # detached again: the plain path, bit for bit
+        b.set_surrogate(None, depth=1)
+        b.run()
+        assert np.array_equal(b.download()["rad"], plain["rad"])
+    finally:
+        sur.close()
+        b.close()
+        m.close()
