@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 C_SRCS = ["model_host.c", "formod.c", "optprop.c", "compat.c"]
 CU_SRCS = ["model_dev.cu", "batch.cu", "ega_g2.cu", "ega_g4.cu", "ega_g8.cu",
-           "ega_gmax.cu", "ega_lane_s.cu", "ega_lane_l.cu", "noalloc.cu", "surrogate.cu",
+           "ega_gmax.cu", "ega_lane_s.cu", "ega_lane_l.cu", "ega_ray.cu", "noalloc.cu", "surrogate.cu",
            "surrogate_tc.cu", "mie.cu"]
 HEADERS = ["jsc_internal.h", "physics.h", "ckd_tables.h", "jsc_model.h",
            "cuda_util.cuh", "device_common.cuh", "kernels.cuh", "ega_kernel.cuh",

@@ -54,6 +54,9 @@ extern "C" void jsc_batch_destroy(jsc_batch *b) {
   batch_free_los(b);
   cudaFree(b->d_tsurf);
   cudaFree(b->d_tp);
+  cudaFree(b->d_rkeys);
+  cudaFree(b->d_rorder);
+  cudaFree(b->d_rtmp);
   cudaFree(b->d_rad);
   cudaFree(b->d_tau);
   cudaFree(b->d_status);
@@ -163,6 +166,15 @@ extern "C" int jsc_batch_create(jsc_model *m, const ctl_t *ctl, int max_atm,
   st = st ? st : jsc_dmalloc(&b->d_los_off, (size_t)max_rays + 1);
   st = st ? st : jsc_dmalloc(&b->d_tsurf, (size_t)max_rays);
   st = st ? st : jsc_dmalloc(&b->d_tp, (size_t)max_rays * 3);
+  st = st ? st : jsc_dmalloc(&b->d_rkeys, (size_t)max_rays * 2);
+  st = st ? st : jsc_dmalloc(&b->d_rorder, (size_t)max_rays * 2);
+  if (!st) {
+    b->rtmp_bytes = jsc_ray_order_tmp_bytes(max_rays);
+    if (cudaMalloc(&b->d_rtmp, b->rtmp_bytes ? b->rtmp_bytes : 16) != cudaSuccess) {
+      jsc_set_error(JSC_ERR_NOMEM, "device allocation of %zu bytes", b->rtmp_bytes);
+      st = JSC_ERR_NOMEM;
+    }
+  }
   st = st ? st : jsc_dmalloc(&b->d_rad, (size_t)max_rays * ctl->nd);
   st = st ? st : jsc_dmalloc(&b->d_tau, (size_t)max_rays * ctl->nd);
   st = st ? st : jsc_dmalloc(&b->d_status, 1);
@@ -545,16 +557,25 @@ extern "C" int jsc_scan_selftest(int device, int n, unsigned budget, int stall) 
 // number sets the register budget, i.e. the trade between occupancy and
 // spills, the rolled loop trades registers and instruction-cache footprint
 // for local-memory path state.  9-13: ega_lane_kernel, a lane per
-// (ray, channel, emitter), after ctm_src_kernel.  jsc_batch_autotune picks
-// one.
-struct EgaVariant { int blk, minb, roll, lane; };
+// (ray, channel, emitter), after ctm_src_kernel.  14-15: ega_ray_kernel,
+// lanes over a tile of 32 ordered rays, a warp per emitter (block size
+// 32 (emitter warps + 1); blk 0 here), after ctm_src_kernel; more than 16
+// emitters run the lane variant 13 instead.  jsc_batch_autotune picks one.
+struct EgaVariant { int blk, minb, roll, lane, ray; };
 static const EgaVariant kEgaVariants[] = {
-    {128, 4, 0, 0}, {128, 6, 0, 0}, {128, 8, 0, 0}, {256, 3, 0, 0}, {256, 4, 0, 0},
-    {128, 8, 1, 0}, {128, 12, 1, 0}, {256, 4, 1, 0}, {256, 6, 1, 0},
-    {128, 12, 0, 1}, {128, 8, 0, 1}, {256, 4, 0, 1}, {256, 5, 0, 1}, {512, 2, 0, 1}};
-static const int kNumEgaVariants = 14;
+    {128, 4, 0, 0, 0}, {128, 6, 0, 0, 0}, {128, 8, 0, 0, 0}, {256, 3, 0, 0, 0},
+    {256, 4, 0, 0, 0}, {128, 8, 1, 0, 0}, {128, 12, 1, 0, 0}, {256, 4, 1, 0, 0},
+    {256, 6, 1, 0, 0}, {128, 12, 0, 1, 0}, {128, 8, 0, 1, 0}, {256, 4, 0, 1, 0},
+    {256, 5, 0, 1, 0}, {512, 2, 0, 1, 0}, {0, 3, 0, 1, 1}, {0, 4, 0, 1, 1}};
+static const int kNumEgaVariants = 16;
 static_assert(kNumEgaVariants <= 32, "ega_variant_ms holds 32 timings");
 static const int kLaneBase = 9;
+static const int kRayBase = 14;
+
+// Emitter warps of the ray-tile kernel for ng emitters (0: not available).
+static int ray_warps(int ng) {
+  return ng <= 2 ? 2 : ng <= 4 ? 4 : ng <= 8 ? 8 : ng <= 16 ? 16 : 0;
+}
 static const int kEgaDefault = JSC_EGA_DEFAULT_VARIANT;  // default of clear-air runs
 
 // Default launch variant of runs with aerosol/cloud layers (the scattering
@@ -583,8 +604,13 @@ static int launch_ega(const EgaArgs &ea, int nr, int ndp, int ng, int variant,
   const unsigned g256 = (unsigned)((threads + 255) / 256);
   const int v = (variant >= 0 && variant < kNumEgaVariants) ? variant : kEgaDefault;
   const bool dig = ea.digest != nullptr;  // index digests (every variant has them)
+  if (kEgaVariants[v].ray && ray_warps(ng) && ea.order) {
+    jsc_ega_ray_launch(ea, v - kRayBase, dig, s);
+    JSC_LAUNCH_CHECK();
+    return JSC_OK;
+  }
   if (kEgaVariants[v].lane) {
-    const int lv = v - kLaneBase;
+    const int lv = kEgaVariants[v].ray ? 4 : v - kLaneBase;
     if (ng <= 4) jsc_ega_lane_launch_s(ea, lv, dig, s);
     else jsc_ega_lane_launch_l(ea, lv, dig, s);
     JSC_LAUNCH_CHECK();
@@ -1650,7 +1676,17 @@ static int batch_run(jsc_batch *b, cudaStream_t s) {
   ea.sp_off = (scattering && (b->n_sp > 0 || b->fixed)) ? b->d_sp_off : nullptr;
   ea.beta_ctm = b->d_ctm;
   ea.src_pl = b->d_srcp;
+  ea.order = nullptr;
   const int variant = run_variant(b);
+  if (kEgaVariants[variant].ray && ray_warps(m->ng)) {
+    int e = jsc_ray_order(nr, b->d_ray_atm, b->d_nlos, b->d_tsurf, b->d_tp, b->d_rkeys,
+                          b->d_rorder, b->d_rtmp, b->rtmp_bytes, s);
+    if (e) {
+      jsc_set_error(JSC_ERR_CUDA, "ray order: %s", cudaGetErrorString((cudaError_t)e));
+      return JSC_ERR_CUDA;
+    }
+    ea.order = b->d_rorder;
+  }
   if (lane_variant(variant)) {
     // continuum extinction and Planck source per (LOS point, channel)
     CtmArgs ca;
@@ -1761,6 +1797,15 @@ extern "C" int jsc_batch_autotune(jsc_batch *b, void *stream) {
   if (st) return st;
   EgaArgs ea = b->last_ega;
   ea.digest = nullptr;
+  if (ray_warps(b->m->ng)) {
+    int e = jsc_ray_order(b->n_rays, b->d_ray_atm, b->d_nlos, b->d_tsurf, b->d_tp, b->d_rkeys,
+                          b->d_rorder, b->d_rtmp, b->rtmp_bytes, s);
+    if (e) {
+      jsc_set_error(JSC_ERR_CUDA, "ray order: %s", cudaGetErrorString((cudaError_t)e));
+      return JSC_ERR_CUDA;
+    }
+    ea.order = b->d_rorder;
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   JSC_CUDA_TRY(cudaEventCreate(&e0));
   if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -1813,8 +1858,11 @@ extern "C" int jsc_batch_variant(const jsc_batch *b, int *variant, int *blk, int
   if (!b) return JSC_ERR_ARG;
   const int v = run_variant(b);
   if (variant) *variant = v;
-  if (blk) *blk = kEgaVariants[v].blk;
-  if (minb) *minb = kEgaVariants[v].minb;
+  const int rw = kEgaVariants[v].ray ? ray_warps(b->m->ng) : 0;
+  if (blk) *blk = kEgaVariants[v].ray ? (rw ? 32 * (rw + 1) : kEgaVariants[kLaneBase + 4].blk)
+                                      : kEgaVariants[v].blk;
+  if (minb) *minb = kEgaVariants[v].ray && !rw ? kEgaVariants[kLaneBase + 4].minb
+                                               : kEgaVariants[v].minb;
   return JSC_OK;
 }
 

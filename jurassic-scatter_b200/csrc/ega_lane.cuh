@@ -47,6 +47,115 @@ static __global__ void __launch_bounds__(256) ctm_src_kernel(CtmArgs A) {
   }
 }
 
+// Path state of one (ray, channel, emitter) along its ray: the emitter's
+// path transmittance, a 16-bit interval hint per (p, T) corner row and the
+// bracket code the hints belong to, the forward distances j - k of the
+// rows (8 bits each), the index digest and the EGA evaluation count.
+struct EgaPath {
+  double tp;
+  unsigned long long hint;
+  int hcode;
+  unsigned djp;
+  unsigned long long dig;
+  unsigned n_ega;
+};
+
+__device__ __forceinline__ EgaPath ega_path_start() {
+  EgaPath ps;
+  ps.tp = 1;
+  ps.hint = 0;
+  ps.hcode = -1;
+  ps.djp = 0;
+  ps.dig = 0;
+  ps.n_ega = 0;
+  return ps;
+}
+
+// The emissivity table of (channel d, emitter g): its grid id (ok: the
+// table exists), its (ip, it) row descriptors with the stride of one slot,
+// and its pressure and temperature grids.
+struct EgaTable {
+  int gid;
+  bool ok;
+  const jsc_row *__restrict__ rows_dg;
+  size_t rs;
+  const double *__restrict__ gp;
+  const double *__restrict__ gt;
+};
+
+__device__ __forceinline__ EgaTable ega_table(const jsc_dev_model &m, int d, int g) {
+  EgaTable tb;
+  const bool has_g = g < m.ng;
+  tb.gid = has_g ? m.tab_grid[d * m.ng + g] : -1;
+  tb.ok = tb.gid >= 0;
+  tb.rows_dg = m.rows + (size_t)(has_g ? g : 0) * m.nd + d;
+  tb.rs = (size_t)m.ng * m.nd;
+  tb.gp = m.grid_p + (size_t)(tb.ok ? tb.gid : 0) * TBLNPMAX;
+  tb.gt = m.grid_t + (size_t)(tb.ok ? tb.gid : 0) * TBLNPMAX * TBLNTMAX;
+  return tb;
+}
+
+// Segment emissivity of one emitter at the LOS point rec (intpol_tbl,
+// src/forwardmodel.c:409-502): the four (p, T) corner rows, each an
+// inverse lookup of the path emissivity and a forward lookup of the
+// extended column (ega_node), interpolated in T, then in p; the path
+// state's hints and digest advance.  The caller multiplies ps.tp by
+// (1 - eps).
+template <bool DIG>
+__device__ __forceinline__ double ega_lane_eps(const jsc_dev_model &m, bool single_grid,
+                                               const EgaTable &tb, int g,
+                                               const double *__restrict__ rec, EgaPath &ps) {
+  const double P = rec[REC_P], T = rec[REC_T];
+  double eps = 0;
+  if (tb.ok) {
+    if (ps.tp < 1e-9) {
+      eps = 1;
+    } else {
+      const int code = single_grid
+                           ? (int)rec[REC_GRID]
+                           : grid_code(m.grid_np[tb.gid], tb.gp,
+                                       m.grid_nt + (size_t)tb.gid * TBLNPMAX, tb.gt, P, T);
+      if (code & (1 << 16)) {
+        const int ipr = (code >> 10) & 63, it0 = (code >> 5) & 31, it1 = code & 31;
+        const jsc_row r00 = tb.rows_dg[(size_t)(ipr * TBLNTMAX + it0) * tb.rs];
+        const jsc_row r01 = tb.rows_dg[(size_t)(ipr * TBLNTMAX + it0 + 1) * tb.rs];
+        const jsc_row r10 = tb.rows_dg[(size_t)((ipr + 1) * TBLNTMAX + it1) * tb.rs];
+        const jsc_row r11 = tb.rows_dg[(size_t)((ipr + 1) * TBLNTMAX + it1 + 1) * tb.rs];
+        if ((r00.nf & 0xffff) >= 2 && (r01.nf & 0xffff) >= 2 && (r10.nf & 0xffff) >= 2 &&
+            (r11.nf & 0xffff) >= 2) {
+          const double x1 = 1 - ps.tp, useg = rec[REC_K + m.nw + g];
+          if (DIG) ps.dig = ps.dig * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
+          if (ps.hcode >= 0 && ps.hcode != code) ps.hint = remap_hints(ps.hint, ps.hcode, code);
+          int k00, k01, k10, k11, j00, j01, j10, j11;
+          const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(ps.hint & 0xffff),
+                                           (int)(ps.djp & 0xff), &k00, &j00, &ps.dig);
+          const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((ps.hint >> 16) & 0xffff),
+                                           (int)((ps.djp >> 8) & 0xff), &k01, &j01, &ps.dig);
+          const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((ps.hint >> 32) & 0xffff),
+                                           (int)((ps.djp >> 16) & 0xff), &k10, &j10, &ps.dig);
+          const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(ps.hint >> 48),
+                                           (int)(ps.djp >> 24), &k11, &j11, &ps.dig);
+          ps.hint = (unsigned long long)(j00 & 0xffff) |
+                    ((unsigned long long)(j01 & 0xffff) << 16) |
+                    ((unsigned long long)(j10 & 0xffff) << 32) |
+                    ((unsigned long long)(j11 & 0xffff) << 48);
+          ps.hcode = code;
+          ps.djp = (unsigned)min(j00 - k00, 255) | ((unsigned)min(j01 - k01, 255) << 8) |
+                   ((unsigned)min(j10 - k10, 255) << 16) | ((unsigned)min(j11 - k11, 255) << 24);
+          double ea = jsc_clamp01(jsc_lin(tb.gt[ipr * TBLNTMAX + it0], e00,
+                                          tb.gt[ipr * TBLNTMAX + it0 + 1], e01, T));
+          const double eb = jsc_clamp01(jsc_lin(tb.gt[(ipr + 1) * TBLNTMAX + it1], e10,
+                                                tb.gt[(ipr + 1) * TBLNTMAX + it1 + 1], e11, T));
+          ea = jsc_clamp01(jsc_lin(tb.gp[ipr], ea, tb.gp[ipr + 1], eb, P));
+          eps = 1 - (1 - ea) / ps.tp;
+          ps.n_ega++;
+        }
+      }
+    }
+  }
+  return eps;
+}
+
 template <int GP, bool DIG, int BLK, int MINB>
 __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
   const jsc_dev_model &m = A.m;
@@ -61,20 +170,9 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
   const unsigned gbase = lane & ~(unsigned)(GP - 1);
   const unsigned gmask = GP == 32 ? 0xffffffffu : (((1u << GP) - 1u) << gbase);
 
-  const bool has_g = g < ng;
-  const int gid = has_g ? m.tab_grid[d * ng + g] : -1;
-  const bool ok = gid >= 0;  // the table of (channel, emitter) exists
-  const jsc_row *__restrict__ rows_dg = m.rows + (size_t)(has_g ? g : 0) * nd + d;
-  const size_t rs = (size_t)ng * nd;  // stride of one (ip, it) slot
-  const double *__restrict__ gp = m.grid_p + (size_t)(ok ? gid : 0) * TBLNPMAX;
-  const double *__restrict__ gt = m.grid_t + (size_t)(ok ? gid : 0) * TBLNPMAX * TBLNTMAX;
-
-  double tp = 1, rad = 0, tau = 1;
-  unsigned long long hint = 0;  // 16-bit interval hint per (p, T) corner row
-  int hcode = -1;               // the bracket code the hints belong to
-  unsigned djp = 0;             // forward distances j - k of the rows, 8 bits each
-  unsigned long long dig = 0;
-  unsigned n_ega = 0;
+  const EgaTable tb = ega_table(m, d, g);
+  EgaPath ps = ega_path_start();
+  double rad = 0, tau = 1;
   const int np = A.nlos[r];
   const int64_t off = A.los_off[r];
   const double *__restrict__ rec = A.pts + off * A.W;
@@ -83,52 +181,9 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
   const double *__restrict__ ssrc = A.src_sca ? A.src_sca + (size_t)A.sp_off[r] * nd + d : nullptr;
 
   for (int ip = 0; ip < np; ip++, rec += A.W, bc += nd, sp += nd) {
-    const double P = rec[REC_P], T = rec[REC_T], DS = rec[REC_DS];
-    double eps = 0;
-    if (ok) {
-      if (tp < 1e-9) {
-        eps = 1;
-      } else {
-        const int code = A.single_grid
-                             ? (int)rec[REC_GRID]
-                             : grid_code(m.grid_np[gid], gp, m.grid_nt + (size_t)gid * TBLNPMAX, gt, P, T);
-        if (code & (1 << 16)) {
-          const int ipr = (code >> 10) & 63, it0 = (code >> 5) & 31, it1 = code & 31;
-          const jsc_row r00 = rows_dg[(size_t)(ipr * TBLNTMAX + it0) * rs];
-          const jsc_row r01 = rows_dg[(size_t)(ipr * TBLNTMAX + it0 + 1) * rs];
-          const jsc_row r10 = rows_dg[(size_t)((ipr + 1) * TBLNTMAX + it1) * rs];
-          const jsc_row r11 = rows_dg[(size_t)((ipr + 1) * TBLNTMAX + it1 + 1) * rs];
-          if ((r00.nf & 0xffff) >= 2 && (r01.nf & 0xffff) >= 2 && (r10.nf & 0xffff) >= 2 &&
-              (r11.nf & 0xffff) >= 2) {
-            const double x1 = 1 - tp, useg = rec[REC_K + m.nw + g];
-            if (DIG) dig = dig * 1000003ull + (unsigned long long)(ipr * 961 + it0 * 31 + it1);
-            if (hcode >= 0 && hcode != code) hint = remap_hints(hint, hcode, code);
-            int k00, k01, k10, k11, j00, j01, j10, j11;
-            const double e00 = ega_node<DIG>(m.nodes, r00, x1, useg, (int)(hint & 0xffff),
-                                             (int)(djp & 0xff), &k00, &j00, &dig);
-            const double e01 = ega_node<DIG>(m.nodes, r01, x1, useg, (int)((hint >> 16) & 0xffff),
-                                             (int)((djp >> 8) & 0xff), &k01, &j01, &dig);
-            const double e10 = ega_node<DIG>(m.nodes, r10, x1, useg, (int)((hint >> 32) & 0xffff),
-                                             (int)((djp >> 16) & 0xff), &k10, &j10, &dig);
-            const double e11 = ega_node<DIG>(m.nodes, r11, x1, useg, (int)(hint >> 48),
-                                             (int)(djp >> 24), &k11, &j11, &dig);
-            hint = (unsigned long long)(j00 & 0xffff) | ((unsigned long long)(j01 & 0xffff) << 16) |
-                   ((unsigned long long)(j10 & 0xffff) << 32) | ((unsigned long long)(j11 & 0xffff) << 48);
-            hcode = code;
-            djp = (unsigned)min(j00 - k00, 255) | ((unsigned)min(j01 - k01, 255) << 8) |
-                  ((unsigned)min(j10 - k10, 255) << 16) | ((unsigned)min(j11 - k11, 255) << 24);
-            double ea = jsc_clamp01(jsc_lin(gt[ipr * TBLNTMAX + it0], e00,
-                                            gt[ipr * TBLNTMAX + it0 + 1], e01, T));
-            const double eb = jsc_clamp01(jsc_lin(gt[(ipr + 1) * TBLNTMAX + it1], e10,
-                                                  gt[(ipr + 1) * TBLNTMAX + it1 + 1], e11, T));
-            ea = jsc_clamp01(jsc_lin(gp[ipr], ea, gp[ipr + 1], eb, P));
-            eps = 1 - (1 - ea) / tp;
-            n_ega++;
-          }
-        }
-      }
-    }
-    tp = tp * (1 - eps);
+    const double DS = rec[REC_DS];
+    const double eps = ega_lane_eps<DIG>(m, A.single_grid, tb, g, rec, ps);
+    ps.tp = ps.tp * (1 - eps);
     // Segment transmittance: the product over emitters in emitter order,
     // as the reference accumulates it (lanes past ng hold eps = 0).
     // All GP factors are fetched first (independent shuffles), then
@@ -178,8 +233,8 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
   if (DIG) {
     // per-channel digest: fold of the per-emitter digests in emitter order
     unsigned long long dd = 0;
-    for (int j = 0; j < ng; j++) dd = dd * 1000003ull + __shfl_sync(gmask, dig, gbase + j);
-    dig = dd;
+    for (int j = 0; j < ng; j++) dd = dd * 1000003ull + __shfl_sync(gmask, ps.dig, gbase + j);
+    ps.dig = dd;
   }
   if (g == 0) {
     const double ts = A.tsurf[r];
@@ -189,11 +244,143 @@ __global__ void __launch_bounds__(BLK, MINB) ega_lane_kernel(EgaArgs A) {
     }
     A.rad[(size_t)r * nd + d] = rad;
     A.tau[(size_t)r * nd + d] = tau;
-    if (DIG) A.digest[(size_t)r * nd + d] = dig;
+    if (DIG) A.digest[(size_t)r * nd + d] = ps.dig;
   }
   const unsigned mask = __activemask();
-  const unsigned tot = __reduce_add_sync(mask, n_ega);
+  const unsigned tot = __reduce_add_sync(mask, ps.n_ega);
   if (lane == (unsigned)(__ffs(mask) - 1)) atomicAdd(&A.counters[1], (unsigned long long)tot);
+}
+
+// Warp-level barrier of the NT threads of a block (barrier 1): the emitter
+// warps and the transfer warp of ega_ray_kernel reach it from different
+// code paths, which a named barrier with an explicit count allows.
+__device__ __forceinline__ void ray_barrier(int nt) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+}
+
+// The EGA + radiative-transfer kernel with lanes over rays: a block takes
+// a tile of 32 rays (ordered so that rays of one profile and similar
+// geometry sit side by side) and one channel.  Warp g < NGW evaluates
+// emitter g's EGA for the tile's 32 rays at one LOS point after another,
+// so the lanes of a warp read the same (channel, emitter) table at nearby
+// (p, T) rows and intervals; warp NGW runs the radiative-transfer step one
+// point behind, from the emitters' transmittance factors in shared memory
+// (two buffers, one barrier per point), multiplying them in emitter order
+// as the reference does (src/forwardmodel.c:302-399).
+template <int NGW, bool DIG, int MINB>
+__global__ void __launch_bounds__(32 * (NGW + 1), MINB) ega_ray_kernel(EgaArgs A) {
+  constexpr int NT = 32 * (NGW + 1);
+  __shared__ double sf[2][NGW][32];
+  __shared__ unsigned long long sdig[DIG ? NGW : 1][32];
+  const jsc_dev_model &m = A.m;
+  const int nd = m.nd, ng = m.ng;
+  const int tile = (int)(blockIdx.x / (unsigned)nd);
+  const int d = (int)(blockIdx.x - (unsigned)tile * nd);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int slot = tile * 32 + lane;
+  const int r = slot < A.n_rays ? A.order[slot] : -1;
+  const int np = r >= 0 ? A.nlos[r] : 0;
+  int npmax = np;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) npmax = max(npmax, __shfl_xor_sync(0xffffffffu, npmax, o));
+  const int64_t off = r >= 0 ? A.los_off[r] : 0;
+
+  if (w < NGW) {
+    // emitter warp: the EGA of emitter w for the tile's rays
+    const EgaTable tb = ega_table(m, d, w);
+    EgaPath ps = ega_path_start();
+    const double *__restrict__ rec = A.pts + off * A.W;
+    for (int ip = 0; ip < npmax; ip++, rec += A.W) {
+      double f = 1;
+      if (ip < np) {
+        const double eps = ega_lane_eps<DIG>(m, A.single_grid, tb, w, rec, ps);
+        ps.tp = ps.tp * (1 - eps);
+        f = 1 - eps;
+      }
+      sf[ip & 1][w][lane] = f;
+      ray_barrier(NT);
+    }
+    if (DIG) sdig[w][lane] = ps.dig;
+    const unsigned tot = __reduce_add_sync(0xffffffffu, ps.n_ega);
+    if (lane == 0 && tot) atomicAdd(&A.counters[1], (unsigned long long)tot);
+    if (DIG) ray_barrier(NT);
+    return;
+  }
+
+  // transfer warp: the radiance of (ray, channel d) one point behind
+  double rad = 0, tau = 1;
+  const double *__restrict__ rec = A.pts + off * A.W;
+  const double *__restrict__ bc = A.beta_ctm + off * nd + d;
+  const double *__restrict__ sp = A.src_pl + off * nd + d;
+  const double *__restrict__ ssrc =
+      (A.src_sca && r >= 0) ? A.src_sca + (size_t)A.sp_off[r] * nd + d : nullptr;
+  for (int ip = 0; ip < npmax; ip++) {
+    ray_barrier(NT);  // the factors of point ip are in sf[ip & 1]
+    if (ip >= np) continue;
+    double tau_gas = sf[ip & 1][0][lane];
+    for (int j = 1; j < ng; j++) tau_gas *= sf[ip & 1][j][lane];
+    const double DS = rec[REC_DS];
+    const double beta = *bc, src = *sp;
+    const double af = rec[REC_AF];
+    if (ssrc && af > 0) {
+      // scattering point (src/forwardmodel.c:317-363)
+      if (tau_gas > 0) {
+        const int ia = (int)rec[REC_AI];
+        const double be = A.beta[ia * nd + d], bs = A.beta[A.aero_nl * nd + ia * nd + d];
+        const double bext = (-1.) * log(tau_gas) / DS + beta + af * be;
+        const double e = 1 - exp(-1 * bext * DS);
+        const double src_all = ((bext - af * bs) * src + af * bs * *ssrc) / bext;
+        rad += tau * e * src_all;
+        tau *= exp(-1. * bext * DS);
+      }
+      ssrc += nd;
+    } else if (tau_gas > 0) {
+      // clear air, or aerosol/cloud extinction (src/forwardmodel.c:365-389)
+      double e;
+      if (A.cfg.sca_n == 0 || af == 0) {
+        e = 1 - tau_gas * exp(-1. * beta * DS);
+      } else {
+        const int ia = (int)rec[REC_AI];
+        const double bx = A.beta[(A.cfg.sca_ext_beta_a ? 2 : 0) * A.aero_nl * nd + ia * nd + d];
+        e = 1 - tau_gas * exp(-1. * (beta + af * bx) * DS);
+      }
+      rad += src * e * tau;
+      tau *= (1 - e);
+    }
+    rec += A.W;
+    bc += nd;
+    sp += nd;
+  }
+  if (DIG) ray_barrier(NT);  // the emitter warps' digests are in sdig
+  if (r < 0) return;
+  const double ts = A.tsurf[r];
+  if (ts > 0) {
+    const int its = planck_index(ts);
+    rad += planck_src(m, d, its, ts) * tau;
+  }
+  A.rad[(size_t)r * nd + d] = rad;
+  A.tau[(size_t)r * nd + d] = tau;
+  if (DIG) {
+    // per-channel digest: fold of the per-emitter digests in emitter order
+    unsigned long long dd = 0;
+    for (int j = 0; j < ng; j++) dd = dd * 1000003ull + sdig[j][lane];
+    A.digest[(size_t)r * nd + d] = dd;
+  }
+}
+
+// Ray-tile variants: (warps over emitters, minimum resident blocks per SM).
+template <int NGW, bool DIG>
+static void ega_ray_launch(const EgaArgs &ea, int v, cudaStream_t s) {
+  const unsigned blocks = (unsigned)(((int64_t)ea.n_rays + 31) / 32 * ea.m.nd);
+  constexpr int NT = 32 * (NGW + 1);
+  if (v == 1) ega_ray_kernel<NGW, DIG, 4><<<blocks, NT, 0, s>>>(ea);
+  else ega_ray_kernel<NGW, DIG, 3><<<blocks, NT, 0, s>>>(ea);
+}
+
+template <int NGW>
+static void ega_ray_variant(const EgaArgs &ea, int v, bool dig, cudaStream_t s) {
+  if (dig) ega_ray_launch<NGW, true>(ea, v, s);
+  else ega_ray_launch<NGW, false>(ea, v, s);
 }
 
 // Launch variants of ega_lane_kernel: (threads per block, minimum resident
@@ -221,4 +408,12 @@ static void ega_lane_variant(const EgaArgs &ea, int v, bool dig, cudaStream_t s)
 void jsc_ega_lane_launch_s(const EgaArgs &ea, int v, bool dig, cudaStream_t s);
 void jsc_ega_lane_launch_l(const EgaArgs &ea, int v, bool dig, cudaStream_t s);
 void jsc_ctm_src_launch(const CtmArgs &ca, cudaStream_t s);
+// Ray-tile kernel (ega_ray.cu) for up to 16 emitters, and the ray order it
+// reads (sorted keys: profile, surface hit, LOS point count, tangent
+// altitude).
+void jsc_ega_ray_launch(const EgaArgs &ea, int v, bool dig, cudaStream_t s);
+int jsc_ray_order(int n_rays, const int *ray_atm, const int *nlos, const double *tsurf,
+                  const double *tpz, unsigned long long *keys, int *order, void *tmp,
+                  size_t tmp_bytes, cudaStream_t s);
+size_t jsc_ray_order_tmp_bytes(int max_rays);
 #define JSC_LANE_VARIANTS 5

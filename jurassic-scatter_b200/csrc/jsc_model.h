@@ -61,6 +61,9 @@ struct EgaArgs {
   // Continuum extinction and Planck source per (LOS point, channel),
   // [n_points][nd] (read by the lane kernel).
   const double *beta_ctm, *src_pl;
+  // Ray order of the ray-tile kernel: tile t holds rays order[32 t ..
+  // 32 t + 31] (rays of one profile and similar geometry side by side).
+  const int *order;
 };
 
 // Kernel timers of a batch.
@@ -173,6 +176,10 @@ struct jsc_batch {
   int64_t n_points;         // LOS points of the current run
   double *d_tsurf;          // [max_rays]
   double *d_tp;             // [3][max_rays]
+  unsigned long long *d_rkeys;  // [2][max_rays] ray sort keys (ray-tile EGA variants)
+  int *d_rorder;                // [2][max_rays] ray order of the tiles
+  void *d_rtmp;                 // sort scratch
+  size_t rtmp_bytes;
 
   // Outputs and status.
   double *d_rad, *d_tau;    // [max_rays][nd]

@@ -124,8 +124,8 @@ def test_curtain_aerosol_extinction(workdir, ip):
 
 # EGA kernel families: -1 the default (variant 6 for clear air, 10 with
 # aerosol/cloud layers), 6 a thread per (ray, channel), 9 a lane per (ray,
-# channel, emitter)
-VARIANTS = [-1, 6, 9]
+# channel, emitter), 14 lanes over a tile of rays with a warp per emitter
+VARIANTS = [-1, 6, 9, 14]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
@@ -267,8 +267,9 @@ def _aero_for(aero, g, nus):
 
 
 # Every launch variant the autotuner can pick: 0-8 a thread per (ray,
-# channel), 9-13 a lane per (ray, channel, emitter).
-ALL_VARIANTS = list(range(14))
+# channel), 9-13 a lane per (ray, channel, emitter), 14-15 lanes over a
+# tile of rays with a warp per emitter.
+ALL_VARIANTS = list(range(16))
 
 
 @pytest.fixture(scope="module", params=["headline_batch", "continuum_bands"])
