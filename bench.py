@@ -58,7 +58,7 @@ def parse():
                     help="rays of the depth-2 scattering workload; 0 skips it")
     ap.add_argument("--ms-train-rays", type=int, default=3_000,
                     help="rays of the depth-2 surrogate's training batch")
-    ap.add_argument("--ms-epochs", type=int, default=300,
+    ap.add_argument("--ms-epochs", type=int, default=500,
                     help="training epochs of the depth-2 surrogate")
     ap.add_argument("--ms-plain-rays", type=int, default=1_000,
                     help="rays of the depth-2 workload timed on the plain path (its first ones)")
@@ -148,10 +148,42 @@ def make_workload(n_rays, seed_offset=0):
 
 
 # ncu dram__bytes (read + write) per EGA evaluation of one 20k-ray launch of
-# this workload (1.8536e9 evaluations), per kernel family: a thread per
-# (ray, channel) (variant 6: 194.5 + 74.3 GB) and a lane per (ray,
-# channel, emitter) (variant 13: 27.8 + 0.6 GB)
-TRAFFIC_PER_EGA = {"thread": 268.8e9 / 1.8536e9, "lane": 28.4e9 / 1.8536e9}
+# this workload (1.8536e9 evaluations), per kernel family, with the digest
+# of the kernel sources the capture was taken with (kernel_sources_sha).  A
+# capture describes the kernel only while those sources are unchanged; for
+# any other source the line reports traffic null.  Families: a thread per
+# (ray, channel) (variants 0-8), a lane per (ray, channel, emitter) (9-13),
+# lanes over a tile of 32 rays (14-20).
+TRAFFIC_PER_EGA = {}
+KERNEL_SOURCES = {
+    "thread": ["ega_kernel.cuh", "device_common.cuh"],
+    "lane": ["ega_lane.cuh", "device_common.cuh"],
+    "ray": ["ega_lane.cuh", "device_common.cuh"],
+}
+
+
+def kernel_family(variant):
+    return "thread" if variant < 9 else ("lane" if variant < 14 else "ray")
+
+
+def kernel_sources_sha(family):
+    """First 16 hex digits of the sha256 of the kernel family's sources."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in KERNEL_SOURCES[family]:
+        with open(os.path.join(REPO, "jurassic-scatter_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def dram_traffic(variant, n_ega):
+    """DRAM bytes per launch from the family's capture, scaled by the EGA
+    evaluations, or None (no capture of the current sources)."""
+    fam = kernel_family(variant)
+    cap = TRAFFIC_PER_EGA.get(fam)
+    if cap is None or cap[1] != kernel_sources_sha(fam):
+        return None
+    return cap[0] * n_ega
 
 
 def algorithmic_bytes(n_ega, n_points, n_rays, nd, ng):
@@ -1145,8 +1177,7 @@ def main():
     achieved = B / (ega / 1e3) / 1e9
     # DRAM bytes per launch: the captured bytes per EGA evaluation of the
     # chosen kernel family, scaled by the EGA evaluations here
-    family = "lane" if tuned.get("variant", 0) >= 9 else "thread"
-    traffic = TRAFFIC_PER_EGA[family] * n_ega
+    traffic = dram_traffic(tuned.get("variant", 0), n_ega)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,

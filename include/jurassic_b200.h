@@ -540,11 +540,13 @@ int jsc_batch_graph_capture(jsc_batch *b, const jsc_batch_input *in,
                             const jsc_batch_output *out, void *stream);
 int jsc_batch_graph_launch(jsc_batch *b, void *stream);
 
-/* Select the EGA launch variant by hand (-1: the default, variant 6 for
- * clear air and 10 for runs with aerosol/cloud layers).  Variants 0-8
+/* Select the EGA launch variant by hand (-1: the default, variant 17, or
+ * the lane variant 13 above 16 emitters).  Variants 0-8
  * run a thread per (ray, channel) with every emitter's path state; 9-13 a
- * lane per (ray, channel, emitter) after a separate continuum/Planck pass.
- * All variants compute the same operations in the same order. */
+ * lane per (ray, channel, emitter) after a separate continuum/Planck pass;
+ * 14-20 (up to 16 emitters) lanes over a tile of 32 rays sorted by
+ * geometry, a warp per emitter, after the same pass.  All variants compute
+ * the same operations in the same order. */
 int jsc_batch_set_variant(jsc_batch *b, int variant);
 double jsc_batch_variant_ms(const jsc_batch *b, int variant);
 

@@ -557,17 +557,23 @@ extern "C" int jsc_scan_selftest(int device, int n, unsigned budget, int stall) 
 // number sets the register budget, i.e. the trade between occupancy and
 // spills, the rolled loop trades registers and instruction-cache footprint
 // for local-memory path state.  9-13: ega_lane_kernel, a lane per
-// (ray, channel, emitter), after ctm_src_kernel.  14-15: ega_ray_kernel,
-// lanes over a tile of 32 ordered rays, a warp per emitter (block size
-// 32 (emitter warps + 1); blk 0 here), after ctm_src_kernel; more than 16
-// emitters run the lane variant 13 instead.  jsc_batch_autotune picks one.
+// (ray, channel, emitter), after ctm_src_kernel.  14-20: lanes over a
+// tile of 32 ordered rays, a warp per emitter, after ctm_src_kernel
+// (blk 0 here: the block size follows the emitter count); ray 1:
+// ega_ray_kernel with a transfer warp (block 32 (emitter warps + 1)),
+// ray 2: ega_ray_rot_kernel, the emitter warps take the transfer step in
+// turn (block 32 emitter warps); 16 and 19-20 order the blocks
+// channel-major.  More than 16 emitters run the lane variant 13 instead.
+// jsc_batch_autotune picks one.
 struct EgaVariant { int blk, minb, roll, lane, ray; };
 static const EgaVariant kEgaVariants[] = {
     {128, 4, 0, 0, 0}, {128, 6, 0, 0, 0}, {128, 8, 0, 0, 0}, {256, 3, 0, 0, 0},
     {256, 4, 0, 0, 0}, {128, 8, 1, 0, 0}, {128, 12, 1, 0, 0}, {256, 4, 1, 0, 0},
     {256, 6, 1, 0, 0}, {128, 12, 0, 1, 0}, {128, 8, 0, 1, 0}, {256, 4, 0, 1, 0},
-    {256, 5, 0, 1, 0}, {512, 2, 0, 1, 0}, {0, 3, 0, 1, 1}, {0, 4, 0, 1, 1}};
-static const int kNumEgaVariants = 16;
+    {256, 5, 0, 1, 0}, {512, 2, 0, 1, 0}, {0, 3, 0, 1, 1}, {0, 4, 0, 1, 1},
+    {0, 4, 0, 1, 1},   {0, 4, 0, 1, 2},   {0, 5, 0, 1, 2}, {0, 4, 0, 1, 2},
+    {0, 5, 0, 1, 2}};
+static const int kNumEgaVariants = 21;
 static_assert(kNumEgaVariants <= 32, "ega_variant_ms holds 32 timings");
 static const int kLaneBase = 9;
 static const int kRayBase = 14;
@@ -576,14 +582,17 @@ static const int kRayBase = 14;
 static int ray_warps(int ng) {
   return ng <= 2 ? 2 : ng <= 4 ? 4 : ng <= 8 ? 8 : ng <= 16 ? 16 : 0;
 }
-static const int kEgaDefault = JSC_EGA_DEFAULT_VARIANT;  // default of clear-air runs
+// Default launch variant of clear-air runs: the ray-tile kernel with the
+// transfer step taken in turn (422 ms against 631 ms for the fastest lane
+// variant and 716 ms for the thread-per-channel variant 6 on 100k rays,
+// 8 emitters, 64 channels).
+static const int kEgaDefault = 17;
 
 // Default launch variant of runs with aerosol/cloud layers (the scattering
-// path and its child batches): the lane family, 10 % faster than the
-// clear-air default on the single-scattering workload (640 vs 715 ms for
-// 2000 limb rays, 16 channels, 2 emitters).  Clear-air runs keep
-// kEgaDefault.
-static const int kScatterDefault = 10;
+// path and its child batches): the same ray-tile kernel (819 ms per plain
+// single-scattering step of 4000 limb rays, 16 channels, 2 emitters,
+// against 847 ms for the lane variant 10).
+static const int kScatterDefault = 17;
 
 // The variant a run of b launches (-1 resolves to the default for its
 // configuration).
@@ -723,7 +732,10 @@ static __global__ void status_or_kernel(unsigned *dst, const unsigned *src) { *d
 // of this batch's scattering points, with room for max_rays rays.
 static int ensure_child(jsc_batch *b, jsc_batch **pc, int max_rays, int depth, int los_per_ray = 128) {
   jsc_batch *c = *pc;
-  if (c && c->max_rays >= max_rays && c->max_seg >= (int64_t)max_rays * los_per_ray) return JSC_OK;
+  if (c && c->max_rays >= max_rays && c->max_seg >= (int64_t)max_rays * los_per_ray) {
+    c->ega_variant = b->ega_variant;  // the parent's current launch variant
+    return JSC_OK;
+  }
   jsc_batch_destroy(c);
   *pc = nullptr;
   int st = jsc_batch_create(b->m, b->ctl, b->max_atm, b->max_levels, max_rays,
@@ -1859,8 +1871,10 @@ extern "C" int jsc_batch_variant(const jsc_batch *b, int *variant, int *blk, int
   const int v = run_variant(b);
   if (variant) *variant = v;
   const int rw = kEgaVariants[v].ray ? ray_warps(b->m->ng) : 0;
-  if (blk) *blk = kEgaVariants[v].ray ? (rw ? 32 * (rw + 1) : kEgaVariants[kLaneBase + 4].blk)
-                                      : kEgaVariants[v].blk;
+  if (blk)
+    *blk = kEgaVariants[v].ray
+               ? (rw ? 32 * (rw + (kEgaVariants[v].ray == 1)) : kEgaVariants[kLaneBase + 4].blk)
+               : kEgaVariants[v].blk;
   if (minb) *minb = kEgaVariants[v].ray && !rw ? kEgaVariants[kLaneBase + 4].minb
                                                : kEgaVariants[v].minb;
   return JSC_OK;

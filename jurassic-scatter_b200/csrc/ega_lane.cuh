@@ -258,6 +258,60 @@ __device__ __forceinline__ void ray_barrier(int nt) {
   asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
 }
 
+// Radiative-transfer step of one (ray, channel) at one LOS point rec, from
+// the point's gas transmittance (the emitters' factors multiplied in
+// emitter order), its continuum extinction beta and Planck source src
+// (src/forwardmodel.c:302-399); ssrc walks the ray's scattering sources.
+__device__ __forceinline__ void rt_point(const EgaArgs &A, int d, int nd,
+                                         const double *__restrict__ rec, double tau_gas,
+                                         double beta, double src,
+                                         const double *__restrict__ &ssrc, double &rad,
+                                         double &tau) {
+  const double DS = rec[REC_DS];
+  const double af = rec[REC_AF];
+  if (ssrc && af > 0) {
+    // scattering point (src/forwardmodel.c:317-363)
+    if (tau_gas > 0) {
+      const int ia = (int)rec[REC_AI];
+      const double be = A.beta[ia * nd + d], bs = A.beta[A.aero_nl * nd + ia * nd + d];
+      const double bext = (-1.) * log(tau_gas) / DS + beta + af * be;
+      const double e = 1 - exp(-1 * bext * DS);
+      const double src_all = ((bext - af * bs) * src + af * bs * *ssrc) / bext;
+      rad += tau * e * src_all;
+      tau *= exp(-1. * bext * DS);
+    }
+    ssrc += nd;
+  } else if (tau_gas > 0) {
+    // clear air, or aerosol/cloud extinction (src/forwardmodel.c:365-389)
+    double e;
+    if (A.cfg.sca_n == 0 || af == 0) {
+      e = 1 - tau_gas * exp(-1. * beta * DS);
+    } else {
+      const int ia = (int)rec[REC_AI];
+      const double bx = A.beta[(A.cfg.sca_ext_beta_a ? 2 : 0) * A.aero_nl * nd + ia * nd + d];
+      e = 1 - tau_gas * exp(-1. * (beta + af * bx) * DS);
+    }
+    rad += src * e * tau;
+    tau *= (1 - e);
+  }
+}
+
+// Tile and channel of a ray-tile block: tile-major (ORD 0, the blocks of
+// one tile side by side) or channel-major (ORD 1, the blocks of one
+// channel side by side, so that the blocks resident at a time read the
+// tables of few channels).
+template <int ORD>
+__device__ __forceinline__ void ray_block(int n_rays, int nd, int *tile, int *d) {
+  if (ORD == 0) {
+    *tile = (int)(blockIdx.x / (unsigned)nd);
+    *d = (int)(blockIdx.x - (unsigned)*tile * nd);
+  } else {
+    const unsigned nt = (unsigned)((n_rays + 31) / 32);
+    *d = (int)(blockIdx.x / nt);
+    *tile = (int)(blockIdx.x - (unsigned)*d * nt);
+  }
+}
+
 // The EGA + radiative-transfer kernel with lanes over rays: a block takes
 // a tile of 32 rays (ordered so that rays of one profile and similar
 // geometry sit side by side) and one channel.  Warp g < NGW evaluates
@@ -267,19 +321,21 @@ __device__ __forceinline__ void ray_barrier(int nt) {
 // point behind, from the emitters' transmittance factors in shared memory
 // (two buffers, one barrier per point), multiplying them in emitter order
 // as the reference does (src/forwardmodel.c:302-399).
-template <int NGW, bool DIG, int MINB>
+template <int NGW, bool DIG, int MINB, int ORD>
 __global__ void __launch_bounds__(32 * (NGW + 1), MINB) ega_ray_kernel(EgaArgs A) {
   constexpr int NT = 32 * (NGW + 1);
   __shared__ double sf[2][NGW][32];
   __shared__ unsigned long long sdig[DIG ? NGW : 1][32];
   const jsc_dev_model &m = A.m;
   const int nd = m.nd, ng = m.ng;
-  const int tile = (int)(blockIdx.x / (unsigned)nd);
-  const int d = (int)(blockIdx.x - (unsigned)tile * nd);
+  int tile, d;
+  ray_block<ORD>(A.n_rays, nd, &tile, &d);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int slot = tile * 32 + lane;
   const int r = slot < A.n_rays ? A.order[slot] : -1;
   const int np = r >= 0 ? A.nlos[r] : 0;
+  // every warp of the block computes the same npmax, so every warp takes
+  // the same number of barriers
   int npmax = np;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) npmax = max(npmax, __shfl_xor_sync(0xffffffffu, npmax, o));
@@ -319,34 +375,7 @@ __global__ void __launch_bounds__(32 * (NGW + 1), MINB) ega_ray_kernel(EgaArgs A
     if (ip >= np) continue;
     double tau_gas = sf[ip & 1][0][lane];
     for (int j = 1; j < ng; j++) tau_gas *= sf[ip & 1][j][lane];
-    const double DS = rec[REC_DS];
-    const double beta = *bc, src = *sp;
-    const double af = rec[REC_AF];
-    if (ssrc && af > 0) {
-      // scattering point (src/forwardmodel.c:317-363)
-      if (tau_gas > 0) {
-        const int ia = (int)rec[REC_AI];
-        const double be = A.beta[ia * nd + d], bs = A.beta[A.aero_nl * nd + ia * nd + d];
-        const double bext = (-1.) * log(tau_gas) / DS + beta + af * be;
-        const double e = 1 - exp(-1 * bext * DS);
-        const double src_all = ((bext - af * bs) * src + af * bs * *ssrc) / bext;
-        rad += tau * e * src_all;
-        tau *= exp(-1. * bext * DS);
-      }
-      ssrc += nd;
-    } else if (tau_gas > 0) {
-      // clear air, or aerosol/cloud extinction (src/forwardmodel.c:365-389)
-      double e;
-      if (A.cfg.sca_n == 0 || af == 0) {
-        e = 1 - tau_gas * exp(-1. * beta * DS);
-      } else {
-        const int ia = (int)rec[REC_AI];
-        const double bx = A.beta[(A.cfg.sca_ext_beta_a ? 2 : 0) * A.aero_nl * nd + ia * nd + d];
-        e = 1 - tau_gas * exp(-1. * (beta + af * bx) * DS);
-      }
-      rad += src * e * tau;
-      tau *= (1 - e);
-    }
+    rt_point(A, d, nd, rec, tau_gas, *bc, *sp, ssrc, rad, tau);
     rec += A.W;
     bc += nd;
     sp += nd;
@@ -368,13 +397,118 @@ __global__ void __launch_bounds__(32 * (NGW + 1), MINB) ega_ray_kernel(EgaArgs A
   }
 }
 
-// Ray-tile variants: (warps over emitters, minimum resident blocks per SM).
+// The same tile of 32 rays and one channel without a transfer warp: the
+// NGW emitter warps take the radiative-transfer step in turn, warp
+// ip mod NGW at LOS point ip right after the point's barrier, with the
+// running radiance, transmittance and scattering-source position of the
+// tile's rays in shared memory.  The next point's barrier orders one step
+// after the other (the warp of step ip reaches barrier ip + 1 only after
+// it), and the factor buffer of point ip is rewritten only after barrier
+// ip + 1.  Every register of the block goes to EGA warps.
+template <int NGW, bool DIG, int MINB, int ORD>
+__global__ void __launch_bounds__(32 * NGW, MINB) ega_ray_rot_kernel(EgaArgs A) {
+  constexpr int NT = 32 * NGW;
+  __shared__ double sf[2][NGW][32];
+  __shared__ double srad[32], stau[32];
+  __shared__ int ssca[32];
+  __shared__ unsigned long long sdig[DIG ? NGW : 1][32];
+  const jsc_dev_model &m = A.m;
+  const int nd = m.nd, ng = m.ng;
+  int tile, d;
+  ray_block<ORD>(A.n_rays, nd, &tile, &d);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int slot = tile * 32 + lane;
+  const int r = slot < A.n_rays ? A.order[slot] : -1;
+  const int np = r >= 0 ? A.nlos[r] : 0;
+  int npmax = np;  // the same in every warp: every warp takes npmax + 1 barriers
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) npmax = max(npmax, __shfl_xor_sync(0xffffffffu, npmax, o));
+  const int64_t off = r >= 0 ? A.los_off[r] : 0;
+  if (w == 0) {
+    srad[lane] = 0;
+    stau[lane] = 1;
+    ssca[lane] = 0;
+  }
+  const EgaTable tb = ega_table(m, d, w);
+  EgaPath ps = ega_path_start();
+  const double *__restrict__ rec = A.pts + off * A.W;
+  const bool sca = A.src_sca && r >= 0;
+  int turn = 0;  // ip mod NGW
+  for (int ip = 0; ip < npmax; ip++, rec += A.W) {
+    double f = 1;
+    if (ip < np) {
+      const double eps = ega_lane_eps<DIG>(m, A.single_grid, tb, w, rec, ps);
+      ps.tp = ps.tp * (1 - eps);
+      f = 1 - eps;
+    }
+    sf[ip & 1][w][lane] = f;
+    ray_barrier(NT);  // the factors of point ip are in sf[ip & 1]
+    if (w == turn && ip < np) {
+      double tau_gas = sf[ip & 1][0][lane];
+      for (int j = 1; j < ng; j++) tau_gas *= sf[ip & 1][j][lane];
+      double rad = srad[lane], tau = stau[lane];
+      const int isp = ssca[lane];
+      const double *__restrict__ ssrc =
+          sca ? A.src_sca + ((size_t)A.sp_off[r] + isp) * nd + d : nullptr;
+      const double *__restrict__ s0 = ssrc;
+      const size_t pc = (size_t)(off + ip) * nd + d;
+      rt_point(A, d, nd, rec, tau_gas, A.beta_ctm[pc], A.src_pl[pc], ssrc, rad, tau);
+      srad[lane] = rad;
+      stau[lane] = tau;
+      if (ssrc != s0) ssca[lane] = isp + 1;
+    }
+    turn = turn + 1 == NGW ? 0 : turn + 1;
+  }
+  if (DIG) sdig[w][lane] = ps.dig;
+  const unsigned tot = __reduce_add_sync(0xffffffffu, ps.n_ega);
+  if (lane == 0 && tot) atomicAdd(&A.counters[1], (unsigned long long)tot);
+  ray_barrier(NT);  // the last step and the digests are in shared memory
+  if (w != 0 || r < 0) return;
+  double rad = srad[lane];
+  const double tau = stau[lane];
+  const double ts = A.tsurf[r];
+  if (ts > 0) {
+    const int its = planck_index(ts);
+    rad += planck_src(m, d, its, ts) * tau;
+  }
+  A.rad[(size_t)r * nd + d] = rad;
+  A.tau[(size_t)r * nd + d] = tau;
+  if (DIG) {
+    unsigned long long dd = 0;
+    for (int j = 0; j < ng; j++) dd = dd * 1000003ull + sdig[j][lane];
+    A.digest[(size_t)r * nd + d] = dd;
+  }
+}
+
+// Ray-tile variants v: 0-2 with a transfer warp, (resident blocks per SM
+// at 8 emitters, block order) = (3, tile-major), (4, tile-major), (4,
+// channel-major); 3-6 with the step taken in turn: (4, tile), (5, tile),
+// (4, channel), (5, channel).  Other emitter counts keep the threads per
+// SM of 8 emitters, i.e. the register budget per thread.
+template <int NGW, bool DIG, int MINB8, int ORD>
+static void ega_ray_tr(const EgaArgs &ea, unsigned blocks, cudaStream_t s) {
+  constexpr int MB = MINB8 * 9 / (NGW + 1) > 1 ? MINB8 * 9 / (NGW + 1) : 1;
+  ega_ray_kernel<NGW, DIG, MB, ORD><<<blocks, 32 * (NGW + 1), 0, s>>>(ea);
+}
+
+template <int NGW, bool DIG, int MINB8, int ORD>
+static void ega_ray_rot(const EgaArgs &ea, unsigned blocks, cudaStream_t s) {
+  constexpr int MB = MINB8 * 8 / NGW > 1 ? MINB8 * 8 / NGW : 1;
+  ega_ray_rot_kernel<NGW, DIG, MB, ORD><<<blocks, 32 * NGW, 0, s>>>(ea);
+}
+
 template <int NGW, bool DIG>
 static void ega_ray_launch(const EgaArgs &ea, int v, cudaStream_t s) {
   const unsigned blocks = (unsigned)(((int64_t)ea.n_rays + 31) / 32 * ea.m.nd);
-  constexpr int NT = 32 * (NGW + 1);
-  if (v == 1) ega_ray_kernel<NGW, DIG, 4><<<blocks, NT, 0, s>>>(ea);
-  else ega_ray_kernel<NGW, DIG, 3><<<blocks, NT, 0, s>>>(ea);
+  switch (v) {
+    case 0: ega_ray_tr<NGW, DIG, 3, 0>(ea, blocks, s); break;
+    case 1: ega_ray_tr<NGW, DIG, 4, 0>(ea, blocks, s); break;
+    case 2: ega_ray_tr<NGW, DIG, 4, 1>(ea, blocks, s); break;
+    case 3: ega_ray_rot<NGW, DIG, 4, 0>(ea, blocks, s); break;
+    case 4: ega_ray_rot<NGW, DIG, 5, 0>(ea, blocks, s); break;
+    case 5: ega_ray_rot<NGW, DIG, 4, 1>(ea, blocks, s); break;
+    default: ega_ray_rot<NGW, DIG, 5, 1>(ea, blocks, s); break;
+  }
 }
 
 template <int NGW>

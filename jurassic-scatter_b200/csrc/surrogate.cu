@@ -70,8 +70,9 @@ static __global__ void sur_features_kernel(int n, const double *sp, float *feat)
 // C[M][N] (ldc) = op(A) op(B) (+ bias[n]) with op(A)(m,k) = TA ? A[k*lda+m]
 // : A[m*lda+k] and op(B)(k,n) = TB ? B[n*ldb+k] : B[k*ldb+n].  256 threads,
 // a 64 x 64 tile per block, 4 x 4 outputs per thread.  With gridDim.z > 1
-// the K range is split over blockIdx.z and the partial products are added
-// atomically into C (zeroed by the caller; no bias).
+// the K range is split over blockIdx.z and block z writes its partial
+// product to the slice C + z M ldc (no bias); ksum_kernel adds the slices
+// in order, so training is deterministic.
 template <bool TA, bool TB>
 static __global__ void __launch_bounds__(256)
 sgemm_kernel(int M, int N, int K, const float *A, int lda, const float *B, int ldb, float *C,
@@ -116,19 +117,39 @@ sgemm_kernel(int M, int N, int K, const float *A, int lda, const float *B, int l
     for (int j = 0; j < 4; j++) {
       const int m = m0 + ty * 4 + i, n = n0 + tx * 4 + j;
       if (m < M && n < N) {
-        if (gridDim.z > 1) atomicAdd(&C[(size_t)m * ldc + n], acc[i][j]);
+        if (gridDim.z > 1) C[((size_t)blockIdx.z * M + m) * ldc + n] = acc[i][j];
         else C[(size_t)m * ldc + n] = acc[i][j] + (bias ? bias[n] : 0.f);
       }
     }
 }
 
-// ksplit > 1: split-K (C zeroed here, bias ignored) for products with a
-// long K and a small output (the weight gradients: K = batch).
+// C[i] = sum over z = 0 .. nz-1, in that order, of ws[z mn + i].
+static __global__ void ksum_kernel(int64_t mn, int nz, const float *ws, float *c) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= mn) return;
+  float t = 0;
+  for (int z = 0; z < nz; z++) t += ws[(size_t)z * mn + i];
+  c[i] = t;
+}
+
+// Most K slices of a split product (sizes the workspace).
+#define SUR_KSPLIT_MAX 64
+
+// ksplit > 1: split-K for products with a long K and a small output (the
+// weight gradients: K = batch), partial products in ws (ksplit M ldc
+// floats, ksplit <= SUR_KSPLIT_MAX), bias ignored.
 template <bool TA, bool TB>
 static void sgemm(int M, int N, int K, const float *A, int lda, const float *B, int ldb, float *C,
-                  int ldc, const float *bias, cudaStream_t s, int ksplit = 1) {
-  dim3 grid((N + TG_N - 1) / TG_N, (M + TG_M - 1) / TG_M, ksplit);
-  if (ksplit > 1) cudaMemsetAsync(C, 0, (size_t)M * ldc * sizeof(float), s);
+                  int ldc, const float *bias, cudaStream_t s, int ksplit = 1,
+                  float *ws = nullptr) {
+  if (ksplit > 1 && ws) {
+    dim3 grid((N + TG_N - 1) / TG_N, (M + TG_M - 1) / TG_M, ksplit);
+    sgemm_kernel<TA, TB><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, ws, ldc, nullptr);
+    const int64_t mn = (int64_t)M * ldc;
+    ksum_kernel<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(mn, ksplit, ws, C);
+    return;
+  }
+  dim3 grid((N + TG_N - 1) / TG_N, (M + TG_M - 1) / TG_M, 1);
   sgemm_kernel<TA, TB><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc, bias);
 }
 
@@ -407,6 +428,7 @@ struct jsc_surrogate {
   float *d_h[5];            // activations per layer, [max_batch][width]
   float *d_dh[2];           // two ping-pong gradient buffers [max_batch][SUR_W]
   float *d_xb, *d_tb, *d_part;
+  float *d_ksum;            // split-K partial products of the weight gradients
   int *d_idx;               // [max_batch] (gradient checks)
   int *d_perm;              // [n_train] per-epoch permutation
   float *d_X, *d_T;         // device copy of the training set
@@ -426,8 +448,9 @@ static void free_train(jsc_surrogate *s) {
   // d_xb is the first activation buffer d_h[0], freed above
   cudaFree(s->d_tb);
   cudaFree(s->d_part);
+  cudaFree(s->d_ksum);
   cudaFree(s->d_idx);
-  s->d_xb = s->d_tb = s->d_part = nullptr;
+  s->d_xb = s->d_tb = s->d_part = s->d_ksum = nullptr;
   s->d_idx = nullptr;
   s->max_batch = 0;
 }
@@ -586,6 +609,8 @@ static int ensure_train(jsc_surrogate *s, int batch) {
   st = st ? st : jsc_dmalloc(&s->d_tb, (size_t)batch * s->nout);
   st = st ? st : jsc_dmalloc(&s->d_part, (size_t)(batch * SUR_NOUT_MAX + 255) / 256 + 1);
   st = st ? st : jsc_dmalloc(&s->d_idx, (size_t)batch);
+  st = st ? st : jsc_dmalloc(&s->d_ksum, (size_t)SUR_KSPLIT_MAX * SUR_W *
+                                             (SUR_NOUT_MAX > SUR_W ? SUR_NOUT_MAX : SUR_W));
   if (st) {
     free_train(s);
     return st;
@@ -617,8 +642,9 @@ static int forward_backward(jsc_surrogate *s, int n, cudaStream_t st, float *los
     const int tiles = ((s->out[l] + TG_M - 1) / TG_M) * ((s->in[l] + TG_N - 1) / TG_N);
     int ksplit = 296 / tiles;  // about two blocks per SM
     if (ksplit > n / 64) ksplit = n / 64 > 0 ? n / 64 : 1;
+    if (ksplit > SUR_KSPLIT_MAX) ksplit = SUR_KSPLIT_MAX;
     sgemm<true, false>(s->out[l], s->in[l], n, dcur, s->out[l], s->d_h[l], s->in[l],
-                       s->d_g[l][0], s->in[l], nullptr, st, ksplit > 1 ? ksplit : 1);
+                       s->d_g[l][0], s->in[l], nullptr, st, ksplit > 1 ? ksplit : 1, s->d_ksum);
     colsum_kernel<<<(s->out[l] + 31) / 32, 256, 0, st>>>(n, s->out[l], dcur, s->d_g[l][1]);
     if (l > 0) {
       // dH_l = dZ W_l, then dZ_{l-1} = dH_l (1 - H_l^2)

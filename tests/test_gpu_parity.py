@@ -122,9 +122,10 @@ def test_curtain_aerosol_extinction(workdir, ip):
     assert max_rel(S.arr(obs.tau)[:nd, :nr].T, g["tau"]) <= REL_TOL
 
 
-# EGA kernel families: -1 the default (variant 6 for clear air, 10 with
-# aerosol/cloud layers), 6 a thread per (ray, channel), 9 a lane per (ray,
-# channel, emitter), 14 lanes over a tile of rays with a warp per emitter
+# EGA kernel families: -1 the default (variant 17, lanes over a tile of
+# rays with the transfer step taken in turn by the emitter warps), 6 a
+# thread per (ray, channel), 9 a lane per (ray, channel, emitter), 14 lanes
+# over a tile of rays with a transfer warp
 VARIANTS = [-1, 6, 9, 14]
 
 
@@ -267,9 +268,10 @@ def _aero_for(aero, g, nus):
 
 
 # Every launch variant the autotuner can pick: 0-8 a thread per (ray,
-# channel), 9-13 a lane per (ray, channel, emitter), 14-15 lanes over a
-# tile of rays with a warp per emitter.
-ALL_VARIANTS = list(range(16))
+# channel), 9-13 a lane per (ray, channel, emitter), 14-20 lanes over a
+# tile of rays with a warp per emitter (14-16 with a transfer warp, 17-20
+# with the transfer step taken in turn).
+ALL_VARIANTS = list(range(21))
 
 
 @pytest.fixture(scope="module", params=["headline_batch", "continuum_bands"])

@@ -246,7 +246,7 @@ def test_order1_surrogate_inside_double_scattering(workdir):
         b.run()
         feat, src = b.scatter_samples(depth=1)
         assert len(feat) > 10000 and np.all(np.isfinite(src))
-        sur.train(feat, src, epochs=40, batch=4096, lr=3e-3)
+        sur.train(feat, src, epochs=80, batch=4096, lr=3e-3)
         b.upload(test)
         b.run()
         plain = b.download()
