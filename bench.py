@@ -58,7 +58,7 @@ def parse():
                     help="rays of the depth-2 scattering workload; 0 skips it")
     ap.add_argument("--ms-train-rays", type=int, default=3_000,
                     help="rays of the depth-2 surrogate's training batch")
-    ap.add_argument("--ms-epochs", type=int, default=500,
+    ap.add_argument("--ms-epochs", type=int, default=300,
                     help="training epochs of the depth-2 surrogate")
     ap.add_argument("--ms-plain-rays", type=int, default=1_000,
                     help="rays of the depth-2 workload timed on the plain path (its first ones)")
@@ -148,13 +148,15 @@ def make_workload(n_rays, seed_offset=0):
 
 
 # ncu dram__bytes (read + write) per EGA evaluation of one 20k-ray launch of
-# this workload (1.8536e9 evaluations), per kernel family, with the digest
+# this workload (1.8536e9 evaluations), per launch variant, with the digest
 # of the kernel sources the capture was taken with (kernel_sources_sha).  A
 # capture describes the kernel only while those sources are unchanged; for
-# any other source the line reports traffic null.  Families: a thread per
-# (ray, channel) (variants 0-8), a lane per (ray, channel, emitter) (9-13),
-# lanes over a tile of 32 rays (14-20).
-TRAFFIC_PER_EGA = {}
+# any other source or variant the line reports traffic null.  Variant 17
+# (ega_ray_rot_kernel<8, 0, 4, 0>): 6.199 GB read + 0.142 GB written.
+TRAFFIC_PER_EGA = {17: ((6.198689e9 + 0.141950e9) / 1.853620866e9, "8def761b6c704d73")}
+# Sources per kernel family: a thread per (ray, channel) (variants 0-8), a
+# lane per (ray, channel, emitter) (9-13), lanes over a tile of 32 rays
+# (14-20).
 KERNEL_SOURCES = {
     "thread": ["ega_kernel.cuh", "device_common.cuh"],
     "lane": ["ega_lane.cuh", "device_common.cuh"],
@@ -177,11 +179,10 @@ def kernel_sources_sha(family):
 
 
 def dram_traffic(variant, n_ega):
-    """DRAM bytes per launch from the family's capture, scaled by the EGA
+    """DRAM bytes per launch from the variant's capture, scaled by the EGA
     evaluations, or None (no capture of the current sources)."""
-    fam = kernel_family(variant)
-    cap = TRAFFIC_PER_EGA.get(fam)
-    if cap is None or cap[1] != kernel_sources_sha(fam):
+    cap = TRAFFIC_PER_EGA.get(variant)
+    if cap is None or cap[1] != kernel_sources_sha(kernel_family(variant)):
         return None
     return cap[0] * n_ega
 
