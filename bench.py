@@ -60,6 +60,8 @@ def parse():
                     help="rays of the depth-2 surrogate's training batch")
     ap.add_argument("--ms-epochs", type=int, default=300,
                     help="training epochs of the depth-2 surrogate")
+    ap.add_argument("--ms1-epochs", type=int, default=80,
+                    help="training epochs of the depth-2 workload's order-1 surrogate")
     ap.add_argument("--ms-plain-rays", type=int, default=1_000,
                     help="rays of the depth-2 workload timed on the plain path (its first ones)")
     ap.add_argument("--requests", type=int, default=512,
@@ -491,7 +493,7 @@ def multiple_scattering_bench(args, local, torch):
     r2 = timed_surrogate(2, sur2)
     sur1 = api.Surrogate(nd, device=local, seed=7)
     t0 = time.perf_counter()
-    sur1.train(X1, Y1, epochs=args.sca_epochs, batch=4096, lr=3e-3)
+    sur1.train(X1, Y1, epochs=args.ms1_epochs, batch=4096, lr=3e-3)
     t1 = time.perf_counter() - t0
     r1 = timed_surrogate(1, sur1)
     res = {"workload": MS_WORKLOAD, "rays": n, "channels": nd,
@@ -500,7 +502,7 @@ def multiple_scattering_bench(args, local, torch):
                      "sample": "the first %d of the %d rays (about 20 ms per ray)" % (npl, n)},
            "surrogate_order2": dict(r2, training={"samples": int(len(X2)), "epochs": args.ms_epochs,
                                                   "seconds": t2}),
-           "surrogate_order1": dict(r1, training={"samples": int(len(X1)), "epochs": args.sca_epochs,
+           "surrogate_order1": dict(r1, training={"samples": int(len(X1)), "epochs": args.ms1_epochs,
                                                   "seconds": t1}),
            "training_rays": args.ms_train_rays,
            "pencils_per_point": {"depth %d" % d: na for d, na in MS_NALPHA.items()}}
