@@ -3,7 +3,7 @@ forward model (oracle/_ref/libjurassic_ref.so, compiled from the
 reference's own sources by oracle/Makefile) on the seeded synthetic
 workloads of jscat.synth.
 
-    make -C oracle ref && python tests/golden/make_golden.py [headline|points [kind...]|ice2|jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
+    make -C oracle ref && python tests/golden/make_golden.py [headline|emitters|points [kind...]|ice2|jacobian|aero|fov|aerojac|ip|ipjac|ip3d]
 
 Each fixture stores the reference's outputs in full FP64 precision, the
 per-(ray, channel) EGA table-index digests of the C restatement (checked
@@ -64,6 +64,21 @@ def band_case(workdir):
     nadir interleaved): exercises ctmn2 and ctmo2."""
     return synth.batched_case(workdir, n_rays=60, rays_per_atm=30, seed=20261205,
                               emitters=synth.CFG0_EMITTERS, nus=BAND_NU)
+
+
+# Emitter sets beyond the benchmark's eight (the reference holds up to
+# NGMAX = 25): the first eight names of the benchmark, then generic gases
+# with a flat 1 ppbv profile.
+def many_emitters(n):
+    return synth.CFG1_EMITTERS + ["GAS%02d" % i for i in range(9, n + 1)]
+
+
+def emitters_case(workdir, n):
+    """n emitters (12: the ray-tile kernels' 16-warp form; 20: the 32-lane
+    groups and the widest thread-per-channel kernel), 4 channels of the
+    64-channel grid, 2 profiles x 20 rays (limb and nadir interleaved)."""
+    return synth.batched_case(workdir, n_rays=40, rays_per_atm=20, seed=20261207 + n,
+                              emitters=many_emitters(n), nus=synth.CFG1_NU[3::16])
 
 
 def reference_ctl(ctlkw):
@@ -443,10 +458,22 @@ def headline_fixtures(workdir):
         save(name, ctlkw, atms, ray_atm, geom, ref, port)
 
 
+def emitters_fixtures(workdir):
+    """emitters12 and emitters20: more emitters than the benchmark's eight."""
+    for n in (12, 20):
+        ctlkw, atms, ray_atm, geom = emitters_case(workdir, n)
+        ref = refrun.run(reference_ctl(ctlkw), atms, ray_atm, geom, los=True)
+        port = refrun.run_port(ctlkw, atms, ray_atm, geom, los=True)
+        save("emitters%d" % n, ctlkw, atms, ray_atm, geom, ref, port)
+
+
 def main():
     workdir = os.environ.get("JSC_WORKDIR", "/tmp/jsc")
     if sys.argv[1:] == ["headline"]:
         headline_fixtures(workdir)
+        return
+    if sys.argv[1:] == ["emitters"]:
+        emitters_fixtures(workdir)
         return
     if sys.argv[1:] == ["ice2"]:
         ice_depth2_fixture(workdir)

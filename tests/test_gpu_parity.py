@@ -274,16 +274,24 @@ def _aero_for(aero, g, nus):
 ALL_VARIANTS = list(range(21))
 
 
-@pytest.fixture(scope="module", params=["headline_batch", "continuum_bands"])
+@pytest.fixture(scope="module",
+                params=["headline_batch", "continuum_bands", "emitters12", "emitters20"])
 def shape_case(request, workdir):
     """The benchmark's 64-channel, 8-emitter shape (O2 continuum in its top
-    channels) and the O2/N2 continuum-band case, with one device model per
-    case shared by all launch variants."""
+    channels), the O2/N2 continuum-band case and two cases with more
+    emitters than the benchmark (12: the ray-tile kernels' 16-warp form;
+    20: above the ray-tile kernels' 16, the 32-lane groups of the lane
+    kernel and the widest thread-per-channel kernel), with one device model
+    per case shared by all launch variants."""
     from jscat import api, structs as S, synth
-    from make_golden_shim import band_case, headline_case
+    from make_golden_shim import band_case, emitters_case, headline_case
     name = request.param
     g = _load(name)
-    ctlkw, atms, ray_atm, geom = (headline_case if name == "headline_batch" else band_case)(workdir)
+    if name.startswith("emitters"):
+        ctlkw, atms, ray_atm, geom = emitters_case(workdir, int(name[len("emitters"):]))
+    else:
+        ctlkw, atms, ray_atm, geom = (headline_case if name == "headline_batch"
+                                      else band_case)(workdir)
     _check_tables(g, ctlkw)
     ctl = S.make_ctl(**ctlkw)
     m = api.Model(ctl)
@@ -293,9 +301,10 @@ def shape_case(request, workdir):
 
 @pytest.mark.parametrize("variant", ALL_VARIANTS)
 def test_every_launch_variant(shape_case, variant):
-    """Each launch variant on the headline shape and on the continuum-band
-    channels: LOS point counts and every EGA table index (digests) exactly
-    the reference's, radiances within 1e-9 relative and 0.01 K."""
+    """Each launch variant on the headline shape, the continuum-band
+    channels and the many-emitter cases: LOS point counts and every EGA
+    table index (digests) exactly the reference's, radiances within 1e-9
+    relative and 0.01 K."""
     from jscat import api
     name, g, ctlkw, ctl, inp, m = shape_case
     out = api.formod_batch(ctl, inp, model=m, digest=True, variant=variant)
