@@ -1190,7 +1190,9 @@ def main():
                        "channels": nd, "emitters": ng, "los_points": n_points,
                        "ega_evaluations": n_ega, "l2": "inputs larger than L2, no flush",
                        "parallelism": "rays sharded per GPU, no collective",
-                       "ega_launch": tuned},
+                       "ega_launch": tuned,
+                       "gpu_launches_note": "this library's kernels; the ray-tile variants' "
+                                            "ray order adds the launches of a CUB radix sort"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),

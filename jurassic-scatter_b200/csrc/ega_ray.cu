@@ -46,6 +46,7 @@ int jsc_ray_order(int n_rays, const int *ray_atm, const int *nlos, const double 
   int *i_in = order + n_rays;
   ray_key_kernel<<<(n_rays + 255) / 256, 256, 0, s>>>(n_rays, ray_atm, nlos, tsurf, tpz, k_in,
                                                       i_in);
+  jsc_count_launch();  // the CUB sort's own launches are not counted
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
   size_t bytes = tmp_bytes;
